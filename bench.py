@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark: MLoD surface projection, queries projected per second.
+
+Default workload (the precision configuration): 2M points on a seeded
+12-blob RBF implicit surface translated 1e3 x diagonal from the origin,
+multi-Gaussian kernel (sigma_1 = 0.01 diag, factor 2, 4 sigmas), cutoff 3,
+2M queries = points + N(0, (0.01 diag)^2), 10 projection iterations each.
+A step projects all queries through the MLoD kernel (device buffers in HBM).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank holds a replica of the tree and projects
+its own query set (weak scaling, no collective on the data path); the time is
+the max over ranks.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "queries projected/s & p50/p99 latency at <=1e-5*diag err vs FP64, 1 B200"
+UNIT = "queries/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n-points", type=int, default=2_000_000)
+    ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--check-queries", type=int, default=2048, help="queries checked against the FP64 oracle")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n_points: int, rank: int):
+    from mlodsurfaces_b200 import Kernel, synth
+
+    pts, nrm = synth.rbf_blobs(n_points, seed=2)
+    pts = synth.make_tie_free(pts)
+    q = synth.perturbed_queries(pts, 0.01, seed=3 + rank)
+    diag = synth.bbox_diag(pts)
+    k = Kernel()
+    k.type = Kernel.GAUSSIAN_MULTIPLE
+    k.sigmas = [0.01 * diag * 2.0**i for i in range(4)]
+    return pts, nrm, q, diag, k
+
+
+def config_dict(args, tree_mb=None):
+    d = {
+        "workload": "precision: RBF-blob surface translated 1e3*diag, multi-Gaussian MLoD",
+        "n_points": args.n_points,
+        "n_queries_per_gpu": args.n_points,
+        "iterations": args.iters,
+        "kernel": "multi-Gaussian sigma1=0.01*diag factor 2 x4",
+        "cutoff": 3.0,
+        "blend_rule": "GPU (Fastapss)",
+        "parallelism": f"replicated tree, queries sharded, {args.gpus} GPU(s)",
+        "l2": "L2 flushed (256 MB write) before every timed step",
+    }
+    if tree_mb is not None:
+        d["tree_mb"] = round(tree_mb, 1)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        finally:
+            os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out):
+    """CPU baseline leg: the reference's own CPU path (oracle/_ref) timed on a
+    bounded query sample with every host thread, and the GPU outputs checked
+    against the FP64 oracle on a sample of queries."""
+    import oracle
+
+    out = {}
+    rng = np.random.default_rng(123)
+    cores = os.cpu_count() or 1
+    if oracle.ref_available():
+        t0 = time.time()
+        rt = oracle.RefTree(pts, nrm, 12)
+        build_s = time.time() - t0
+        sel = rng.choice(len(q), 256, replace=False)
+        _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+        per_q = max(s0 / 256, 1e-7)
+        ns = int(min(len(q), max(256, args.cpu_seconds / per_q)))
+        sel = rng.choice(len(q), ns, replace=False)
+        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+        out["cpu_baseline"] = {"value": ns / secs, "unit": UNIT, "cores": cores, "kind": "reference",
+                               "sample": f"{ns} random queries of the workload, {args.iters} iterations, "
+                                         f"APSSOctree::projectCPU under OpenMP; tree build {build_s:.1f} s "
+                                         f"single-threaded, not included"}
+        del rt
+    # accuracy of the GPU result against the FP64 oracle
+    ot = oracle.OracleTree(pts, nrm, 12)
+    sel = rng.choice(len(q), min(args.check_queries, len(q)), replace=False)
+    x64, _ = ot.project_mlod(q[sel], args.iters, kernel, rule=0, cutoff=3.0)
+    x = gpu_out[sel].astype(np.float64)
+    err = np.linalg.norm(x - x64, axis=1) / diag
+    half_ulp = np.abs(np.spacing(x64.astype(np.float32)).astype(np.float64)) / 2
+    excess = np.linalg.norm(np.maximum(np.abs(x - x64) - half_ulp, 0.0), axis=1) / diag
+    out["err_vs_fp64"] = {"max": float(err.max()), "p99": float(np.percentile(err, 99)),
+                          "max_beyond_f32_output_rounding": float(excess.max()),
+                          "p99_beyond_f32_output_rounding": float(np.percentile(excess, 99)),
+                          "queries_checked": int(len(sel))}
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from mlodsurfaces_b200 import APSSOctree, Fastapss
+    from mlodsurfaces_b200 import _capi as capi
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    pts, nrm, q, diag, kernel = workload(args.n_points, rank)
+    tree = APSSOctree()
+    tree.build(pts, nrm)
+    inf = tree.info()
+    tree_mb = inf.device_bytes / 2**20
+    f = Fastapss(tree, kernel, len(q))
+    f.setScalingProtectionSphere(3.0)
+    lib = capi.load()
+
+    d_q = torch.from_numpy(q).to(dev)
+    d_p = torch.empty_like(d_q)
+    d_n = torch.empty_like(d_q)
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        f.project_device(d_q, d_p, d_n, args.iters, stream=sptr)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = lib.mlods_kernel_launches()
+    step_ms, kern_ms, visits = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        st = f.last_stats()
+        kern_ms.append(st["kernel_ms"])
+        visits.append(st["node_visits"])
+        if st["overflows"]:
+            raise RuntimeError(f"{st['overflows']} queries overflowed the traversal stack")
+    torch.cuda.synchronize(dev)
+    launches = lib.mlods_kernel_launches() - launches0
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+
+    total_ms = float(sum(step_ms))
+    t = torch.tensor([total_ms, max(step_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms_max = float(t[0])
+    value = world * len(q) * args.steps / (total_ms_max / 1e3)
+
+    # ---- end to end through the public C ABI with host buffers (Fastapss protocol)
+    h_q = torch.from_numpy(q).pin_memory()
+    h_p = torch.empty_like(h_q).pin_memory()
+    h_n = torch.empty_like(h_q).pin_memory()
+    e2e_ms = []
+    h = tree.handle
+    f._sync_params()
+    default = torch.cuda.default_stream(dev)
+    for i in range(args.e2e_steps + 1):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(default)
+        capi.check(lib.mlods_queries_upload(h, len(q), C.c_void_p(h_q.data_ptr()), None))
+        capi.check(lib.mlods_project(h, len(q), args.iters, -1.0, C.c_void_p(h_p.data_ptr()),
+                                     C.c_void_p(h_n.data_ptr()), None))
+        e1.record(default)
+        e1.synchronize()
+        if i > 0:  # first call allocates the query buffer
+            e2e_ms.append(e0.elapsed_time(e1))
+    te = torch.tensor([statistics.mean(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * len(q) / (float(te[0]) / 1e3)
+    out_host = d_p.cpu().numpy()
+
+    # ---- roofline of the projection kernel (algorithmic bytes per launch)
+    mean_visits = statistics.mean(visits)
+    bytes_per_launch = len(q) * (12 + 24) + 64 * mean_visits
+    kms = statistics.mean(kern_ms)
+    achieved = bytes_per_launch / (kms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (f64 sphere solve)",
+        "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag; queries = points + "
+                "N(0, 0.01 diag)",
+        "config": config_dict(args, tree_mb),
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                       "per": f"request of {len(q)} queries x {args.iters} iterations"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h_q.numel() * 4),
+                "d2h_bytes_per_step": int(h_p.numel() * 4 + h_n.numel() * 4),
+                "path": "mlods_queries_upload + mlods_project (host pinned in/out)"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None,
+                     "note": f"algorithmic bytes = 36 per query + 64 per node visit ({mean_visits / len(q) / args.iters:.0f}"
+                             f" visits per query-iteration); peak {peak_kind}; node records are mostly served "
+                             f"from L1/L2"},
+        "kernel_ms": kms,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result.update(cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, out_host))
+    return result
+
+
+def run_reference(args, rank):
+    """Reference arm: the reference's own CPU implementation (oracle/_ref,
+    APSSOctree::projectCPU under OpenMP) on the same workload, each step a
+    bounded random sample of the queries."""
+    import oracle
+
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "reference CPU shim oracle/_ref/libmlods_ref.so not built"}
+    pts, nrm, q, diag, kernel = workload(args.n_points, rank)
+    cores = os.cpu_count() or 1
+    rt = oracle.RefTree(pts, nrm, 12)
+    rng = np.random.default_rng(7)
+    sel = rng.choice(len(q), 256, replace=False)
+    _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+    per_q = max(s0 / 256, 1e-7)
+    budget = 150.0 / max(args.steps + args.warmup, 1)
+    ns = int(min(len(q), max(256, budget / per_q)))
+    times = []
+    for i in range(args.warmup + args.steps):
+        sel = rng.choice(len(q), ns, replace=False)
+        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+        if i >= args.warmup:
+            times.append(secs)
+    value = ns * len(times) / sum(times)
+    sample = f"{ns} random queries per step, {args.iters} iterations, APSSOctree::projectCPU under OpenMP"
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag",
+        "config": config_dict(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args, rank)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        res = run_ours(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

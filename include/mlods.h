@@ -1,0 +1,161 @@
+/*
+ * mlods.h -- C ABI of libmlods.so, a B200 (sm_100a) implementation of the
+ * point-set surface projection path of "Moving Level-of-Detail Surfaces"
+ * (reference project: CorentinMercier/MlodSurfaces).
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status
+ * (MLODS_OK on success); mlods_last_error() gives the message of the last
+ * failure on the calling thread.  `stream` is a cudaStream_t passed as void*
+ * (NULL = the legacy default stream).  Host pointers are ordinary (pageable or
+ * pinned) memory; arguments named d_* are device pointers.
+ *
+ * Coordinates are float xyz triples (the layout of std::vector<glm::vec3>).
+ */
+#ifndef MLODS_H
+#define MLODS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define MLODS_OK 0
+#define MLODS_ERR_INVALID 1   /* bad argument (null handle, n == 0, unknown enum, ...) */
+#define MLODS_ERR_CUDA 2      /* a CUDA call failed; see mlods_last_error() */
+#define MLODS_ERR_STATE 3     /* call out of protocol order (e.g. project before upload) */
+#define MLODS_ERR_CAPACITY 4  /* a request exceeds a fixed capacity */
+
+/* ---- weight kernels (Kernel.h:37, Kernel.cpp:64-83) ------------------- */
+#define MLODS_GAUSSIAN 0
+#define MLODS_SINGULAR 1          /* the reference's "rational" kernel */
+#define MLODS_GAUSSIAN_MULTIPLE 2
+#define MLODS_MAX_SIGMAS 16
+
+/* ---- projection modes (APSS subclasses and APSSOctree modes) ----------- */
+#define MLODS_MODE_MLOD 0    /* Fastapss::project (Fastapss.cu:439-455) */
+#define MLODS_MODE_GLOBAL 1  /* GlobalAPSS::project (GlobalAPSS.cu:203-235) */
+#define MLODS_MODE_KNN 2     /* APSSOctree::knnMode + projectAPSSCPU (CPUUtils.cpp:674-737) */
+#define MLODS_MODE_BALL 3    /* APSSOctree::ballMode + projectAPSSCPU (CPUUtils.cpp:682-737) */
+
+/* ---- blend rules of the MLoD traversal --------------------------------- */
+#define MLODS_BLEND_GPU 0  /* parent weight w * a_child / a_node, |u4| < 1e-6 (Fastapss.cu:244, :362) */
+#define MLODS_BLEND_CPU 1  /* parent weight w / #children, |u4| < 1e-12 (CPUUtils.cpp:485, :751) */
+
+/* Kernel value type; mirrors class Kernel (Kernel.h:24-60).  sigma and sigmas
+ * are absolute lengths (already multiplied by the box radius, as
+ * scene::setNewKernel does, scene.cpp:1025-1033). */
+typedef struct mlods_kernel {
+    int32_t type;            /* MLODS_GAUSSIAN / _SINGULAR / _GAUSSIAN_MULTIPLE */
+    float sigma;             /* Kernel::sigma */
+    float exponent;          /* Kernel::exponent */
+    float constant_shift;    /* Kernel::constant_shift */
+    int32_t n_sigmas;        /* Kernel::sigmas.size(), <= MLODS_MAX_SIGMAS */
+    float sigmas[MLODS_MAX_SIGMAS];
+} mlods_kernel;
+
+/* Projection options; mirror APSS::setScalingProtectionSphere / setMinDepth
+ * (GPUUtils.h:40-43) and APSSOctree::knnMode / ballMode (CPUUtils.h:191-192). */
+typedef struct mlods_params {
+    float cutoff;        /* scalingProtectionSphere: a node is an aggregate when |q-c| > cutoff*r (default 2) */
+    int32_t min_depth;   /* nodes shallower than this are always opened (default 0) */
+    int32_t mode;        /* MLODS_MODE_* */
+    int32_t knn;         /* k for MLODS_MODE_KNN (default 20) */
+    float ball_radius;   /* radius for MLODS_MODE_BALL; < 0 uses 3 * sigmas[0] (default 0.1) */
+    int32_t blend_rule;  /* MLODS_BLEND_GPU (default) or MLODS_BLEND_CPU */
+    int32_t reorder;     /* 1: process queries in Morton order (results are identical) */
+    float prune_tol;     /* > 0: skip MLoD subtrees whose weight bound is below prune_tol
+                            times the running total (extension; 0 = off, reference behaviour) */
+} mlods_params;
+
+typedef struct mlods_tree_s* mlods_tree;
+
+/* Tree statistics. */
+typedef struct mlods_tree_info {
+    int64_t n_points;
+    int64_t n_nodes;       /* reference node count (APSSOctree nbOfNodes, CPUUtils.cpp:177-184) */
+    int64_t n_extra;       /* point records of multi-point leaves */
+    int32_t depth;         /* octreeNode::computeDepth of the root (CPUUtils.cpp:254-261) */
+    int32_t max_depth;
+    int64_t n_ties;        /* points lying exactly on a split they were classified by (sent low) */
+    float bbox_min[3];     /* root box, BBOX (CPUUtils.h:70-99) */
+    float bbox_max[3];
+    double origin[3];      /* local frame origin (centre of the root box) */
+    int64_t device_bytes;  /* device memory held by the tree */
+} mlods_tree_info;
+
+/* ---- library ------------------------------------------------------------ */
+const char* mlods_last_error(void);
+int mlods_version(void);
+
+/* ---- tree (APSSOctree::build, CPUUtils.cpp:540-569) ----------------------
+ * Builds the octree on the device: Morton codes on the reference's split
+ * lattice, radix sort, level-wise node creation, area weights and bottom-up
+ * moments.  Topology and breadth-first order equal the reference's (points
+ * exactly on a split go to the low child).  max_depth <= 12 (MAX_DEPTH).
+ * mlods_tree_build takes host arrays (copied in); mlods_tree_build_device
+ * takes device arrays (read, not kept). */
+int mlods_tree_build(const float* pts, const float* nrm, int64_t n, int32_t max_depth, void* stream,
+                     mlods_tree* out);
+int mlods_tree_build_device(const float* d_pts, const float* d_nrm, int64_t n, int32_t max_depth, void* stream,
+                            mlods_tree* out);
+/* Frees everything the tree holds (Fastapss::eraseFromGPU + APSS::erasePointsFromGPU,
+ * Fastapss.cu:486-511, GPUUtils.cu:452-464). */
+int mlods_tree_free(mlods_tree t);
+int mlods_tree_get_info(mlods_tree t, mlods_tree_info* info);
+
+/* Downloads the topology in breadth-first order for parity checks.  Arrays
+ * are n_nodes long (perm: n_points): father/firstChild/nextBrother as
+ * octreeNode::getRelations (CPUUtils.cpp:213-234); leaf_off/leaf_cnt index
+ * into perm, which lists each leaf's original point indices in ascending
+ * order; bmin/bmax are the float boxes (3 per node); mom holds 9 doubles per
+ * node {m0, pbar[3] (world), n[3], cpn, cpp}.  Any pointer may be NULL. */
+int mlods_tree_export(mlods_tree t, int32_t* depth, int32_t* parent, int32_t* first_child, int32_t* n_children,
+                      int32_t* next_brother, int32_t* leaf_off, int32_t* leaf_cnt, int32_t* perm, float* bmin,
+                      float* bmax, double* mom, float* area);
+
+/* ---- kernel and options ---------------------------------------------------
+ * mlods_set_kernel replaces the device kernel (APSS::updateKernel,
+ * GPUUtils.cu:466-472, without its leak).  mlods_set_params replaces all
+ * options at once; mlods_default_params fills the reference defaults. */
+int mlods_set_kernel(mlods_tree t, const mlods_kernel* k);
+void mlods_default_params(mlods_params* p);
+int mlods_set_params(mlods_tree t, const mlods_params* p);
+
+/* ---- query buffer protocol (Fastapss::copyToGPU/project, APSS::copyPointsToGPU) ----
+ * mlods_queries_upload copies n host points into the tree's device query
+ * buffer (APSS::copyPointsToGPU, GPUUtils.cu:406-411; an earlier buffer is
+ * replaced, not leaked).  mlods_project runs n_iterations projection steps in
+ * place on that buffer, so repeated calls continue from the last positions,
+ * and copies positions/normals back when the host pointers are non-NULL
+ * (Fastapss::project, Fastapss.cu:439-455).  step_max < 0 selects the root box
+ * radius.  n must not exceed the uploaded count.  mlods_queries_free releases
+ * the buffer (APSS::erasePointsFromGPU). */
+int mlods_queries_upload(mlods_tree t, int64_t n, const float* pts, void* stream);
+int mlods_project(mlods_tree t, int64_t n, int32_t n_iterations, float step_max, float* out_pts, float* out_nrm,
+                  void* stream);
+int mlods_queries_free(mlods_tree t);
+
+/* ---- device-buffer projection (no host traffic) ---------------------------
+ * Projects n queries d_q (device, xyz) into d_out_pts / d_out_nrm (device).
+ * d_out_pts may equal d_q (in place).  Asynchronous on `stream`. */
+int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out_pts, float* d_out_nrm,
+                         int32_t n_iterations, float step_max, void* stream);
+
+/* ---- per-launch statistics of the last projection on this tree ------------
+ * node visits summed over queries and iterations, largest traversal stack,
+ * queries whose traversal stack overflowed (their result is the input point
+ * with a zero normal), and the device time of the projection kernel itself
+ * in milliseconds (CUDA events on the launching stream).  Synchronises. */
+int mlods_last_stats(mlods_tree t, int64_t* node_visits, int32_t* max_stack, int64_t* overflows,
+                     float* kernel_ms);
+
+/* Number of kernels this library has launched in this process (diagnostics). */
+int64_t mlods_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MLODS_H */

@@ -1,0 +1,12 @@
+"""mlodsurfaces_b200 -- B200 (sm_100a) point-set surface projection.
+
+The Moving Level-of-Detail (MLoD) and APSS projection path of
+CorentinMercier/MlodSurfaces, rebuilt around hand-written CUDA kernels in
+``libmlods.so`` (C ABI: ``include/mlods.h``).  This package is the Python
+mirror of the reference's C++ projection API (``Kernel``, ``APSSOctree``,
+``APSS``/``Fastapss``) plus seeded synthetic inputs (``synth``).
+"""
+from .apss import APSS, APSSOctree, Fastapss, Kernel  # noqa: F401
+from . import synth  # noqa: F401
+
+__all__ = ["APSS", "APSSOctree", "Fastapss", "Kernel", "synth"]

@@ -1,0 +1,140 @@
+"""ctypes bindings of libmlods.so (the C ABI in include/mlods.h).
+
+The library is loaded from ``mlodsurfaces_b200/_lib/libmlods.so``.  There is
+no fallback: if the library is missing the import fails with the build
+command to run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libmlods.so"
+
+MLODS_OK = 0
+MLODS_ERR_INVALID = 1
+MLODS_ERR_CUDA = 2
+MLODS_ERR_STATE = 3
+MLODS_ERR_CAPACITY = 4
+
+GAUSSIAN = 0
+SINGULAR = 1
+GAUSSIAN_MULTIPLE = 2
+MAX_SIGMAS = 16
+
+MODE_MLOD = 0
+MODE_GLOBAL = 1
+MODE_KNN = 2
+MODE_BALL = 3
+
+BLEND_GPU = 0
+BLEND_CPU = 1
+
+
+class mlods_kernel(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("sigma", C.c_float),
+        ("exponent", C.c_float),
+        ("constant_shift", C.c_float),
+        ("n_sigmas", C.c_int32),
+        ("sigmas", C.c_float * MAX_SIGMAS),
+    ]
+
+
+class mlods_params(C.Structure):
+    _fields_ = [
+        ("cutoff", C.c_float),
+        ("min_depth", C.c_int32),
+        ("mode", C.c_int32),
+        ("knn", C.c_int32),
+        ("ball_radius", C.c_float),
+        ("blend_rule", C.c_int32),
+        ("reorder", C.c_int32),
+        ("prune_tol", C.c_float),
+    ]
+
+
+class mlods_tree_info(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int64),
+        ("n_nodes", C.c_int64),
+        ("n_extra", C.c_int64),
+        ("depth", C.c_int32),
+        ("max_depth", C.c_int32),
+        ("n_ties", C.c_int64),
+        ("bbox_min", C.c_float * 3),
+        ("bbox_max", C.c_float * 3),
+        ("origin", C.c_double * 3),
+        ("device_bytes", C.c_int64),
+    ]
+
+
+class MlodsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"mlods error {code}: {msg}")
+        self.code = code
+
+
+_P = C.c_void_p
+_F = C.POINTER(C.c_float)
+_D = C.POINTER(C.c_double)
+_I32 = C.POINTER(C.c_int32)
+_I64 = C.POINTER(C.c_int64)
+
+# name -> (restype, argtypes); the full exported surface of include/mlods.h
+SIGNATURES = {
+    "mlods_last_error": (C.c_char_p, []),
+    "mlods_version": (C.c_int, []),
+    "mlods_tree_build": (C.c_int, [_P, _P, C.c_int64, C.c_int32, _P, C.POINTER(_P)]),
+    "mlods_tree_build_device": (C.c_int, [_P, _P, C.c_int64, C.c_int32, _P, C.POINTER(_P)]),
+    "mlods_tree_free": (C.c_int, [_P]),
+    "mlods_tree_get_info": (C.c_int, [_P, C.POINTER(mlods_tree_info)]),
+    "mlods_tree_export": (C.c_int, [_P] + [_P] * 12),
+    "mlods_set_kernel": (C.c_int, [_P, C.POINTER(mlods_kernel)]),
+    "mlods_default_params": (None, [C.POINTER(mlods_params)]),
+    "mlods_set_params": (C.c_int, [_P, C.POINTER(mlods_params)]),
+    "mlods_queries_upload": (C.c_int, [_P, C.c_int64, _P, _P]),
+    "mlods_project": (C.c_int, [_P, C.c_int64, C.c_int32, C.c_float, _P, _P, _P]),
+    "mlods_queries_free": (C.c_int, [_P]),
+    "mlods_project_device": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
+    "mlods_last_stats": (C.c_int, [_P, _I64, _I32, _I64, C.POINTER(C.c_float)]),
+    "mlods_kernel_launches": (C.c_int64, []),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libmlods.so once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m mlodsurfaces_b200.build` "
+            "(there is no CPU fallback)"
+        )
+    lib = C.CDLL(os.fspath(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != MLODS_OK:
+        msg = load().mlods_last_error().decode(errors="replace")
+        raise MlodsError(rc, msg)
+
+
+def ptr(a) -> C.c_void_p:
+    """Address of a numpy array or torch tensor (None -> NULL)."""
+    if a is None:
+        return C.c_void_p(0)
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return C.c_void_p(a.ctypes.data)

@@ -1,0 +1,350 @@
+"""Python mirror of the reference's projection API over libmlods.so.
+
+Class and method names follow the reference's C++ classes so that code (and
+tests) written against them read the same:
+
+* :class:`Kernel` -- ``class Kernel`` (sources/apss/Kernel.h:24-60)
+* :class:`APSSOctree` -- ``class APSSOctree`` (sources/apss/CPUUtils.h:166-229);
+  ``build`` runs on the device.
+* :class:`APSS`, :class:`Fastapss` -- ``class APSS`` (sources/apss/GPUUtils.h:22-67)
+  and ``class Fastapss`` (sources/apss/Fastapss.h:32-51): upload queries,
+  project them in place ``n_iterations`` steps per call, copy back on demand.
+
+Arrays are numpy ``float32`` arrays of shape (n, 3) on the host.  Errors raise
+:class:`~mlodsurfaces_b200._capi.MlodsError` (the reference exits the process).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _capi as capi
+
+
+def _f32x3(a, name: str) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    if a.ndim != 2 or a.shape[1] != 3:
+        raise ValueError(f"{name} must have shape (n, 3)")
+    return a
+
+
+class Kernel:
+    """Weight kernel value type (Kernel.h:24-60, Kernel.cpp:76-190)."""
+
+    GAUSSIAN = capi.GAUSSIAN
+    SINGULAR = capi.SINGULAR
+    GAUSSIAN_MULTIPLE = capi.GAUSSIAN_MULTIPLE
+
+    def __init__(self):
+        # Kernel::Kernel(), Kernel.cpp:76-79
+        self.type = Kernel.GAUSSIAN
+        self.sigma = 2.0
+        self.exponent = 1.0
+        self.constant_shift = 0.0
+        self.sigmas: list[float] = []
+        self.fixedSigmas: list[float] = []
+        self.beginningSigma = 0.0
+        self.factor = 0.0
+        self.nbOfComputedSigmas = 1
+
+    def copy(self) -> "Kernel":
+        k = Kernel()
+        k.__dict__.update({key: (list(v) if isinstance(v, list) else v) for key, v in self.__dict__.items()})
+        return k
+
+    def updateSigmas(self, computedSigmas: bool = True, radius: float = 1.0) -> None:
+        """Kernel::updateSigmas (Kernel.cpp:172-190), float arithmetic."""
+        f32 = np.float32
+        if computedSigmas:
+            s = [f32(self.beginningSigma)]
+            for _ in range(1, self.nbOfComputedSigmas):
+                s.append(f32(s[-1] * f32(self.factor)))
+            self.sigmas = [float(v) for v in s]
+        else:
+            self.sigmas = list(self.fixedSigmas)
+        self.sigma = float(f32(self.sigma) * f32(radius))
+        self.sigmas = [float(f32(v) * f32(radius)) for v in self.sigmas]
+
+    def w(self, p, eta) -> float:
+        """Kernel::w (Kernel.cpp:64-83), evaluated in double on the host."""
+        d2 = float(sum((float(a) - float(b)) ** 2 for a, b in zip(p, eta)))
+        if self.type == Kernel.GAUSSIAN_MULTIPLE:
+            s = sum(math.exp(-d2 / (2.0 * sg * sg)) / (sg * sg * sg) for sg in self.sigmas)
+            return s if s != 0 else self.constant_shift
+        if self.type == Kernel.GAUSSIAN:
+            return math.exp(-d2 / (2.0 * self.sigma * self.sigma)) + self.constant_shift
+        if self.type == Kernel.SINGULAR:
+            v = max(self.constant_shift, 1e-4)
+            return v**self.exponent / (d2 + self.constant_shift) ** self.exponent
+        return 1.0
+
+    def to_c(self) -> capi.mlods_kernel:
+        if len(self.sigmas) > capi.MAX_SIGMAS:
+            raise ValueError(f"at most {capi.MAX_SIGMAS} sigmas are supported")
+        k = capi.mlods_kernel()
+        k.type = int(self.type)
+        k.sigma = float(self.sigma)
+        k.exponent = float(self.exponent)
+        k.constant_shift = float(self.constant_shift)
+        k.n_sigmas = len(self.sigmas)
+        for i, s in enumerate(self.sigmas):
+            k.sigmas[i] = float(s)
+        return k
+
+
+class APSSOctree:
+    """Device-resident octree with per-node weighted moments (CPUUtils.h:166-229)."""
+
+    def __init__(self):
+        self._h = C.c_void_p(0)
+        self._lib = capi.load()
+        self.m_scalingProtectionSphere = 2.0  # CPUUtils.h:206
+        self.m_minDepth = 0
+        self.m_knnMode = False
+        self.m_knn = 20
+        self.m_ballMode = False
+        self.m_ballRadius = 0.1
+        self._info = None
+
+    # -- lifetime
+    def build(self, points, normals, updateRootBoundingBox: bool = True, maxDepth: int = 12,
+              maxNumberOfPointsPerLeaf: int = 1, stream=None) -> None:
+        """APSSOctree::build (CPUUtils.cpp:540-569), on the device."""
+        if not updateRootBoundingBox:
+            raise ValueError("a fixed root box is not supported (the reference never uses it)")
+        if maxNumberOfPointsPerLeaf != 1:
+            raise ValueError("only one point per leaf is supported (the reference's only setting)")
+        pts = _f32x3(points, "points")
+        nrm = _f32x3(normals, "normals")
+        if len(pts) != len(nrm) or len(pts) == 0:
+            raise ValueError("points and normals must be non-empty and of equal length")
+        self.free()
+        h = C.c_void_p(0)
+        capi.check(self._lib.mlods_tree_build(capi.ptr(pts), capi.ptr(nrm), len(pts), int(maxDepth),
+                                              C.c_void_p(stream or 0), C.byref(h)))
+        self._h = h
+        self._info = None
+
+    def build_device(self, d_points, d_normals, maxDepth: int = 12, stream=None) -> None:
+        """Build from device tensors (torch CUDA float32, shape (n, 3))."""
+        self.free()
+        h = C.c_void_p(0)
+        capi.check(self._lib.mlods_tree_build_device(capi.ptr(d_points), capi.ptr(d_normals), int(d_points.shape[0]),
+                                                     int(maxDepth), C.c_void_p(stream or 0), C.byref(h)))
+        self._h = h
+        self._info = None
+
+    def free(self) -> None:
+        if self._h:
+            self._lib.mlods_tree_free(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise RuntimeError("tree not built")
+        return self._h
+
+    # -- queries
+    def info(self) -> capi.mlods_tree_info:
+        if self._info is None:
+            inf = capi.mlods_tree_info()
+            capi.check(self._lib.mlods_tree_get_info(self.handle, C.byref(inf)))
+            self._info = inf
+        return self._info
+
+    def getBoundingBox(self):
+        inf = self.info()
+        return np.array(inf.bbox_min[:], np.float32), np.array(inf.bbox_max[:], np.float32)
+
+    def radius(self) -> float:
+        """BBOX::radius of the root box, float arithmetic (CPUUtils.h:85)."""
+        bb, BB = self.getBoundingBox()
+        d = (BB - bb).astype(np.float32)
+        d2 = np.float32(np.float32(d[0] * d[0] + d[1] * d[1]) + d[2] * d[2])
+        return float(np.float32(np.sqrt(d2)) / np.float32(2.0))
+
+    def nbOfNodes(self) -> int:
+        return int(self.info().n_nodes)
+
+    def computeDepth(self) -> int:
+        return int(self.info().depth)
+
+    def numTies(self) -> int:
+        return int(self.info().n_ties)
+
+    def getScalingProtectionSphere(self) -> float:
+        return self.m_scalingProtectionSphere
+
+    def setScalingProtectionSphere(self, val: float) -> None:
+        self.m_scalingProtectionSphere = float(val)
+
+    def getMinDepth(self) -> int:
+        return self.m_minDepth
+
+    def setMinDepth(self, val: int) -> None:
+        self.m_minDepth = int(val)
+
+    def knnMode(self, setMode: bool, knn: int = 20) -> None:
+        """CPUUtils.cpp:674-680."""
+        self.m_knnMode = bool(setMode)
+        if self.m_knnMode:
+            self.m_ballMode = False
+        self.m_knn = int(knn)
+
+    def ballMode(self, setMode: bool, ballRadius: float = 0.1) -> None:
+        """CPUUtils.cpp:682-688."""
+        self.m_ballMode = bool(setMode)
+        if self.m_ballMode:
+            self.m_knnMode = False
+        self.m_ballRadius = float(ballRadius)
+
+    def isAPSS(self) -> bool:
+        return self.m_knnMode or self.m_ballMode
+
+    def export(self) -> dict:
+        """Topology and moments in breadth-first order (see mlods_tree_export)."""
+        inf = self.info()
+        nn, n = int(inf.n_nodes), int(inf.n_points)
+        out = {
+            "depth": np.empty(nn, np.int32), "parent": np.empty(nn, np.int32),
+            "first_child": np.empty(nn, np.int32), "n_children": np.empty(nn, np.int32),
+            "next_brother": np.empty(nn, np.int32), "leaf_off": np.empty(nn, np.int32),
+            "leaf_cnt": np.empty(nn, np.int32), "perm": np.empty(n, np.int32),
+            "bmin": np.empty((nn, 3), np.float32), "bmax": np.empty((nn, 3), np.float32),
+            "mom": np.empty((nn, 9), np.float64), "area": np.empty(n, np.float32),
+        }
+        keys = ["depth", "parent", "first_child", "n_children", "next_brother", "leaf_off", "leaf_cnt", "perm",
+                "bmin", "bmax", "mom", "area"]
+        capi.check(self._lib.mlods_tree_export(self.handle, *[capi.ptr(out[k]) for k in keys]))
+        return out
+
+
+class APSS:
+    """Projection interface (GPUUtils.h:22-67) over a device octree."""
+
+    mode = capi.MODE_MLOD
+
+    def __init__(self, apssOctree: APSSOctree, kernel: Kernel | None = None, nbOfVectors: int = 0):
+        self.m_apssOctree = apssOctree
+        self._lib = capi.load()
+        self.m_scalingProtectionSphere = 2.0  # GPUUtils.h:63
+        self.m_minDepth = 0
+        self.blend_rule = capi.BLEND_GPU
+        self.reorder = True
+        self.prune_tol = 0.0
+        self._n_uploaded = 0
+        if kernel is not None:
+            self.copyToGPU(kernel, nbOfVectors)
+
+    def _params(self) -> capi.mlods_params:
+        p = capi.mlods_params()
+        self._lib.mlods_default_params(C.byref(p))
+        t = self.m_apssOctree
+        p.cutoff = float(self.m_scalingProtectionSphere)
+        p.min_depth = int(self.m_minDepth)
+        p.mode = int(self._mode())
+        p.knn = int(t.m_knn)
+        p.ball_radius = float(t.m_ballRadius)
+        p.blend_rule = int(self.blend_rule)
+        p.reorder = 1 if self.reorder else 0
+        p.prune_tol = float(self.prune_tol)
+        return p
+
+    def _mode(self) -> int:
+        t = self.m_apssOctree
+        if t.m_knnMode:
+            return capi.MODE_KNN
+        if t.m_ballMode:
+            return capi.MODE_BALL
+        return self.mode
+
+    def _sync_params(self) -> None:
+        p = self._params()
+        capi.check(self._lib.mlods_set_params(self.m_apssOctree.handle, C.byref(p)))
+
+    # -- GPUUtils.h:29-51
+    def copyToGPU(self, kernel: Kernel, nbOfVectors: int = 0) -> None:
+        self.updateKernel(kernel)
+
+    def updateKernel(self, kernel: Kernel) -> None:
+        k = kernel.to_c()
+        capi.check(self._lib.mlods_set_kernel(self.m_apssOctree.handle, C.byref(k)))
+
+    def eraseFromGPU(self) -> None:
+        self.erasePointsFromGPU()
+
+    def copyPointsToGPU(self, nbOfVectors: int, outputPoints) -> None:
+        pts = _f32x3(outputPoints, "points")[:nbOfVectors]
+        capi.check(self._lib.mlods_queries_upload(self.m_apssOctree.handle, int(nbOfVectors), capi.ptr(pts),
+                                                  C.c_void_p(0)))
+        self._n_uploaded = int(nbOfVectors)
+
+    def erasePointsFromGPU(self) -> None:
+        if self.m_apssOctree._h:
+            self._lib.mlods_queries_free(self.m_apssOctree.handle)
+        self._n_uploaded = 0
+
+    def project(self, nbOfVectors: int, outputPoints, outputNormals, n_iterations: int, kernel: Kernel | None = None,
+                stepMaxSize: float = -1.0) -> None:
+        """Fastapss::project (Fastapss.cu:439-455): iterate in place on the device
+        buffer, copy back into the given float32 (n, 3) arrays when not None.
+        As in the reference, ``kernel`` is ignored: the device kernel is the
+        one from copyToGPU/updateKernel."""
+        self._sync_params()
+        op = outputPoints if outputPoints is not None else None
+        on = outputNormals if outputNormals is not None else None
+        for a in (op, on):
+            if a is not None and (a.dtype != np.float32 or not a.flags.c_contiguous or a.shape[0] < nbOfVectors):
+                raise ValueError("output arrays must be C-contiguous float32 with at least n rows")
+        capi.check(self._lib.mlods_project(self.m_apssOctree.handle, int(nbOfVectors), int(n_iterations),
+                                           float(stepMaxSize), capi.ptr(op), capi.ptr(on), C.c_void_p(0)))
+
+    def project_device(self, d_q, d_out_p, d_out_n, n_iterations: int, stepMaxSize: float = -1.0,
+                       stream=None) -> None:
+        """Device-buffer projection (torch CUDA tensors), asynchronous."""
+        self._sync_params()
+        capi.check(self._lib.mlods_project_device(self.m_apssOctree.handle, int(d_q.shape[0]), capi.ptr(d_q),
+                                                  capi.ptr(d_out_p), capi.ptr(d_out_n), int(n_iterations),
+                                                  float(stepMaxSize), C.c_void_p(stream or 0)))
+
+    def last_stats(self):
+        v = C.c_int64(0)
+        m = C.c_int32(0)
+        o = C.c_int64(0)
+        ms = C.c_float(0)
+        capi.check(self._lib.mlods_last_stats(self.m_apssOctree.handle, C.byref(v), C.byref(m), C.byref(o),
+                                              C.byref(ms)))
+        return {"node_visits": v.value, "max_stack": m.value, "overflows": o.value, "kernel_ms": ms.value}
+
+    # -- options, GPUUtils.h:40-43
+    def setScalingProtectionSphere(self, val: float) -> None:
+        self.m_scalingProtectionSphere = float(val)
+        self.m_apssOctree.setScalingProtectionSphere(val)
+
+    def getScalingProtectionSphere(self) -> float:
+        return self.m_scalingProtectionSphere
+
+    def setMinDepth(self, val: int) -> None:
+        self.m_minDepth = int(val)
+        self.m_apssOctree.setMinDepth(val)
+
+    def getMinDepth(self) -> int:
+        return self.m_minDepth
+
+    def CPU(self) -> APSSOctree:
+        return self.m_apssOctree
+
+
+class Fastapss(APSS):
+    """MLoD projection (Fastapss.h:32-51)."""
+
+    mode = capi.MODE_MLOD

@@ -1,0 +1,409 @@
+// capi.cu -- extern "C" entry points of libmlods.so (declared in include/mlods.h).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "project.cuh"
+#include "tree.cuh"
+
+namespace mlods
+{
+namespace
+{
+thread_local char g_err[1024] = "";
+std::atomic<int64_t> g_launches{0};
+
+int sm_count_for_current_device()
+{
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (dev < 64 && cache[dev]) return cache[dev];
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    if (dev < 64) cache[dev] = v;
+    return v;
+}
+
+inline size_t al256(size_t v) { return (v + 255) / 256 * 256; }
+
+}  // namespace
+
+void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void set_last_error(const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line)
+{
+    set_last_error("CUDA error %d (%s) in %s at %s:%d", int(e), cudaGetErrorString(e), what, file, line);
+    return MLODS_ERR_CUDA;
+}
+
+KernelConsts make_kernel_consts(const mlods_kernel& k)
+{
+    KernelConsts c;
+    std::memset(&c, 0, sizeof c);
+    const double log2e = 1.4426950408889634;
+    c.type = k.type;
+    c.shift = k.constant_shift;
+    c.exponent = k.exponent;
+    c.nsig = k.n_sigmas;
+    const double sg = k.sigma;
+    c.g_scale = float(-log2e / (2.0 * sg * sg));
+    const double v = std::max(double(k.constant_shift), 1e-4);
+    c.num = float(std::pow(v, double(k.exponent)));
+    for (int i = 0; i < k.n_sigmas && i < MLODS_MAX_SIGMAS; ++i) {
+        const double s = k.sigmas[i];
+        c.ms_scale[i] = float(-log2e / (2.0 * s * s));
+        c.ms_w[i] = float(1.0 / (s * s * s));
+    }
+    return c;
+}
+
+// Ensures the tree's projection scratch holds `bytes` bytes (plus the stats
+// block at its start).
+static int ensure_scratch(mlods_tree_s* T, size_t bytes)
+{
+    const size_t need = al256(8 * sizeof(int64_t)) + bytes;
+    if (T->d_scratch && T->scratch_bytes >= need) return MLODS_OK;
+    if (T->d_scratch) cudaFree(T->d_scratch);
+    T->d_scratch = nullptr;
+    T->scratch_bytes = 0;
+    MLODS_CUDA(cudaMalloc(&T->d_scratch, need));
+    T->scratch_bytes = need;
+    T->d_stats = static_cast<int64_t*>(T->d_scratch);
+    return MLODS_OK;
+}
+
+static int project_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
+                        float step_max, cudaStream_t s)
+{
+    if (!T->kernel_set) {
+        set_last_error("project: no kernel set (call mlods_set_kernel first)");
+        return MLODS_ERR_STATE;
+    }
+    if (n <= 0 || n >= (int64_t(1) << 32)) {
+        set_last_error("project: n=%lld out of range [1, 2^32)", (long long)n);
+        return MLODS_ERR_INVALID;
+    }
+    if (iters < 0) {
+        set_last_error("project: negative iteration count");
+        return MLODS_ERR_INVALID;
+    }
+    if (T->params.mode != MLODS_MODE_MLOD) {
+        set_last_error("project: mode %d not available in this build", T->params.mode);
+        return MLODS_ERR_INVALID;
+    }
+    const bool reorder = T->params.reorder != 0 && n > 1;
+    const size_t order_bytes = reorder ? al256(size_t(n) * 4) + query_order_temp_bytes(n) : 0;
+    int rc = ensure_scratch(T, order_bytes);
+    if (rc != MLODS_OK) return rc;
+    char* base = static_cast<char*>(T->d_scratch) + al256(8 * sizeof(int64_t));
+    MLODS_CUDA(cudaMemsetAsync(T->d_stats, 0, 8 * sizeof(int64_t), s));
+    uint32_t* d_order = nullptr;
+    if (reorder) {
+        d_order = reinterpret_cast<uint32_t*>(base);
+        float ext = 0.f;
+        for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
+        MLODS_CUDA(compute_query_order(d_q, n, T->origin, ext, d_order, base + al256(size_t(n) * 4), s));
+    }
+    ProjectArgs a;
+    a.nodes = T->d_nodes;
+    a.q_in = d_q;
+    a.out_p = d_out_p;
+    a.out_n = d_out_n;
+    a.order = d_order;
+    a.nq = n;
+    a.n_iter = iters;
+    a.cutoff = T->params.cutoff;
+    a.min_depth = T->params.min_depth;
+    a.step_max = step_max < 0.f ? T->root_radius : step_max;
+    a.o0 = T->origin[0];
+    a.o1 = T->origin[1];
+    a.o2 = T->origin[2];
+    a.kc = T->kc;
+    a.counter = reinterpret_cast<unsigned int*>(T->d_stats + 3);
+    a.stats = T->d_stats;
+    if (!T->ev_start) {
+        MLODS_CUDA(cudaEventCreate(&T->ev_start));
+        MLODS_CUDA(cudaEventCreate(&T->ev_stop));
+    }
+    MLODS_CUDA(cudaEventRecord(T->ev_start, s));
+    MLODS_CUDA(launch_mlod_project(a, T->kc.type, T->params.blend_rule, sm_count_for_current_device(), s));
+    MLODS_CUDA(cudaEventRecord(T->ev_stop, s));
+    T->timed = true;
+    return MLODS_OK;
+}
+
+}  // namespace mlods
+
+using namespace mlods;
+
+#define CHECK_TREE(t)                                  \
+    do {                                               \
+        if (!(t)) {                                    \
+            set_last_error("null tree handle");        \
+            return MLODS_ERR_INVALID;                  \
+        }                                              \
+    } while (0)
+
+extern "C" {
+
+const char* mlods_last_error(void) { return g_err; }
+
+int mlods_version(void) { return 100; }
+
+void mlods_default_params(mlods_params* p)
+{
+    if (!p) return;
+    p->cutoff = 2.f;        // GPUUtils.h:63
+    p->min_depth = 0;       // GPUUtils.h:64
+    p->mode = MLODS_MODE_MLOD;
+    p->knn = 20;            // CPUUtils.h:211
+    p->ball_radius = 0.1f;  // CPUUtils.h:214
+    p->blend_rule = MLODS_BLEND_GPU;
+    p->reorder = 1;
+    p->prune_tol = 0.f;
+}
+
+int mlods_tree_build_device(const float* d_pts, const float* d_nrm, int64_t n, int32_t max_depth, void* stream,
+                            mlods_tree* out)
+{
+    if (!out || !d_pts || !d_nrm) {
+        set_last_error("tree build: null argument");
+        return MLODS_ERR_INVALID;
+    }
+    *out = nullptr;
+    auto* T = new (std::nothrow) mlods_tree_s();
+    if (!T) {
+        set_last_error("tree build: host allocation failed");
+        return MLODS_ERR_CAPACITY;
+    }
+    mlods_default_params(&T->params);
+    const int rc = build_tree(T, d_pts, d_nrm, n, max_depth, static_cast<cudaStream_t>(stream));
+    if (rc != MLODS_OK) {
+        free_tree_device(T);
+        delete T;
+        return rc;
+    }
+    *out = T;
+    return MLODS_OK;
+}
+
+int mlods_tree_build(const float* pts, const float* nrm, int64_t n, int32_t max_depth, void* stream,
+                     mlods_tree* out)
+{
+    if (!out || !pts || !nrm) {
+        set_last_error("tree build: null argument");
+        return MLODS_ERR_INVALID;
+    }
+    if (n <= 0) {
+        set_last_error("tree build: n must be positive");
+        return MLODS_ERR_INVALID;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float* d = nullptr;
+    MLODS_CUDA(cudaMalloc(&d, size_t(n) * 6 * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(d, pts, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d + 3 * n, nrm, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_fail(e, "tree build upload", __FILE__, __LINE__);
+    }
+    const int rc = mlods_tree_build_device(d, d + 3 * n, n, max_depth, stream, out);
+    cudaStreamSynchronize(s);
+    cudaFree(d);
+    return rc;
+}
+
+int mlods_tree_free(mlods_tree t)
+{
+    if (!t) return MLODS_OK;
+    free_tree_device(t);
+    cudaFree(t->d_q);
+    cudaFree(t->d_qn);
+    cudaFree(t->d_scratch);
+    if (t->ev_start) cudaEventDestroy(t->ev_start);
+    if (t->ev_stop) cudaEventDestroy(t->ev_stop);
+    delete t;
+    return MLODS_OK;
+}
+
+int mlods_tree_get_info(mlods_tree t, mlods_tree_info* info)
+{
+    CHECK_TREE(t);
+    if (!info) {
+        set_last_error("null info");
+        return MLODS_ERR_INVALID;
+    }
+    info->n_points = t->n_pts;
+    info->n_nodes = t->n_nodes;
+    info->n_extra = t->n_extra;
+    info->depth = t->depth;
+    info->max_depth = t->max_depth;
+    info->n_ties = t->n_ties;
+    for (int a = 0; a < 3; ++a) {
+        info->bbox_min[a] = t->bb[a];
+        info->bbox_max[a] = t->BB[a];
+        info->origin[a] = t->origin[a];
+    }
+    info->device_bytes = t->device_bytes;
+    return MLODS_OK;
+}
+
+int mlods_tree_export(mlods_tree t, int32_t* depth, int32_t* parent, int32_t* first_child, int32_t* n_children,
+                      int32_t* next_brother, int32_t* leaf_off, int32_t* leaf_cnt, int32_t* perm, float* bmin,
+                      float* bmax, double* mom, float* area)
+{
+    CHECK_TREE(t);
+    return export_tree(t, depth, parent, first_child, n_children, next_brother, leaf_off, leaf_cnt, perm, bmin, bmax,
+                       mom, area);
+}
+
+int mlods_set_kernel(mlods_tree t, const mlods_kernel* k)
+{
+    CHECK_TREE(t);
+    if (!k) {
+        set_last_error("null kernel");
+        return MLODS_ERR_INVALID;
+    }
+    if (k->type != MLODS_GAUSSIAN && k->type != MLODS_SINGULAR && k->type != MLODS_GAUSSIAN_MULTIPLE) {
+        set_last_error("unknown kernel type %d", k->type);
+        return MLODS_ERR_INVALID;
+    }
+    if (k->n_sigmas < 0 || k->n_sigmas > MLODS_MAX_SIGMAS) {
+        set_last_error("n_sigmas=%d out of range [0, %d]", k->n_sigmas, MLODS_MAX_SIGMAS);
+        return MLODS_ERR_CAPACITY;
+    }
+    if (k->type == MLODS_GAUSSIAN_MULTIPLE && k->n_sigmas == 0) {
+        set_last_error("multi-Gaussian kernel needs at least one sigma");
+        return MLODS_ERR_INVALID;
+    }
+    if (k->type == MLODS_GAUSSIAN && !(k->sigma > 0.f)) {
+        set_last_error("Gaussian kernel needs sigma > 0");
+        return MLODS_ERR_INVALID;
+    }
+    t->kernel = *k;
+    t->kc = make_kernel_consts(*k);
+    t->kernel_set = true;
+    return MLODS_OK;
+}
+
+int mlods_set_params(mlods_tree t, const mlods_params* p)
+{
+    CHECK_TREE(t);
+    if (!p) {
+        set_last_error("null params");
+        return MLODS_ERR_INVALID;
+    }
+    if (p->mode < MLODS_MODE_MLOD || p->mode > MLODS_MODE_BALL || (p->blend_rule != MLODS_BLEND_GPU &&
+                                                                   p->blend_rule != MLODS_BLEND_CPU)) {
+        set_last_error("invalid mode %d or blend rule %d", p->mode, p->blend_rule);
+        return MLODS_ERR_INVALID;
+    }
+    if (p->min_depth < 0) {
+        set_last_error("min_depth must be >= 0");
+        return MLODS_ERR_INVALID;
+    }
+    t->params = *p;
+    return MLODS_OK;
+}
+
+int mlods_queries_upload(mlods_tree t, int64_t n, const float* pts, void* stream)
+{
+    CHECK_TREE(t);
+    if (n <= 0 || !pts) {
+        set_last_error("queries upload: n must be positive and pts non-null");
+        return MLODS_ERR_INVALID;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (t->q_n < n || !t->d_q) {
+        cudaFree(t->d_q);
+        cudaFree(t->d_qn);
+        t->d_q = t->d_qn = nullptr;
+        t->q_n = 0;
+        MLODS_CUDA(cudaMalloc(&t->d_q, size_t(n) * 3 * sizeof(float)));
+        MLODS_CUDA(cudaMalloc(&t->d_qn, size_t(n) * 3 * sizeof(float)));
+    }
+    t->q_n = n;
+    MLODS_CUDA(cudaMemcpyAsync(t->d_q, pts, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
+    MLODS_CUDA(cudaMemsetAsync(t->d_qn, 0, size_t(n) * 3 * sizeof(float), s));
+    return MLODS_OK;
+}
+
+int mlods_project(mlods_tree t, int64_t n, int32_t n_iterations, float step_max, float* out_pts, float* out_nrm,
+                  void* stream)
+{
+    CHECK_TREE(t);
+    if (n == 0) {
+        set_last_error("No points to project");  // Fastapss.cu:441-445
+        return MLODS_ERR_INVALID;
+    }
+    if (!t->d_q || n > t->q_n) {
+        set_last_error("project: %lld queries requested, %lld uploaded", (long long)n, (long long)t->q_n);
+        return MLODS_ERR_STATE;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = project_impl(t, n, t->d_q, t->d_q, t->d_qn, n_iterations, step_max, s);
+    if (rc != MLODS_OK) return rc;
+    if (out_pts)
+        MLODS_CUDA(cudaMemcpyAsync(out_pts, t->d_q, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (out_nrm)
+        MLODS_CUDA(cudaMemcpyAsync(out_nrm, t->d_qn, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    MLODS_CUDA(cudaStreamSynchronize(s));
+    return MLODS_OK;
+}
+
+int mlods_queries_free(mlods_tree t)
+{
+    CHECK_TREE(t);
+    cudaFree(t->d_q);
+    cudaFree(t->d_qn);
+    t->d_q = t->d_qn = nullptr;
+    t->q_n = 0;
+    return MLODS_OK;
+}
+
+int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out_pts, float* d_out_nrm,
+                         int32_t n_iterations, float step_max, void* stream)
+{
+    CHECK_TREE(t);
+    if (!d_q || !d_out_pts || !d_out_nrm) {
+        set_last_error("project_device: null buffer");
+        return MLODS_ERR_INVALID;
+    }
+    return project_impl(t, n, d_q, d_out_pts, d_out_nrm, n_iterations, step_max, static_cast<cudaStream_t>(stream));
+}
+
+int mlods_last_stats(mlods_tree t, int64_t* node_visits, int32_t* max_stack, int64_t* overflows,
+                     float* kernel_ms)
+{
+    CHECK_TREE(t);
+    int64_t h[4] = {0, 0, 0, 0};
+    float ms = 0.f;
+    if (t->timed) {
+        MLODS_CUDA(cudaEventSynchronize(t->ev_stop));
+        MLODS_CUDA(cudaEventElapsedTime(&ms, t->ev_start, t->ev_stop));
+    }
+    if (t->d_stats) MLODS_CUDA(cudaMemcpy(h, t->d_stats, sizeof h, cudaMemcpyDeviceToHost));
+    if (node_visits) *node_visits = h[0];
+    if (max_stack) *max_stack = int32_t(h[1]);
+    if (overflows) *overflows = h[2];
+    if (kernel_ms) *kernel_ms = ms;
+    return MLODS_OK;
+}
+
+int64_t mlods_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// tree.cuh -- the tree handle behind mlods_tree.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mlods_internal.cuh"
+
+struct mlods_tree_s {
+    int device = 0;
+    int64_t n_pts = 0;
+    int max_depth = 0;
+    int depth = 0;
+    int64_t n_nodes = 0;   // reference nodes
+    int64_t n_extra = 0;   // point records of multi-point leaves
+    int64_t n_ties = 0;
+    float bb[3] = {0, 0, 0};
+    float BB[3] = {0, 0, 0};
+    double origin[3] = {0, 0, 0};
+    float root_radius = 0.f;  // BBOX::radius of the root box, float as the reference
+
+    // device data
+    mlods::DNode* d_nodes = nullptr;       // n_nodes + n_extra records
+    int32_t* d_node_head = nullptr;        // sorted position of each node's first point
+    uint64_t* d_codes = nullptr;           // Morton codes in sorted order
+    uint32_t* d_perm = nullptr;            // sorted position -> original point index
+    float* d_area = nullptr;               // per original point (float, as the reference)
+    float4* d_spts = nullptr;              // sorted points, local frame: xyz, w = original index bits
+    float4* d_snrm = nullptr;              // sorted normals
+    float* d_bounds = nullptr;             // per-axis float bound tables (3 x table size)
+    int64_t bounds_stride = 0;
+
+    // configuration
+    mlods_kernel kernel{};
+    mlods::KernelConsts kc{};
+    mlods_params params{};
+    bool kernel_set = false;
+
+    // query buffer of the copyPointsToGPU protocol
+    float* d_q = nullptr;
+    float* d_qn = nullptr;
+    int64_t q_n = 0;
+
+    // reusable scratch for projection (grown on demand)
+    void* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int64_t* d_stats = nullptr;  // [0] visits, [1] max stack, [2] overflows, [3] work counter
+    int64_t last_visits = 0;
+    int32_t last_max_stack = 0;
+    int64_t last_overflows = 0;
+
+    int64_t device_bytes = 0;
+
+    // CUDA events bracketing the last projection kernel (created on first use)
+    cudaEvent_t ev_start = nullptr;
+    cudaEvent_t ev_stop = nullptr;
+    bool timed = false;
+};
+
+namespace mlods
+{
+// Builds the tree from device arrays (xyz float triples).
+int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t n, int max_depth, cudaStream_t s);
+void free_tree_device(mlods_tree_s* T);
+int export_tree(mlods_tree_s* T, int32_t* depth, int32_t* parent, int32_t* first_child, int32_t* n_children,
+                int32_t* next_brother, int32_t* leaf_off, int32_t* leaf_cnt, int32_t* perm, float* bmin, float* bmax,
+                double* mom, float* area);
+}  // namespace mlods

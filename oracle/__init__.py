@@ -1,0 +1,248 @@
+"""Test infrastructure: the CPU checkers of the projection path.
+
+* ``liboracle`` -- oracle/mlods_oracle.c, an FP64 restatement of the
+  reference's algorithm (tree build, MLoD traversal with both blend rules,
+  sphere fit, global/kNN/ball APSS, DC corner field and vertex).
+* ``libref`` -- the reference's own CPU code (sources/apss/CPUUtils.cpp,
+  Kernel.cpp, kdTreeNN.h) compiled by oracle/Makefile behind ref_shim.cpp.
+
+Only tests, the smoke test and the benchmark's CPU-baseline/reference arms
+use this module; the library never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libmlods_oracle.so"
+REF_SO = HERE / "_ref" / "libmlods_ref.so"
+REF_ROOT = Path(os.environ.get("MLODS_REF_ROOT", "/root/reference"))
+
+_P = C.c_void_p
+_orc = None
+_ref = None
+
+
+def build(with_ref: bool = True) -> None:
+    """Compile the oracle (and the reference shim when the sources exist)."""
+    targets = ["oracle"]
+    if with_ref and (REF_ROOT / "sources" / "apss").is_dir():
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF_ROOT={REF_ROOT}"] + targets, check=True)
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def _ptr(a):
+    return C.c_void_p(0) if a is None else C.c_void_p(a.ctypes.data)
+
+
+def orc() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORACLE_SO.exists():
+            build(with_ref=False)
+        lib = C.CDLL(os.fspath(ORACLE_SO))
+        lib.orc_tree_build.restype = _P
+        lib.orc_tree_build.argtypes = [_P, _P, C.c_int64, C.c_int]
+        lib.orc_tree_free.argtypes = [_P]
+        lib.orc_tree_num_nodes.restype = C.c_int64
+        lib.orc_tree_num_nodes.argtypes = [_P]
+        lib.orc_tree_num_ties.restype = C.c_int64
+        lib.orc_tree_num_ties.argtypes = [_P]
+        lib.orc_tree_radius.restype = C.c_double
+        lib.orc_tree_radius.argtypes = [_P]
+        lib.orc_tree_export.argtypes = [_P] + [_P] * 12
+        lib.orc_project_mlod.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         _P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, _P, _P, _P]
+        lib.orc_project_global.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                           _P, C.c_int, C.c_double, _P, _P]
+        lib.orc_knn.argtypes = [_P, C.c_int64, _P, C.c_int64, C.c_int, _P, _P, _P]
+        lib.orc_project_apss.argtypes = [_P, _P, C.c_int64, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_double,
+                                         C.c_int, C.c_double, C.c_double, C.c_double, _P, C.c_int, C.c_double, _P, _P]
+        lib.orc_dc_field.argtypes = [_P, _P, _P, C.c_int64, _P]
+        lib.orc_dc_vertex.argtypes = [_P, C.c_double, _P, _P, _P]
+        _orc = lib
+    return _orc
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (needs the reference sources)")
+        lib = C.CDLL(os.fspath(REF_SO))
+        lib.ref_tree_build.restype = _P
+        lib.ref_tree_build.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_uint]
+        lib.ref_tree_free.argtypes = [_P]
+        lib.ref_tree_num_nodes.restype = C.c_int64
+        lib.ref_tree_num_nodes.argtypes = [_P]
+        lib.ref_tree_depth.restype = C.c_int
+        lib.ref_tree_depth.argtypes = [_P]
+        lib.ref_tree_export.argtypes = [_P] + [_P] * 12
+        lib.ref_project.restype = C.c_double
+        lib.ref_project.argtypes = [_P, _P, _P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, _P,
+                                    C.c_int, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int, C.c_float, C.c_int]
+        lib.ref_kdtree_knn.argtypes = [_P, C.c_int64, _P, C.c_int64, C.c_int, _P, _P]
+        _ref = lib
+    return _ref
+
+
+def _kargs(kernel):
+    """(type, sigma, exponent, shift, sigmas float64 array, nsig) of a Kernel-like object."""
+    sig = np.ascontiguousarray(np.asarray(kernel.sigmas if len(kernel.sigmas) else [0.0], np.float64))
+    return int(kernel.type), float(kernel.sigma), float(kernel.exponent), float(kernel.constant_shift), sig, \
+        len(kernel.sigmas)
+
+
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, np.float32))
+
+
+EXPORT_KEYS = ["depth", "parent", "first_child", "n_children", "next_brother", "leaf_off", "leaf_cnt", "perm",
+               "bmin", "bmax"]
+
+
+class OracleTree:
+    """FP64 restatement of APSSOctree (oracle/mlods_oracle.c)."""
+
+    def __init__(self, pts, nrm, max_depth: int = 12):
+        self.pts = _f32(pts)
+        self.nrm = _f32(nrm)
+        self._h = orc().orc_tree_build(_ptr(self.pts), _ptr(self.nrm), len(self.pts), int(max_depth))
+        if not self._h:
+            raise ValueError("oracle tree build failed")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            orc().orc_tree_free(self._h)
+            self._h = None
+
+    @property
+    def n_nodes(self) -> int:
+        return int(orc().orc_tree_num_nodes(self._h))
+
+    @property
+    def n_ties(self) -> int:
+        return int(orc().orc_tree_num_ties(self._h))
+
+    @property
+    def radius(self) -> float:
+        return float(orc().orc_tree_radius(self._h))
+
+    def export(self) -> dict:
+        nn, n = self.n_nodes, len(self.pts)
+        out = {k: np.empty(nn, np.int32) for k in EXPORT_KEYS[:7]}
+        out["perm"] = np.empty(n, np.int32)
+        out["bmin"] = np.empty((nn, 3), np.float32)
+        out["bmax"] = np.empty((nn, 3), np.float32)
+        out["mom"] = np.empty((nn, 9), np.float64)
+        out["area"] = np.empty(n, np.float64)
+        keys = EXPORT_KEYS + ["mom", "area"]
+        orc().orc_tree_export(self._h, *[_ptr(out[k]) for k in keys])
+        return out
+
+    def project_mlod(self, q, n_iter, kernel, rule=0, cutoff=2.0, min_depth=0, step_max=-1.0, visited=False):
+        q = _f32(q)
+        n = len(q)
+        op = np.empty((n, 3), np.float64)
+        on = np.empty((n, 3), np.float64)
+        vis = np.empty(n, np.int64) if visited else None
+        t, s, e, sh, sig, ns = _kargs(kernel)
+        orc().orc_project_mlod(self._h, _ptr(q), n, int(n_iter), t, s, e, sh, _ptr(sig), ns, int(rule),
+                               float(cutoff), int(min_depth), float(step_max), _ptr(op), _ptr(on), _ptr(vis))
+        return (op, on, vis) if visited else (op, on)
+
+    def project_global(self, q, n_iter, kernel, step_max=-1.0):
+        q = _f32(q)
+        n = len(q)
+        op = np.empty((n, 3), np.float64)
+        on = np.empty((n, 3), np.float64)
+        t, s, e, sh, sig, ns = _kargs(kernel)
+        orc().orc_project_global(self._h, _ptr(q), n, int(n_iter), t, s, e, sh, _ptr(sig), ns, float(step_max),
+                                 _ptr(op), _ptr(on))
+        return op, on
+
+
+def knn(pts, q, k):
+    """Exact kNN (brute force, kdTreeNN distance arithmetic); (idx, d2, tie)."""
+    pts, q = _f32(pts), _f32(q)
+    idx = np.empty((len(q), k), np.int32)
+    d2 = np.empty((len(q), k), np.float64)
+    tie = np.empty(len(q), np.int32)
+    orc().orc_knn(_ptr(pts), len(pts), _ptr(q), len(q), int(k), _ptr(idx), _ptr(d2), _ptr(tie))
+    return idx, d2, tie
+
+
+def project_apss(pts, nrm, q, n_iter, kernel, mode, k=20, ball_r=0.1, step_max=1.0):
+    """kNN (mode 0) / ball (mode 1) APSS restatement (CPUUtils.cpp:690-737)."""
+    pts, nrm, q = _f32(pts), _f32(nrm), _f32(q)
+    op = np.empty((len(q), 3), np.float64)
+    on = np.empty((len(q), 3), np.float64)
+    t, s, e, sh, sig, ns = _kargs(kernel)
+    orc().orc_project_apss(_ptr(pts), _ptr(nrm), len(pts), _ptr(q), len(q), int(n_iter), int(mode), int(k),
+                           float(ball_r), t, s, e, sh, _ptr(sig), ns, float(step_max), _ptr(op), _ptr(on))
+    return op, on
+
+
+class RefTree:
+    """The reference's own APSSOctree, built and run on the CPU (oracle/_ref)."""
+
+    def __init__(self, pts, nrm, max_depth: int = 12, seed: int = 0):
+        self.pts = _f32(pts)
+        self.nrm = _f32(nrm)
+        self._h = ref().ref_tree_build(_ptr(self.pts), _ptr(self.nrm), len(self.pts), int(max_depth), int(seed))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            ref().ref_tree_free(self._h)
+            self._h = None
+
+    @property
+    def n_nodes(self) -> int:
+        return int(ref().ref_tree_num_nodes(self._h))
+
+    @property
+    def depth(self) -> int:
+        return int(ref().ref_tree_depth(self._h))
+
+    def export(self) -> dict:
+        nn, n = self.n_nodes, len(self.pts)
+        out = {k: np.empty(nn, np.int32) for k in EXPORT_KEYS[:7]}
+        out["perm"] = np.empty(n, np.int32)
+        out["bmin"] = np.empty((nn, 3), np.float32)
+        out["bmax"] = np.empty((nn, 3), np.float32)
+        out["stats"] = np.empty((nn, 9), np.float32)
+        out["area"] = np.empty(n, np.float32)
+        keys = EXPORT_KEYS + ["stats", "area"]
+        ref().ref_tree_export(self._h, *[_ptr(out[k]) for k in keys])
+        return out
+
+    def project(self, q, n_iter, kernel, cutoff=2.0, min_depth=0, step_max=-1.0, mode=0, k=20, ball_r=0.1,
+                nthreads=0):
+        """Returns (points, normals, seconds) from APSSOctree::projectCPU."""
+        q = _f32(q)
+        n = len(q)
+        op = np.empty((n, 3), np.float32)
+        on = np.empty((n, 3), np.float32)
+        sig = np.ascontiguousarray(np.asarray(kernel.sigmas if len(kernel.sigmas) else [0.0], np.float32))
+        secs = ref().ref_project(self._h, _ptr(q), _ptr(op), _ptr(on), n, int(n_iter), int(kernel.type),
+                                 float(kernel.sigma), float(kernel.exponent), float(kernel.constant_shift), _ptr(sig),
+                                 len(kernel.sigmas), float(cutoff), int(min_depth), float(step_max), int(mode),
+                                 int(k), float(ball_r), int(nthreads))
+        return op, on, secs
+
+
+def ref_kdtree_knn(pts, q, k):
+    pts, q = _f32(pts), _f32(q)
+    idx = np.empty((len(q), k), np.int32)
+    d2 = np.empty((len(q), k), np.float64)
+    ref().ref_kdtree_knn(_ptr(pts), len(pts), _ptr(q), len(q), int(k), _ptr(idx), _ptr(d2))
+    return idx, d2

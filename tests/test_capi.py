@@ -1,0 +1,57 @@
+"""libmlods.so loads, exports every entry point include/mlods.h declares, and
+validates arguments before touching the GPU (no device needed)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from mlodsurfaces_b200 import _capi as capi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "mlods.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mlods_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "mlods_tree_build" in names and "mlods_project" in names
+    assert len(names) >= 15
+
+
+def test_library_exports_every_declared_symbol():
+    lib = capi.load()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_bindings_cover_the_header():
+    assert set(declared_functions()) == set(capi.SIGNATURES)
+
+
+def test_null_handles_are_rejected_without_a_gpu():
+    lib = capi.load()
+    assert lib.mlods_set_kernel(None, None) == capi.MLODS_ERR_INVALID
+    assert b"null" in lib.mlods_last_error()
+    assert lib.mlods_project(None, 10, 1, -1.0, None, None, None) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_tree_build(None, None, 0, 12, None, C.byref(C.c_void_p())) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_tree_free(None) == capi.MLODS_OK
+
+
+def test_default_params_follow_the_reference():
+    lib = capi.load()
+    p = capi.mlods_params()
+    lib.mlods_default_params(C.byref(p))
+    assert p.cutoff == pytest.approx(2.0)  # GPUUtils.h:63
+    assert p.min_depth == 0
+    assert p.knn == 20 and p.ball_radius == pytest.approx(0.1)
+    assert p.blend_rule == capi.BLEND_GPU and p.mode == capi.MODE_MLOD
+
+
+def test_error_raises():
+    with pytest.raises(capi.MlodsError):
+        capi.check(capi.load().mlods_set_params(None, None))
