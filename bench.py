@@ -219,7 +219,7 @@ def run_ours(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
     launches0 = lib.mlods_kernel_launches()
-    step_ms, kern_ms, visits = [], [], []
+    step_ms, kern_ms, visits, rounds, max_stack = [], [], [], [], 0
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -232,6 +232,8 @@ def run_ours(args, rank, world, local_rank):
         st = f.last_stats()
         kern_ms.append(st["kernel_ms"])
         visits.append(st["node_visits"])
+        rounds.append(st["rounds"])
+        max_stack = max(max_stack, st["max_stack"])
         if st["overflows"]:
             raise RuntimeError(f"{st['overflows']} queries overflowed the traversal stack")
     torch.cuda.synchronize(dev)
@@ -253,14 +255,15 @@ def run_ours(args, rank, world, local_rank):
     h_n = torch.empty_like(h_q).pin_memory()
     e2e_ms = []
     h = tree.handle
+    qb = f._q
     f._sync_params()
     default = torch.cuda.default_stream(dev)
     for i in range(args.e2e_steps + 1):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(default)
-        capi.check(lib.mlods_queries_upload(h, len(q), C.c_void_p(h_q.data_ptr()), None))
-        capi.check(lib.mlods_project(h, len(q), args.iters, -1.0, C.c_void_p(h_p.data_ptr()),
+        capi.check(lib.mlods_queries_upload(qb, len(q), C.c_void_p(h_q.data_ptr()), None))
+        capi.check(lib.mlods_project(h, qb, len(q), args.iters, -1.0, C.c_void_p(h_p.data_ptr()),
                                      C.c_void_p(h_n.data_ptr()), None))
         e1.record(default)
         e1.synchronize()
@@ -306,6 +309,9 @@ def run_ours(args, rank, world, local_rank):
                              f" visits per query-iteration); peak {peak_kind}; node records are mostly served "
                              f"from L1/L2"},
         "kernel_ms": kms,
+        "traversal": {"visits_per_query_iteration": mean_visits / len(q) / args.iters,
+                      "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),
+                      "max_stack_ranges": max_stack},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

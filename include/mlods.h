@@ -124,18 +124,40 @@ void mlods_default_params(mlods_params* p);
 int mlods_set_params(mlods_tree t, const mlods_params* p);
 
 /* ---- query buffer protocol (Fastapss::copyToGPU/project, APSS::copyPointsToGPU) ----
- * mlods_queries_upload copies n host points into the tree's device query
- * buffer (APSS::copyPointsToGPU, GPUUtils.cu:406-411; an earlier buffer is
- * replaced, not leaked).  mlods_project runs n_iterations projection steps in
- * place on that buffer, so repeated calls continue from the last positions,
- * and copies positions/normals back when the host pointers are non-NULL
- * (Fastapss::project, Fastapss.cu:439-455).  step_max < 0 selects the root box
- * radius.  n must not exceed the uploaded count.  mlods_queries_free releases
- * the buffer (APSS::erasePointsFromGPU). */
-int mlods_queries_upload(mlods_tree t, int64_t n, const float* pts, void* stream);
-int mlods_project(mlods_tree t, int64_t n, int32_t n_iterations, float step_max, float* out_pts, float* out_nrm,
-                  void* stream);
-int mlods_queries_free(mlods_tree t);
+ * A query buffer is owned by its projection object, as APSS owns m_outPts and
+ * m_outNmls (GPUUtils.h:56-57); a tree can serve several buffers.
+ * mlods_queries_upload copies n host points into the buffer's device memory
+ * (APSS::copyPointsToGPU, GPUUtils.cu:406-411; an earlier upload is replaced,
+ * not leaked).  mlods_project runs n_iterations projection steps in place on
+ * that buffer, so repeated calls continue from the last positions, and
+ * copies positions/normals back when the host pointers are non-NULL
+ * (Fastapss::project, Fastapss.cu:439-455).  step_max < 0 selects the root
+ * box radius.  n must not exceed the uploaded count.  mlods_queries_free
+ * releases the device memory (APSS::erasePointsFromGPU) and keeps the handle;
+ * mlods_queries_destroy releases both. */
+typedef struct mlods_queries_s* mlods_queries;
+int mlods_queries_create(mlods_queries* out);
+int mlods_queries_destroy(mlods_queries q);
+int mlods_queries_upload(mlods_queries q, int64_t n, const float* pts, void* stream);
+int mlods_queries_free(mlods_queries q);
+int mlods_project(mlods_tree t, mlods_queries q, int64_t n, int32_t n_iterations, float step_max, float* out_pts,
+                  float* out_nrm, void* stream);
+
+/* Swaps the queries listed in invalid[0..n_invalid) with the tail of the first
+ * end_valid queries of the buffer, so that the valid ones come first
+ * (APSS::reorganizePoints and the reorganizePts kernel, GPUUtils.cu:413-424,
+ * :503-517).  invalid is a host array. */
+int mlods_queries_reorganize(mlods_queries q, int64_t n_invalid, const uint32_t* invalid, uint32_t end_valid,
+                             void* stream);
+
+/* ---- one-off host projection ---------------------------------------------
+ * Projects n host queries into host outputs without touching the query
+ * buffer (synchronous).  blend_rule overrides the tree's rule (-1 keeps it);
+ * the C++ mirror's projectCPU uses MLODS_BLEND_CPU here, the reference's CPU
+ * semantics (APSSOctree::projectCPU, CPUUtils.cpp:621-636), evaluated on the
+ * device. */
+int mlods_project_host(mlods_tree t, int64_t n, const float* q, float* out_pts, float* out_nrm, int32_t n_iterations,
+                       float step_max, int32_t blend_rule, void* stream);
 
 /* ---- device-buffer projection (no host traffic) ---------------------------
  * Projects n queries d_q (device, xyz) into d_out_pts / d_out_nrm (device).
@@ -143,12 +165,24 @@ int mlods_queries_free(mlods_tree t);
 int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out_pts, float* d_out_nrm,
                          int32_t n_iterations, float step_max, void* stream);
 
+/* ---- neighbour gathers -----------------------------------------------------
+ * k nearest neighbours of n device query points (world xyz), as the
+ * reference kd-tree's knearest (kdTreeNN.h:416-461, :590-600) which
+ * APSSOctree::knnMode uses: squared distances evaluated in float exactly as
+ * the kd-tree does, so the sets are equal except at exact distance ties at
+ * the k-th place (resolved here to the lower point index).  Rows are sorted
+ * by (distance, index); d_idx holds original point indices (-1 past the
+ * point count).  k <= MLODS_MAX_KNN.  Asynchronous. */
+#define MLODS_MAX_KNN 32
+int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_idx, float* d_d2, void* stream);
+
 /* ---- per-launch statistics of the last projection on this tree ------------
- * node visits summed over queries and iterations, largest traversal stack,
- * queries whose traversal stack overflowed (their result is the input point
- * with a zero normal), and the device time of the projection kernel itself
- * in milliseconds (CUDA events on the launching stream).  Synchronises. */
-int mlods_last_stats(mlods_tree t, int64_t* node_visits, int32_t* max_stack, int64_t* overflows,
+ * node visits summed over queries and iterations, warp rounds (32 lanes each)
+ * that evaluated them, largest traversal stack, queries whose traversal stack
+ * overflowed (their result is the input point with a zero normal), and the
+ * device time of the projection kernel itself in milliseconds (CUDA events on
+ * the launching stream).  Any pointer may be NULL.  Synchronises. */
+int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_t* max_stack, int64_t* overflows,
                      float* kernel_ms);
 
 /* Number of kernels this library has launched in this process (diagnostics). */

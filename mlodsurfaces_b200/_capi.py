@@ -22,6 +22,7 @@ GAUSSIAN = 0
 SINGULAR = 1
 GAUSSIAN_MULTIPLE = 2
 MAX_SIGMAS = 16
+MAX_KNN = 32
 
 MODE_MLOD = 0
 MODE_GLOBAL = 1
@@ -95,12 +96,17 @@ SIGNATURES = {
     "mlods_set_kernel": (C.c_int, [_P, C.POINTER(mlods_kernel)]),
     "mlods_default_params": (None, [C.POINTER(mlods_params)]),
     "mlods_set_params": (C.c_int, [_P, C.POINTER(mlods_params)]),
+    "mlods_queries_create": (C.c_int, [C.POINTER(_P)]),
+    "mlods_queries_destroy": (C.c_int, [_P]),
     "mlods_queries_upload": (C.c_int, [_P, C.c_int64, _P, _P]),
-    "mlods_project": (C.c_int, [_P, C.c_int64, C.c_int32, C.c_float, _P, _P, _P]),
+    "mlods_project": (C.c_int, [_P, _P, C.c_int64, C.c_int32, C.c_float, _P, _P, _P]),
     "mlods_queries_free": (C.c_int, [_P]),
     "mlods_project_device": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
-    "mlods_last_stats": (C.c_int, [_P, _I64, _I32, _I64, C.POINTER(C.c_float)]),
+    "mlods_queries_reorganize": (C.c_int, [_P, C.c_int64, _P, C.c_uint32, _P]),
+    "mlods_project_host": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, C.c_int32, _P]),
+    "mlods_last_stats": (C.c_int, [_P, _I64, _I64, _I32, _I64, C.POINTER(C.c_float)]),
     "mlods_kernel_launches": (C.c_int64, []),
+    "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),
 }
 
 _lib = None

@@ -210,6 +210,24 @@ class APSSOctree:
     def isAPSS(self) -> bool:
         return self.m_knnMode or self.m_ballMode
 
+    def knearest(self, queries, k: int):
+        """k nearest neighbours of host queries (kdTree::knearest semantics,
+        kdTreeNN.h:590-600): (indices int32 (n, k), squared distances float32)."""
+        import torch
+
+        q = torch.from_numpy(_f32x3(queries, "queries")).cuda()
+        idx = torch.empty((len(q), k), dtype=torch.int32, device=q.device)
+        d2 = torch.empty((len(q), k), dtype=torch.float32, device=q.device)
+        capi.check(self._lib.mlods_knn(self.handle, len(q), capi.ptr(q), int(k), capi.ptr(idx), capi.ptr(d2),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        torch.cuda.current_stream().synchronize()
+        return idx.cpu().numpy(), d2.cpu().numpy()
+
+    def getKnn(self, x, k: int):
+        """APSSOctree::getKnn (CPUUtils.cpp:665-672): the k nearest points of x."""
+        idx, _ = self.knearest(np.asarray(x, np.float32).reshape(1, 3), k)
+        return idx[0]
+
     def export(self) -> dict:
         """Topology and moments in breadth-first order (see mlods_tree_export)."""
         inf = self.info()
@@ -242,8 +260,19 @@ class APSS:
         self.reorder = True
         self.prune_tol = 0.0
         self._n_uploaded = 0
+        q = C.c_void_p(0)
+        capi.check(self._lib.mlods_queries_create(C.byref(q)))
+        self._q = q  # the device query buffer this object owns (APSS::m_outPts, GPUUtils.h:56)
         if kernel is not None:
             self.copyToGPU(kernel, nbOfVectors)
+
+    def __del__(self):
+        try:
+            if getattr(self, "_q", None):
+                self._lib.mlods_queries_destroy(self._q)
+                self._q = None
+        except Exception:
+            pass
 
     def _params(self) -> capi.mlods_params:
         p = capi.mlods_params()
@@ -284,14 +313,18 @@ class APSS:
 
     def copyPointsToGPU(self, nbOfVectors: int, outputPoints) -> None:
         pts = _f32x3(outputPoints, "points")[:nbOfVectors]
-        capi.check(self._lib.mlods_queries_upload(self.m_apssOctree.handle, int(nbOfVectors), capi.ptr(pts),
-                                                  C.c_void_p(0)))
+        capi.check(self._lib.mlods_queries_upload(self._q, int(nbOfVectors), capi.ptr(pts), C.c_void_p(0)))
         self._n_uploaded = int(nbOfVectors)
 
     def erasePointsFromGPU(self) -> None:
-        if self.m_apssOctree._h:
-            self._lib.mlods_queries_free(self.m_apssOctree.handle)
+        capi.check(self._lib.mlods_queries_free(self._q))
         self._n_uploaded = 0
+
+    def reorganizePoints(self, invalidPts, endValid: int) -> None:
+        """APSS::reorganizePoints (GPUUtils.cu:503-517)."""
+        inv = np.ascontiguousarray(np.asarray(invalidPts, np.uint32))
+        capi.check(self._lib.mlods_queries_reorganize(self._q, len(inv), capi.ptr(inv), int(endValid),
+                                                      C.c_void_p(0)))
 
     def project(self, nbOfVectors: int, outputPoints, outputNormals, n_iterations: int, kernel: Kernel | None = None,
                 stepMaxSize: float = -1.0) -> None:
@@ -305,7 +338,7 @@ class APSS:
         for a in (op, on):
             if a is not None and (a.dtype != np.float32 or not a.flags.c_contiguous or a.shape[0] < nbOfVectors):
                 raise ValueError("output arrays must be C-contiguous float32 with at least n rows")
-        capi.check(self._lib.mlods_project(self.m_apssOctree.handle, int(nbOfVectors), int(n_iterations),
+        capi.check(self._lib.mlods_project(self.m_apssOctree.handle, self._q, int(nbOfVectors), int(n_iterations),
                                            float(stepMaxSize), capi.ptr(op), capi.ptr(on), C.c_void_p(0)))
 
     def project_device(self, d_q, d_out_p, d_out_n, n_iterations: int, stepMaxSize: float = -1.0,
@@ -318,12 +351,14 @@ class APSS:
 
     def last_stats(self):
         v = C.c_int64(0)
+        r = C.c_int64(0)
         m = C.c_int32(0)
         o = C.c_int64(0)
         ms = C.c_float(0)
-        capi.check(self._lib.mlods_last_stats(self.m_apssOctree.handle, C.byref(v), C.byref(m), C.byref(o),
-                                              C.byref(ms)))
-        return {"node_visits": v.value, "max_stack": m.value, "overflows": o.value, "kernel_ms": ms.value}
+        capi.check(self._lib.mlods_last_stats(self.m_apssOctree.handle, C.byref(v), C.byref(r), C.byref(m),
+                                              C.byref(o), C.byref(ms)))
+        return {"node_visits": v.value, "rounds": r.value, "max_stack": m.value, "overflows": o.value,
+                "kernel_ms": ms.value}
 
     # -- options, GPUUtils.h:40-43
     def setScalingProtectionSphere(self, val: float) -> None:
@@ -348,3 +383,9 @@ class Fastapss(APSS):
     """MLoD projection (Fastapss.h:32-51)."""
 
     mode = capi.MODE_MLOD
+
+
+class GlobalAPSS(APSS):
+    """APSS over every point, no level of detail (GlobalAPSS.h:19-43)."""
+
+    mode = capi.MODE_GLOBAL

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 
+#include "gather.cuh"
 #include "project.cuh"
 #include "tree.cuh"
 
@@ -85,8 +86,118 @@ static int ensure_scratch(mlods_tree_s* T, size_t bytes)
     return MLODS_OK;
 }
 
+// Pruning margin of the neighbour searches: points may sit up to half a
+// world-frame ulp outside their cell box (the reference classifies against the
+// double split but stores the float one), and local coordinates are rounded.
+static float gather_eps(const mlods_tree_s* T)
+{
+    float m = 0.f, ext = 0.f;
+    for (int a = 0; a < 3; ++a) {
+        m = std::max(m, std::max(std::fabs(T->bb[a]), std::fabs(T->BB[a])));
+        ext = std::max(ext, T->BB[a] - T->bb[a]);
+    }
+    const float ulp = std::nextafter(m, INFINITY) - m;
+    return 2.f * ulp + 1e-6f * ext + 1e-30f;
+}
+
+static void fill_gather_args(mlods_tree_s* T, GatherArgs& g)
+{
+    g.nodes = T->d_nodes;
+    g.node_head = T->d_node_head;
+    g.codes = T->d_codes;
+    g.wspts = T->d_wspts;
+    g.spts = T->d_spts;
+    g.snrm = T->d_snrm;
+    g.bounds = T->d_bounds;
+    g.bounds_stride = T->bounds_stride;
+    g.max_depth = T->max_depth;
+    g.n_pts = T->n_pts;
+    g.eps = gather_eps(T);
+    g.o0 = T->origin[0];
+    g.o1 = T->origin[1];
+    g.o2 = T->origin[2];
+    g.kc = T->kc;
+    g.counter = reinterpret_cast<unsigned int*>(T->d_stats + 3);
+    g.stats = T->d_stats;
+    g.out_idx = nullptr;
+    g.out_d2 = nullptr;
+}
+
+static int ensure_events(mlods_tree_s* T)
+{
+    if (!T->ev_start) {
+        MLODS_CUDA(cudaEventCreate(&T->ev_start));
+        MLODS_CUDA(cudaEventCreate(&T->ev_stop));
+    }
+    return MLODS_OK;
+}
+
+// Global, kNN and ball APSS projections (GlobalAPSS::project, GlobalAPSS.cu:203-235;
+// APSSOctree::projectAPSSCPU, CPUUtils.cpp:690-737).
+static int project_apss_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
+                             float step_max, cudaStream_t s)
+{
+    int rc = ensure_scratch(T, 0);
+    if (rc != MLODS_OK) return rc;
+    rc = ensure_events(T);
+    if (rc != MLODS_OK) return rc;
+    MLODS_CUDA(cudaMemsetAsync(T->d_stats, 0, 8 * sizeof(int64_t), s));
+    const float sm = step_max < 0.f ? T->root_radius : step_max;
+    const int mode = T->params.mode;
+    if (mode == MLODS_MODE_GLOBAL) {
+        GlobalArgs g;
+        g.spts = T->d_spts;
+        g.snrm = T->d_snrm;
+        g.area = T->d_area;
+        g.n_pts = T->n_pts;
+        g.q_in = d_q;
+        g.nq = n;
+        g.out_p = d_out_p;
+        g.out_n = d_out_n;
+        g.n_iter = iters;
+        g.step_max = sm;
+        g.o0 = T->origin[0];
+        g.o1 = T->origin[1];
+        g.o2 = T->origin[2];
+        g.kc = T->kc;
+        MLODS_CUDA(cudaEventRecord(T->ev_start, s));
+        MLODS_CUDA(launch_global_apss(g, T->kc.type, s));
+        MLODS_CUDA(cudaEventRecord(T->ev_stop, s));
+        T->timed = true;
+        return MLODS_OK;
+    }
+    GatherArgs g;
+    fill_gather_args(T, g);
+    g.q_in = d_q;
+    g.nq = n;
+    g.out_p = d_out_p;
+    g.out_n = d_out_n;
+    g.n_iter = iters;
+    g.step_max = sm;
+    g.k = T->params.knn;
+    if (mode == MLODS_MODE_KNN && (g.k < 1 || g.k > MLODS_MAX_KNN)) {
+        set_last_error("kNN: k=%d out of range [1, %d]", g.k, MLODS_MAX_KNN);
+        return MLODS_ERR_CAPACITY;
+    }
+    g.ball_r = T->params.ball_radius;
+    if (mode == MLODS_MODE_BALL && g.ball_r < 0.f) {
+        // CPUUtils.cpp:706-707: a negative radius means 3 * sigmas[0]
+        if (T->kernel.n_sigmas < 1) {
+            set_last_error("ball mode: radius < 0 needs a kernel with sigmas");
+            return MLODS_ERR_INVALID;
+        }
+        g.ball_r = T->kernel.sigmas[0] * 3;
+    }
+    MLODS_CUDA(cudaEventRecord(T->ev_start, s));
+    MLODS_CUDA(launch_gather(g, mode == MLODS_MODE_KNN ? kGatherKnnApss : kGatherBallApss, T->kc.type,
+                             sm_count_for_current_device(), s));
+    MLODS_CUDA(cudaEventRecord(T->ev_stop, s));
+    T->timed = true;
+    return MLODS_OK;
+}
+
 static int project_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
-                        float step_max, cudaStream_t s)
+                        float step_max, cudaStream_t s, int rule_override = -1)
 {
     if (!T->kernel_set) {
         set_last_error("project: no kernel set (call mlods_set_kernel first)");
@@ -100,10 +211,8 @@ static int project_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_o
         set_last_error("project: negative iteration count");
         return MLODS_ERR_INVALID;
     }
-    if (T->params.mode != MLODS_MODE_MLOD) {
-        set_last_error("project: mode %d not available in this build", T->params.mode);
-        return MLODS_ERR_INVALID;
-    }
+    if (T->params.mode != MLODS_MODE_MLOD)
+        return project_apss_impl(T, n, d_q, d_out_p, d_out_n, iters, step_max, s);
     const bool reorder = T->params.reorder != 0 && n > 1;
     const size_t order_bytes = reorder ? al256(size_t(n) * 4) + query_order_temp_bytes(n) : 0;
     int rc = ensure_scratch(T, order_bytes);
@@ -134,12 +243,11 @@ static int project_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_o
     a.kc = T->kc;
     a.counter = reinterpret_cast<unsigned int*>(T->d_stats + 3);
     a.stats = T->d_stats;
-    if (!T->ev_start) {
-        MLODS_CUDA(cudaEventCreate(&T->ev_start));
-        MLODS_CUDA(cudaEventCreate(&T->ev_stop));
-    }
+    rc = ensure_events(T);
+    if (rc != MLODS_OK) return rc;
     MLODS_CUDA(cudaEventRecord(T->ev_start, s));
-    MLODS_CUDA(launch_mlod_project(a, T->kc.type, T->params.blend_rule, sm_count_for_current_device(), s));
+    const int rule = rule_override >= 0 ? rule_override : T->params.blend_rule;
+    MLODS_CUDA(launch_mlod_project(a, T->kc.type, rule, sm_count_for_current_device(), s));
     MLODS_CUDA(cudaEventRecord(T->ev_stop, s));
     T->timed = true;
     return MLODS_OK;
@@ -231,8 +339,6 @@ int mlods_tree_free(mlods_tree t)
 {
     if (!t) return MLODS_OK;
     free_tree_device(t);
-    cudaFree(t->d_q);
-    cudaFree(t->d_qn);
     cudaFree(t->d_scratch);
     if (t->ev_start) cudaEventDestroy(t->ev_start);
     if (t->ev_stop) cudaEventDestroy(t->ev_stop);
@@ -320,58 +426,141 @@ int mlods_set_params(mlods_tree t, const mlods_params* p)
     return MLODS_OK;
 }
 
-int mlods_queries_upload(mlods_tree t, int64_t n, const float* pts, void* stream)
+int mlods_queries_create(mlods_queries* out)
 {
-    CHECK_TREE(t);
-    if (n <= 0 || !pts) {
-        set_last_error("queries upload: n must be positive and pts non-null");
+    if (!out) {
+        set_last_error("queries_create: null argument");
         return MLODS_ERR_INVALID;
     }
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (t->q_n < n || !t->d_q) {
-        cudaFree(t->d_q);
-        cudaFree(t->d_qn);
-        t->d_q = t->d_qn = nullptr;
-        t->q_n = 0;
-        MLODS_CUDA(cudaMalloc(&t->d_q, size_t(n) * 3 * sizeof(float)));
-        MLODS_CUDA(cudaMalloc(&t->d_qn, size_t(n) * 3 * sizeof(float)));
+    *out = new (std::nothrow) mlods_queries_s();
+    if (!*out) {
+        set_last_error("queries_create: host allocation failed");
+        return MLODS_ERR_CAPACITY;
     }
-    t->q_n = n;
-    MLODS_CUDA(cudaMemcpyAsync(t->d_q, pts, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
-    MLODS_CUDA(cudaMemsetAsync(t->d_qn, 0, size_t(n) * 3 * sizeof(float), s));
     return MLODS_OK;
 }
 
-int mlods_project(mlods_tree t, int64_t n, int32_t n_iterations, float step_max, float* out_pts, float* out_nrm,
-                  void* stream)
+int mlods_queries_free(mlods_queries q)
+{
+    if (!q) {
+        set_last_error("null query buffer");
+        return MLODS_ERR_INVALID;
+    }
+    cudaFree(q->d_q);
+    cudaFree(q->d_qn);
+    q->d_q = q->d_qn = nullptr;
+    q->n = q->cap = 0;
+    return MLODS_OK;
+}
+
+int mlods_queries_destroy(mlods_queries q)
+{
+    if (!q) return MLODS_OK;
+    mlods_queries_free(q);
+    delete q;
+    return MLODS_OK;
+}
+
+int mlods_queries_upload(mlods_queries q, int64_t n, const float* pts, void* stream)
+{
+    if (!q || n <= 0 || !pts) {
+        set_last_error("queries upload: null buffer, n <= 0 or null points");
+        return MLODS_ERR_INVALID;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (q->cap < n) {
+        mlods_queries_free(q);
+        MLODS_CUDA(cudaMalloc(&q->d_q, size_t(n) * 3 * sizeof(float)));
+        MLODS_CUDA(cudaMalloc(&q->d_qn, size_t(n) * 3 * sizeof(float)));
+        q->cap = n;
+    }
+    q->n = n;
+    MLODS_CUDA(cudaMemcpyAsync(q->d_q, pts, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
+    MLODS_CUDA(cudaMemsetAsync(q->d_qn, 0, size_t(n) * 3 * sizeof(float), s));
+    return MLODS_OK;
+}
+
+int mlods_project(mlods_tree t, mlods_queries q, int64_t n, int32_t n_iterations, float step_max, float* out_pts,
+                  float* out_nrm, void* stream)
 {
     CHECK_TREE(t);
+    if (!q) {
+        set_last_error("null query buffer");
+        return MLODS_ERR_INVALID;
+    }
     if (n == 0) {
         set_last_error("No points to project");  // Fastapss.cu:441-445
         return MLODS_ERR_INVALID;
     }
-    if (!t->d_q || n > t->q_n) {
-        set_last_error("project: %lld queries requested, %lld uploaded", (long long)n, (long long)t->q_n);
+    if (!q->d_q || n > q->n) {
+        set_last_error("project: %lld queries requested, %lld uploaded", (long long)n, (long long)q->n);
         return MLODS_ERR_STATE;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc = project_impl(t, n, t->d_q, t->d_q, t->d_qn, n_iterations, step_max, s);
+    int rc = project_impl(t, n, q->d_q, q->d_q, q->d_qn, n_iterations, step_max, s);
     if (rc != MLODS_OK) return rc;
     if (out_pts)
-        MLODS_CUDA(cudaMemcpyAsync(out_pts, t->d_q, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+        MLODS_CUDA(cudaMemcpyAsync(out_pts, q->d_q, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
     if (out_nrm)
-        MLODS_CUDA(cudaMemcpyAsync(out_nrm, t->d_qn, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+        MLODS_CUDA(cudaMemcpyAsync(out_nrm, q->d_qn, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
     MLODS_CUDA(cudaStreamSynchronize(s));
     return MLODS_OK;
 }
 
-int mlods_queries_free(mlods_tree t)
+int mlods_queries_reorganize(mlods_queries q, int64_t n_invalid, const uint32_t* invalid, uint32_t end_valid,
+                             void* stream)
+{
+    if (!q) {
+        set_last_error("null query buffer");
+        return MLODS_ERR_INVALID;
+    }
+    if (n_invalid == 0) return MLODS_OK;
+    if (n_invalid < 0 || !invalid || int64_t(end_valid) > q->n || n_invalid > int64_t(end_valid)) {
+        set_last_error("queries_reorganize: bad arguments (n_invalid=%lld end_valid=%u uploaded=%lld)",
+                       (long long)n_invalid, end_valid, (long long)q->n);
+        return MLODS_ERR_INVALID;
+    }
+    for (int64_t i = 0; i < n_invalid; ++i)
+        if (invalid[i] >= end_valid) {
+            set_last_error("queries_reorganize: index %u >= end_valid %u", invalid[i], end_valid);
+            return MLODS_ERR_INVALID;
+        }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t* d_inv = nullptr;
+    MLODS_CUDA(cudaMalloc(&d_inv, size_t(n_invalid) * 4));
+    cudaError_t e = cudaMemcpyAsync(d_inv, invalid, size_t(n_invalid) * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = launch_reorganize(q->d_q, d_inv, n_invalid, end_valid, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_inv);
+    if (e != cudaSuccess) return cuda_fail(e, "queries_reorganize", __FILE__, __LINE__);
+    return MLODS_OK;
+}
+
+int mlods_project_host(mlods_tree t, int64_t n, const float* q, float* out_pts, float* out_nrm, int32_t n_iterations,
+                       float step_max, int32_t blend_rule, void* stream)
 {
     CHECK_TREE(t);
-    cudaFree(t->d_q);
-    cudaFree(t->d_qn);
-    t->d_q = t->d_qn = nullptr;
-    t->q_n = 0;
+    if (n <= 0 || !q || !out_pts) {
+        set_last_error("project_host: n must be positive, q and out_pts non-null");
+        return MLODS_ERR_INVALID;
+    }
+    if (blend_rule != -1 && blend_rule != MLODS_BLEND_GPU && blend_rule != MLODS_BLEND_CPU) {
+        set_last_error("project_host: unknown blend rule %d", blend_rule);
+        return MLODS_ERR_INVALID;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float* d = nullptr;
+    MLODS_CUDA(cudaMalloc(&d, size_t(n) * 9 * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(d, q, size_t(n) * 12, cudaMemcpyHostToDevice, s);
+    int rc = MLODS_OK;
+    if (e == cudaSuccess) rc = project_impl(t, n, d, d + 3 * n, d + 6 * n, n_iterations, step_max, s, blend_rule);
+    if (e == cudaSuccess && rc == MLODS_OK) e = cudaMemcpyAsync(out_pts, d + 3 * n, size_t(n) * 12, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && rc == MLODS_OK && out_nrm)
+        e = cudaMemcpyAsync(out_nrm, d + 6 * n, size_t(n) * 12, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (rc != MLODS_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "project_host", __FILE__, __LINE__);
     return MLODS_OK;
 }
 
@@ -386,11 +575,43 @@ int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out
     return project_impl(t, n, d_q, d_out_pts, d_out_nrm, n_iterations, step_max, static_cast<cudaStream_t>(stream));
 }
 
-int mlods_last_stats(mlods_tree t, int64_t* node_visits, int32_t* max_stack, int64_t* overflows,
+int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_idx, float* d_d2, void* stream)
+{
+    CHECK_TREE(t);
+    if (n <= 0 || n >= (int64_t(1) << 32) || !d_q || !d_idx || !d_d2) {
+        set_last_error("knn: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    if (k < 1 || k > MLODS_MAX_KNN) {
+        set_last_error("knn: k=%d out of range [1, %d]", k, MLODS_MAX_KNN);
+        return MLODS_ERR_CAPACITY;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = ensure_scratch(t, 0);
+    if (rc != MLODS_OK) return rc;
+    MLODS_CUDA(cudaMemsetAsync(t->d_stats, 0, 8 * sizeof(int64_t), s));
+    GatherArgs g;
+    fill_gather_args(t, g);
+    g.q_in = d_q;
+    g.nq = n;
+    g.out_p = nullptr;
+    g.out_n = nullptr;
+    g.out_idx = d_idx;
+    g.out_d2 = d_d2;
+    g.k = k;
+    g.ball_r = 0.f;
+    g.n_iter = 1;
+    g.step_max = 0.f;
+    MLODS_CUDA(launch_gather(g, kGatherKnnOnly, t->kernel_set ? t->kc.type : MLODS_GAUSSIAN,
+                             sm_count_for_current_device(), s));
+    return MLODS_OK;
+}
+
+int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_t* max_stack, int64_t* overflows,
                      float* kernel_ms)
 {
     CHECK_TREE(t);
-    int64_t h[4] = {0, 0, 0, 0};
+    int64_t h[5] = {0, 0, 0, 0, 0};
     float ms = 0.f;
     if (t->timed) {
         MLODS_CUDA(cudaEventSynchronize(t->ev_stop));
@@ -398,6 +619,7 @@ int mlods_last_stats(mlods_tree t, int64_t* node_visits, int32_t* max_stack, int
     }
     if (t->d_stats) MLODS_CUDA(cudaMemcpy(h, t->d_stats, sizeof h, cudaMemcpyDeviceToHost));
     if (node_visits) *node_visits = h[0];
+    if (rounds) *rounds = h[4];
     if (max_stack) *max_stack = int32_t(h[1]);
     if (overflows) *overflows = h[2];
     if (kernel_ms) *kernel_ms = ms;

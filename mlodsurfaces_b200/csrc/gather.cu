@@ -1,0 +1,602 @@
+// gather.cu -- kNN and ball gathers over the device octree and the APSS
+// projection built on them (APSSOctree::projectAPSSCPU, CPUUtils.cpp:690-737),
+// plus the all-points (global) APSS projection (GlobalAPSS.cu:113-235).
+//
+// One warp per query.  Neighbour candidates are ranked by the squared
+// distance evaluated exactly as the reference kd-tree does (kdTreeNN.h:424):
+// float differences of the world coordinates, float products, left-to-right
+// float sums, no contraction.  The k best (k <= 32) live one per lane, sorted
+// across the warp; batches of candidates are merged with a bitonic network
+// (keys (distance, original index), so ties at the k-th distance resolve to
+// the lower index; the reference resolves them by kd-tree visiting order).
+// The search starts from the 32 points around the query's Morton position
+// (an upper bound for the k-th distance) and walks the octree with the
+// bounding sphere of each node box, widened by the float rounding of the
+// local frame.  The fit is the reference's CPU one (|u4| < 1e-12).
+#include <cfloat>
+#include <cmath>
+
+#include "gather.cuh"
+#include "tree.cuh"
+
+namespace mlods
+{
+namespace
+{
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr uint32_t kGCount = 0x7FFFFFFFu;
+constexpr uint32_t kGPoints = 1u << 31;  // entry is a range of sorted point positions
+constexpr int kGatherCap = 128;          // stack entries per warp
+
+struct GStack {
+    uint32_t first[kGatherCap];
+    uint32_t cnt[kGatherCap];
+};
+
+__device__ __forceinline__ float kd_dist2(const float4 p, float qx, float qy, float qz)
+{
+    const float dx = __fsub_rn(p.x, qx), dy = __fsub_rn(p.y, qy), dz = __fsub_rn(p.z, qz);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ bool key_less(float da, uint32_t oa, float db, uint32_t ob)
+{
+    return da < db || (da == db && oa < ob);
+}
+
+// Bitonic sort of one (d, o, p) per lane; ascending unless `desc`.
+__device__ __forceinline__ void warp_sort(float& d, uint32_t& o, uint32_t& p, bool desc)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const float od = __shfl_xor_sync(kFull, d, j);
+            const uint32_t oo = __shfl_xor_sync(kFull, o, j);
+            const uint32_t op = __shfl_xor_sync(kFull, p, j);
+            const bool up = (((lane & k) == 0) != desc);
+            const bool lower = (lane & j) == 0;
+            const bool other_less = key_less(od, oo, d, o);
+            const bool take = (lower == up) ? other_less : (!other_less && (od != d || oo != o));
+            if (take) {
+                d = od;
+                o = oo;
+                p = op;
+            }
+        }
+    }
+}
+
+// Ascending best list (d, o, p) merged with candidate batch (cd, co, cp).
+__device__ __forceinline__ void warp_merge(float& d, uint32_t& o, uint32_t& p, float cd, uint32_t co, uint32_t cp)
+{
+    const int lane = threadIdx.x & 31;
+    warp_sort(cd, co, cp, true);
+    if (key_less(cd, co, d, o)) {
+        d = cd;
+        o = co;
+        p = cp;
+    }
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        const float od = __shfl_xor_sync(kFull, d, j);
+        const uint32_t oo = __shfl_xor_sync(kFull, o, j);
+        const uint32_t op = __shfl_xor_sync(kFull, p, j);
+        const bool lower = (lane & j) == 0;
+        const bool other_less = key_less(od, oo, d, o);
+        if (lower ? other_less : (!other_less && (od != d || oo != o))) {
+            d = od;
+            o = oo;
+            p = op;
+        }
+    }
+}
+
+__device__ __forceinline__ float warp_sum_f(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int warp_incl_scan_i(int v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int n = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += n;
+    }
+    return v;
+}
+
+// Morton code of a world point on the tree's split lattice (the descent of
+// the build, with the split recomputed from the float bound table).
+__device__ uint64_t lattice_code(const GatherArgs& a, float wx, float wy, float wz)
+{
+    const float w[3] = {wx, wy, wz};
+    uint32_t cell[3];
+    for (int ax = 0; ax < 3; ++ax) {
+        const float* B = a.bounds + ax * a.bounds_stride;
+        const double x = double(w[ax]);
+        uint32_t k = 0;
+        for (int d = 0; d < a.max_depth; ++d) {
+            const int64_t off = ((int64_t(1) << d) - 1) + d;
+            const double s = (double(__ldg(B + off + k)) + double(__ldg(B + off + k + 1))) / 2.0;
+            k = 2u * k + (x > s ? 1u : 0u);
+        }
+        cell[ax] = k;
+    }
+    uint64_t code = 0;
+    for (int d = 0; d < a.max_depth; ++d) {
+        const int b = a.max_depth - 1 - d;
+        const uint64_t g = ((cell[0] >> b) & 1u) | (((cell[1] >> b) & 1u) << 1) | (((cell[2] >> b) & 1u) << 2);
+        code |= g << (3 * b);
+    }
+    return code;
+}
+
+// First sorted position whose code is > qcode, found with 32-way splits.
+__device__ int64_t warp_upper_bound(const uint64_t* __restrict__ codes, int64_t n, uint64_t qcode)
+{
+    const int lane = threadIdx.x & 31;
+    int64_t lo = 0, hi = n;  // answer in [lo, hi]
+    while (hi - lo > 32) {
+        const int64_t step = (hi - lo) / 32;
+        const int64_t idx = lo + step * lane;
+        const bool le = __ldg(codes + idx) <= qcode;
+        const uint32_t m = __ballot_sync(kFull, le);
+        const int last = m ? 31 - __clz(m) : -1;  // last lane with code <= q
+        if (last < 0) {
+            hi = lo;
+            break;
+        }
+        const int64_t nlo = lo + step * last + 1;
+        const int64_t nhi = last == 31 ? hi : lo + step * (last + 1);
+        lo = nlo;
+        hi = nhi;
+    }
+    const int64_t idx = lo + lane;
+    const bool le = idx < hi && __ldg(codes + idx) <= qcode;
+    const uint32_t m = __ballot_sync(kFull, le);
+    return lo + __popc(m);
+}
+
+template <int KTYPE>
+__device__ __forceinline__ float weight_cpu(const KernelConsts& kc, float d2)
+{
+    float w = kernel_weight<KTYPE>(kc, d2);
+    if (KTYPE == MLODS_GAUSSIAN_MULTIPLE && w == 0.f) w = kc.shift;  // Kernel.cpp:70-74
+    return w;
+}
+
+// CPU-rule fit (CPUUtils.cpp:744-781) of the query-frame sums, in double.
+__device__ bool fit_cpu(const float* s, double step_max, double x[3], float nrm[3])
+{
+    const double Sw = s[0];
+    const double Sn[3] = {s[1], s[2], s[3]};
+    const double Sp[3] = {s[4], s[5], s[6]};
+    const double Spn = s[7], Spp = s[8];
+    const double u4 = 0.5 * (Spn - (Sp[0] * Sn[0] + Sp[1] * Sn[1] + Sp[2] * Sn[2]) / Sw) /
+                      (Spp - (Sp[0] * Sp[0] + Sp[1] * Sp[1] + Sp[2] * Sp[2]) / Sw);
+    double u123[3];
+    for (int c = 0; c < 3; ++c) u123[c] = (Sn[c] - 2.0 * u4 * Sp[c]) / Sw;
+    const double u0 = -((Sp[0] * u123[0] + Sp[1] * u123[1] + Sp[2] * u123[2]) + u4 * Spp) / Sw;
+    double nv[3];
+    if (fabs(u4) < 1e-12) {
+        const double m[3] = {-u123[0], -u123[1], -u123[2]};
+        const double lambda = u0 / (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        for (int c = 0; c < 3; ++c) x[c] = lambda * m[c];
+        for (int c = 0; c < 3; ++c) nv[c] = Sn[c];
+    } else {
+        double cc[3];
+        for (int c = 0; c < 3; ++c) cc[c] = u123[c] / (-2.0 * u4);
+        const double r2 = cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2] - u0 / u4;
+        const double rad = sqrt(r2 > 0.0 ? r2 : 0.0);
+        const double pl = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+        for (int c = 0; c < 3; ++c) x[c] = cc[c] + rad * (-cc[c] / pl);
+        for (int c = 0; c < 3; ++c) nv[c] = u123[c] + 2.0 * u4 * x[c];
+    }
+    const double nl = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+    for (int c = 0; c < 3; ++c) nv[c] /= nl;
+    if (isnan(x[0]) || isnan(x[1]) || isnan(x[2])) return false;
+    const double step = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    if (step > step_max)
+        for (int c = 0; c < 3; ++c) x[c] *= step_max / step;
+    for (int c = 0; c < 3; ++c) nrm[c] = float(nv[c]);
+    return true;
+}
+
+// MODE: 0 = kNN APSS projection, 1 = ball APSS projection, 2 = kNN sets only.
+template <int KTYPE, int MODE>
+__global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
+{
+    __shared__ GStack stacks[kGatherThreads / 32];
+    const int lane = threadIdx.x & 31;
+    GStack& st = stacks[threadIdx.x >> 5];
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const int k = a.k;
+    const double r2ball = double(a.ball_r) * double(a.ball_r);
+    const int n_iter = MODE == 2 ? 1 : a.n_iter;
+    int64_t overflows = 0;
+
+    for (;;) {
+        unsigned int qs = 0;
+        if (lane == 0) qs = atomicAdd(a.counter, 1u);
+        qs = __shfl_sync(kFull, qs, 0);
+        if (int64_t(qs) >= a.nq) break;
+        const int64_t qi = qs;
+        const float q0[3] = {a.q_in[3 * qi], a.q_in[3 * qi + 1], a.q_in[3 * qi + 2]};
+        double xd[3] = {double(q0[0]) - a.o0, double(q0[1]) - a.o1, double(q0[2]) - a.o2};
+        float nrm[3] = {0.f, 0.f, 0.f};
+        bool failed = false, empty = false, overflow = false;
+        float best_d = INFINITY;
+        uint32_t best_o = 0xFFFFFFFFu, best_p = 0xFFFFFFFFu;
+        for (int it = 0; it < n_iter && !failed; ++it) {
+            // the reference keeps the iterate as a float glm::vec3
+            const float wx = it == 0 ? q0[0] : float(xd[0] + a.o0);
+            const float wy = it == 0 ? q0[1] : float(xd[1] + a.o1);
+            const float wz = it == 0 ? q0[2] : float(xd[2] + a.o2);
+            const float lx = float(double(wx) - a.o0), ly = float(double(wy) - a.o1), lz = float(double(wz) - a.o2);
+            float acc[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) acc[c] = 0.f;
+            int found = 0;
+            int64_t w0 = 0, w1 = 0;  // Morton window already in the best list
+            float bound;             // squared search radius
+            best_d = INFINITY;
+            best_o = best_p = 0xFFFFFFFFu;
+            if (MODE != 1) {
+                const uint64_t qc = lattice_code(a, wx, wy, wz);
+                const int64_t pos = warp_upper_bound(a.codes, a.n_pts, qc);
+                w0 = pos - 16 < 0 ? 0 : pos - 16;
+                w1 = w0 + 32 > a.n_pts ? a.n_pts : w0 + 32;
+                w0 = w1 - 32 < 0 ? 0 : w1 - 32;
+                const int64_t j = w0 + lane;
+                if (j < w1) {
+                    const float4 p = __ldg(a.wspts + j);
+                    best_d = kd_dist2(p, wx, wy, wz);
+                    best_o = __float_as_uint(p.w);
+                    best_p = uint32_t(j);
+                }
+                warp_sort(best_d, best_o, best_p, false);
+                bound = __shfl_sync(kFull, best_d, k - 1);
+            } else {
+                bound = float(r2ball) * (1.f + 1e-6f);
+            }
+            // ---- octree walk
+            int top = 1;
+            if (lane == 0) {
+                st.first[0] = 0;
+                st.cnt[0] = 1u;
+            }
+            __syncwarp();
+            while (top > 0) {
+                uint32_t e_first = 0, e_cnt = 0;
+                int c = 0;
+                if (lane < top) {
+                    e_first = st.first[top - 1 - lane];
+                    e_cnt = st.cnt[top - 1 - lane];
+                    c = int(e_cnt & kGCount);
+                }
+                const int incl = warp_incl_scan_i(c);
+                const uint32_t fit = __ballot_sync(kFull, lane < top && incl <= 32);
+                int npop = __popc(fit);
+                const bool partial = npop == 0;
+                int total;
+                uint32_t headbit;
+                if (partial) {
+                    total = 32;
+                    headbit = lane == 0 ? 1u : 0u;
+                } else {
+                    total = __shfl_sync(kFull, incl, npop - 1);
+                    headbit = lane < npop ? (1u << (incl - c)) : 0u;
+                }
+                const uint32_t heads = __reduce_or_sync(kFull, headbit);
+                const bool active = lane < total;
+                const int e = active ? __popc(heads & (lane == 31 ? kFull : ((2u << lane) - 1u))) - 1 : 0;
+                const uint32_t r_first = __shfl_sync(kFull, e_first, e);
+                const uint32_t r_cnt = __shfl_sync(kFull, e_cnt, e);
+                const int r_start = partial ? 0 : __shfl_sync(kFull, incl - c, e);
+                if (partial) {
+                    if (lane == 0) {
+                        st.first[top - 1] = e_first + 32u;
+                        st.cnt[top - 1] = e_cnt - 32u;
+                    }
+                } else {
+                    top -= npop;
+                }
+                const uint32_t idx = r_first + uint32_t(lane - r_start);
+                // candidate point of this lane (sorted position), if any
+                int64_t cpos = -1;
+                bool push = false;
+                uint32_t p_first = 0, p_cnt = 0;
+                if (active) {
+                    if (r_cnt & kGPoints) {
+                        cpos = idx;
+                    } else {
+                        const DNode nd = a.nodes[idx];
+                        if (nd.info & kLeafBit) {
+                            const int cnt = int(node_count(nd.info));
+                            const int64_t head = __ldg(a.node_head + idx);
+                            if (cnt == 1) {
+                                cpos = head;
+                            } else {
+                                push = true;
+                                p_first = uint32_t(head);
+                                p_cnt = uint32_t(cnt) | kGPoints;
+                            }
+                        } else {
+                            const float cx = nd.cx - lx, cy = nd.cy - ly, cz = nd.cz - lz;
+                            const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
+                            const float lo = dc - nd.r - a.eps;
+                            if (!(lo > 0.f && lo * lo > bound)) {
+                                push = true;
+                                p_first = nd.first;
+                                p_cnt = node_count(nd.info);
+                            }
+                        }
+                    }
+                }
+                float cd = INFINITY;
+                uint32_t co = 0xFFFFFFFFu, cp = 0xFFFFFFFFu;
+                if (cpos >= 0 && !(MODE != 1 && cpos >= w0 && cpos < w1)) {
+                    const float4 p = __ldg(a.wspts + cpos);
+                    const float d2 = kd_dist2(p, wx, wy, wz);
+                    if (MODE == 1) {
+                        if (double(d2) <= r2ball) {
+                            const float4 pl = __ldg(a.spts + cpos);
+                            const float4 nn = __ldg(a.snrm + cpos);
+                            const float dx = pl.x - lx, dy = pl.y - ly, dz = pl.z - lz;
+                            const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float w = weight_cpu<KTYPE>(a.kc, dd);
+                            acc[0] += w;
+                            acc[1] = fmaf(w, nn.x, acc[1]);
+                            acc[2] = fmaf(w, nn.y, acc[2]);
+                            acc[3] = fmaf(w, nn.z, acc[3]);
+                            acc[4] = fmaf(w, dx, acc[4]);
+                            acc[5] = fmaf(w, dy, acc[5]);
+                            acc[6] = fmaf(w, dz, acc[6]);
+                            acc[7] = fmaf(w, fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z)), acc[7]);
+                            acc[8] = fmaf(w, dd, acc[8]);
+                            ++found;
+                        }
+                    } else if (d2 <= bound) {
+                        cd = d2;
+                        co = __float_as_uint(p.w);
+                        cp = uint32_t(cpos);
+                    }
+                }
+                if (MODE != 1) {
+                    if (__any_sync(kFull, cd <= bound && cd < INFINITY)) {
+                        warp_merge(best_d, best_o, best_p, cd, co, cp);
+                        bound = __shfl_sync(kFull, best_d, k - 1);
+                    }
+                }
+                const uint32_t pm = __ballot_sync(kFull, push);
+                const int npush = __popc(pm);
+                if (top + npush > kGatherCap) {
+                    overflow = true;
+                } else {
+                    if (push) {
+                        const int pos = top + __popc(pm & lt_mask);
+                        st.first[pos] = p_first;
+                        st.cnt[pos] = p_cnt;
+                    }
+                    top += npush;
+                }
+                __syncwarp();
+            }
+            if (overflow) {
+                failed = true;
+                break;
+            }
+            if (MODE == 2) break;
+            if (MODE == 0) {
+                if (lane < k && best_p != 0xFFFFFFFFu) {
+                    const float4 pl = __ldg(a.spts + best_p);
+                    const float4 nn = __ldg(a.snrm + best_p);
+                    const float dx = pl.x - lx, dy = pl.y - ly, dz = pl.z - lz;
+                    const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float w = weight_cpu<KTYPE>(a.kc, dd);
+                    acc[0] = w;
+                    acc[1] = w * nn.x;
+                    acc[2] = w * nn.y;
+                    acc[3] = w * nn.z;
+                    acc[4] = w * dx;
+                    acc[5] = w * dy;
+                    acc[6] = w * dz;
+                    acc[7] = w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
+                    acc[8] = w * dd;
+                }
+            } else {
+                // CPUUtils.cpp:711-716: an empty ball returns the start point, normal 0
+                const int tot = __reduce_add_sync(kFull, found);
+                if (tot == 0) {
+                    empty = true;
+                    failed = true;
+                    break;
+                }
+            }
+            float s[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) s[c] = warp_sum_f(acc[c]);
+            double x[3];
+            if (!fit_cpu(s, double(a.step_max), x, nrm)) {
+                // NaN: the iterate stays, normal 0 (CPUUtils.cpp:770-776)
+                nrm[0] = nrm[1] = nrm[2] = 0.f;
+                xd[0] = double(wx) - a.o0;
+                xd[1] = double(wy) - a.o1;
+                xd[2] = double(wz) - a.o2;
+                continue;
+            }
+            xd[0] = double(lx) + x[0];
+            xd[1] = double(ly) + x[1];
+            xd[2] = double(lz) + x[2];
+        }
+        if (MODE == 2) {
+            if (lane < k) {
+                const bool ok = best_p != 0xFFFFFFFFu && !overflow;
+                a.out_idx[qi * k + lane] = ok ? int32_t(best_o) : -1;
+                a.out_d2[qi * k + lane] = ok ? best_d : -1.f;
+            }
+        } else if (lane == 0) {
+            float* op = a.out_p + 3 * qi;
+            float* on = a.out_n + 3 * qi;
+            if (empty || overflow) {
+                op[0] = q0[0];
+                op[1] = q0[1];
+                op[2] = q0[2];
+                on[0] = on[1] = on[2] = 0.f;
+            } else {
+                op[0] = float(xd[0] + a.o0);
+                op[1] = float(xd[1] + a.o1);
+                op[2] = float(xd[2] + a.o2);
+                on[0] = nrm[0];
+                on[1] = nrm[1];
+                on[2] = nrm[2];
+            }
+        }
+        if (overflow) ++overflows;
+    }
+    if (lane == 0 && a.stats && overflows)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[2]), (unsigned long long)overflows);
+}
+
+// ---------------------------------------------------------------- global APSS
+
+constexpr int kGlobalThreads = 128;
+constexpr int kGlobalTile = 512;
+
+// One thread per query; every point of the cloud contributes
+// w(p_i, q) a_i {1, n_i, p_i, p_i.n_i, |p_i|^2} (APSSOctree::APSSStats,
+// CPUUtils.cpp:515-528).  Points stream through shared memory in tiles;
+// per-tile float partial sums are accumulated in double.
+template <int KTYPE>
+__global__ void __launch_bounds__(kGlobalThreads) global_apss_kernel(GlobalArgs a)
+{
+    __shared__ float4 s_p[kGlobalTile];
+    __shared__ float4 s_n[kGlobalTile];
+    const int64_t qi = int64_t(blockIdx.x) * kGlobalThreads + threadIdx.x;
+    const bool valid = qi < a.nq;
+    double xd[3] = {0, 0, 0};
+    float q0[3] = {0, 0, 0};
+    if (valid) {
+        for (int c = 0; c < 3; ++c) {
+            q0[c] = a.q_in[3 * qi + c];
+            xd[c] = double(q0[c]) - (c == 0 ? a.o0 : (c == 1 ? a.o1 : a.o2));
+        }
+    }
+    float nrm[3] = {0.f, 0.f, 0.f};
+    bool failed = false;
+    for (int it = 0; it < a.n_iter; ++it) {
+        const float lx = float(xd[0]), ly = float(xd[1]), lz = float(xd[2]);
+        double tot[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int64_t base = 0; base < a.n_pts; base += kGlobalTile) {
+            __syncthreads();
+            for (int j = threadIdx.x; j < kGlobalTile; j += kGlobalThreads) {
+                const int64_t g = base + j;
+                if (g < a.n_pts) {
+                    const float4 p = __ldg(a.spts + g);
+                    const float4 nn = __ldg(a.snrm + g);
+                    const float ar = __ldg(a.area + __float_as_uint(p.w));
+                    s_p[j] = make_float4(p.x, p.y, p.z, ar);
+                    s_n[j] = nn;
+                } else {
+                    s_p[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    s_n[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+            __syncthreads();
+            float acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int j = 0; j < kGlobalTile; ++j) {
+                const float4 p = s_p[j];
+                const float4 nn = s_n[j];
+                const float dx = p.x - lx, dy = p.y - ly, dz = p.z - lz;
+                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float w = kernel_weight<KTYPE>(a.kc, dd) * p.w;
+                acc[0] += w;
+                acc[1] = fmaf(w, nn.x, acc[1]);
+                acc[2] = fmaf(w, nn.y, acc[2]);
+                acc[3] = fmaf(w, nn.z, acc[3]);
+                acc[4] = fmaf(w, dx, acc[4]);
+                acc[5] = fmaf(w, dy, acc[5]);
+                acc[6] = fmaf(w, dz, acc[6]);
+                acc[7] = fmaf(w, fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z)), acc[7]);
+                acc[8] = fmaf(w, dd, acc[8]);
+            }
+            for (int c = 0; c < 9; ++c) tot[c] += double(acc[c]);
+        }
+        if (!valid || failed) continue;
+        float s[9];
+        for (int c = 0; c < 9; ++c) s[c] = float(tot[c]);
+        double x[3];
+        if (!fit_cpu(s, double(a.step_max), x, nrm)) {
+            nrm[0] = nrm[1] = nrm[2] = 0.f;
+            failed = true;
+            continue;
+        }
+        xd[0] = double(lx) + x[0];
+        xd[1] = double(ly) + x[1];
+        xd[2] = double(lz) + x[2];
+    }
+    if (valid) {
+        a.out_p[3 * qi] = float(xd[0] + a.o0);
+        a.out_p[3 * qi + 1] = float(xd[1] + a.o1);
+        a.out_p[3 * qi + 2] = float(xd[2] + a.o2);
+        a.out_n[3 * qi] = nrm[0];
+        a.out_n[3 * qi + 1] = nrm[1];
+        a.out_n[3 * qi + 2] = nrm[2];
+    }
+}
+
+template <int KTYPE, int MODE>
+cudaError_t launch_gather_typed(const GatherArgs& a, int sm_count, cudaStream_t s)
+{
+    auto kern = gather_kernel<KTYPE, MODE>;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kGatherThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const int64_t want = (a.nq + kGatherThreads / 32 - 1) / (kGatherThreads / 32);
+    int64_t grid = int64_t(per_sm) * sm_count;
+    if (grid > want) grid = want;
+    if (grid < 1) grid = 1;
+    kern<<<unsigned(grid), kGatherThreads, 0, s>>>(a);
+    note_launch();
+    return cudaGetLastError();
+}
+
+template <int MODE>
+cudaError_t launch_gather_mode(const GatherArgs& a, int ktype, int sm_count, cudaStream_t s)
+{
+    switch (ktype) {
+    case MLODS_GAUSSIAN: return launch_gather_typed<MLODS_GAUSSIAN, MODE>(a, sm_count, s);
+    case MLODS_SINGULAR: return launch_gather_typed<MLODS_SINGULAR, MODE>(a, sm_count, s);
+    default: return launch_gather_typed<MLODS_GAUSSIAN_MULTIPLE, MODE>(a, sm_count, s);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_gather(const GatherArgs& a, int mode, int ktype, int sm_count, cudaStream_t s)
+{
+    if (mode == kGatherKnnApss) return launch_gather_mode<0>(a, ktype, sm_count, s);
+    if (mode == kGatherBallApss) return launch_gather_mode<1>(a, ktype, sm_count, s);
+    return launch_gather_mode<2>(a, ktype, sm_count, s);
+}
+
+cudaError_t launch_global_apss(const GlobalArgs& a, int ktype, cudaStream_t s)
+{
+    const unsigned grid = unsigned((a.nq + kGlobalThreads - 1) / kGlobalThreads);
+    switch (ktype) {
+    case MLODS_GAUSSIAN: global_apss_kernel<MLODS_GAUSSIAN><<<grid, kGlobalThreads, 0, s>>>(a); break;
+    case MLODS_SINGULAR: global_apss_kernel<MLODS_SINGULAR><<<grid, kGlobalThreads, 0, s>>>(a); break;
+    default: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE><<<grid, kGlobalThreads, 0, s>>>(a); break;
+    }
+    note_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace mlods

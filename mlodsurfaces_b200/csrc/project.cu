@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(kProjectThreads) mlod_project_kernel(ProjectAr
     const int min_depth = a.min_depth;
 
     int64_t visits = 0;
+    int64_t rounds = 0;
     int max_top = 0;
     int64_t overflows = 0;
 
@@ -223,6 +224,7 @@ __global__ void __launch_bounds__(kProjectThreads) mlod_project_kernel(ProjectAr
                     top -= npop;
                 }
                 visits += total;
+                ++rounds;
 
                 // ---- evaluate one node per lane
                 const uint32_t node = r_first + uint32_t(lane - r_start);
@@ -366,6 +368,7 @@ __global__ void __launch_bounds__(kProjectThreads) mlod_project_kernel(ProjectAr
     }
     if (lane == 0 && a.stats) {
         atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[0]), (unsigned long long)visits);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[4]), (unsigned long long)rounds);
         atomicMax(reinterpret_cast<unsigned long long*>(&a.stats[1]), (unsigned long long)max_top);
         if (overflows) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[2]), (unsigned long long)overflows);
     }
@@ -417,7 +420,28 @@ __global__ void query_codes_kernel(const float* __restrict__ q, int64_t n, doubl
     idx[i] = uint32_t(i);
 }
 
+__global__ void reorganize_kernel(float* __restrict__ q, const uint32_t* __restrict__ inv, int64_t n_inv,
+                                  uint32_t end_valid)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n_inv) return;
+    const int64_t a = inv[i], b = int64_t(end_valid) - 1 - i;
+    for (int c = 0; c < 3; ++c) {
+        const float t = q[3 * a + c];
+        q[3 * a + c] = q[3 * b + c];
+        q[3 * b + c] = t;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_invalid, uint32_t end_valid,
+                              cudaStream_t s)
+{
+    reorganize_kernel<<<unsigned((n_invalid + 255) / 256), 256, 0, s>>>(d_q, d_invalid, n_invalid, end_valid);
+    note_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int sm_count, cudaStream_t s)
 {

@@ -26,10 +26,14 @@ struct ProjectArgs {
     double o0, o1, o2;       // local frame origin
     KernelConsts kc;
     unsigned int* counter;   // work counter, zero before launch
-    int64_t* stats;          // [0] node visits, [1] max stack, [2] overflows (may be nullptr)
+    int64_t* stats;          // [0] node visits, [1] max stack, [2] overflows, [3] work counter, [4] rounds
 };
 
 cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int sm_count, cudaStream_t s);
+
+// Swaps query points invalid[i] and end_valid-1-i (GPUUtils.cu:413-424).
+cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_invalid, uint32_t end_valid,
+                              cudaStream_t s);
 
 // Morton order of queries on a 1024^3 grid over the root box (the reference
 // orders its queries on a 64^3 grid, Pn.cpp:388-445).  d_order receives the

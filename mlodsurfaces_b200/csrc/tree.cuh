@@ -27,6 +27,7 @@ struct mlods_tree_s {
     float* d_area = nullptr;               // per original point (float, as the reference)
     float4* d_spts = nullptr;              // sorted points, local frame: xyz, w = original index bits
     float4* d_snrm = nullptr;              // sorted normals
+    float4* d_wspts = nullptr;             // sorted points, world frame (exact neighbour distances)
     float* d_bounds = nullptr;             // per-axis float bound tables (3 x table size)
     int64_t bounds_stride = 0;
 
@@ -35,11 +36,6 @@ struct mlods_tree_s {
     mlods::KernelConsts kc{};
     mlods_params params{};
     bool kernel_set = false;
-
-    // query buffer of the copyPointsToGPU protocol
-    float* d_q = nullptr;
-    float* d_qn = nullptr;
-    int64_t q_n = 0;
 
     // reusable scratch for projection (grown on demand)
     void* d_scratch = nullptr;
@@ -55,6 +51,15 @@ struct mlods_tree_s {
     cudaEvent_t ev_start = nullptr;
     cudaEvent_t ev_stop = nullptr;
     bool timed = false;
+};
+
+// Device query buffer of the copyPointsToGPU / project protocol, owned by the
+// projection object (APSS::m_outPts, m_outNmls, GPUUtils.h:56-57).
+struct mlods_queries_s {
+    float* d_q = nullptr;
+    float* d_qn = nullptr;
+    int64_t n = 0;    // uploaded queries
+    int64_t cap = 0;  // allocated queries
 };
 
 namespace mlods

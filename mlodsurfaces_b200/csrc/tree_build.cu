@@ -466,7 +466,8 @@ __global__ void write_point_records_kernel(int64_t n_nodes, const int32_t* __res
 
 __global__ void sorted_points_kernel(int64_t n, const uint32_t* __restrict__ perm, const float* __restrict__ pts,
                                      const float* __restrict__ nrm, double o0, double o1, double o2,
-                                     float4* __restrict__ spts, float4* __restrict__ snrm)
+                                     float4* __restrict__ spts, float4* __restrict__ snrm,
+                                     float4* __restrict__ wspts)
 {
     int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -474,6 +475,7 @@ __global__ void sorted_points_kernel(int64_t n, const uint32_t* __restrict__ per
     spts[j] = make_float4(float(double(pts[3 * i]) - o0), float(double(pts[3 * i + 1]) - o1),
                           float(double(pts[3 * i + 2]) - o2), __uint_as_float(i));
     snrm[j] = make_float4(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2], 0.f);
+    wspts[j] = make_float4(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], __uint_as_float(i));
 }
 
 inline size_t al(size_t v) { return (v + 255) / 256 * 256; }
@@ -502,6 +504,7 @@ void free_tree_device(mlods_tree_s* T)
     cudaFree(T->d_area);
     cudaFree(T->d_spts);
     cudaFree(T->d_snrm);
+    cudaFree(T->d_wspts);
     cudaFree(T->d_bounds);
     T->d_nodes = nullptr;
     T->d_node_head = nullptr;
@@ -510,6 +513,7 @@ void free_tree_device(mlods_tree_s* T)
     T->d_area = nullptr;
     T->d_spts = nullptr;
     T->d_snrm = nullptr;
+    T->d_wspts = nullptr;
     T->d_bounds = nullptr;
 }
 
@@ -775,8 +779,9 @@ int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t 
     NODE_CHECK(cudaMemcpyAsync(T->d_perm, perm, size_t(n) * 4, cudaMemcpyDeviceToDevice, s), "copy perm");
     NODE_CHECK(cudaMalloc(&T->d_spts, size_t(n) * sizeof(float4)), "alloc spts");
     NODE_CHECK(cudaMalloc(&T->d_snrm, size_t(n) * sizeof(float4)), "alloc snrm");
+    NODE_CHECK(cudaMalloc(&T->d_wspts, size_t(n) * sizeof(float4)), "alloc wspts");
     sorted_points_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(n, perm, d_pts, d_nrm, T->origin[0], T->origin[1],
-                                                                    T->origin[2], T->d_spts, T->d_snrm);
+                                                                    T->origin[2], T->d_spts, T->d_snrm, T->d_wspts);
     note_launch();
     NODE_CHECK(cudaGetLastError(), "sorted points");
     NODE_CHECK(cudaStreamSynchronize(s), "sync build");
@@ -784,7 +789,7 @@ int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t 
     cudaFree(bump.base);
 #undef NODE_CHECK
 #undef BUILD_CHECK
-    T->device_bytes = int64_t((nn + h_extra) * sizeof(DNode)) + nn * 4 + n * (8 + 4 + 4 + 32) +
+    T->device_bytes = int64_t((nn + h_extra) * sizeof(DNode)) + nn * 4 + n * (8 + 4 + 4 + 48) +
                       3 * bound_stride * 4;
     return MLODS_OK;
 }

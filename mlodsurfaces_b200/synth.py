@@ -203,11 +203,16 @@ def count_split_ties(points: np.ndarray, depth: int = 12) -> int:
 
 
 def make_tie_free(points: np.ndarray, depth: int = 12, max_rounds: int = 8) -> np.ndarray:
-    """Return a copy where no coordinate equals a split value on its path."""
+    """Return a copy where no coordinate equals a split value on its path.
+
+    Axes on which all points are equal are left alone (every split of such an
+    axis equals the coordinate)."""
     p = np.array(points, dtype=F32, copy=True)
     for _ in range(max_rounds):
         changed = False
         for a in range(3):
+            if p[:, a].min() == p[:, a].max():
+                continue  # a flat axis ties everywhere; nudging would only move the box
             x = p[:, a].astype(np.float64)
             splits, _ = split_tables(p[:, a].min(), p[:, a].max(), depth)
             k = np.zeros(len(x), dtype=np.int64)

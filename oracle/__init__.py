@@ -246,3 +246,61 @@ def ref_kdtree_knn(pts, q, k):
     d2 = np.empty((len(q), k), np.float64)
     ref().ref_kdtree_knn(_ptr(pts), len(pts), _ptr(q), len(q), int(k), _ptr(idx), _ptr(d2))
     return idx, d2
+
+
+REFGPU_SO = HERE / "_ref" / "libmlods_refgpu.so"
+_refgpu = None
+
+
+def refgpu_available() -> bool:
+    return REFGPU_SO.exists()
+
+
+def refgpu() -> C.CDLL:
+    global _refgpu
+    if _refgpu is None:
+        if not REFGPU_SO.exists():
+            raise FileNotFoundError(f"{REFGPU_SO} not built (needs the reference sources and nvcc)")
+        lib = C.CDLL(os.fspath(REFGPU_SO))
+        lib.refgpu_create.restype = _P
+        lib.refgpu_create.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, _P,
+                                      C.c_int, C.c_float, C.c_int, C.c_char_p, C.c_int]
+        lib.refgpu_project.restype = C.c_double
+        lib.refgpu_project.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, _P, _P]
+        lib.refgpu_free.argtypes = [_P]
+        _refgpu = lib
+    return _refgpu
+
+
+class RefGpu:
+    """The reference's own Fastapss (GPU) on the reference's host-built tree.
+    Refuses trees of depth >= 12 (the reference kernel would index its
+    per-depth array out of bounds there)."""
+
+    def __init__(self, pts, nrm, kernel, cutoff=2.0, min_depth=0, max_depth=12):
+        self.pts = _f32(pts)
+        self.nrm = _f32(nrm)
+        sig = np.ascontiguousarray(np.asarray(kernel.sigmas if len(kernel.sigmas) else [0.0], np.float32))
+        err = C.create_string_buffer(256)
+        self._h = refgpu().refgpu_create(_ptr(self.pts), _ptr(self.nrm), len(self.pts), int(max_depth),
+                                         int(kernel.type), float(kernel.sigma), float(kernel.exponent),
+                                         float(kernel.constant_shift), _ptr(sig), len(kernel.sigmas), float(cutoff),
+                                         int(min_depth), err, 256)
+        if not self._h:
+            raise ValueError(err.value.decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            refgpu().refgpu_free(self._h)
+            self._h = None
+
+    def project(self, q, calls=10, iters_per_call=1, step_max=-1.0):
+        """(points, normals, device milliseconds of the project calls)."""
+        q = _f32(q)
+        op = np.empty((len(q), 3), np.float32)
+        on = np.empty((len(q), 3), np.float32)
+        ms = refgpu().refgpu_project(self._h, _ptr(q), len(q), int(calls), int(iters_per_call), float(step_max),
+                                     _ptr(op), _ptr(on))
+        if ms < 0:
+            raise ValueError("query count out of the reference's launch range")
+        return op, on, ms

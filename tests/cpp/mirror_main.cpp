@@ -1,0 +1,57 @@
+// Drives the C++ mirror (include/mlods.hpp) the way scene::projectPoints and
+// scene::projectPointsOnCPU drive the reference classes: build the octree,
+// upload queries, project in place one iteration per call, read back; and
+// projectCPU per query.  Reads points/normals/queries from raw float files and
+// writes the projections for the test to compare.
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "mlods.hpp"
+
+using mlods::vec3;
+
+static std::vector<vec3> read_vec3(const char* path)
+{
+    std::vector<vec3> v;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) std::exit(2);
+    vec3 x;
+    while (std::fread(&x, sizeof x, 1, f) == 1) v.push_back(x);
+    std::fclose(f);
+    return v;
+}
+
+static void write_vec3(const char* path, const std::vector<vec3>& v)
+{
+    FILE* f = std::fopen(path, "wb");
+    std::fwrite(v.data(), sizeof(vec3), v.size(), f);
+    std::fclose(f);
+}
+
+int main(int argc, char** argv)
+{
+    if (argc < 7) return 1;  // pts nrm queries out_gpu out_cpu sigma_rel
+    const std::vector<vec3> pts = read_vec3(argv[1]), nrm = read_vec3(argv[2]);
+    std::vector<vec3> q = read_vec3(argv[3]);
+    const float sigma_rel = float(std::atof(argv[6]));
+    auto* tree = new mlods::APSSOctree();
+    tree->build(pts, nrm);
+    mlods::Kernel k;
+    k.type = mlods::Kernel::GAUSSIAN;
+    k.sigma = sigma_rel;
+    k.updateSigmas(true, tree->getBoundingBox().radius());  // scene::setNewKernel scales by the box radius
+    mlods::Fastapss apss(tree, k, unsigned(q.size()));
+    apss.setScalingProtectionSphere(3.f);
+    apss.copyPointsToGPU(unsigned(q.size()), q.data());
+    std::vector<vec3> out(q.size()), outn(q.size());
+    for (int tick = 0; tick < 10; ++tick) apss.project(unsigned(q.size()), nullptr, nullptr, 1, k);
+    apss.project(unsigned(q.size()), out.data(), outn.data(), 0, k);
+    write_vec3(argv[4], out);
+    std::vector<vec3> cpu(q.size()), cpun(q.size());
+    for (size_t i = 0; i < q.size(); ++i) apss.projectCPU(q[i], cpu[i], cpun[i], 10, k);
+    write_vec3(argv[5], cpu);
+    std::printf("nodes %u depth %u\n", tree->nbOfNodes(), tree->computeDepth());
+    delete tree;
+    return 0;
+}

@@ -37,7 +37,9 @@ def test_null_handles_are_rejected_without_a_gpu():
     lib = capi.load()
     assert lib.mlods_set_kernel(None, None) == capi.MLODS_ERR_INVALID
     assert b"null" in lib.mlods_last_error()
-    assert lib.mlods_project(None, 10, 1, -1.0, None, None, None) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_project(None, None, 10, 1, -1.0, None, None, None) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_queries_upload(None, 10, None, None) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_queries_destroy(None) == capi.MLODS_OK
     assert lib.mlods_tree_build(None, None, 0, 12, None, C.byref(C.c_void_p())) == capi.MLODS_ERR_INVALID
     assert lib.mlods_tree_free(None) == capi.MLODS_OK
 

@@ -1,0 +1,131 @@
+"""Neighbour gathers (c) and the APSS projections built on them, against the
+oracle and the reference's own kd-tree/APSS results.
+
+kNN sets: exact (same float distance arithmetic as kdTreeNN.h:424) except at
+an exact tie between the k-th and (k+1)-th distance.  Projections: within
+1e-5 of the bounding-box diagonal."""
+import numpy as np
+import pytest
+
+import oracle
+from mlodsurfaces_b200 import APSSOctree, Fastapss, GlobalAPSS, synth
+from conftest import TOL_DIAG, golden_kernel, make_kernel, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def tree_of(pts, nrm):
+    t = APSSOctree()
+    t.build(pts, nrm)
+    return t
+
+
+def assert_knn_sets(pts, q, k, t=None):
+    t = t or tree_of(pts, np.tile(np.array([[0, 0, 1]], np.float32), (len(pts), 1)))
+    idx, d2 = t.knearest(q, k)
+    oi, od, tie = oracle.knn(pts, q, k)
+    kk = min(k, len(pts))
+    assert np.array_equal(d2[:, :kk].astype(np.float64), od[:, :kk])
+    for i in range(len(q)):
+        if tie[i]:
+            continue
+        assert set(idx[i, :kk].tolist()) == set(oi[i, :kk].tolist()), i
+    if kk < k:
+        assert (idx[:, kk:] == -1).all()
+    return idx, d2
+
+
+@pytest.mark.parametrize("k", [1, 8, 20, 32])
+def test_knn_sets_match_bruteforce(k):
+    pts, nrm = synth.torus(30000, seed=71)
+    q = synth.perturbed_queries(pts, 0.01, seed=72)[:500]
+    assert_knn_sets(pts, q, k, tree_of(pts, nrm))
+
+
+def test_knn_sets_match_reference_kdtree_golden(golden):
+    t = tree_of(golden["pts"], golden["nrm"])
+    idx, d2 = t.knearest(golden["q"], 32)
+    ref = golden["kd_knn32_idx"]
+    _, _, tie = oracle.knn(golden["pts"], golden["q"], 32)
+    for i in range(len(idx)):
+        if not tie[i]:
+            assert set(idx[i].tolist()) == set(ref[i].tolist())
+    assert np.array_equal(np.sort(d2, 1).astype(np.float64), np.sort(golden["kd_knn32_d2"], 1))
+
+
+def test_knn_translated_cloud_and_fewer_points_than_k():
+    pts, nrm = synth.rbf_blobs(20000, seed=73)
+    q = synth.perturbed_queries(pts, 0.01, seed=74)[:300]
+    assert_knn_sets(pts, q, 32, tree_of(pts, nrm))
+    small = pts[:10]
+    assert_knn_sets(small, q[:20], 20)
+
+
+def apss_gpu(pts, nrm, q, kernel, mode, iters=3, k=32, ball_r=0.1):
+    t = tree_of(pts, nrm)
+    if mode == "knn":
+        t.knnMode(True, k)
+    else:
+        t.ballMode(True, ball_r)
+    f = Fastapss(t, kernel, len(q))
+    f.copyPointsToGPU(len(q), q)
+    op = np.empty((len(q), 3), np.float32)
+    on = np.empty((len(q), 3), np.float32)
+    f.project(len(q), op, on, iters, kernel)
+    return op, on, t
+
+
+def test_knn_apss_matches_reference_golden(golden):
+    k = golden_kernel(golden, "gauss")
+    diag = float(golden["diag"])
+    op, on, _ = apss_gpu(golden["pts"], golden["nrm"], golden["q"], k, "knn", iters=3, k=32)
+    o64, _ = oracle.project_apss(golden["pts"], golden["nrm"], golden["q"], 3, k, mode=0, k=32,
+                                 step_max=float(golden["radius"]))
+    assert rel_err(op, o64, diag).max() < TOL_DIAG
+    assert rel_err(op, golden["knn32_gauss_p"], diag).max() < TOL_DIAG
+
+
+def test_ball_apss_matches_reference_golden(golden):
+    k = golden_kernel(golden, "gauss")
+    diag = float(golden["diag"])
+    r = float(golden["ball_r"])
+    op, on, _ = apss_gpu(golden["pts"], golden["nrm"], golden["q"], k, "ball", iters=3, ball_r=r)
+    o64, _ = oracle.project_apss(golden["pts"], golden["nrm"], golden["q"], 3, k, mode=1, ball_r=r,
+                                 step_max=float(golden["radius"]))
+    assert rel_err(op, o64, diag).max() < TOL_DIAG
+    assert rel_err(op, golden["ball_gauss_p"], diag).max() < TOL_DIAG
+
+
+@pytest.mark.parametrize("kind", ["multi", "singular"])
+def test_knn_apss_matches_oracle(kind):
+    pts, nrm = synth.torus(30000, seed=75)
+    q = synth.perturbed_queries(pts, 0.01, seed=76)[:400]
+    diag = synth.bbox_diag(pts)
+    k = make_kernel(kind, diag)
+    op, on, t = apss_gpu(pts, nrm, q, k, "knn", iters=5, k=20)
+    o64, n64 = oracle.project_apss(pts, nrm, q, 5, k, mode=0, k=20, step_max=t.radius())
+    assert rel_err(op, o64, diag).max() < TOL_DIAG
+
+
+def test_empty_ball_returns_start_point():
+    pts, nrm = synth.torus(5000, seed=77)
+    k = make_kernel("gauss", synth.bbox_diag(pts))
+    q = np.array([[3.0, 3.0, 3.0], [1.35, 0.0, 0.0]], np.float32)
+    op, on, _ = apss_gpu(pts, nrm, q, k, "ball", iters=2, ball_r=0.05)
+    assert np.array_equal(op[0], q[0]) and np.all(on[0] == 0)
+    assert np.linalg.norm(on[1]) > 0.5
+
+
+def test_global_apss_matches_oracle_and_reference(golden):
+    k = golden_kernel(golden, "gauss")
+    diag = float(golden["diag"])
+    t = tree_of(golden["pts"], golden["nrm"])
+    g = GlobalAPSS(t, k)
+    q = golden["q"][:100]
+    g.copyPointsToGPU(len(q), q)
+    op = np.empty((len(q), 3), np.float32)
+    on = np.empty((len(q), 3), np.float32)
+    g.project(len(q), op, on, 2, k)
+    o64, _ = oracle.OracleTree(golden["pts"], golden["nrm"], 12).project_global(q, 2, k)
+    assert rel_err(op, o64, diag).max() < TOL_DIAG
+    assert rel_err(op, golden["global_gauss_p"], diag).max() < TOL_DIAG

@@ -23,9 +23,10 @@ def excess_err(x, x64, diag):
     return np.linalg.norm(e, axis=1) / diag
 
 
-def run_gpu(pts, nrm, q, kernel, iters=10, cutoff=3.0, rule=BLEND_GPU, min_depth=0, reorder=True, step_max=-1.0):
+def run_gpu(pts, nrm, q, kernel, iters=10, cutoff=3.0, rule=BLEND_GPU, min_depth=0, reorder=True, step_max=-1.0,
+            depth=12):
     t = APSSOctree()
-    t.build(pts, nrm)
+    t.build(pts, nrm, maxDepth=depth)
     f = Fastapss(t)
     f.copyToGPU(kernel, len(q))
     f.setScalingProtectionSphere(cutoff)

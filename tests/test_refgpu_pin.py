@@ -1,0 +1,37 @@
+"""Pins the GPU blend rule (Fastapss.cu) of the oracle and of the kernel
+against the reference's own GPU code, compiled for sm_100a from its sources
+(oracle/_ref/libmlods_refgpu.so) and run on trees of depth <= 11 only."""
+import numpy as np
+import pytest
+
+import oracle
+from mlodsurfaces_b200 import synth
+from mlodsurfaces_b200._capi import BLEND_GPU
+from conftest import TOL_DIAG, make_kernel, rel_err
+from test_project_gpu import run_gpu
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not oracle.refgpu_available(), reason="reference GPU shim not built")]
+
+
+@pytest.mark.parametrize("kind", ["gauss", "multi", "singular"])
+def test_gpu_rule_matches_reference_gpu_kernel(kind):
+    pts, nrm = synth.torus(20000, seed=61)
+    pts = synth.make_tie_free(pts)
+    depth = 11  # keeps every leaf shallower than the reference kernel's 12-entry array
+    q = synth.perturbed_queries(pts, 0.01, seed=62)[:1000]
+    diag = synth.bbox_diag(pts)
+    k = make_kernel(kind, diag)
+    ref = oracle.RefGpu(pts, nrm, k, cutoff=3.0, max_depth=depth)
+    rp, rn, _ = ref.project(q, calls=10, iters_per_call=1)
+    ot = oracle.OracleTree(pts, nrm, depth)
+    o64, _ = ot.project_mlod(q, 10, k, rule=0, cutoff=3.0)
+    # the oracle restates the reference's GPU rule: agreement to the
+    # reference's own float noise
+    e_ref = rel_err(rp, o64, diag)
+    assert np.percentile(e_ref, 99) < 5e-6, np.percentile(e_ref, 99)
+    # the kernel agrees with the reference wherever the reference is accurate
+    op, _, _, _ = run_gpu(pts, nrm, q, k, rule=BLEND_GPU, depth=depth)
+    ok = e_ref < 5e-6
+    assert ok.mean() > 0.98
+    assert rel_err(op, rp, diag)[ok].max() < TOL_DIAG
