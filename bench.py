@@ -134,6 +134,31 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# DRAM bytes (read + write) of one projection launch of the default workload
+# (2M points, 2M queries, 10 iterations), from a single-pass ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum: see
+# profiles/mlod_project_kernel_precision_2M_launches.md.
+PROFILED_TRAFFIC = {(2_000_000, 10): 465.77e6 + 130.46e6}
+
+
+def max_over_ranks(values, world: int, device):
+    """Element-wise max of per-rank timings (the slowest rank sets the job
+    time); identity on one rank."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def job_throughput(world: int, queries_per_rank: int, steps: int, total_ms_max: float) -> float:
+    """Whole-job queries/s: every rank projects its own queries_per_rank
+    queries per step (weak scaling) and the job lasts as long as its slowest
+    rank."""
+    return world * queries_per_rank * steps / (total_ms_max / 1e3)
+
+
 def measured_peak_hbm():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -242,12 +267,8 @@ def run_ours(args, rank, world, local_rank):
         torch.distributed.barrier()
     clk = clocks.stop()
 
-    total_ms = float(sum(step_ms))
-    t = torch.tensor([total_ms, max(step_ms)], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms_max = float(t[0])
-    value = world * len(q) * args.steps / (total_ms_max / 1e3)
+    total_ms_max = max_over_ranks([float(sum(step_ms))], world, dev)[0]
+    value = job_throughput(world, len(q), args.steps, total_ms_max)
 
     # ---- end to end through the public C ABI with host buffers (Fastapss protocol)
     h_q = torch.from_numpy(q).pin_memory()
@@ -269,10 +290,8 @@ def run_ours(args, rank, world, local_rank):
         e1.synchronize()
         if i > 0:  # first call allocates the query buffer
             e2e_ms.append(e0.elapsed_time(e1))
-    te = torch.tensor([statistics.mean(e2e_ms)], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * len(q) / (float(te[0]) / 1e3)
+    e2e_ms_max = max_over_ranks([statistics.mean(e2e_ms)], world, dev)[0]
+    e2e_value = job_throughput(world, len(q), 1, e2e_ms_max)
     out_host = d_p.cpu().numpy()
 
     # ---- roofline of the projection kernel (algorithmic bytes per launch)
@@ -304,10 +323,10 @@ def run_ours(args, rank, world, local_rank):
                 "path": "mlods_queries_upload + mlods_project (host pinned in/out)"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None,
+                     "traffic": PROFILED_TRAFFIC.get((args.n_points, args.iters)),
                      "note": f"algorithmic bytes = 36 per query + 64 per node visit ({mean_visits / len(q) / args.iters:.0f}"
-                             f" visits per query-iteration); peak {peak_kind}; node records are mostly served "
-                             f"from L1/L2"},
+                             f" visits per query-iteration); peak {peak_kind}; traffic = DRAM bytes per launch from "
+                             f"ncu: the node arrays are read from DRAM about once, later visits hit L1/L2"},
         "kernel_ms": kms,
         "traversal": {"visits_per_query_iteration": mean_visits / len(q) / args.iters,
                       "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),
@@ -380,7 +399,7 @@ def main():
         import torch
 
         torch.cuda.set_device(local_rank)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local_rank))
     try:
         res = run_ours(args, rank, world, local_rank)

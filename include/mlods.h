@@ -57,6 +57,12 @@ typedef struct mlods_kernel {
 
 /* Projection options; mirror APSS::setScalingProtectionSphere / setMinDepth
  * (GPUUtils.h:40-43) and APSSOctree::knnMode / ballMode (CPUUtils.h:191-192). */
+/* ---- convergence modes (extension; the reference always runs n_iterations) ---- */
+#define MLODS_CONVERGE_OFF 0    /* run every iteration (reference behaviour) */
+#define MLODS_CONVERGE_EXACT 1  /* stop a query once its float iterate repeats: the remaining iterations
+                                   would return the same result, so outputs are bit-identical */
+#define MLODS_CONVERGE_TOL 2    /* stop a query once its step is shorter than converge_tol */
+
 typedef struct mlods_params {
     float cutoff;        /* scalingProtectionSphere: a node is an aggregate when |q-c| > cutoff*r (default 2) */
     int32_t min_depth;   /* nodes shallower than this are always opened (default 0) */
@@ -65,8 +71,9 @@ typedef struct mlods_params {
     float ball_radius;   /* radius for MLODS_MODE_BALL; < 0 uses 3 * sigmas[0] (default 0.1) */
     int32_t blend_rule;  /* MLODS_BLEND_GPU (default) or MLODS_BLEND_CPU */
     int32_t reorder;     /* 1: process queries in Morton order (results are identical) */
-    float prune_tol;     /* > 0: skip MLoD subtrees whose weight bound is below prune_tol
-                            times the running total (extension; 0 = off, reference behaviour) */
+    float prune_tol;     /* reserved (0) */
+    int32_t converge;    /* MLODS_CONVERGE_* (default MLODS_CONVERGE_OFF) */
+    float converge_tol;  /* step length for MLODS_CONVERGE_TOL (absolute units) */
 } mlods_params;
 
 typedef struct mlods_tree_s* mlods_tree;
@@ -176,6 +183,39 @@ int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out
 #define MLODS_MAX_KNN 32
 int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_idx, float* d_d2, void* stream);
 
+/* ---- dual contouring --------------------------------------------------------
+ * Cells are octree nodes (depth, x, y, z) as octree_id (octree.h:18-44) over
+ * the unit cube; their corners sit on the integer lattice of the deepest
+ * level, max_depth.
+ *
+ * mlods_dcgrid_from_points builds the DC grid of the reference's `-b` path:
+ * OctreeGenerator::generateFromPoints (upsample.cpp:128-144: the cells at
+ * max_depth enclosing the points inside [box_min, box_max], the reference uses
+ * [-1,1]^3) followed by uniformizeFromPoints (upsample.cpp:253-260: grade,
+ * regularize_up, regularize_siblings), cells in sorted_octree order
+ * (node_comparator, octree.h:147-154).  Host code. */
+typedef struct mlods_dcgrid_s* mlods_dcgrid;
+int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, const float* box_min,
+                             const float* box_max, mlods_dcgrid* out);
+int mlods_dcgrid_info(mlods_dcgrid g, int64_t* n_cells, int32_t* max_depth);
+int mlods_dcgrid_cells(mlods_dcgrid g, int32_t* cells);  /* 4 int32 per cell */
+int mlods_dcgrid_free(mlods_dcgrid g);
+
+/* Signed field at the 8 corners of every cell and the per-cell vertex
+ * (scene.cpp:1346-1394, dual_contouring.h:124-176).  xform is the 3x4
+ * row-major map from the unit cube to the tree's frame (the top rows of
+ * new2bbox, scene.cpp:1313).  Every unique corner is projected once (one MLoD
+ * iteration with the tree's kernel and options); corner_f[8 c + k] =
+ * (corner - projection).normal, NaN when the projection failed.  vertex[3 c]
+ * is the cell's vertex in the unit cube and n_cross[c] its number of edge
+ * crossings: with use_normals = 0 the reference's zero normal field, i.e. the
+ * mass point of the crossings (the cell centre without crossings); with
+ * use_normals = 1 a full QEF on the interpolated projected normals, solved in
+ * double (extension).  Host arrays in and out; synchronous. */
+int mlods_dc_evaluate(mlods_tree t, int64_t n_cells, const int32_t* cells, int32_t max_depth, const float* xform,
+                      int32_t use_normals, float* corner_f, float* vertex, int32_t* n_cross,
+                      int64_t* n_unique_corners, void* stream);
+
 /* ---- per-launch statistics of the last projection on this tree ------------
  * node visits summed over queries and iterations, warp rounds (32 lanes each)
  * that evaluated them, largest traversal stack, queries whose traversal stack
@@ -184,6 +224,33 @@ int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_i
  * the launching stream).  Any pointer may be NULL.  Synchronises. */
 int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_t* max_stack, int64_t* overflows,
                      float* kernel_ms);
+
+/* ---- batched projection over many resident trees (extension) ---------------
+ * No counterpart in the reference, which projects one tree per launch
+ * (Fastapss::project, Fastapss.cu:439-455).  A batch holds a fixed list of
+ * trees; mlods_batch_project projects, in ONE persistent kernel launch, the
+ * device query buffer d_q (float xyz, concatenated per tree: tree i owns
+ * queries [offsets[i], offsets[i+1]), offsets is a HOST array of n_trees + 1
+ * entries starting at 0) onto their trees, writing d_out_pts/d_out_nrm in the
+ * same layout.  Every tree must be in MLODS_MODE_MLOD with a kernel set; each
+ * tree's own cutoff, min_depth, blend rule and convergence mode apply, and the
+ * step clamp is each tree's root box radius.  Results equal per-tree
+ * mlods_project_device calls bit for bit.  With use_graph != 0 the work is
+ * captured once in a CUDA graph and replayed while buffers, offsets, tree
+ * settings and n_iterations stay the same (the stream must not be capturing).
+ * mlods_batch_tune times a few launch shapes on the given buffers (it runs the
+ * projection four times) and keeps the fastest for later calls.  The trees
+ * must outlive the batch and must not be rebuilt while it exists. */
+typedef struct mlods_batch_s* mlods_batch;
+int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* out);
+int mlods_batch_free(mlods_batch b);
+int mlods_batch_project(mlods_batch b, const int64_t* offsets, const float* d_q, float* d_out_pts, float* d_out_nrm,
+                        int32_t n_iterations, int32_t use_graph, void* stream);
+int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, float* d_out_pts, float* d_out_nrm,
+                     int32_t n_iterations, void* stream);
+/* Statistics of the last batch launch (synchronises); any pointer may be NULL. */
+int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
+                      int32_t* reorder, int32_t* grid_pct);
 
 /* Number of kernels this library has launched in this process (diagnostics). */
 int64_t mlods_kernel_launches(void);

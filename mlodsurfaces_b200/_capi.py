@@ -10,7 +10,9 @@ import ctypes as C
 import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libmlods.so"
+# MLODS_LIBRARY selects another build of the same library (e.g. a variant
+# compiled with different tuning constants); the default is the in-tree build.
+LIB_PATH = Path(os.environ.get("MLODS_LIBRARY", Path(__file__).resolve().parent / "_lib" / "libmlods.so"))
 
 MLODS_OK = 0
 MLODS_ERR_INVALID = 1
@@ -31,6 +33,10 @@ MODE_BALL = 3
 
 BLEND_GPU = 0
 BLEND_CPU = 1
+
+CONVERGE_OFF = 0
+CONVERGE_EXACT = 1
+CONVERGE_TOL = 2
 
 
 class mlods_kernel(C.Structure):
@@ -54,6 +60,8 @@ class mlods_params(C.Structure):
         ("blend_rule", C.c_int32),
         ("reorder", C.c_int32),
         ("prune_tol", C.c_float),
+        ("converge", C.c_int32),
+        ("converge_tol", C.c_float),
     ]
 
 
@@ -107,6 +115,16 @@ SIGNATURES = {
     "mlods_last_stats": (C.c_int, [_P, _I64, _I64, _I32, _I64, C.POINTER(C.c_float)]),
     "mlods_kernel_launches": (C.c_int64, []),
     "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),
+    "mlods_dcgrid_from_points": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, C.POINTER(_P)]),
+    "mlods_dcgrid_info": (C.c_int, [_P, _I64, _I32]),
+    "mlods_dcgrid_cells": (C.c_int, [_P, _P]),
+    "mlods_dcgrid_free": (C.c_int, [_P]),
+    "mlods_dc_evaluate": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, C.c_int32, _P, _P, _P, _I64, _P]),
+    "mlods_batch_create": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
+    "mlods_batch_free": (C.c_int, [_P]),
+    "mlods_batch_project": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, _P]),
+    "mlods_batch_tune": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
+    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32]),
 }
 
 _lib = None

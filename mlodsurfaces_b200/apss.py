@@ -246,6 +246,42 @@ class APSSOctree:
         return out
 
 
+class DCGrid:
+    """Dual-contouring cells from points (OctreeGenerator::generateFromPoints +
+    uniformizeFromPoints, upsample.cpp:128-144, :253-260), built on the host by
+    the library.  ``cells`` is an int32 (n, 4) array of (depth, x, y, z) in
+    sorted_octree order; ``max_depth`` the deepest level."""
+
+    def __init__(self, points, max_depth: int, box_min=(-1.0, -1.0, -1.0), box_max=(1.0, 1.0, 1.0)):
+        lib = capi.load()
+        pts = _f32x3(points, "points")
+        bmin = np.asarray(box_min, np.float32)
+        bmax = np.asarray(box_max, np.float32)
+        g = C.c_void_p(0)
+        capi.check(lib.mlods_dcgrid_from_points(capi.ptr(pts), len(pts), int(max_depth), capi.ptr(bmin),
+                                                capi.ptr(bmax), C.byref(g)))
+        try:
+            n = C.c_int64(0)
+            d = C.c_int32(0)
+            capi.check(lib.mlods_dcgrid_info(g, C.byref(n), C.byref(d)))
+            self.cells = np.empty((n.value, 4), np.int32)
+            capi.check(lib.mlods_dcgrid_cells(g, capi.ptr(self.cells)))
+            self.max_depth = int(d.value)
+        finally:
+            lib.mlods_dcgrid_free(g)
+
+
+def unit2bbox(box_min=(-1.0, -1.0, -1.0), box_max=(1.0, 1.0, 1.0)) -> np.ndarray:
+    """3x4 map from the unit cube to the octree zone box (scene.cpp:1257-1269)."""
+    bmin = np.asarray(box_min, np.float32)
+    d = (np.asarray(box_max, np.float32) - bmin).astype(np.float32)
+    m = np.zeros((3, 4), np.float32)
+    for a in range(3):
+        m[a, a] = d[a]
+        m[a, 3] = bmin[a]
+    return m
+
+
 class APSS:
     """Projection interface (GPUUtils.h:22-67) over a device octree."""
 
@@ -259,6 +295,8 @@ class APSS:
         self.blend_rule = capi.BLEND_GPU
         self.reorder = True
         self.prune_tol = 0.0
+        self.converge = capi.CONVERGE_OFF
+        self.converge_tol = 0.0
         self._n_uploaded = 0
         q = C.c_void_p(0)
         capi.check(self._lib.mlods_queries_create(C.byref(q)))
@@ -286,6 +324,8 @@ class APSS:
         p.blend_rule = int(self.blend_rule)
         p.reorder = 1 if self.reorder else 0
         p.prune_tol = float(self.prune_tol)
+        p.converge = int(self.converge)
+        p.converge_tol = float(self.converge_tol)
         return p
 
     def _mode(self) -> int:
@@ -349,6 +389,23 @@ class APSS:
                                                   capi.ptr(d_out_p), capi.ptr(d_out_n), int(n_iterations),
                                                   float(stepMaxSize), C.c_void_p(stream or 0)))
 
+    def dc_evaluate(self, cells, max_depth: int, xform=None, use_normals: bool = False):
+        """Corner field and per-cell vertex of a DC grid (scene.cpp:1346-1394,
+        dual_contouring.h:124-176): (corner_f (n, 8), vertex (n, 3) in the unit
+        cube, n_cross (n,), number of unique corners projected)."""
+        self._sync_params()
+        cells = np.ascontiguousarray(np.asarray(cells, np.int32).reshape(-1, 4))
+        xf = np.ascontiguousarray(unit2bbox() if xform is None else np.asarray(xform, np.float32).reshape(3, 4))
+        n = len(cells)
+        cf = np.empty((n, 8), np.float32)
+        vx = np.empty((n, 3), np.float32)
+        nc = np.empty(n, np.int32)
+        nu = C.c_int64(0)
+        capi.check(self._lib.mlods_dc_evaluate(self.m_apssOctree.handle, n, capi.ptr(cells), int(max_depth),
+                                               capi.ptr(xf), 1 if use_normals else 0, capi.ptr(cf), capi.ptr(vx),
+                                               capi.ptr(nc), C.byref(nu), C.c_void_p(0)))
+        return cf, vx, nc, nu.value
+
     def last_stats(self):
         v = C.c_int64(0)
         r = C.c_int64(0)
@@ -389,3 +446,71 @@ class GlobalAPSS(APSS):
     """APSS over every point, no level of detail (GlobalAPSS.h:19-43)."""
 
     mode = capi.MODE_GLOBAL
+
+
+class FastapssBatch:
+    """Many resident Fastapss objects projected in one kernel launch.
+
+    No counterpart in the reference (one ``Fastapss::project`` launch per tree,
+    Fastapss.cu:439-455).  ``projectors`` are :class:`Fastapss` objects whose
+    kernel has been set; each keeps its own settings (cutoff, min depth, blend
+    rule, convergence mode).  :meth:`project_device` takes one concatenated
+    device query buffer (torch CUDA tensors, float32 (n, 3)) and the per-tree
+    query counts, and gives results identical to one ``project_device`` call
+    per tree.  The projectors must outlive the batch.
+    """
+
+    def __init__(self, projectors):
+        self._lib = capi.load()
+        self._projectors = list(projectors)
+        if not self._projectors:
+            raise ValueError("need at least one projector")
+        for p in self._projectors:
+            if p._mode() != capi.MODE_MLOD:
+                raise ValueError("batched projection supports the MLoD mode only")
+        handles = (C.c_void_p * len(self._projectors))(*[p.m_apssOctree.handle.value for p in self._projectors])
+        b = C.c_void_p(0)
+        capi.check(self._lib.mlods_batch_create(handles, len(self._projectors), C.byref(b)))
+        self._b = b
+
+    def __del__(self):
+        try:
+            if getattr(self, "_b", None):
+                self._lib.mlods_batch_free(self._b)
+                self._b = None
+        except Exception:
+            pass
+
+    def _offsets(self, counts) -> np.ndarray:
+        counts = np.asarray(counts, np.int64)
+        if counts.shape != (len(self._projectors),) or (counts < 0).any():
+            raise ValueError("counts must give one non-negative count per projector")
+        return np.ascontiguousarray(np.concatenate([[0], np.cumsum(counts)]).astype(np.int64))
+
+    def project_device(self, counts, d_q, d_out_p, d_out_n, n_iterations: int, use_graph: bool = False,
+                       stream=None) -> None:
+        for p in self._projectors:
+            p._sync_params()
+        off = self._offsets(counts)
+        capi.check(self._lib.mlods_batch_project(self._b, capi.ptr(off), capi.ptr(d_q), capi.ptr(d_out_p),
+                                                 capi.ptr(d_out_n), int(n_iterations), 1 if use_graph else 0,
+                                                 C.c_void_p(stream or 0)))
+
+    def tune(self, counts, d_q, d_out_p, d_out_n, n_iterations: int, stream=None) -> None:
+        for p in self._projectors:
+            p._sync_params()
+        off = self._offsets(counts)
+        capi.check(self._lib.mlods_batch_tune(self._b, capi.ptr(off), capi.ptr(d_q), capi.ptr(d_out_p),
+                                              capi.ptr(d_out_n), int(n_iterations), C.c_void_p(stream or 0)))
+
+    def last_stats(self):
+        v = C.c_int64(0)
+        r = C.c_int64(0)
+        o = C.c_int64(0)
+        ms = C.c_float(0)
+        ro = C.c_int32(0)
+        gp = C.c_int32(0)
+        capi.check(self._lib.mlods_batch_stats(self._b, C.byref(v), C.byref(r), C.byref(o), C.byref(ms),
+                                               C.byref(ro), C.byref(gp)))
+        return {"node_visits": v.value, "rounds": r.value, "overflows": o.value, "kernel_ms": ms.value,
+                "reorder": ro.value, "grid_pct": gp.value}

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 
+#include "dc.h"
 #include "gather.cuh"
 #include "project.cuh"
 #include "tree.cuh"
@@ -17,6 +18,7 @@ namespace
 {
 thread_local char g_err[1024] = "";
 std::atomic<int64_t> g_launches{0};
+}  // namespace
 
 int sm_count_for_current_device()
 {
@@ -30,11 +32,13 @@ int sm_count_for_current_device()
     return v;
 }
 
+namespace
+{
 inline size_t al256(size_t v) { return (v + 255) / 256 * 256; }
-
 }  // namespace
 
 void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_last_error(const char* fmt, ...)
 {
@@ -47,6 +51,9 @@ void set_last_error(const char* fmt, ...)
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line)
 {
     set_last_error("CUDA error %d (%s) in %s at %s:%d", int(e), cudaGetErrorString(e), what, file, line);
+    // reset the runtime's last-error slot so that a later launch check does
+    // not report this (non-sticky) error again
+    (void)cudaGetLastError();
     return MLODS_ERR_CUDA;
 }
 
@@ -86,6 +93,26 @@ static int ensure_scratch(mlods_tree_s* T, size_t bytes)
     return MLODS_OK;
 }
 
+void fill_cloud_args(const mlods_tree_s* T, CloudArgs& c, const float* d_q, float* d_out_p, float* d_out_n,
+                     int iters, float step_max, int rule)
+{
+    c.nodes = T->nodes;
+    c.o0 = T->origin[0];
+    c.o1 = T->origin[1];
+    c.o2 = T->origin[2];
+    c.kc = T->kc;
+    c.cutoff = T->params.cutoff;
+    c.min_depth = T->params.min_depth;
+    c.step_max = step_max < 0.f ? T->root_radius : step_max;
+    c.rule = rule;
+    c.n_iter = iters;
+    c.conv_mode = T->params.converge;
+    c.conv_tol = T->params.converge_tol;
+    c.q_in = d_q;
+    c.out_p = d_out_p;
+    c.out_n = d_out_n;
+}
+
 // Pruning margin of the neighbour searches: points may sit up to half a
 // world-frame ulp outside their cell box (the reference classifies against the
 // double split but stores the float one), and local coordinates are rounded.
@@ -102,7 +129,7 @@ static float gather_eps(const mlods_tree_s* T)
 
 static void fill_gather_args(mlods_tree_s* T, GatherArgs& g)
 {
-    g.nodes = T->d_nodes;
+    g.nodes = T->nodes;
     g.node_head = T->d_node_head;
     g.codes = T->d_codes;
     g.wspts = T->d_wspts;
@@ -196,8 +223,8 @@ static int project_apss_impl(mlods_tree_s* T, int64_t n, const float* d_q, float
     return MLODS_OK;
 }
 
-static int project_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
-                        float step_max, cudaStream_t s, int rule_override = -1)
+int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
+                    float step_max, cudaStream_t s, int rule_override)
 {
     if (!T->kernel_set) {
         set_last_error("project: no kernel set (call mlods_set_kernel first)");
@@ -226,27 +253,16 @@ static int project_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_o
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
         MLODS_CUDA(compute_query_order(d_q, n, T->origin, ext, d_order, base + al256(size_t(n) * 4), s));
     }
+    const int rule = rule_override >= 0 ? rule_override : T->params.blend_rule;
     ProjectArgs a;
-    a.nodes = T->d_nodes;
-    a.q_in = d_q;
-    a.out_p = d_out_p;
-    a.out_n = d_out_n;
+    fill_cloud_args(T, a.cloud, d_q, d_out_p, d_out_n, iters, step_max, rule);
     a.order = d_order;
     a.nq = n;
-    a.n_iter = iters;
-    a.cutoff = T->params.cutoff;
-    a.min_depth = T->params.min_depth;
-    a.step_max = step_max < 0.f ? T->root_radius : step_max;
-    a.o0 = T->origin[0];
-    a.o1 = T->origin[1];
-    a.o2 = T->origin[2];
-    a.kc = T->kc;
     a.counter = reinterpret_cast<unsigned int*>(T->d_stats + 3);
     a.stats = T->d_stats;
     rc = ensure_events(T);
     if (rc != MLODS_OK) return rc;
     MLODS_CUDA(cudaEventRecord(T->ev_start, s));
-    const int rule = rule_override >= 0 ? rule_override : T->params.blend_rule;
     MLODS_CUDA(launch_mlod_project(a, T->kc.type, rule, sm_count_for_current_device(), s));
     MLODS_CUDA(cudaEventRecord(T->ev_stop, s));
     T->timed = true;
@@ -282,6 +298,8 @@ void mlods_default_params(mlods_params* p)
     p->blend_rule = MLODS_BLEND_GPU;
     p->reorder = 1;
     p->prune_tol = 0.f;
+    p->converge = MLODS_CONVERGE_OFF;
+    p->converge_tol = 0.f;
 }
 
 int mlods_tree_build_device(const float* d_pts, const float* d_nrm, int64_t n, int32_t max_depth, void* stream,
@@ -422,6 +440,10 @@ int mlods_set_params(mlods_tree t, const mlods_params* p)
         set_last_error("min_depth must be >= 0");
         return MLODS_ERR_INVALID;
     }
+    if (p->converge < MLODS_CONVERGE_OFF || p->converge > MLODS_CONVERGE_TOL) {
+        set_last_error("unknown convergence mode %d", p->converge);
+        return MLODS_ERR_INVALID;
+    }
     t->params = *p;
     return MLODS_OK;
 }
@@ -497,7 +519,7 @@ int mlods_project(mlods_tree t, mlods_queries q, int64_t n, int32_t n_iterations
         return MLODS_ERR_STATE;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc = project_impl(t, n, q->d_q, q->d_q, q->d_qn, n_iterations, step_max, s);
+    int rc = project_buffers(t, n, q->d_q, q->d_q, q->d_qn, n_iterations, step_max, s);
     if (rc != MLODS_OK) return rc;
     if (out_pts)
         MLODS_CUDA(cudaMemcpyAsync(out_pts, q->d_q, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -553,7 +575,7 @@ int mlods_project_host(mlods_tree t, int64_t n, const float* q, float* out_pts, 
     MLODS_CUDA(cudaMalloc(&d, size_t(n) * 9 * sizeof(float)));
     cudaError_t e = cudaMemcpyAsync(d, q, size_t(n) * 12, cudaMemcpyHostToDevice, s);
     int rc = MLODS_OK;
-    if (e == cudaSuccess) rc = project_impl(t, n, d, d + 3 * n, d + 6 * n, n_iterations, step_max, s, blend_rule);
+    if (e == cudaSuccess) rc = project_buffers(t, n, d, d + 3 * n, d + 6 * n, n_iterations, step_max, s, blend_rule);
     if (e == cudaSuccess && rc == MLODS_OK) e = cudaMemcpyAsync(out_pts, d + 3 * n, size_t(n) * 12, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && rc == MLODS_OK && out_nrm)
         e = cudaMemcpyAsync(out_nrm, d + 6 * n, size_t(n) * 12, cudaMemcpyDeviceToHost, s);
@@ -572,7 +594,7 @@ int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out
         set_last_error("project_device: null buffer");
         return MLODS_ERR_INVALID;
     }
-    return project_impl(t, n, d_q, d_out_pts, d_out_nrm, n_iterations, step_max, static_cast<cudaStream_t>(stream));
+    return project_buffers(t, n, d_q, d_out_pts, d_out_nrm, n_iterations, step_max, static_cast<cudaStream_t>(stream));
 }
 
 int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_idx, float* d_d2, void* stream)
@@ -605,6 +627,68 @@ int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_i
     MLODS_CUDA(launch_gather(g, kGatherKnnOnly, t->kernel_set ? t->kc.type : MLODS_GAUSSIAN,
                              sm_count_for_current_device(), s));
     return MLODS_OK;
+}
+
+int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, const float* box_min,
+                             const float* box_max, mlods_dcgrid* out)
+{
+    if (!out || !box_min || !box_max) {
+        set_last_error("dcgrid: null argument");
+        return MLODS_ERR_INVALID;
+    }
+    *out = nullptr;
+    auto* g = new (std::nothrow) mlods_dcgrid_s();
+    if (!g) {
+        set_last_error("dcgrid: host allocation failed");
+        return MLODS_ERR_CAPACITY;
+    }
+    const int rc = dcgrid_from_points(pts, n, max_depth, box_min, box_max, g->cells, g->max_depth);
+    if (rc != MLODS_OK) {
+        delete g;
+        return rc;
+    }
+    *out = g;
+    return MLODS_OK;
+}
+
+int mlods_dcgrid_info(mlods_dcgrid g, int64_t* n_cells, int32_t* max_depth)
+{
+    if (!g) {
+        set_last_error("null dc grid");
+        return MLODS_ERR_INVALID;
+    }
+    if (n_cells) *n_cells = int64_t(g->cells.size() / 4);
+    if (max_depth) *max_depth = g->max_depth;
+    return MLODS_OK;
+}
+
+int mlods_dcgrid_cells(mlods_dcgrid g, int32_t* cells)
+{
+    if (!g || !cells) {
+        set_last_error("null dc grid or output");
+        return MLODS_ERR_INVALID;
+    }
+    std::memcpy(cells, g->cells.data(), g->cells.size() * sizeof(int32_t));
+    return MLODS_OK;
+}
+
+int mlods_dcgrid_free(mlods_dcgrid g)
+{
+    delete g;
+    return MLODS_OK;
+}
+
+int mlods_dc_evaluate(mlods_tree t, int64_t n_cells, const int32_t* cells, int32_t max_depth, const float* xform,
+                      int32_t use_normals, float* corner_f, float* vertex, int32_t* n_cross,
+                      int64_t* n_unique_corners, void* stream)
+{
+    CHECK_TREE(t);
+    if (!t->kernel_set) {
+        set_last_error("dc evaluate: no kernel set (call mlods_set_kernel first)");
+        return MLODS_ERR_STATE;
+    }
+    return dc_evaluate(t, n_cells, cells, max_depth, xform, use_normals, corner_f, vertex, n_cross, n_unique_corners,
+                       static_cast<cudaStream_t>(stream));
 }
 
 int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_t* max_stack, int64_t* overflows,

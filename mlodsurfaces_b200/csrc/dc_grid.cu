@@ -1,0 +1,154 @@
+// dc_grid.cu -- the dual-contouring cell grid built from points (host).
+//
+// OctreeGenerator::generateFromPoints (upsample.cpp:128-144) then
+// uniformizeFromPoints (upsample.cpp:253-260): the cells enclosing the points
+// at max_depth, graded (grade, upsample.cpp:67-93), completed with all their
+// ancestors (regularize_up, :40-46) and with the siblings of every non-root
+// cell (regularize_siblings, :48-65), in sorted_octree order (node_comparator,
+// octree.h:147-154: depth, then z, y, x).  Integer set work on a few million
+// cells; the device evaluates the field on the result.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "dc.h"
+#include "mlods_internal.cuh"
+
+namespace mlods
+{
+namespace
+{
+struct Cell {
+    int depth, x, y, z;
+    bool operator==(const Cell& o) const { return depth == o.depth && x == o.x && y == o.y && z == o.z; }
+};
+
+// node_comparator, octree.h:147-154
+inline bool cell_less(const Cell& a, const Cell& b)
+{
+    if (a.depth != b.depth) return a.depth < b.depth;
+    if (a.z != b.z) return a.z < b.z;
+    if (a.y != b.y) return a.y < b.y;
+    return a.x < b.x;
+}
+
+// octree_id::parent, octree.h:547-559 (division rounded towards -infinity)
+inline int floor_half(int v) { return (v < 0 && (v % 2) != 0) ? v / 2 - 1 : v / 2; }
+inline Cell parent(const Cell& c) { return Cell{c.depth - 1, floor_half(c.x), floor_half(c.y), floor_half(c.z)}; }
+inline Cell child(const Cell& c, int k)
+{
+    return Cell{c.depth + 1, 2 * c.x + (k & 1), 2 * c.y + ((k >> 1) & 1), 2 * c.z + ((k >> 2) & 1)};
+}
+// octree_id::neighbor, octree.h:591-602
+inline Cell neighbor(const Cell& c, int n)
+{
+    const int z = n / 9, y = (n - 9 * z) / 3, x = n - 9 * z - 3 * y;
+    return Cell{c.depth, c.x + x - 1, c.y + y - 1, c.z + z - 1};
+}
+
+void remove_duplicates(std::vector<Cell>& v)
+{
+    std::sort(v.begin(), v.end(), cell_less);
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+}
+
+void remove_duplicates_reverse(std::vector<Cell>& v)
+{
+    std::sort(v.rbegin(), v.rend(), cell_less);
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+}
+
+// grade, upsample.cpp:67-93
+void grade(std::vector<Cell>& nodes)
+{
+    static const int corners[8] = {0, 2, 6, 8, 18, 20, 24, 26};
+    if (nodes.empty()) return;
+    std::sort(nodes.rbegin(), nodes.rend(), cell_less);
+    size_t i = 0;
+    int current = nodes[0].depth;
+    while (i < nodes.size()) {
+        if (current != nodes[i].depth) {
+            remove_duplicates_reverse(nodes);
+            current = nodes[i].depth;
+        }
+        if (nodes[i].depth > 0)
+            for (int c : corners) nodes.push_back(parent(neighbor(nodes[i], c)));
+        ++i;
+    }
+    remove_duplicates(nodes);
+}
+
+// regularize_up, upsample.cpp:40-46
+void regularize_up(std::vector<Cell>& nodes)
+{
+    for (size_t t = 0; t < nodes.size(); ++t)
+        if (nodes[t].depth != 0) nodes.push_back(parent(nodes[t]));
+    remove_duplicates(nodes);
+}
+
+// regularize_siblings, upsample.cpp:48-65 (entries of depth-0 cells stay the
+// default octree_id, the root)
+void regularize_siblings(std::vector<Cell>& nodes)
+{
+    const size_t s = nodes.size();
+    nodes.resize(9 * s, Cell{0, 0, 0, 0});
+    for (size_t t = 0; t < s; ++t) {
+        if (nodes[t].depth <= 0) continue;
+        const Cell p = parent(nodes[t]);
+        for (int k = 0; k < 8; ++k) nodes[s + 8 * t + k] = child(p, k);
+    }
+    remove_duplicates(nodes);
+}
+
+}  // namespace
+
+int dcgrid_from_points(const float* pts, int64_t n, int max_depth, const float box_min[3], const float box_max[3],
+                       std::vector<int32_t>& cells_out, int& depth_out)
+{
+    if (n <= 0 || !pts) {
+        set_last_error("dc grid: no points");
+        return MLODS_ERR_INVALID;
+    }
+    if (max_depth < 0 || max_depth > 16) {
+        set_last_error("dc grid: max_depth=%d out of range [0, 16]", max_depth);
+        return MLODS_ERR_INVALID;
+    }
+    float diag[3];
+    for (int a = 0; a < 3; ++a) {
+        diag[a] = box_max[a] - box_min[a];
+        if (!(diag[a] > 0.f)) {
+            set_last_error("dc grid: empty box");
+            return MLODS_ERR_INVALID;
+        }
+    }
+    // aabb_octree::enclosing, octree.h:957-965: P = (pos - min) / diag / w, floored
+    const float w = 1.0f / float(1 << max_depth);
+    std::vector<Cell> nodes(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) {
+        int c[3];
+        for (int a = 0; a < 3; ++a) {
+            const float t = (pts[3 * i + a] - box_min[a]) / diag[a] / w;
+            c[a] = int(std::floor(t));
+        }
+        nodes[size_t(i)] = Cell{max_depth, c[0], c[1], c[2]};
+    }
+    remove_duplicates(nodes);
+    grade(nodes);
+    regularize_up(nodes);
+    regularize_siblings(nodes);
+    depth_out = 0;
+    cells_out.resize(nodes.size() * 4);
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        cells_out[4 * i] = nodes[i].depth;
+        cells_out[4 * i + 1] = nodes[i].x;
+        cells_out[4 * i + 2] = nodes[i].y;
+        cells_out[4 * i + 3] = nodes[i].z;
+        depth_out = std::max(depth_out, nodes[i].depth);
+    }
+    return MLODS_OK;
+}
+
+}  // namespace mlods

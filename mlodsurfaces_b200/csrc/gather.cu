@@ -316,9 +316,11 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
                     if (r_cnt & kGPoints) {
                         cpos = idx;
                     } else {
-                        const DNode nd = a.nodes[idx];
-                        if (nd.info & kLeafBit) {
-                            const int cnt = int(node_count(nd.info));
+                        const float4 g4 = __ldg(a.nodes.geom + idx);
+                        const float4 x4 = __ldg(a.nodes.aux + idx);
+                        const uint32_t info = __float_as_uint(x4.z);
+                        if (info & kLeafBit) {
+                            const int cnt = int(node_count(info));
                             const int64_t head = __ldg(a.node_head + idx);
                             if (cnt == 1) {
                                 cpos = head;
@@ -328,13 +330,13 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
                                 p_cnt = uint32_t(cnt) | kGPoints;
                             }
                         } else {
-                            const float cx = nd.cx - lx, cy = nd.cy - ly, cz = nd.cz - lz;
+                            const float cx = g4.x - lx, cy = g4.y - ly, cz = g4.z - lz;
                             const float dc = sqrtf(cx * cx + cy * cy + cz * cz);
-                            const float lo = dc - nd.r - a.eps;
+                            const float lo = dc - g4.w - a.eps;
                             if (!(lo > 0.f && lo * lo > bound)) {
                                 push = true;
-                                p_first = nd.first;
-                                p_cnt = node_count(nd.info);
+                                p_first = __float_as_uint(x4.y);
+                                p_cnt = node_count(info);
                             }
                         }
                     }

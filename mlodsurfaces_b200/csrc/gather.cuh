@@ -15,7 +15,7 @@ constexpr int kGatherBallApss = 1;
 constexpr int kGatherKnnOnly = 2;
 
 struct GatherArgs {
-    const DNode* nodes;
+    NodeArrays nodes;
     const int32_t* node_head;  // sorted position of each node's first point
     const uint64_t* codes;     // sorted Morton codes
     const float4* wspts;       // sorted points, world frame, w = original index bits

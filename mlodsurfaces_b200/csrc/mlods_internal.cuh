@@ -45,6 +45,44 @@ struct __align__(16) DNode {
 };
 static_assert(sizeof(DNode) == 64, "DNode must stay 64 bytes");
 
+// The nodes live in HBM as four float4 arrays (structure of arrays), so that
+// the loads of one sibling range are contiguous per array:
+//   geom[i] = {cx, cy, cz, r}      pm[i] = {px, py, pz, m0}
+//   nc[i]   = {nx, ny, nz, cpn}    aux[i] = {cpp, first, info, parent}
+struct NodeArrays {
+    float4* geom;
+    float4* pm;
+    float4* nc;
+    float4* aux;
+};
+
+__device__ inline void store_node(const NodeArrays& a, int64_t i, const DNode& n)
+{
+    a.geom[i] = make_float4(n.cx, n.cy, n.cz, n.r);
+    a.pm[i] = make_float4(n.px, n.py, n.pz, n.m0);
+    a.nc[i] = make_float4(n.nx, n.ny, n.nz, n.cpn);
+    float4 x;
+    x.x = n.cpp;
+    x.y = __uint_as_float(n.first);
+    x.z = __uint_as_float(n.info);
+    x.w = __uint_as_float(n.parent);
+    a.aux[i] = x;
+}
+
+__device__ inline DNode load_node_all(const NodeArrays& a, int64_t i)
+{
+    const float4 g = a.geom[i], p = a.pm[i], c = a.nc[i], x = a.aux[i];
+    DNode n;
+    n.cx = g.x; n.cy = g.y; n.cz = g.z; n.r = g.w;
+    n.px = p.x; n.py = p.y; n.pz = p.z; n.m0 = p.w;
+    n.nx = c.x; n.ny = c.y; n.nz = c.z; n.cpn = c.w;
+    n.cpp = x.x;
+    n.first = __float_as_uint(x.y);
+    n.info = __float_as_uint(x.z);
+    n.parent = __float_as_uint(x.w);
+    return n;
+}
+
 __host__ __device__ inline uint32_t node_count(uint32_t info) { return info & kCountMask; }
 __host__ __device__ inline int node_depth(uint32_t info) { return int((info >> kDepthShift) & kDepthMask); }
 
@@ -80,6 +118,10 @@ __device__ __forceinline__ float kernel_weight(const KernelConsts& kc, float d2)
 
 // Counts kernel launches made by the library (mlods_kernel_launches).
 void note_launch(int n = 1);
+// Kernel launches so far (all threads); graphs add their kernel count per replay.
+int64_t launches_so_far();
+// Multiprocessor count of the current device (cached per device).
+int sm_count_for_current_device();
 
 // Error-reporting helpers (host).
 void set_last_error(const char* fmt, ...);

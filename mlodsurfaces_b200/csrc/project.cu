@@ -24,6 +24,11 @@
 // (S_p = sum c m0 (pbar - q), S_pn = sum c (cpn + (pbar - q).n),
 // S_pp = sum c (cpp + |pbar - q|^2 m0)), reduced across the warp, and the
 // algebraic sphere is solved in double (Fastapss.cu:354-395).
+//
+// Two kernels share the per-query walk: one for a single tree, and a batched
+// one that serves many resident trees (each with its own kernel and options)
+// from one persistent launch.
+#include <algorithm>
 #include <cmath>
 
 #include "primitives.cuh"
@@ -40,14 +45,13 @@ constexpr uint32_t kEntNoBlend = 1u << 31;
 constexpr uint32_t kEntLastOnly = 1u << 30;  // CPU rule multi-point leaf: only the last point is weighted
 constexpr float kPiRef = 3.14159265f;         // the reference's literal (Fastapss.cu:93)
 
+// Per-warp stack of sibling ranges.  e = {first, count|flags, f, A},
+// pg = {dP, g}; cnt repeats the count word so the pop scan reads 4 bytes.
 template <int CAP>
 struct WarpStack {
-    uint32_t first[CAP];
+    uint4 e[CAP];
+    float2 pg[CAP];
     uint32_t cnt[CAP];
-    float f[CAP];
-    float A[CAP];
-    float dP[CAP];
-    float g[CAP];
 };
 
 __device__ __forceinline__ int warp_incl_scan_i(int v)
@@ -68,26 +72,10 @@ __device__ __forceinline__ float warp_sum_f(float v)
     return v;
 }
 
-__device__ __forceinline__ DNode load_node(const DNode* __restrict__ nodes, uint32_t i)
-{
-    const float4* p = reinterpret_cast<const float4*>(nodes + i);
-    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
-    DNode n;
-    n.cx = a.x; n.cy = a.y; n.cz = a.z; n.r = a.w;
-    n.px = b.x; n.py = b.y; n.pz = b.z; n.m0 = b.w;
-    n.nx = c.x; n.ny = c.y; n.nz = c.z; n.cpn = c.w;
-    n.cpp = d.x;
-    n.first = __float_as_uint(d.y);
-    n.info = __float_as_uint(d.z);
-    n.parent = __float_as_uint(d.w);
-    return n;
-}
-
 // Sphere fit + projection of the query (frame origin) in double; mirrors
 // Fastapss.cu:354-395 (GPU rule) and CPUUtils.cpp:744-781 (CPU rule).
 // Returns false when the result is NaN (caller keeps the input, normal 0).
-template <int RULE>
-__device__ __forceinline__ bool fit_sphere(const float* s, double step_max, double x[3], float nrm[3])
+__device__ __forceinline__ bool fit_sphere(const float* s, double step_max, bool gpu_rule, double x[3], float nrm[3])
 {
     const double Sw = s[0];
     const double Sn[3] = {s[1], s[2], s[3]};
@@ -98,7 +86,7 @@ __device__ __forceinline__ bool fit_sphere(const float* s, double step_max, doub
     double u123[3];
     for (int a = 0; a < 3; ++a) u123[a] = (Sn[a] - 2.0 * u4 * Sp[a]) / Sw;
     const double u0 = -((Sp[0] * u123[0] + Sp[1] * u123[1] + Sp[2] * u123[2]) + u4 * Spp) / Sw;
-    const double thr = RULE == MLODS_BLEND_GPU ? 1e-6 : 1e-12;
+    const double thr = gpu_rule ? 1e-6 : 1e-12;
     double nv[3];
     if (fabs(u4) < thr) {
         const double m[3] = {-u123[0], -u123[1], -u123[2]};
@@ -112,7 +100,7 @@ __device__ __forceinline__ bool fit_sphere(const float* s, double step_max, doub
         const double rad = sqrt(r2 > 0.0 ? r2 : 0.0);
         double pc[3] = {-c[0], -c[1], -c[2]};
         const double pl = sqrt(pc[0] * pc[0] + pc[1] * pc[1] + pc[2] * pc[2]);
-        if (pl != 0.0 || RULE == MLODS_BLEND_CPU)
+        if (pl != 0.0 || !gpu_rule)
             for (int a = 0; a < 3; ++a) pc[a] /= pl;
         else
             pc[0] = pc[1] = pc[2] = 0.0;
@@ -120,7 +108,7 @@ __device__ __forceinline__ bool fit_sphere(const float* s, double step_max, doub
         for (int a = 0; a < 3; ++a) nv[a] = u123[a] + 2.0 * u4 * x[a];
     }
     const double nl = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-    if (nl != 0.0 || RULE == MLODS_BLEND_CPU)
+    if (nl != 0.0 || !gpu_rule)
         for (int a = 0; a < 3; ++a) nv[a] /= nl;
     else
         nv[0] = nv[1] = nv[2] = 0.0;
@@ -132,275 +120,352 @@ __device__ __forceinline__ bool fit_sphere(const float* s, double step_max, doub
     return true;
 }
 
-template <int KTYPE, int RULE, int CAP>
-__global__ void __launch_bounds__(kProjectThreads) mlod_project_kernel(ProjectArgs a)
+// Weight with the number of multi-Gaussian terms fixed at compile time
+// (NSIG > 0) or read at run time (NSIG == 0); KTYPE < 0 reads the kernel type
+// at run time too (uniform across a warp).
+template <int KTYPE, int NSIG>
+__device__ __forceinline__ float weight_n(const KernelConsts& kc, float d2)
+{
+    if (KTYPE < 0) {
+        if (kc.type == MLODS_GAUSSIAN) return kernel_weight<MLODS_GAUSSIAN>(kc, d2);
+        if (kc.type == MLODS_SINGULAR) return kernel_weight<MLODS_SINGULAR>(kc, d2);
+        return kernel_weight<MLODS_GAUSSIAN_MULTIPLE>(kc, d2);
+    }
+    if (KTYPE == MLODS_GAUSSIAN_MULTIPLE && NSIG > 0) {
+        float s = 0.f;
+#pragma unroll
+        for (int i = 0; i < NSIG; ++i) s = fmaf(exp2f(d2 * kc.ms_scale[i]), kc.ms_w[i], s);
+        return s;
+    }
+    return kernel_weight<KTYPE>(kc, d2);
+}
+
+struct WalkStats {
+    uint32_t visits = 0, rounds = 0, iterations = 0;
+    int max_top = 0;
+    bool overflow = false;
+};
+
+// Projects query qi of one tree: n_iter iterations (fewer with a convergence
+// mode), result written to out_p/out_n (world frame).  KTYPE / RULE < 0 take
+// the kernel type / blend rule from c at run time.
+template <int KTYPE, int NSIG, int RULE, int CAP>
+__device__ __forceinline__ void project_query(const CloudArgs& c, uint32_t qi, WarpStack<CAP>& st, WalkStats& ws)
+{
+    const bool gpu_rule = RULE < 0 ? c.rule == MLODS_BLEND_GPU : RULE == MLODS_BLEND_GPU;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t le_mask = lane == 31 ? kFull : ((2u << lane) - 1u);
+    const float4* __restrict__ ngeom = c.nodes.geom;
+    const float4* __restrict__ npm = c.nodes.pm;
+    const float4* __restrict__ nnc = c.nodes.nc;
+    const float4* __restrict__ naux = c.nodes.aux;
+    const float cutoff = c.cutoff;
+    const int min_depth = c.min_depth;
+
+    // the iterate, in the tree's local frame, in double
+    double qd[3] = {double(c.q_in[3 * int64_t(qi)]) - c.o0, double(c.q_in[3 * int64_t(qi) + 1]) - c.o1,
+                    double(c.q_in[3 * int64_t(qi) + 2]) - c.o2};
+    float nrm[3] = {0.f, 0.f, 0.f};
+    bool failed = false;
+    for (int it = 0; it < c.n_iter && !failed; ++it) {
+        const float qx = float(qd[0]), qy = float(qd[1]), qz = float(qd[2]);
+        float acc[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[k] = 0.f;
+        int top = 1;
+        if (lane == 0) {
+            st.e[0] = make_uint4(0u, 1u | kEntNoBlend, __float_as_uint(1.f), 0u);
+            st.pg[0] = make_float2(0.f, 0.f);
+            st.cnt[0] = 1u | kEntNoBlend;
+        }
+        __syncwarp();
+        while (top > 0) {
+            // ---- pop sibling ranges from the top until 32 lanes are filled
+            int cn = 0;
+            if (lane < top) cn = int(st.cnt[top - 1 - lane] & kEntCount);
+            const int incl = warp_incl_scan_i(cn);
+            const uint32_t fit = __ballot_sync(kFull, lane < top && incl <= 32);
+            const int npop = __popc(fit);
+            const bool partial = npop == 0;  // top range wider than a warp (multi-point leaf)
+            const int total = partial ? 32 : __shfl_sync(kFull, incl, npop - 1);
+            const uint32_t heads = partial ? 1u : __reduce_or_sync(kFull, lane < npop ? (1u << (incl - cn)) : 0u);
+            const bool active = lane < total;
+            // entry of this lane: the e-th popped range, which starts at the
+            // highest head bit at or below the lane
+            const uint32_t hb = heads & le_mask;
+            const int e = __popc(hb) - 1;
+            const int r_start = 31 - __clz(hb);
+            const int slot = top - 1 - e;
+            const uint4 E = st.e[slot];
+            const float2 PG = st.pg[slot];
+            const uint32_t r_first = E.x, r_cnt = E.y;
+            const float r_f = __uint_as_float(E.z), r_A = __uint_as_float(E.w);
+            const float r_dP = PG.x, r_g = PG.y;
+            const int r_len = partial ? 32 : int(r_cnt & kEntCount);
+            const int old_top = top;
+            if (!partial) top -= npop;
+            ws.visits += uint32_t(total);
+            ++ws.rounds;
+
+            // ---- evaluate one node per lane
+            const uint32_t node = r_first + uint32_t(lane - r_start);
+            float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f), p4 = g4;
+            float4 x4 = make_float4(0.f, 0.f, __uint_as_float(kLeafBit | 1u), 0.f);
+            if (active) {
+                g4 = __ldg(ngeom + node);
+                p4 = __ldg(npm + node);
+                x4 = __ldg(naux + node);
+            }
+            const float cr = cutoff * g4.w;
+            const float cx = g4.x - qx, cy = g4.y - qy, cz = g4.z - qz;
+            const float dist = sqrtf(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
+            float beta = 1.f, kcon = 0.f;
+            if (active && !(r_cnt & kEntNoBlend)) {
+                const float dC = fmaxf(dist - cr, 0.f);
+                const float t = __fdividef(r_dP, r_dP + dC);
+                beta = 0.5f - 0.5f * __cosf(kPiRef * t);
+                kcon = (1.f - beta) * r_g * (gpu_rule ? p4.w : 1.f);
+            }
+            // segmented sum over the range (blend ranges hold <= 8 lanes)
+            {
+                const int seg_end = r_start + r_len;
+#pragma unroll
+                for (int o = 1; o < 8; o <<= 1) {
+                    const float nv = __shfl_down_sync(kFull, kcon, o);
+                    if (lane + o < seg_end) kcon += nv;
+                }
+            }
+            const float K = __shfl_sync(kFull, kcon, r_start);
+            float f = r_f * beta;
+            const float A = r_A + K;
+            if (!gpu_rule && (r_cnt & kEntLastOnly) && (partial || node != r_first + uint32_t(r_len) - 1u))
+                f = 0.f;
+
+            const float px = p4.x - qx, py = p4.y - qy, pz = p4.z - qz;
+            const float d2 = fmaf(px, px, fmaf(py, py, pz * pz));
+            const float w = weight_n<KTYPE, NSIG>(c.kc, d2);
+            const uint32_t info = __float_as_uint(x4.z);
+            const uint32_t nfirst = __float_as_uint(x4.y);
+            const bool leaf = (info & kLeafBit) != 0;
+            const bool multi = (info & kMultiBit) != 0;
+            const uint32_t cnt = node_count(info);
+            bool terminal = false, push = false;
+            uint32_t p_cnt = 0;
+            float p_dP = 0.f, p_g = 0.f;
+            if (active) {
+                if (leaf) {
+                    if (!multi) {
+                        terminal = true;
+                    } else {
+                        push = true;
+                        p_cnt = cnt | kEntNoBlend | (gpu_rule ? 0u : kEntLastOnly);
+                    }
+                } else if (node_depth(info) < min_depth) {
+                    push = true;
+                    p_cnt = cnt | kEntNoBlend;
+                } else if (dist > cr) {
+                    terminal = true;
+                } else {
+                    push = true;
+                    p_cnt = cnt;
+                    p_dP = cr - dist;
+                    p_g = f * w / (gpu_rule ? p4.w : float(cnt));
+                }
+            }
+            if (terminal) {
+                const float4 n4 = __ldg(nnc + node);
+                const float coef = fmaf(f, w, A);
+                const float cm = coef * p4.w;
+                acc[0] += cm;
+                acc[1] = fmaf(coef, n4.x, acc[1]);
+                acc[2] = fmaf(coef, n4.y, acc[2]);
+                acc[3] = fmaf(coef, n4.z, acc[3]);
+                acc[4] = fmaf(cm, px, acc[4]);
+                acc[5] = fmaf(cm, py, acc[5]);
+                acc[6] = fmaf(cm, pz, acc[6]);
+                acc[7] = fmaf(coef, fmaf(px, n4.x, fmaf(py, n4.y, fmaf(pz, n4.z, n4.w))), acc[7]);
+                acc[8] = fmaf(coef, fmaf(d2, p4.w, x4.x), acc[8]);
+            }
+            // ---- push child ranges (every lane has read its entry: the
+            // shuffles above depend on those reads)
+            __syncwarp();
+            if (partial && lane == 0) {
+                uint4 rest = st.e[old_top - 1];
+                rest.x += 32u;
+                rest.y -= 32u;
+                st.e[old_top - 1] = rest;
+                st.cnt[old_top - 1] = rest.y;
+            }
+            const uint32_t pm = __ballot_sync(kFull, push);
+            const int npush = __popc(pm);
+            if (top + npush > CAP) {
+                ws.overflow = true;  // the query is reported as failed
+            } else {
+                if (push) {
+                    const int pos = top + __popc(pm & lt_mask);
+                    st.e[pos] = make_uint4(nfirst, p_cnt, __float_as_uint(f), __float_as_uint(A));
+                    st.pg[pos] = make_float2(p_dP, p_g);
+                    st.cnt[pos] = p_cnt;
+                }
+                top += npush;
+            }
+            if (top > ws.max_top) ws.max_top = top;
+            __syncwarp();
+        }
+        ++ws.iterations;
+        float s[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) s[k] = warp_sum_f(acc[k]);
+        double x[3];
+        if (ws.overflow || !fit_sphere(s, double(c.step_max), gpu_rule, x, nrm)) {
+            failed = true;
+            break;
+        }
+        // the projection of the float query just evaluated
+        qd[0] = double(qx) + x[0];
+        qd[1] = double(qy) + x[1];
+        qd[2] = double(qz) + x[2];
+        if (c.conv_mode == MLODS_CONVERGE_EXACT) {
+            // the next iteration would evaluate the same float query: every
+            // remaining iteration returns this result again
+            if (float(qd[0]) == qx && float(qd[1]) == qy && float(qd[2]) == qz) break;
+        } else if (c.conv_mode == MLODS_CONVERGE_TOL) {
+            if (x[0] * x[0] + x[1] * x[1] + x[2] * x[2] < double(c.conv_tol) * double(c.conv_tol)) break;
+        }
+    }
+    if (lane == 0) {
+        float* op = c.out_p + 3 * int64_t(qi);
+        float* on = c.out_n + 3 * int64_t(qi);
+        // on failure (Fastapss.cu:385-391) the point stays where the failing
+        // iteration started and the normal is zero
+        op[0] = float(qd[0] + c.o0);
+        op[1] = float(qd[1] + c.o1);
+        op[2] = float(qd[2] + c.o2);
+        on[0] = failed ? 0.f : nrm[0];
+        on[1] = failed ? 0.f : nrm[1];
+        on[2] = failed ? 0.f : nrm[2];
+    }
+}
+
+__device__ __forceinline__ void flush_stats(int64_t* stats, int64_t visits, int64_t rounds, int max_top,
+                                            int64_t overflows, int64_t iterations)
+{
+    if ((threadIdx.x & 31) != 0 || !stats) return;
+    atomicAdd(reinterpret_cast<unsigned long long*>(&stats[0]), (unsigned long long)visits);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&stats[4]), (unsigned long long)rounds);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&stats[5]), (unsigned long long)iterations);
+    atomicMax(reinterpret_cast<unsigned long long*>(&stats[1]), (unsigned long long)max_top);
+    if (overflows) atomicAdd(reinterpret_cast<unsigned long long*>(&stats[2]), (unsigned long long)overflows);
+}
+
+template <int KTYPE, int NSIG, int RULE, int CAP>
+__global__ void __launch_bounds__(kProjectThreads, kProjectMinBlocks) mlod_project_kernel(ProjectArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    WarpStack<CAP>& st = reinterpret_cast<WarpStack<CAP>*>(smem_raw)[warp];
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    const DNode* __restrict__ nodes = a.nodes;
-    const float cutoff = a.cutoff;
-    const int min_depth = a.min_depth;
-
-    int64_t visits = 0;
-    int64_t rounds = 0;
+    WarpStack<CAP>& st = reinterpret_cast<WarpStack<CAP>*>(smem_raw)[threadIdx.x >> 5];
+    int64_t visits = 0, rounds = 0, overflows = 0, iterations = 0;
     int max_top = 0;
-    int64_t overflows = 0;
-
     for (;;) {
         unsigned int qs = 0;
         if (lane == 0) qs = atomicAdd(a.counter, 1u);
         qs = __shfl_sync(kFull, qs, 0);
         if (int64_t(qs) >= a.nq) break;
         const uint32_t qi = a.order ? a.order[qs] : qs;
-        // iterate in the tree's local frame, in double
-        double qd[3] = {double(a.q_in[3 * int64_t(qi)]) - a.o0, double(a.q_in[3 * int64_t(qi) + 1]) - a.o1,
-                        double(a.q_in[3 * int64_t(qi) + 2]) - a.o2};
-        float nrm[3] = {0.f, 0.f, 0.f};
-        bool failed = false;
-        bool overflow = false;
-        for (int it = 0; it < a.n_iter && !failed; ++it) {
-            const float qx = float(qd[0]), qy = float(qd[1]), qz = float(qd[2]);
-            float acc[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) acc[k] = 0.f;
-            int top = 1;
-            if (lane == 0) {
-                st.first[0] = 0;
-                st.cnt[0] = 1u | kEntNoBlend;
-                st.f[0] = 1.f;
-                st.A[0] = 0.f;
-                st.dP[0] = 0.f;
-                st.g[0] = 0.f;
-            }
-            __syncwarp();
-            while (top > 0) {
-                // ---- pop sibling ranges from the top until 32 lanes are filled
-                uint32_t e_first = 0, e_cnt = 0;
-                float e_f = 0.f, e_A = 0.f, e_dP = 0.f, e_g = 0.f;
-                int c = 0;
-                if (lane < top) {
-                    const int slot = top - 1 - lane;
-                    e_first = st.first[slot];
-                    e_cnt = st.cnt[slot];
-                    e_f = st.f[slot];
-                    e_A = st.A[slot];
-                    e_dP = st.dP[slot];
-                    e_g = st.g[slot];
-                    c = int(e_cnt & kEntCount);
-                }
-                const int incl = warp_incl_scan_i(c);
-                const uint32_t fit = __ballot_sync(kFull, lane < top && incl <= 32);
-                int npop = __popc(fit);
-                const bool partial = npop == 0;  // top range wider than a warp (multi-point leaf)
-                int total;
-                uint32_t headbit;
-                if (partial) {
-                    total = 32;
-                    headbit = lane == 0 ? 1u : 0u;
-                } else {
-                    total = __shfl_sync(kFull, incl, npop - 1);
-                    headbit = lane < npop ? (1u << (incl - c)) : 0u;
-                }
-                const uint32_t heads = __reduce_or_sync(kFull, headbit);
-                const bool active = lane < total;
-                const int e = active ? __popc(heads & (lane == 31 ? kFull : ((2u << lane) - 1u))) - 1 : 0;
-                const uint32_t r_first = __shfl_sync(kFull, e_first, e);
-                const uint32_t r_cnt = __shfl_sync(kFull, e_cnt, e);
-                const float r_f = __shfl_sync(kFull, e_f, e);
-                const float r_A = __shfl_sync(kFull, e_A, e);
-                const float r_dP = __shfl_sync(kFull, e_dP, e);
-                const float r_g = __shfl_sync(kFull, e_g, e);
-                const int r_start = partial ? 0 : __shfl_sync(kFull, incl - c, e);
-                const int r_len = partial ? 32 : int(r_cnt & kEntCount);
-                if (partial) {
-                    if (lane == 0) {
-                        st.first[top - 1] = e_first + 32u;
-                        st.cnt[top - 1] = e_cnt - 32u;
-                    }
-                } else {
-                    top -= npop;
-                }
-                visits += total;
-                ++rounds;
-
-                // ---- evaluate one node per lane
-                const uint32_t node = r_first + uint32_t(lane - r_start);
-                DNode nd;
-                if (active) {
-                    nd = load_node(nodes, node);
-                } else {
-                    nd.cx = nd.cy = nd.cz = 0.f;
-                    nd.r = 0.f;
-                    nd.px = nd.py = nd.pz = 0.f;
-                    nd.m0 = 0.f;
-                    nd.nx = nd.ny = nd.nz = nd.cpn = nd.cpp = 0.f;
-                    nd.first = 0;
-                    nd.info = kLeafBit | 1u;
-                    nd.parent = 0;
-                }
-                const float cx = nd.cx - qx, cy = nd.cy - qy, cz = nd.cz - qz;
-                const float dist = sqrtf(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
-                float beta = 1.f, kcon = 0.f;
-                if (active && !(r_cnt & kEntNoBlend)) {
-                    const float dC = fmaxf(dist - cutoff * nd.r, 0.f);
-                    const float t = __fdividef(r_dP, r_dP + dC);
-                    beta = 0.5f - 0.5f * __cosf(kPiRef * t);
-                    kcon = (1.f - beta) * r_g * (RULE == MLODS_BLEND_GPU ? nd.m0 : 1.f);
-                }
-                // segmented sum over the range (blend ranges hold <= 8 lanes)
-                {
-                    const int seg_end = r_start + r_len;
-#pragma unroll
-                    for (int o = 1; o < 8; o <<= 1) {
-                        const float nv = __shfl_down_sync(kFull, kcon, o);
-                        if (lane + o < seg_end) kcon += nv;
-                    }
-                }
-                const float K = __shfl_sync(kFull, kcon, r_start);
-                float f = r_f * beta;
-                const float A = r_A + K;
-                if (RULE == MLODS_BLEND_CPU && (r_cnt & kEntLastOnly) && node != r_first + uint32_t(r_len) - 1u &&
-                    !partial)
-                    f = 0.f;
-                if (RULE == MLODS_BLEND_CPU && (r_cnt & kEntLastOnly) && partial) f = 0.f;
-
-                const float px = nd.px - qx, py = nd.py - qy, pz = nd.pz - qz;
-                const float d2 = fmaf(px, px, fmaf(py, py, pz * pz));
-                const float w = kernel_weight<KTYPE>(a.kc, d2);
-                const uint32_t info = nd.info;
-                const bool leaf = (info & kLeafBit) != 0;
-                const bool multi = (info & kMultiBit) != 0;
-                const int cnt = int(node_count(info));
-                bool terminal = false, push = false;
-                uint32_t p_first = 0, p_cnt = 0;
-                float p_dP = 0.f, p_g = 0.f;
-                if (active) {
-                    if (leaf) {
-                        if (!multi) {
-                            terminal = true;
-                        } else {
-                            push = true;
-                            p_first = nd.first;
-                            p_cnt = uint32_t(cnt) | kEntNoBlend | (RULE == MLODS_BLEND_CPU ? kEntLastOnly : 0u);
-                        }
-                    } else if (node_depth(info) < min_depth) {
-                        push = true;
-                        p_first = nd.first;
-                        p_cnt = uint32_t(cnt) | kEntNoBlend;
-                    } else if (dist > cutoff * nd.r) {
-                        terminal = true;
-                    } else {
-                        push = true;
-                        p_first = nd.first;
-                        p_cnt = uint32_t(cnt);
-                        p_dP = cutoff * nd.r - dist;
-                        p_g = f * w / (RULE == MLODS_BLEND_GPU ? nd.m0 : float(cnt));
-                    }
-                }
-                if (terminal) {
-                    const float coef = fmaf(f, w, A);
-                    const float cm = coef * nd.m0;
-                    acc[0] += cm;
-                    acc[1] = fmaf(coef, nd.nx, acc[1]);
-                    acc[2] = fmaf(coef, nd.ny, acc[2]);
-                    acc[3] = fmaf(coef, nd.nz, acc[3]);
-                    acc[4] = fmaf(cm, px, acc[4]);
-                    acc[5] = fmaf(cm, py, acc[5]);
-                    acc[6] = fmaf(cm, pz, acc[6]);
-                    acc[7] = fmaf(coef, fmaf(px, nd.nx, fmaf(py, nd.ny, fmaf(pz, nd.nz, nd.cpn))), acc[7]);
-                    acc[8] = fmaf(coef, fmaf(d2, nd.m0, nd.cpp), acc[8]);
-                }
-                // ---- push child ranges
-                const uint32_t pm = __ballot_sync(kFull, push);
-                const int npush = __popc(pm);
-                if (top + npush > CAP) {
-                    overflow = true;  // the query is reported as failed
-                } else {
-                    if (push) {
-                        const int pos = top + __popc(pm & lt_mask);
-                        st.first[pos] = p_first;
-                        st.cnt[pos] = p_cnt;
-                        st.f[pos] = f;
-                        st.A[pos] = A;
-                        st.dP[pos] = p_dP;
-                        st.g[pos] = p_g;
-                    }
-                    top += npush;
-                }
-                if (top > max_top) max_top = top;
-                __syncwarp();
-            }
-            float s[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) s[k] = warp_sum_f(acc[k]);
-            double x[3];
-            if (overflow || !fit_sphere<RULE>(s, double(a.step_max), x, nrm)) {
-                failed = true;
-                break;
-            }
-            qd[0] += x[0];
-            qd[1] += x[1];
-            qd[2] += x[2];
-        }
-        if (lane == 0) {
-            float* op = a.out_p + 3 * int64_t(qi);
-            float* on = a.out_n + 3 * int64_t(qi);
-            if (failed) {
-                // Fastapss.cu:385-391: keep the point, zero normal.  The in-place
-                // buffer already holds the start of the failing iteration.
-                op[0] = float(qd[0] + a.o0);
-                op[1] = float(qd[1] + a.o1);
-                op[2] = float(qd[2] + a.o2);
-                on[0] = on[1] = on[2] = 0.f;
-            } else {
-                op[0] = float(qd[0] + a.o0);
-                op[1] = float(qd[1] + a.o1);
-                op[2] = float(qd[2] + a.o2);
-                on[0] = nrm[0];
-                on[1] = nrm[1];
-                on[2] = nrm[2];
-            }
-        }
-        if (overflow) ++overflows;
+        WalkStats ws;
+        project_query<KTYPE, NSIG, RULE, CAP>(a.cloud, qi, st, ws);
+        visits += ws.visits;
+        rounds += ws.rounds;
+        iterations += ws.iterations;
+        max_top = max(max_top, ws.max_top);
+        overflows += ws.overflow ? 1 : 0;
     }
-    if (lane == 0 && a.stats) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[0]), (unsigned long long)visits);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[4]), (unsigned long long)rounds);
-        atomicMax(reinterpret_cast<unsigned long long*>(&a.stats[1]), (unsigned long long)max_top);
-        if (overflows) atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[2]), (unsigned long long)overflows);
-    }
+    flush_stats(a.stats, visits, rounds, max_top, overflows, iterations);
 }
 
-template <int KTYPE, int RULE>
+// Many trees, one launch.  Query slot s (in processing order) belongs to the
+// cloud whose [q_offsets[c], q_offsets[c+1]) holds it; order[s] is the global
+// index of the query in the concatenated buffers.  The weight kernel and the
+// blend rule are read per query (uniform across the warp), so one
+// instantiation serves every cloud.
+template <int CAP>
+__global__ void __launch_bounds__(kProjectThreads, kProjectMinBlocks) mlod_batch_kernel(BatchArgs b)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    WarpStack<CAP>& st = reinterpret_cast<WarpStack<CAP>*>(smem_raw)[threadIdx.x >> 5];
+    int64_t visits = 0, rounds = 0, overflows = 0, iterations = 0;
+    int max_top = 0;
+    for (;;) {
+        unsigned int qs = 0;
+        if (lane == 0) qs = atomicAdd(b.counter, 1u);
+        qs = __shfl_sync(kFull, qs, 0);
+        if (int64_t(qs) >= b.total) break;
+        // cloud of this slot (binary search over the offsets)
+        int lo = 0, hi = b.n_clouds;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (int64_t(qs) >= __ldg(b.q_offsets + mid)) lo = mid; else hi = mid;
+        }
+        const CloudArgs& c = b.clouds[lo];
+        const uint32_t g = b.order ? b.order[qs] : qs;
+        const uint32_t qi = uint32_t(int64_t(g) - b.q_offsets[lo]);
+        WalkStats ws;
+        project_query<-1, 0, -1, CAP>(c, qi, st, ws);
+        visits += ws.visits;
+        rounds += ws.rounds;
+        iterations += ws.iterations;
+        max_top = max(max_top, ws.max_top);
+        overflows += ws.overflow ? 1 : 0;
+    }
+    flush_stats(b.stats, visits, rounds, max_top, overflows, iterations);
+}
+
+template <typename Kern>
+int64_t persistent_grid(Kern kern, size_t smem, int64_t work_warps, int sm_count, cudaError_t* err)
+{
+    int per_sm = 0;
+    *err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kProjectThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int64_t want = (work_warps + kProjectThreads / 32 - 1) / (kProjectThreads / 32);
+    int64_t grid = int64_t(per_sm) * sm_count;
+    if (grid > want) grid = want;
+    return grid < 1 ? 1 : grid;
+}
+
+template <int KTYPE, int NSIG, int RULE>
 cudaError_t launch_typed(const ProjectArgs& a, int sm_count, cudaStream_t s)
 {
     constexpr int CAP = kProjectStackCap;
-    auto kern = mlod_project_kernel<KTYPE, RULE, CAP>;
+    auto kern = mlod_project_kernel<KTYPE, NSIG, RULE, CAP>;
     const size_t smem = size_t(kProjectThreads / 32) * sizeof(WarpStack<CAP>);
-    static bool attr_done[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 64 && !attr_done[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess) return e;
-        attr_done[dev] = true;
-    }
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kProjectThreads, smem);
+    cudaError_t e = cudaSuccess;
+    const int64_t grid = persistent_grid(kern, smem, a.nq, sm_count, &e);
     if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    const int64_t want = (a.nq + kProjectThreads / 32 - 1) / (kProjectThreads / 32);
-    int64_t grid = int64_t(per_sm) * sm_count;
-    if (grid > want) grid = want;
-    if (grid < 1) grid = 1;
     kern<<<unsigned(grid), kProjectThreads, smem, s>>>(a);
     note_launch();
     return cudaGetLastError();
 }
 
+template <int RULE>
+cudaError_t launch_rule(const ProjectArgs& a, int ktype, int sm_count, cudaStream_t s)
+{
+    if (ktype == MLODS_GAUSSIAN) return launch_typed<MLODS_GAUSSIAN, 0, RULE>(a, sm_count, s);
+    if (ktype == MLODS_SINGULAR) return launch_typed<MLODS_SINGULAR, 0, RULE>(a, sm_count, s);
+    switch (a.cloud.kc.nsig) {
+    case 2: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 2, RULE>(a, sm_count, s);
+    case 3: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 3, RULE>(a, sm_count, s);
+    case 4: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 4, RULE>(a, sm_count, s);
+    case 5: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 5, RULE>(a, sm_count, s);
+    case 6: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 6, RULE>(a, sm_count, s);
+    case 8: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 8, RULE>(a, sm_count, s);
+    default: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 0, RULE>(a, sm_count, s);
+    }
+}
+
+// Morton key of a query on a 1024^3 grid over its tree's root box, prefixed
+// by the cloud index in the batched case.
 __global__ void query_codes_kernel(const float* __restrict__ q, int64_t n, double o0, double o1, double o2,
                                    float inv_ext, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx)
 {
@@ -420,6 +485,32 @@ __global__ void query_codes_kernel(const float* __restrict__ q, int64_t n, doubl
     idx[i] = uint32_t(i);
 }
 
+__global__ void batch_codes_kernel(const float* __restrict__ q, int64_t n, const int64_t* __restrict__ q_offsets,
+                                   int n_clouds, const BatchFrame* __restrict__ frames, uint64_t* __restrict__ keys,
+                                   uint32_t* __restrict__ idx)
+{
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = 0, hi = n_clouds;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (i >= q_offsets[mid]) lo = mid; else hi = mid;
+    }
+    const BatchFrame fr = frames[lo];
+    uint32_t c[3];
+    const double o[3] = {fr.o0, fr.o1, fr.o2};
+    for (int k = 0; k < 3; ++k) {
+        float u = float(double(q[3 * i + k]) - o[k]) * fr.inv_ext + 0.5f;
+        u = fminf(fmaxf(u, 0.f), 0.99999994f);
+        c[k] = uint32_t(u * 1024.f);
+    }
+    uint64_t code = uint64_t(lo);
+    for (int b = 9; b >= 0; --b)
+        code = (code << 3) | ((c[0] >> b) & 1u) | (((c[1] >> b) & 1u) << 1) | (((c[2] >> b) & 1u) << 2);
+    keys[i] = code;
+    idx[i] = uint32_t(i);
+}
+
 __global__ void reorganize_kernel(float* __restrict__ q, const uint32_t* __restrict__ inv, int64_t n_inv,
                                   uint32_t end_valid)
 {
@@ -433,6 +524,8 @@ __global__ void reorganize_kernel(float* __restrict__ q, const uint32_t* __restr
     }
 }
 
+inline size_t up256(size_t v) { return (v + 255) / 256 * 256; }
+
 }  // namespace
 
 cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_invalid, uint32_t end_valid,
@@ -445,37 +538,37 @@ cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_i
 
 cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int sm_count, cudaStream_t s)
 {
-    if (rule == MLODS_BLEND_GPU) {
-        switch (ktype) {
-        case MLODS_GAUSSIAN: return launch_typed<MLODS_GAUSSIAN, MLODS_BLEND_GPU>(a, sm_count, s);
-        case MLODS_SINGULAR: return launch_typed<MLODS_SINGULAR, MLODS_BLEND_GPU>(a, sm_count, s);
-        default: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, MLODS_BLEND_GPU>(a, sm_count, s);
-        }
-    }
-    switch (ktype) {
-    case MLODS_GAUSSIAN: return launch_typed<MLODS_GAUSSIAN, MLODS_BLEND_CPU>(a, sm_count, s);
-    case MLODS_SINGULAR: return launch_typed<MLODS_SINGULAR, MLODS_BLEND_CPU>(a, sm_count, s);
-    default: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, MLODS_BLEND_CPU>(a, sm_count, s);
-    }
+    if (rule == MLODS_BLEND_GPU) return launch_rule<MLODS_BLEND_GPU>(a, ktype, sm_count, s);
+    return launch_rule<MLODS_BLEND_CPU>(a, ktype, sm_count, s);
+}
+
+cudaError_t launch_mlod_batch(const BatchArgs& b, int sm_count, int grid_scale_pct, cudaStream_t s)
+{
+    constexpr int CAP = kProjectStackCap;
+    auto kern = mlod_batch_kernel<CAP>;
+    const size_t smem = size_t(kProjectThreads / 32) * sizeof(WarpStack<CAP>);
+    cudaError_t e = cudaSuccess;
+    int64_t grid = persistent_grid(kern, smem, b.total, sm_count, &e);
+    if (e != cudaSuccess) return e;
+    if (grid_scale_pct > 0 && grid_scale_pct < 100) grid = std::max<int64_t>(1, grid * grid_scale_pct / 100);
+    kern<<<unsigned(grid), kProjectThreads, smem, s>>>(b);
+    note_launch();
+    return cudaGetLastError();
 }
 
 size_t query_order_temp_bytes(int64_t n)
 {
-    const size_t al = 256;
-    auto up = [&](size_t v) { return (v + al - 1) / al * al; };
-    return 2 * up(size_t(n) * 8) + up(size_t(n) * 4) + radix_temp_bytes(n);
+    return 2 * up256(size_t(n) * 8) + up256(size_t(n) * 4) + radix_temp_bytes(n);
 }
 
 cudaError_t compute_query_order(const float* d_q, int64_t n, const double origin[3], float extent, uint32_t* d_order,
                                 void* temp, cudaStream_t s)
 {
-    const size_t al = 256;
-    auto up = [&](size_t v) { return (v + al - 1) / al * al; };
     char* t = static_cast<char*>(temp);
     uint64_t* k0 = reinterpret_cast<uint64_t*>(t);
-    uint64_t* k1 = reinterpret_cast<uint64_t*>(t + up(size_t(n) * 8));
-    uint32_t* v1 = reinterpret_cast<uint32_t*>(t + 2 * up(size_t(n) * 8));
-    void* rt = t + 2 * up(size_t(n) * 8) + up(size_t(n) * 4);
+    uint64_t* k1 = reinterpret_cast<uint64_t*>(t + up256(size_t(n) * 8));
+    uint32_t* v1 = reinterpret_cast<uint32_t*>(t + 2 * up256(size_t(n) * 8));
+    void* rt = t + 2 * up256(size_t(n) * 8) + up256(size_t(n) * 4);
     const float inv_ext = extent > 0.f ? 1.f / extent : 1.f;
     query_codes_kernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(d_q, n, origin[0], origin[1], origin[2], inv_ext, k0,
                                                                  d_order);
@@ -484,6 +577,27 @@ cudaError_t compute_query_order(const float* d_q, int64_t n, const double origin
     if (e != cudaSuccess) return e;
     bool alt = false;
     e = radix_sort_pairs_u64(k0, d_order, k1, v1, n, 30, &alt, rt, s);
+    if (e != cudaSuccess) return e;
+    if (alt) e = cudaMemcpyAsync(d_order, v1, size_t(n) * 4, cudaMemcpyDeviceToDevice, s);
+    return e;
+}
+
+cudaError_t compute_batch_order(const float* d_q, int64_t n, const int64_t* d_q_offsets, int n_clouds,
+                                const BatchFrame* d_frames, uint32_t* d_order, void* temp, cudaStream_t s)
+{
+    char* t = static_cast<char*>(temp);
+    uint64_t* k0 = reinterpret_cast<uint64_t*>(t);
+    uint64_t* k1 = reinterpret_cast<uint64_t*>(t + up256(size_t(n) * 8));
+    uint32_t* v1 = reinterpret_cast<uint32_t*>(t + 2 * up256(size_t(n) * 8));
+    void* rt = t + 2 * up256(size_t(n) * 8) + up256(size_t(n) * 4);
+    batch_codes_kernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(d_q, n, d_q_offsets, n_clouds, d_frames, k0, d_order);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int cbits = 1;
+    while ((1 << cbits) < n_clouds) ++cbits;
+    bool alt = false;
+    e = radix_sort_pairs_u64(k0, d_order, k1, v1, n, 30 + cbits, &alt, rt, s);
     if (e != cudaSuccess) return e;
     if (alt) e = cudaMemcpyAsync(d_order, v1, size_t(n) * 4, cudaMemcpyDeviceToDevice, s);
     return e;

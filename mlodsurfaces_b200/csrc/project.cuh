@@ -1,4 +1,4 @@
-// project.cuh -- launch interface of the MLoD projection kernel.
+// project.cuh -- launch interface of the MLoD projection kernels.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -9,27 +9,63 @@
 namespace mlods
 {
 
-constexpr int kProjectThreads = 128;   // 4 warps per block, one query per warp at a time
-constexpr int kProjectStackCap = 192;  // sibling ranges per warp (24 bytes each)
+#ifndef MLODS_PROJECT_MIN_BLOCKS
+#define MLODS_PROJECT_MIN_BLOCKS 8
+#endif
+#ifndef MLODS_PROJECT_STACK_CAP
+#define MLODS_PROJECT_STACK_CAP 160
+#endif
+constexpr int kProjectThreads = 128;                          // 4 warps per block, one query per warp at a time
+constexpr int kProjectMinBlocks = MLODS_PROJECT_MIN_BLOCKS;  // 8 -> 32 warps per SM, <= 64 registers
+constexpr int kProjectStackCap = MLODS_PROJECT_STACK_CAP;    // sibling ranges per warp (28 bytes each)
 
-struct ProjectArgs {
-    const DNode* nodes;
-    const float* q_in;       // world xyz
-    float* out_p;            // world xyz (may alias q_in)
-    float* out_n;
-    const uint32_t* order;   // processing order (Morton), or nullptr
-    int64_t nq;
-    int n_iter;
+// One tree and its projection settings, plus the query buffers it serves.
+struct CloudArgs {
+    NodeArrays nodes;
+    double o0, o1, o2;      // local frame origin
+    KernelConsts kc;
     float cutoff;
     int min_depth;
     float step_max;
-    double o0, o1, o2;       // local frame origin
-    KernelConsts kc;
-    unsigned int* counter;   // work counter, zero before launch
-    int64_t* stats;          // [0] node visits, [1] max stack, [2] overflows, [3] work counter, [4] rounds
+    int rule;               // MLODS_BLEND_*
+    int n_iter;
+    int conv_mode;          // MLODS_CONVERGE_*
+    float conv_tol;
+    const float* q_in;      // world xyz
+    float* out_p;           // world xyz (may alias q_in)
+    float* out_n;
+};
+
+struct ProjectArgs {
+    CloudArgs cloud;
+    const uint32_t* order;  // processing order (Morton), or nullptr
+    int64_t nq;
+    unsigned int* counter;  // work counter, zero before launch
+    int64_t* stats;         // [0] visits, [1] max stack, [2] overflows, [3] counter, [4] rounds, [5] iterations
+};
+
+// Many trees in one launch: clouds[c] serves the global query range
+// [q_offsets[c], q_offsets[c+1]) of the concatenated buffers (each cloud's
+// q_in/out_p/out_n point at the start of its own range).
+struct BatchArgs {
+    const CloudArgs* clouds;
+    const int64_t* q_offsets;  // n_clouds + 1 entries
+    int n_clouds;
+    int64_t total;
+    const uint32_t* order;     // processing order over all queries (grouped by cloud), or nullptr
+    unsigned int* counter;
+    int64_t* stats;
+};
+
+// Per-cloud frame used to key queries in Morton order.
+struct BatchFrame {
+    double o0, o1, o2;
+    float inv_ext;
+    float pad;
 };
 
 cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int sm_count, cudaStream_t s);
+cudaError_t launch_mlod_batch(const BatchArgs& b, int sm_count, int grid_scale_pct, cudaStream_t s);
 
 // Swaps query points invalid[i] and end_valid-1-i (GPUUtils.cu:413-424).
 cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_invalid, uint32_t end_valid,
@@ -41,5 +77,8 @@ cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_i
 size_t query_order_temp_bytes(int64_t n);
 cudaError_t compute_query_order(const float* d_q, int64_t n, const double origin[3], float extent, uint32_t* d_order,
                                 void* temp, cudaStream_t s);
+// Same for a batch: grouped by cloud, Morton order inside each cloud.
+cudaError_t compute_batch_order(const float* d_q, int64_t n, const int64_t* d_q_offsets, int n_clouds,
+                                const BatchFrame* d_frames, uint32_t* d_order, void* temp, cudaStream_t s);
 
 }  // namespace mlods

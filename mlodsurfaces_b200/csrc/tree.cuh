@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "mlods_internal.cuh"
 
 struct mlods_tree_s {
@@ -20,7 +22,7 @@ struct mlods_tree_s {
     float root_radius = 0.f;  // BBOX::radius of the root box, float as the reference
 
     // device data
-    mlods::DNode* d_nodes = nullptr;       // n_nodes + n_extra records
+    mlods::NodeArrays nodes{};             // n_nodes + n_extra records (one allocation at nodes.geom)
     int32_t* d_node_head = nullptr;        // sorted position of each node's first point
     uint64_t* d_codes = nullptr;           // Morton codes in sorted order
     uint32_t* d_perm = nullptr;            // sorted position -> original point index
@@ -62,11 +64,25 @@ struct mlods_queries_s {
     int64_t cap = 0;  // allocated queries
 };
 
+// Dual-contouring cell grid: (depth, x, y, z) per cell in sorted_octree order.
+struct mlods_dcgrid_s {
+    std::vector<int32_t> cells;
+    int max_depth = 0;
+};
+
 namespace mlods
 {
 // Builds the tree from device arrays (xyz float triples).
 int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t n, int max_depth, cudaStream_t s);
 void free_tree_device(mlods_tree_s* T);
+// Projects n device queries through the tree with its current kernel and
+// options (the mode selects MLoD, global, kNN or ball APSS).  Asynchronous.
+int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
+                    float step_max, cudaStream_t s, int rule_override = -1);
+struct CloudArgs;
+// Fills the per-tree part of a projection launch.
+void fill_cloud_args(const mlods_tree_s* T, CloudArgs& c, const float* d_q, float* d_out_p, float* d_out_n,
+                     int iters, float step_max, int rule);
 int export_tree(mlods_tree_s* T, int32_t* depth, int32_t* parent, int32_t* first_child, int32_t* n_children,
                 int32_t* next_brother, int32_t* leaf_off, int32_t* leaf_cnt, int32_t* perm, float* bmin, float* bmax,
                 double* mom, float* area);

@@ -386,7 +386,7 @@ __global__ void write_nodes_kernel(int64_t n_nodes, int D, const uint8_t* __rest
                                    const int32_t* __restrict__ leaf_cnt, const uint32_t* __restrict__ extra_off,
                                    const uint64_t* __restrict__ codes, const uint32_t* __restrict__ perm,
                                    const float* __restrict__ bounds, int64_t stride, const double* __restrict__ mom,
-                                   double o0, double o1, double o2, DNode* __restrict__ nodes)
+                                   double o0, double o1, double o2, NodeArrays nodes)
 {
     int64_t id = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (id >= n_nodes) return;
@@ -428,7 +428,7 @@ __global__ void write_nodes_kernel(int64_t n_nodes, int D, const uint8_t* __rest
     }
     nd.info = info;
     nd.parent = parent[id] < 0 ? 0xFFFFFFFFu : uint32_t(parent[id]);
-    nodes[id] = nd;
+    store_node(nodes, id, nd);
 }
 
 __global__ void write_point_records_kernel(int64_t n_nodes, const int32_t* __restrict__ head,
@@ -436,7 +436,7 @@ __global__ void write_point_records_kernel(int64_t n_nodes, const int32_t* __res
                                            const uint8_t* __restrict__ level, const uint32_t* __restrict__ perm,
                                            const float* __restrict__ pts, const float* __restrict__ nrm,
                                            const float* __restrict__ area, double o0, double o1, double o2,
-                                           DNode* __restrict__ nodes)
+                                           NodeArrays nodes)
 {
     int64_t id = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (id >= n_nodes) return;
@@ -460,7 +460,7 @@ __global__ void write_point_records_kernel(int64_t n_nodes, const int32_t* __res
         pr.first = i;
         pr.info = kLeafBit | 1u | (uint32_t(level[id] + 1 < 31 ? level[id] + 1 : 31) << kDepthShift);
         pr.parent = uint32_t(id);
-        nodes[n_nodes + extra_off[id] + k] = pr;
+        store_node(nodes, n_nodes + extra_off[id] + k, pr);
     }
 }
 
@@ -497,7 +497,7 @@ struct Bump {
 
 void free_tree_device(mlods_tree_s* T)
 {
-    cudaFree(T->d_nodes);
+    cudaFree(T->nodes.geom);
     cudaFree(T->d_node_head);
     cudaFree(T->d_codes);
     cudaFree(T->d_perm);
@@ -506,7 +506,7 @@ void free_tree_device(mlods_tree_s* T)
     cudaFree(T->d_snrm);
     cudaFree(T->d_wspts);
     cudaFree(T->d_bounds);
-    T->d_nodes = nullptr;
+    T->nodes = NodeArrays{};
     T->d_node_head = nullptr;
     T->d_codes = nullptr;
     T->d_perm = nullptr;
@@ -755,17 +755,25 @@ int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t 
     T->n_extra = h_extra;
     T->n_ties = int64_t(h_ties);
 
-    NODE_CHECK(cudaMalloc(&T->d_nodes, size_t(nn + h_extra) * sizeof(DNode)), "alloc nodes");
+    {
+        const size_t rec = size_t(nn + h_extra);
+        float4* base = nullptr;
+        NODE_CHECK(cudaMalloc(&base, rec * 4 * sizeof(float4)), "alloc nodes");
+        T->nodes.geom = base;
+        T->nodes.pm = base + rec;
+        T->nodes.nc = base + 2 * rec;
+        T->nodes.aux = base + 3 * rec;
+    }
     write_nodes_kernel<<<grid_for(nn, kThreads), kThreads, 0, s>>>(nn, D, d_level, d_head, d_parent, d_first, d_nchild,
                                                                    d_lcnt, d_xoff, codes, perm, T->d_bounds,
                                                                    bound_stride, d_mom, T->origin[0], T->origin[1],
-                                                                   T->origin[2], T->d_nodes);
+                                                                   T->origin[2], T->nodes);
     note_launch();
     NODE_CHECK(cudaGetLastError(), "write nodes");
     if (h_extra > 0) {
         write_point_records_kernel<<<grid_for(nn, kThreads), kThreads, 0, s>>>(
             nn, d_head, d_lcnt, d_xoff, d_level, perm, d_pts, d_nrm, T->d_area, T->origin[0], T->origin[1],
-            T->origin[2], T->d_nodes);
+            T->origin[2], T->nodes);
         note_launch();
         NODE_CHECK(cudaGetLastError(), "write point records");
     }
@@ -789,14 +797,14 @@ int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t 
     cudaFree(bump.base);
 #undef NODE_CHECK
 #undef BUILD_CHECK
-    T->device_bytes = int64_t((nn + h_extra) * sizeof(DNode)) + nn * 4 + n * (8 + 4 + 4 + 48) +
+    T->device_bytes = int64_t((nn + h_extra) * 4 * sizeof(float4)) + nn * 4 + n * (8 + 4 + 4 + 48) +
                       3 * bound_stride * 4;
     return MLODS_OK;
 }
 
 namespace
 {
-__global__ void export_kernel(int64_t nn, int D, const DNode* __restrict__ nodes, const int32_t* __restrict__ head,
+__global__ void export_kernel(int64_t nn, int D, NodeArrays nodes, const int32_t* __restrict__ head,
                               const uint64_t* __restrict__ codes, const float* __restrict__ bounds, int64_t stride,
                               double o0, double o1, double o2, int32_t* depth, int32_t* parent, int32_t* first_child,
                               int32_t* n_children, int32_t* next_brother, int32_t* leaf_cnt, float* bmin, float* bmax,
@@ -804,7 +812,7 @@ __global__ void export_kernel(int64_t nn, int D, const DNode* __restrict__ nodes
 {
     int64_t id = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (id >= nn) return;
-    const DNode nd = nodes[id];
+    const DNode nd = load_node_all(nodes, id);
     const int d = node_depth(nd.info);
     const bool leaf = (nd.info & kLeafBit) != 0;
     depth[id] = d;
@@ -813,7 +821,8 @@ __global__ void export_kernel(int64_t nn, int D, const DNode* __restrict__ nodes
     n_children[id] = leaf ? 0 : int32_t(node_count(nd.info));
     leaf_cnt[id] = leaf ? int32_t(node_count(nd.info)) : 0;
     int32_t nb = -1;
-    if (id + 1 < nn && nd.parent != 0xFFFFFFFFu && nodes[id + 1].parent == nd.parent) nb = int32_t(id + 1);
+    if (id + 1 < nn && nd.parent != 0xFFFFFFFFu && __float_as_uint(nodes.aux[id + 1].w) == nd.parent)
+        nb = int32_t(id + 1);
     next_brother[id] = nb;
     float bb[3], BB[3];
     node_box(bounds, stride, codes[head[id]], D, d, bb, BB);
@@ -854,7 +863,7 @@ int export_tree(mlods_tree_s* T, int32_t* depth, int32_t* parent, int32_t* first
     float* d_bmin = reinterpret_cast<float*>(d_lc + nn);
     float* d_bmax = d_bmin + 3 * nn;
     double* d_mom = reinterpret_cast<double*>(d_bmax + 3 * nn);
-    export_kernel<<<grid_for(nn, kThreads), kThreads>>>(nn, T->max_depth, T->d_nodes, T->d_node_head, T->d_codes,
+    export_kernel<<<grid_for(nn, kThreads), kThreads>>>(nn, T->max_depth, T->nodes, T->d_node_head, T->d_codes,
                                                         T->d_bounds, T->bounds_stride, T->origin[0], T->origin[1],
                                                         T->origin[2], d_depth, d_parent, d_first, d_nc, d_nb, d_lc,
                                                         d_bmin, d_bmax, d_mom);
@@ -874,23 +883,26 @@ int export_tree(mlods_tree_s* T, int32_t* depth, int32_t* parent, int32_t* first
     if (e != cudaSuccess) return cuda_fail(e, "export", __FILE__, __LINE__);
     // leaf point lists: single-point leaves hold the point index in `first`,
     // multi-point leaves point at their point records.
-    std::vector<DNode> hn(size_t(nn + T->n_extra));
-    MLODS_CUDA(cudaMemcpy(hn.data(), T->d_nodes, hn.size() * sizeof(DNode), cudaMemcpyDeviceToHost));
+    // aux = {cpp, first, info, parent}
+    std::vector<float4> hx(size_t(nn + T->n_extra));
+    MLODS_CUDA(cudaMemcpy(hx.data(), T->nodes.aux, hx.size() * sizeof(float4), cudaMemcpyDeviceToHost));
+    auto first_of = [&](int64_t i) { uint32_t v; std::memcpy(&v, &hx[i].y, 4); return v; };
+    auto info_of = [&](int64_t i) { uint32_t v; std::memcpy(&v, &hx[i].z, 4); return v; };
     if (perm_out || leaf_off) {
         int32_t pos = 0;
         for (int64_t id = 0; id < nn; ++id) {
-            if (!(hn[id].info & kLeafBit)) {
+            if (!(info_of(id) & kLeafBit)) {
                 if (leaf_off) leaf_off[id] = -1;
                 continue;
             }
             if (leaf_off) leaf_off[id] = pos;
-            const int cnt = int(node_count(hn[id].info));
+            const int cnt = int(node_count(info_of(id)));
             if (cnt == 1) {
-                if (perm_out) perm_out[pos] = int32_t(hn[id].first);
+                if (perm_out) perm_out[pos] = int32_t(first_of(id));
                 ++pos;
             } else {
                 for (int k = 0; k < cnt; ++k) {
-                    if (perm_out) perm_out[pos] = int32_t(hn[hn[id].first + k].first);
+                    if (perm_out) perm_out[pos] = int32_t(first_of(first_of(id) + k));
                     ++pos;
                 }
             }

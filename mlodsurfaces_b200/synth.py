@@ -229,5 +229,20 @@ def make_tie_free(points: np.ndarray, depth: int = 12, max_rounds: int = 8) -> n
     raise RuntimeError("could not remove split ties")
 
 
+def normalize_like_pn(points: np.ndarray) -> np.ndarray:
+    """Pn::normalize (sources/apss/Pn.cpp:262-290) in float: centre on the
+    mean, pad the box by 0.5% of its diagonal, divide by the largest absolute
+    coordinate, so the cloud fits the [-1, 1]^3 zone of the DC grid."""
+    p = np.asarray(points, np.float32)
+    off = p.astype(np.float64).mean(0).astype(np.float32)
+    mx = (p.max(0) - off).astype(np.float32)
+    mn = (p.min(0) - off).astype(np.float32)
+    small = np.float32(np.linalg.norm((mx - mn).astype(np.float32)) * np.float32(0.005))
+    mx = mx + small
+    mn = mn - small
+    norme = np.float32(max(np.abs(mx).max(), np.abs(mn).max()))
+    return ((p - off) / norme).astype(np.float32)
+
+
 def bbox_diag(points: np.ndarray) -> float:
     return _bbox_diag(points)

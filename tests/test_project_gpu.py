@@ -8,7 +8,7 @@ import pytest
 
 import oracle
 from mlodsurfaces_b200 import APSSOctree, Fastapss, synth
-from mlodsurfaces_b200._capi import BLEND_CPU, BLEND_GPU, MlodsError
+from mlodsurfaces_b200._capi import BLEND_CPU, BLEND_GPU, CONVERGE_EXACT, CONVERGE_OFF, CONVERGE_TOL, MlodsError
 from conftest import TOL_DIAG, golden_kernel, make_kernel, rel_err
 
 pytestmark = pytest.mark.gpu
@@ -24,7 +24,7 @@ def excess_err(x, x64, diag):
 
 
 def run_gpu(pts, nrm, q, kernel, iters=10, cutoff=3.0, rule=BLEND_GPU, min_depth=0, reorder=True, step_max=-1.0,
-            depth=12):
+            depth=12, converge=CONVERGE_OFF, converge_tol=0.0):
     t = APSSOctree()
     t.build(pts, nrm, maxDepth=depth)
     f = Fastapss(t)
@@ -33,6 +33,8 @@ def run_gpu(pts, nrm, q, kernel, iters=10, cutoff=3.0, rule=BLEND_GPU, min_depth
     f.setMinDepth(min_depth)
     f.blend_rule = rule
     f.reorder = reorder
+    f.converge = converge
+    f.converge_tol = converge_tol
     f.copyPointsToGPU(len(q), q)
     op = np.empty((len(q), 3), np.float32)
     on = np.empty((len(q), 3), np.float32)
@@ -100,7 +102,9 @@ def test_min_depth_and_step_clamp(torus20k):
     op, _, _, _ = run_gpu(pts, nrm, q[:300], k, iters=3, min_depth=4, step_max=0.002)
     rp, _ = ot.project_mlod(q[:300], 3, k, rule=0, cutoff=3.0, min_depth=4, step_max=0.002)
     assert rel_err(op, rp, diag).max() < TOL_DIAG
-    assert (np.linalg.norm(op.astype(np.float64) - q[:300], axis=1) <= 3 * 0.002 * (1 + 1e-5)).all()
+    # each step is clamped to 0.002; every iterate is rounded to float (as the
+    # reference stores it), which adds up to about one ulp (1.2e-7 here) per step
+    assert (np.linalg.norm(op.astype(np.float64) - q[:300], axis=1) <= 3 * 0.002 + 4e-7).all()
 
 
 def test_far_queries_and_single_query(torus20k):
@@ -121,6 +125,28 @@ def test_reorder_is_bit_identical(torus20k):
     a, an, _, _ = run_gpu(pts, nrm, q, k, reorder=True)
     b, bn, _, _ = run_gpu(pts, nrm, q, k, reorder=False)
     assert np.array_equal(a, b) and np.array_equal(an, bn)
+
+
+@pytest.mark.parametrize("kind", ["gauss", "multi"])
+def test_exact_convergence_is_bit_identical_and_cheaper(torus20k, kind):
+    pts, nrm, q, _ = torus20k
+    k = make_kernel(kind, synth.bbox_diag(pts))
+    a, an, sa, _ = run_gpu(pts, nrm, q, k, iters=30)
+    b, bn, sb, _ = run_gpu(pts, nrm, q, k, iters=30, converge=CONVERGE_EXACT)
+    assert np.array_equal(a, b) and np.array_equal(an, bn)
+    assert sb["node_visits"] < sa["node_visits"]
+
+
+def test_tolerance_convergence_stays_within_tolerance(torus20k):
+    pts, nrm, q, ot = torus20k
+    diag = synth.bbox_diag(pts)
+    k = make_kernel("gauss", diag)
+    tol = 1e-7 * diag
+    b, bn, sb, _ = run_gpu(pts, nrm, q, k, iters=10, converge=CONVERGE_TOL, converge_tol=tol)
+    rp, _ = ot.project_mlod(q, 10, k, rule=BLEND_GPU, cutoff=3.0)
+    assert rel_err(b, rp, diag).max() < TOL_DIAG
+    _, _, sa, _ = run_gpu(pts, nrm, q, k, iters=10)
+    assert sb["node_visits"] < sa["node_visits"]
 
 
 def test_in_place_protocol_continues_from_last_positions(torus20k):
