@@ -10,13 +10,13 @@ namespace mlods
 {
 
 #ifndef MLODS_PROJECT_MIN_BLOCKS
-#define MLODS_PROJECT_MIN_BLOCKS 8
+#define MLODS_PROJECT_MIN_BLOCKS 10
 #endif
 #ifndef MLODS_PROJECT_STACK_CAP
 #define MLODS_PROJECT_STACK_CAP 160
 #endif
 constexpr int kProjectThreads = 128;                          // 4 warps per block, one query per warp at a time
-constexpr int kProjectMinBlocks = MLODS_PROJECT_MIN_BLOCKS;  // 8 -> 32 warps per SM, <= 64 registers
+constexpr int kProjectMinBlocks = MLODS_PROJECT_MIN_BLOCKS;  // 10 -> 40 warps per SM, <= 48 registers
 constexpr int kProjectStackCap = MLODS_PROJECT_STACK_CAP;    // sibling ranges per warp (28 bytes each)
 
 // One tree and its projection settings, plus the query buffers it serves.
