@@ -252,6 +252,27 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
                       int32_t* reorder, int32_t* grid_pct);
 
+/* ---- projection without device allocation (extension) ----------------------
+ * No counterpart in the reference.  Same computation and results as
+ * mlods_project_device (MLoD mode only; the tree's kernel, cutoff, min depth,
+ * blend rule, query ordering and convergence mode apply), but the call
+ * allocates no device memory: its scratch (query order, sort buffers, work
+ * counter) lives in one fixed array of about 13 MB that the library's module
+ * holds on each device, instead of the tree's lazily grown cudaMalloc buffer.
+ * For callers that must not allocate at call time (fixed memory budget, an
+ * allocator that owns the free memory, start-up-only footprint).
+ *   - n is at most MLODS_NOALLOC_MAX_QUERIES per call; larger n returns
+ *     MLODS_ERR_CAPACITY (split the batch).
+ *   - The first call on a device does a one-time setup (it looks up the
+ *     array's address; with CUDA's lazy module loading this is also when the
+ *     array becomes resident); make it outside any stream capture.
+ *   - All calls on a device share the array: calls that overlap in time
+ *     (several streams or host threads) race and must be serialised.
+ *   - mlods_last_stats does not report these calls. */
+#define MLODS_NOALLOC_MAX_QUERIES 524288
+int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float* d_q, float* d_out_pts, float* d_out_nrm,
+                                 int32_t n_iterations, float step_max, void* stream);
+
 /* Number of kernels this library has launched in this process (diagnostics). */
 int64_t mlods_kernel_launches(void);
 

@@ -38,6 +38,8 @@ CONVERGE_OFF = 0
 CONVERGE_EXACT = 1
 CONVERGE_TOL = 2
 
+NOALLOC_MAX_QUERIES = 524288
+
 
 class mlods_kernel(C.Structure):
     _fields_ = [
@@ -125,6 +127,7 @@ SIGNATURES = {
     "mlods_batch_project": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, _P]),
     "mlods_batch_tune": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
     "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32]),
+    "mlods_project_device_noalloc": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
 }
 
 _lib = None

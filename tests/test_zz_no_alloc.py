@@ -1,0 +1,81 @@
+"""mlods_project_device_noalloc against mlods_project_device through the C
+ABI: the same results on two calls in a row, no change in free device memory
+across them, and a clear capacity error beyond the fixed scratch size.
+(Named to be collected last: it must pass after every other test and alone.)"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mlodsurfaces_b200 import APSSOctree, Fastapss, synth
+from mlodsurfaces_b200 import _capi as capi
+from conftest import TOL_DIAG, make_kernel, rel_err
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def cloud():
+    pts, nrm = synth.torus(30000, seed=91)
+    pts = synth.make_tie_free(pts)
+    q = synth.perturbed_queries(pts, 0.01, seed=92)[:20000]
+    t = APSSOctree()
+    t.build(pts, nrm)
+    diag = synth.bbox_diag(pts)
+    f = Fastapss(t, make_kernel("multi", diag))
+    f.setScalingProtectionSphere(3.0)
+    f._sync_params()
+    return t, f, q, diag
+
+
+def _noalloc(lib, t, d_q, d_p, d_n, iters):
+    return lib.mlods_project_device_noalloc(t.handle, int(d_q.shape[0]), capi.ptr(d_q), capi.ptr(d_p),
+                                            capi.ptr(d_n), iters, C.c_float(-1.0), C.c_void_p(0))
+
+
+def test_noalloc_matches_project_device_twice_without_allocating(cloud):
+    t, f, q, diag = cloud
+    lib = capi.load()
+    d_q = torch.from_numpy(q).cuda()
+    ref_p = torch.empty_like(d_q)
+    ref_n = torch.empty_like(d_q)
+    capi.check(lib.mlods_project_device(t.handle, len(q), capi.ptr(d_q), capi.ptr(ref_p), capi.ptr(ref_n), 10,
+                                        C.c_float(-1.0), C.c_void_p(0)))
+    torch.cuda.synchronize()
+    outs = [(torch.full_like(d_q, float("nan")), torch.full_like(d_q, float("nan"))) for _ in range(2)]
+    torch.cuda.synchronize()
+    # first call: one-time setup (the module holding the fixed scratch array
+    # may load here, which takes its memory once)
+    capi.check(_noalloc(lib, t, d_q, *outs[0], 10))
+    torch.cuda.synchronize()
+    # second call: no device memory is taken
+    free_before = torch.cuda.mem_get_info()[0]
+    capi.check(_noalloc(lib, t, d_q, *outs[1], 10))
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert free_after == free_before
+    rp, rn = ref_p.cpu().numpy(), ref_n.cpu().numpy()
+    for d_p, d_n in outs:
+        p, n = d_p.cpu().numpy(), d_n.cpu().numpy()
+        assert rel_err(p, rp, diag).max() < TOL_DIAG
+        assert ((n * rn).sum(1) > 1 - 1e-4).all()
+
+
+def test_noalloc_rejects_too_many_queries_and_other_modes(cloud):
+    t, f, q, diag = cloud
+    lib = capi.load()
+    big = torch.zeros((capi.NOALLOC_MAX_QUERIES + 1, 3), device="cuda")
+    assert _noalloc(lib, t, big, big, big, 1) == capi.MLODS_ERR_CAPACITY
+    assert b"capacity" in lib.mlods_last_error()
+    small = torch.from_numpy(q[:100]).cuda()
+    out = torch.empty_like(small)
+    t.knnMode(True, 8)
+    try:
+        f._sync_params()
+        assert _noalloc(lib, t, small, out, out, 1) == capi.MLODS_ERR_INVALID
+    finally:
+        t.knnMode(False)
+        f._sync_params()
+    assert _noalloc(lib, t, small, out, out, 1) == capi.MLODS_OK
+    torch.cuda.synchronize()
