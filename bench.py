@@ -47,31 +47,66 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--check-queries", type=int, default=2048, help="queries checked against the FP64 oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["precision", "torus", "dc"], default="precision",
+                    help="precision: 2M-point RBF surface, MLoD projection (default); torus: 100k-point torus, "
+                         "CPU-path semantics; dc: 5M-point torus knot, adaptive depth-9 dual contouring")
+    ap.add_argument("--dc-depth", type=int, default=9)
     return ap.parse_args()
 
 
-def workload(n_points: int, rank: int):
+# Projection workloads: the precision configuration (default) and the
+# 100k-point torus configuration evaluated with the CPU path's semantics.
+SPECS = {
+    "precision": {"desc": "precision: RBF-blob surface translated 1e3*diag, multi-Gaussian MLoD",
+                  "kernel_desc": "multi-Gaussian sigma1=0.01*diag factor 2 x4", "cutoff": 3.0, "rule": 0,
+                  "rule_desc": "GPU (Fastapss)",
+                  "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag; queries = points + "
+                          "N(0, 0.01 diag)"},
+    "torus": {"desc": "torus: 100k-point torus, single Gaussian, CPU-path semantics",
+              "kernel_desc": "Gaussian sigma=0.02*diag", "cutoff": 3.0, "rule": 1,
+              "rule_desc": "CPU (APSSOctree::projectCPU)",
+              "data": "synthetic: seeded torus R=1 r=0.35, area-uniform, noise 0.002; queries = the points"},
+}
+
+
+def workload(n_points: int, rank: int, kind: str = "precision"):
     from mlodsurfaces_b200 import Kernel, synth
 
+    k = Kernel()
+    if kind == "torus":
+        pts, nrm = synth.torus(n_points, seed=1)
+        pts = synth.make_tie_free(pts)
+        q = pts.copy() if rank == 0 else synth.perturbed_queries(pts, 0.001, seed=3 + rank)
+        diag = synth.bbox_diag(pts)
+        k.type = Kernel.GAUSSIAN
+        k.sigma = 0.02 * diag
+        return pts, nrm, q, diag, k
     pts, nrm = synth.rbf_blobs(n_points, seed=2)
     pts = synth.make_tie_free(pts)
     q = synth.perturbed_queries(pts, 0.01, seed=3 + rank)
     diag = synth.bbox_diag(pts)
-    k = Kernel()
     k.type = Kernel.GAUSSIAN_MULTIPLE
     k.sigmas = [0.01 * diag * 2.0**i for i in range(4)]
     return pts, nrm, q, diag, k
 
 
+def n_points_for(args):
+    if args.workload == "torus" and args.n_points == 2_000_000:
+        return 100_000
+    return args.n_points
+
+
 def config_dict(args, tree_mb=None):
+    spec = SPECS[args.workload]
+    n = n_points_for(args)
     d = {
-        "workload": "precision: RBF-blob surface translated 1e3*diag, multi-Gaussian MLoD",
-        "n_points": args.n_points,
-        "n_queries_per_gpu": args.n_points,
+        "workload": spec["desc"],
+        "n_points": n,
+        "n_queries_per_gpu": n,
         "iterations": args.iters,
-        "kernel": "multi-Gaussian sigma1=0.01*diag factor 2 x4",
-        "cutoff": 3.0,
-        "blend_rule": "GPU (Fastapss)",
+        "kernel": spec["kernel_desc"],
+        "cutoff": spec["cutoff"],
+        "blend_rule": spec["rule_desc"],
         "parallelism": f"replicated tree, queries sharded, {args.gpus} GPU(s)",
         "l2": "L2 flushed (256 MB write) before every timed step",
     }
@@ -138,7 +173,7 @@ class ClockSampler:
 # (2M points, 2M queries, 10 iterations), from a single-pass ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum: see
 # profiles/mlod_project_kernel_precision_2M_launches.md.
-PROFILED_TRAFFIC = {(2_000_000, 10): 465.77e6 + 130.46e6}
+PROFILED_TRAFFIC = {("precision", 2_000_000, 10): 465.77e6 + 130.46e6}
 
 
 def max_over_ranks(values, world: int, device):
@@ -180,11 +215,12 @@ def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out):
         rt = oracle.RefTree(pts, nrm, 12)
         build_s = time.time() - t0
         sel = rng.choice(len(q), 256, replace=False)
-        _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+        cutoff = SPECS[args.workload]["cutoff"]
+        _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores)
         per_q = max(s0 / 256, 1e-7)
         ns = int(min(len(q), max(256, args.cpu_seconds / per_q)))
         sel = rng.choice(len(q), ns, replace=False)
-        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores)
         out["cpu_baseline"] = {"value": ns / secs, "unit": UNIT, "cores": cores, "kind": "reference",
                                "sample": f"{ns} random queries of the workload, {args.iters} iterations, "
                                          f"APSSOctree::projectCPU under OpenMP; tree build {build_s:.1f} s "
@@ -193,7 +229,8 @@ def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out):
     # accuracy of the GPU result against the FP64 oracle
     ot = oracle.OracleTree(pts, nrm, 12)
     sel = rng.choice(len(q), min(args.check_queries, len(q)), replace=False)
-    x64, _ = ot.project_mlod(q[sel], args.iters, kernel, rule=0, cutoff=3.0)
+    x64, _ = ot.project_mlod(q[sel], args.iters, kernel, rule=SPECS[args.workload]["rule"],
+                             cutoff=SPECS[args.workload]["cutoff"])
     x = gpu_out[sel].astype(np.float64)
     err = np.linalg.norm(x - x64, axis=1) / diag
     half_ulp = np.abs(np.spacing(x64.astype(np.float32)).astype(np.float64)) / 2
@@ -215,13 +252,15 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    pts, nrm, q, diag, kernel = workload(args.n_points, rank)
+    spec = SPECS[args.workload]
+    pts, nrm, q, diag, kernel = workload(n_points_for(args), rank, args.workload)
     tree = APSSOctree()
     tree.build(pts, nrm)
     inf = tree.info()
     tree_mb = inf.device_bytes / 2**20
     f = Fastapss(tree, kernel, len(q))
-    f.setScalingProtectionSphere(3.0)
+    f.setScalingProtectionSphere(spec["cutoff"])
+    f.blend_rule = spec["rule"]
     lib = capi.load()
 
     d_q = torch.from_numpy(q).to(dev)
@@ -313,8 +352,7 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 (f64 sphere solve)",
-        "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag; queries = points + "
-                "N(0, 0.01 diag)",
+        "data": spec["data"],
         "config": config_dict(args, tree_mb),
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                        "per": f"request of {len(q)} queries x {args.iters} iterations"},
@@ -323,7 +361,7 @@ def run_ours(args, rank, world, local_rank):
                 "path": "mlods_queries_upload + mlods_project (host pinned in/out)"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": PROFILED_TRAFFIC.get((args.n_points, args.iters)),
+                     "traffic": PROFILED_TRAFFIC.get((args.workload, n_points_for(args), args.iters)),
                      "note": f"algorithmic bytes = 36 per query + 64 per node visit ({mean_visits / len(q) / args.iters:.0f}"
                              f" visits per query-iteration); peak {peak_kind}; traffic = DRAM bytes per launch from "
                              f"ncu: the node arrays are read from DRAM about once, later visits hit L1/L2"},
@@ -338,6 +376,120 @@ def run_ours(args, rank, world, local_rank):
     return result
 
 
+def run_dc(args):
+    """Dual-contouring workload: 5M points on a torus-knot tube with 20 holes,
+    normalised into [-1, 1]^3 as Pn::normalize does, rational kernel
+    (exponent 4, epsilon 1e-3), cutoff 2, projection-driven grid at depth 9,
+    then the full mesh pipeline.  A step evaluates the corner field of the
+    grid (every unique lattice corner projected once, per-cell vertex)."""
+    import ctypes as C
+
+    import torch
+
+    from mlodsurfaces_b200 import APSSOctree, DCGrid, Fastapss, Kernel, synth
+    from mlodsurfaces_b200 import _capi as capi
+
+    n_points = args.n_points if args.n_points != 2_000_000 else 5_000_000
+    pts, nrm = synth.torus_knot(n_points, seed=4)
+    pts = synth.make_tie_free(synth.normalize_like_pn(pts))
+    diag = synth.bbox_diag(pts)
+    k = Kernel()
+    k.type = Kernel.SINGULAR
+    k.exponent = 4.0
+    k.constant_shift = 1e-3
+    lib = capi.load()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tree = APSSOctree()
+    tree.build(pts, nrm)
+    f = Fastapss(tree, k)
+    f.setScalingProtectionSphere(2.0)
+    torch.cuda.synchronize()
+    build_ms = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    grid = DCGrid.adaptive(f, args.dc_depth)
+    grid_ms = 1e3 * (time.perf_counter() - t0)
+    n_cells = len(grid.cells)
+
+    launches0 = lib.mlods_kernel_launches()
+    clocks = ClockSampler(0)
+    for _ in range(max(args.warmup, 0)):
+        f.dc_evaluate(grid.cells, grid.max_depth, grid.xform)
+    clocks.start()
+    step_ms, proj_ms = [], []
+    n_unique = 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cf, vx, nc, n_unique = f.dc_evaluate(grid.cells, grid.max_depth, grid.xform)
+        step_ms.append(1e3 * (time.perf_counter() - t0))
+        proj_ms.append(f.last_stats()["kernel_ms"])
+    clk = clocks.stop()
+    launches = lib.mlods_kernel_launches() - launches0
+    st = f.last_stats()
+    t0 = time.perf_counter()
+    mesh = f.dc_mesh(grid)
+    mesh_ms = 1e3 * (time.perf_counter() - t0)
+    v, _, tri = mesh.arrays()
+    value = n_unique * len(step_ms) / (sum(step_ms) / 1e3)
+    visits = st["node_visits"]
+    kms = statistics.mean(proj_ms)
+    achieved = (n_unique * 36 + 64 * visits) / (kms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    res = {
+        "metric": "dual contouring: unique grid corners evaluated/s (field + per-cell vertex)",
+        "value": value,
+        "unit": "corners/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": statistics.mean(step_ms),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (f64 sphere solve and vertex)",
+        "data": "synthetic: seeded (2,3) torus-knot tube, 20 spherical holes, normalised into [-1,1]^3",
+        "config": {"workload": "dual contouring: 5M-point torus knot, rational kernel, adaptive grid",
+                   "n_points": n_points, "dc_depth": args.dc_depth, "kernel": "rational exponent 4 epsilon 1e-3",
+                   "cutoff": 2.0, "n_cells": n_cells, "n_unique_corners": int(n_unique),
+                   "corner_projections_saved": f"{8 * n_cells} corner slots -> {n_unique} unique",
+                   "l2": "inputs larger than L2 (tree + corner buffers)"},
+        "stages_ms": {"tree_build": build_ms, "adaptive_grid": grid_ms, "corner_field": statistics.mean(step_ms),
+                      "corner_projection_kernel": kms, "mesh_pipeline": mesh_ms},
+        "mesh": {"vertices": int(len(v)), "triangles": int(len(tri))},
+        "e2e": {"value": value, "unit": "corners/s", "h2d_bytes_per_step": int(grid.cells.nbytes),
+                "d2h_bytes_per_step": int(cf.nbytes + vx.nbytes + nc.nbytes),
+                "path": "mlods_dc_evaluate (host cells in, host corner values and vertices out)"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "note": f"corner projection kernel; 36 B per corner + 64 B per node visit; "
+                                              f"peak {peak_kind}"},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.ref_available():
+            cores = os.cpu_count() or 1
+            rt = oracle.RefTree(pts, nrm, 12)
+            d = grid.cells[:, 0].astype(np.int64)
+            rng = np.random.default_rng(11)
+            sel = rng.choice(n_cells, min(n_cells, 4096), replace=False)
+            u = ((grid.cells[sel, 1:4].astype(np.float64) + 0.5) / (np.int64(1) << d[sel])[:, None])
+            q = (u @ grid.xform[:, :3].T.astype(np.float64) + grid.xform[:, 3]).astype(np.float32)
+            _, _, s0 = rt.project(q, 1, k, cutoff=2.0, nthreads=cores)
+            ns = int(min(n_cells, max(4096, args.cpu_seconds / max(s0 / len(sel), 1e-7))))
+            sel = rng.choice(n_cells, ns, replace=False)
+            u = ((grid.cells[sel, 1:4].astype(np.float64) + 0.5) / (np.int64(1) << d[sel])[:, None])
+            q = (u @ grid.xform[:, :3].T.astype(np.float64) + grid.xform[:, 3]).astype(np.float32)
+            _, _, secs = rt.project(q, 1, k, cutoff=2.0, nthreads=cores)
+            res["cpu_baseline"] = {"value": ns / secs, "unit": "corners/s", "cores": cores, "kind": "reference",
+                                   "sample": f"{ns} grid cell centres projected once (1 iteration) by "
+                                             f"APSSOctree::projectCPU under OpenMP (the reference projects each "
+                                             f"cell's 8 corners without de-duplication)"}
+    return res
+
+
 def run_reference(args, rank):
     """Reference arm: the reference's own CPU implementation (oracle/_ref,
     APSSOctree::projectCPU under OpenMP) on the same workload, each step a
@@ -346,19 +498,21 @@ def run_reference(args, rank):
 
     if not oracle.ref_available():
         return {"impl": "reference", "unavailable": "reference CPU shim oracle/_ref/libmlods_ref.so not built"}
-    pts, nrm, q, diag, kernel = workload(args.n_points, rank)
+    spec = SPECS[args.workload if args.workload in SPECS else "precision"]
+    pts, nrm, q, diag, kernel = workload(n_points_for(args), rank, args.workload if args.workload in SPECS
+                                         else "precision")
     cores = os.cpu_count() or 1
     rt = oracle.RefTree(pts, nrm, 12)
     rng = np.random.default_rng(7)
     sel = rng.choice(len(q), 256, replace=False)
-    _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+    _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=spec["cutoff"], nthreads=cores)
     per_q = max(s0 / 256, 1e-7)
     budget = 150.0 / max(args.steps + args.warmup, 1)
     ns = int(min(len(q), max(256, budget / per_q)))
     times = []
     for i in range(args.warmup + args.steps):
         sel = rng.choice(len(q), ns, replace=False)
-        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=3.0, nthreads=cores)
+        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=spec["cutoff"], nthreads=cores)
         if i >= args.warmup:
             times.append(secs)
     value = ns * len(times) / sum(times)
@@ -376,7 +530,7 @@ def run_reference(args, rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag",
+        "data": spec["data"],
         "config": config_dict(args),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -392,6 +546,10 @@ def main():
         if rank != 0:
             return
         print(json.dumps(run_reference(args, rank)), flush=True)
+        return
+    if args.workload == "dc":
+        if rank == 0:
+            print(json.dumps(run_dc(args)), flush=True)
         return
     if world > 1:
         import datetime

@@ -26,6 +26,7 @@ extern "C" {
 #define MLODS_ERR_CUDA 2      /* a CUDA call failed; see mlods_last_error() */
 #define MLODS_ERR_STATE 3     /* call out of protocol order (e.g. project before upload) */
 #define MLODS_ERR_CAPACITY 4  /* a request exceeds a fixed capacity */
+#define MLODS_ERR_TIMEOUT 5   /* a bounded wait ran out (the operation may still finish) */
 
 /* ---- weight kernels (Kernel.h:37, Kernel.cpp:64-83) ------------------- */
 #define MLODS_GAUSSIAN 0
@@ -200,6 +201,16 @@ int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, con
 int mlods_dcgrid_info(mlods_dcgrid g, int64_t* n_cells, int32_t* max_depth);
 int mlods_dcgrid_cells(mlods_dcgrid g, int32_t* cells);  /* 4 int32 per cell */
 int mlods_dcgrid_free(mlods_dcgrid g);
+/* The projection-driven grid of the reference's default mode
+ * (OctreeGenerator::generate + uniformize, upsample.cpp:228-273): cell
+ * centres projected level by level with the tree's projection (one step, no
+ * step limit), kept where the projection lands, refined with their
+ * neighbours, then graded and regularised; cut != 0 drops cells deeper than
+ * max_depth.  The grid's unit frame maps to the tree's frame by the 3x4
+ * matrix mlods_dcgrid_xform returns (new2bbox, scene.cpp:1311); for
+ * mlods_dcgrid_from_points it is the map of the given box. */
+int mlods_dcgrid_adaptive(mlods_tree t, int32_t max_depth, int32_t cut, void* stream, mlods_dcgrid* out);
+int mlods_dcgrid_xform(mlods_dcgrid g, float* xform, int64_t* n_projected);
 
 /* Signed field at the 8 corners of every cell and the per-cell vertex
  * (scene.cpp:1346-1394, dual_contouring.h:124-176).  xform is the 3x4
@@ -215,6 +226,33 @@ int mlods_dcgrid_free(mlods_dcgrid g);
 int mlods_dc_evaluate(mlods_tree t, int64_t n_cells, const int32_t* cells, int32_t max_depth, const float* xform,
                       int32_t use_normals, float* corner_f, float* vertex, int32_t* n_cross,
                       int64_t* n_unique_corners, void* stream);
+
+/* ---- mesh extraction and refinement (dual_contouring.h:59-87, scene.cpp:1396-1452) ----
+ * mlods_dc_extract builds the dual-contouring mesh of a grid (cells sorted as
+ * mlods_dcgrid_cells gives them) from its corner values and per-cell vertices
+ * (as mlods_dc_evaluate returns them): minimal edges enumerated in the
+ * reference's order (minimal_edges::traverse, octree.h:400-540), two
+ * triangles per sign-changing edge, vertices numbered on first use, vertex
+ * positions in the grid's unit frame.  Runs on the host, no GPU needed.
+ * mlods_mesh_transform applies a 3x4 map, mlods_mesh_smooth and
+ * mlods_mesh_subdivide are mesh::smoothMesh / mesh::subdivideMesh
+ * (upsample.h:55-133), mlods_mesh_project projects the vertices in place
+ * (positions and normals).  mlods_dc_mesh runs the whole reference pipeline
+ * on a grid: corner field, extraction, transform to the tree's frame,
+ * projection (3 iterations), then refine_rounds x (smooth, subdivide,
+ * project 3 iterations); the reference uses 2 rounds. */
+typedef struct mlods_mesh_s* mlods_mesh;
+int mlods_dc_extract(int64_t n_cells, const int32_t* cells, const float* corner_f, const float* cell_vertex,
+                     mlods_mesh* out);
+int mlods_mesh_info(mlods_mesh m, int64_t* n_vertices, int64_t* n_triangles);
+int mlods_mesh_get(mlods_mesh m, float* vertices, float* normals, uint32_t* indices);
+int mlods_mesh_transform(mlods_mesh m, const float* xform);
+int mlods_mesh_smooth(mlods_mesh m);
+int mlods_mesh_subdivide(mlods_mesh m);
+int mlods_mesh_project(mlods_tree t, mlods_mesh m, int32_t n_iterations, void* stream);
+int mlods_mesh_free(mlods_mesh m);
+int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t refine_rounds, void* stream,
+                  mlods_mesh* out);
 
 /* ---- per-launch statistics of the last projection on this tree ------------
  * node visits summed over queries and iterations, warp rounds (32 lanes each)
@@ -272,6 +310,42 @@ int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int6
 #define MLODS_NOALLOC_MAX_QUERIES 524288
 int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float* d_q, float* d_out_pts, float* d_out_nrm,
                                  int32_t n_iterations, float step_max, void* stream);
+
+/* ---- projection server (extension) -----------------------------------------
+ * No counterpart in the reference (one synchronous request at a time).  A
+ * server keeps a fixed list of resident trees (MLoD mode, kernel set; their
+ * settings must not change while it runs) and answers requests from any
+ * host thread: mlods_server_submit queues n host query points for one tree
+ * (optionally with their own weight kernel) and returns a ticket at once;
+ * worker threads, one per CUDA stream, take everything queued whenever they
+ * are free (up to max_batch_queries / max_batch_requests, optionally waiting
+ * max_wait_us for more) and project it with one launch of the multi-tree
+ * kernel; results are written to out_pts / out_nrm (either may be NULL),
+ * identical to mlods_project_host on the same tree and kernel.  The query and
+ * output arrays must stay valid until the ticket is waited for.
+ * Admission: a submit that would leave more than max_pending_queries queued
+ * returns MLODS_ERR_CAPACITY.  mlods_server_wait blocks at most timeout_ms
+ * (MLODS_ERR_TIMEOUT after that; wait again later), returns the request's
+ * status and its latency from submit to results on the host, and retires the
+ * ticket.  mlods_server_free cancels queued requests, lets running batches
+ * finish and joins the workers. */
+typedef struct mlods_server_config {
+    int32_t n_streams;            /* worker threads / CUDA streams (default 2) */
+    int32_t max_batch_requests;   /* requests per launch (default 4096) */
+    int64_t max_batch_queries;    /* queries per launch (default 2^21; a larger request runs alone) */
+    int64_t max_pending_queries;  /* admission bound on queued queries (default 2^26) */
+    int32_t max_wait_us;          /* batching window when less than a batch is queued (default 0) */
+    int32_t reserved;
+} mlods_server_config;
+typedef struct mlods_server_s* mlods_server;
+void mlods_server_default_config(mlods_server_config* c);
+int mlods_server_create(const mlods_tree* trees, int32_t n_trees, const mlods_server_config* cfg, mlods_server* out);
+int mlods_server_submit(mlods_server s, int32_t tree, int64_t n, const float* q, float* out_pts, float* out_nrm,
+                        int32_t n_iterations, const mlods_kernel* kernel, uint64_t* ticket);
+int mlods_server_wait(mlods_server s, uint64_t ticket, int32_t timeout_ms, double* latency_ms);
+int mlods_server_stats(mlods_server s, int64_t* completed, int64_t* batches, int64_t* queries, int64_t* queued,
+                       double* busy_ms);
+int mlods_server_free(mlods_server s);
 
 /* Number of kernels this library has launched in this process (diagnostics). */
 int64_t mlods_kernel_launches(void);

@@ -6,7 +6,7 @@ CorentinMercier/MlodSurfaces, rebuilt around hand-written CUDA kernels in
 mirror of the reference's C++ projection API (``Kernel``, ``APSSOctree``,
 ``APSS``/``Fastapss``) plus seeded synthetic inputs (``synth``).
 """
-from .apss import APSS, APSSOctree, DCGrid, Fastapss, FastapssBatch, GlobalAPSS, Kernel, unit2bbox  # noqa: F401
+from .apss import APSS, APSSOctree, DCGrid, Fastapss, FastapssBatch, GlobalAPSS, Kernel, Mesh, ProjectionServer, unit2bbox  # noqa: F401
 from . import synth  # noqa: F401
 
-__all__ = ["APSS", "APSSOctree", "DCGrid", "Fastapss", "FastapssBatch", "GlobalAPSS", "Kernel", "synth", "unit2bbox"]
+__all__ = ["APSS", "APSSOctree", "DCGrid", "Fastapss", "FastapssBatch", "GlobalAPSS", "Kernel", "Mesh", "ProjectionServer", "synth", "unit2bbox"]

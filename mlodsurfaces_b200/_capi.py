@@ -19,6 +19,7 @@ MLODS_ERR_INVALID = 1
 MLODS_ERR_CUDA = 2
 MLODS_ERR_STATE = 3
 MLODS_ERR_CAPACITY = 4
+MLODS_ERR_TIMEOUT = 5
 
 GAUSSIAN = 0
 SINGULAR = 1
@@ -64,6 +65,17 @@ class mlods_params(C.Structure):
         ("prune_tol", C.c_float),
         ("converge", C.c_int32),
         ("converge_tol", C.c_float),
+    ]
+
+
+class mlods_server_config(C.Structure):
+    _fields_ = [
+        ("n_streams", C.c_int32),
+        ("max_batch_requests", C.c_int32),
+        ("max_batch_queries", C.c_int64),
+        ("max_pending_queries", C.c_int64),
+        ("max_wait_us", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -128,6 +140,24 @@ SIGNATURES = {
     "mlods_batch_tune": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
     "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32]),
     "mlods_project_device_noalloc": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
+    "mlods_dcgrid_adaptive": (C.c_int, [_P, C.c_int32, C.c_int32, _P, C.POINTER(_P)]),
+    "mlods_dcgrid_xform": (C.c_int, [_P, _P, _I64]),
+    "mlods_dc_extract": (C.c_int, [C.c_int64, _P, _P, _P, C.POINTER(_P)]),
+    "mlods_mesh_info": (C.c_int, [_P, _I64, _I64]),
+    "mlods_mesh_get": (C.c_int, [_P, _P, _P, _P]),
+    "mlods_mesh_transform": (C.c_int, [_P, _P]),
+    "mlods_mesh_smooth": (C.c_int, [_P]),
+    "mlods_mesh_subdivide": (C.c_int, [_P]),
+    "mlods_mesh_project": (C.c_int, [_P, _P, C.c_int32, _P]),
+    "mlods_mesh_free": (C.c_int, [_P]),
+    "mlods_dc_mesh": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, C.POINTER(_P)]),
+    "mlods_server_default_config": (None, [C.POINTER(mlods_server_config)]),
+    "mlods_server_create": (C.c_int, [_P, C.c_int32, C.POINTER(mlods_server_config), C.POINTER(_P)]),
+    "mlods_server_submit": (C.c_int, [_P, C.c_int32, C.c_int64, _P, _P, _P, C.c_int32, C.POINTER(mlods_kernel),
+                                      C.POINTER(C.c_uint64)]),
+    "mlods_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int32, C.POINTER(C.c_double)]),
+    "mlods_server_stats": (C.c_int, [_P, _I64, _I64, _I64, _I64, C.POINTER(C.c_double)]),
+    "mlods_server_free": (C.c_int, [_P]),
 }
 
 _lib = None

@@ -247,28 +247,121 @@ class APSSOctree:
 
 
 class DCGrid:
-    """Dual-contouring cells from points (OctreeGenerator::generateFromPoints +
-    uniformizeFromPoints, upsample.cpp:128-144, :253-260), built on the host by
-    the library.  ``cells`` is an int32 (n, 4) array of (depth, x, y, z) in
-    sorted_octree order; ``max_depth`` the deepest level."""
+    """Dual-contouring cell grid.  ``cells`` is an int32 (n, 4) array of
+    (depth, x, y, z) in sorted_octree order, ``max_depth`` the deepest level
+    and ``xform`` the 3x4 map from the grid's unit frame to the tree's frame
+    (new2bbox, scene.cpp:1311).
 
-    def __init__(self, points, max_depth: int, box_min=(-1.0, -1.0, -1.0), box_max=(1.0, 1.0, 1.0)):
+    ``DCGrid(points, max_depth)`` is the grid on the input points
+    (OctreeGenerator::generateFromPoints + uniformizeFromPoints,
+    upsample.cpp:128-144, :253-260; the ``-b`` mode);
+    ``DCGrid.adaptive(apss, max_depth)`` the projection-driven grid of the
+    default mode (OctreeGenerator::generate + uniformize, upsample.cpp:228-273).
+    """
+
+    def __init__(self, points=None, max_depth: int = 0, box_min=(-1.0, -1.0, -1.0), box_max=(1.0, 1.0, 1.0),
+                 _handle=None):
+        self._lib = capi.load()
+        if _handle is None:
+            pts = _f32x3(points, "points")
+            bmin = np.asarray(box_min, np.float32)
+            bmax = np.asarray(box_max, np.float32)
+            g = C.c_void_p(0)
+            capi.check(self._lib.mlods_dcgrid_from_points(capi.ptr(pts), len(pts), int(max_depth), capi.ptr(bmin),
+                                                          capi.ptr(bmax), C.byref(g)))
+        else:
+            g = _handle
+        self._g = g
+        n = C.c_int64(0)
+        d = C.c_int32(0)
+        capi.check(self._lib.mlods_dcgrid_info(g, C.byref(n), C.byref(d)))
+        self.cells = np.empty((n.value, 4), np.int32)
+        if n.value:
+            capi.check(self._lib.mlods_dcgrid_cells(g, capi.ptr(self.cells)))
+        self.max_depth = int(d.value)
+        self.xform = np.empty((3, 4), np.float32)
+        npj = C.c_int64(0)
+        capi.check(self._lib.mlods_dcgrid_xform(g, capi.ptr(self.xform), C.byref(npj)))
+        self.n_projected = int(npj.value)
+
+    @classmethod
+    def adaptive(cls, apss: "APSS", max_depth: int, cut: bool = False, stream=None) -> "DCGrid":
+        apss._sync_params()
         lib = capi.load()
-        pts = _f32x3(points, "points")
-        bmin = np.asarray(box_min, np.float32)
-        bmax = np.asarray(box_max, np.float32)
         g = C.c_void_p(0)
-        capi.check(lib.mlods_dcgrid_from_points(capi.ptr(pts), len(pts), int(max_depth), capi.ptr(bmin),
-                                                capi.ptr(bmax), C.byref(g)))
+        capi.check(lib.mlods_dcgrid_adaptive(apss.m_apssOctree.handle, int(max_depth), 1 if cut else 0,
+                                             C.c_void_p(stream or 0), C.byref(g)))
+        return cls(_handle=g)
+
+    def __del__(self):
         try:
-            n = C.c_int64(0)
-            d = C.c_int32(0)
-            capi.check(lib.mlods_dcgrid_info(g, C.byref(n), C.byref(d)))
-            self.cells = np.empty((n.value, 4), np.int32)
-            capi.check(lib.mlods_dcgrid_cells(g, capi.ptr(self.cells)))
-            self.max_depth = int(d.value)
-        finally:
-            lib.mlods_dcgrid_free(g)
+            if getattr(self, "_g", None):
+                self._lib.mlods_dcgrid_free(self._g)
+                self._g = None
+        except Exception:
+            pass
+
+
+def _mesh_arrays(lib, m):
+    nv = C.c_int64(0)
+    nt = C.c_int64(0)
+    capi.check(lib.mlods_mesh_info(m, C.byref(nv), C.byref(nt)))
+    v = np.empty((nv.value, 3), np.float32)
+    n = np.empty((nv.value, 3), np.float32)
+    t = np.empty((nt.value, 3), np.uint32)
+    capi.check(lib.mlods_mesh_get(m, capi.ptr(v), capi.ptr(n), capi.ptr(t)))
+    return v, n, t
+
+
+class Mesh:
+    """A triangle mesh held by the library (positions, normals, uint32
+    triangles): dual-contouring output and the refinement steps of
+    scene::computeDualContouring (scene.cpp:1396-1452)."""
+
+    def __init__(self, handle):
+        self._lib = capi.load()
+        self._m = handle
+
+    @classmethod
+    def extract(cls, cells, corner_f, cell_vertex) -> "Mesh":
+        """dual_contour::extract over a grid's cells from their corner values
+        and per-cell vertices (host only)."""
+        lib = capi.load()
+        cells = np.ascontiguousarray(np.asarray(cells, np.int32).reshape(-1, 4))
+        cf = np.ascontiguousarray(np.asarray(corner_f, np.float32).reshape(-1, 8))
+        vx = np.ascontiguousarray(np.asarray(cell_vertex, np.float32).reshape(-1, 3))
+        if len(cf) != len(cells) or len(vx) != len(cells):
+            raise ValueError("corner_f and cell_vertex need one row per cell")
+        m = C.c_void_p(0)
+        capi.check(lib.mlods_dc_extract(len(cells), capi.ptr(cells), capi.ptr(cf), capi.ptr(vx), C.byref(m)))
+        return cls(m)
+
+    def arrays(self):
+        """(vertices (n, 3), normals (n, 3), triangles (m, 3) uint32)."""
+        return _mesh_arrays(self._lib, self._m)
+
+    def transform(self, xform) -> None:
+        x = np.ascontiguousarray(np.asarray(xform, np.float32).reshape(3, 4))
+        capi.check(self._lib.mlods_mesh_transform(self._m, capi.ptr(x)))
+
+    def smooth(self) -> None:
+        capi.check(self._lib.mlods_mesh_smooth(self._m))
+
+    def subdivide(self) -> None:
+        capi.check(self._lib.mlods_mesh_subdivide(self._m))
+
+    def project(self, apss: "APSS", n_iterations: int = 3, stream=None) -> None:
+        apss._sync_params()
+        capi.check(self._lib.mlods_mesh_project(apss.m_apssOctree.handle, self._m, int(n_iterations),
+                                                C.c_void_p(stream or 0)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "_m", None):
+                self._lib.mlods_mesh_free(self._m)
+                self._m = None
+        except Exception:
+            pass
 
 
 def unit2bbox(box_min=(-1.0, -1.0, -1.0), box_max=(1.0, 1.0, 1.0)) -> np.ndarray:
@@ -406,6 +499,16 @@ class APSS:
                                                capi.ptr(nc), C.byref(nu), C.c_void_p(0)))
         return cf, vx, nc, nu.value
 
+    def dc_mesh(self, grid: DCGrid, use_normals: bool = False, refine_rounds: int = 2, stream=None) -> Mesh:
+        """scene::computeDualContouring's mesh (scene.cpp:1346-1452): corner
+        field, extraction, transform to the tree's frame, projection, then
+        refine_rounds x (smooth, subdivide, project)."""
+        self._sync_params()
+        m = C.c_void_p(0)
+        capi.check(self._lib.mlods_dc_mesh(self.m_apssOctree.handle, grid._g, 1 if use_normals else 0,
+                                           int(refine_rounds), C.c_void_p(stream or 0), C.byref(m)))
+        return Mesh(m)
+
     def last_stats(self):
         v = C.c_int64(0)
         r = C.c_int64(0)
@@ -514,3 +617,75 @@ class FastapssBatch:
                                                C.byref(ro), C.byref(gp)))
         return {"node_visits": v.value, "rounds": r.value, "overflows": o.value, "kernel_ms": ms.value,
                 "reorder": ro.value, "grid_pct": gp.value}
+
+
+class ProjectionServer:
+    """Asynchronous projection requests over resident trees (no counterpart
+    in the reference).  ``projectors`` are :class:`Fastapss` objects with a
+    kernel set; requests name one of them by index.  :meth:`submit` queues
+    float32 (n, 3) host queries and returns a ticket at once; :meth:`wait`
+    returns (points, normals, latency_ms) once the request has run (results
+    equal ``project`` on the same tree and kernel).  Queued requests run in
+    batches, one multi-tree launch per batch, on ``n_streams`` worker streams.
+    """
+
+    def __init__(self, projectors, n_streams: int = 2, max_batch_queries: int = 1 << 21,
+                 max_batch_requests: int = 4096, max_pending_queries: int = 1 << 26, max_wait_us: int = 0):
+        self._lib = capi.load()
+        self._projectors = list(projectors)
+        for p in self._projectors:
+            if p._mode() != capi.MODE_MLOD:
+                raise ValueError("the server supports the MLoD mode only")
+            p._sync_params()
+        cfg = capi.mlods_server_config()
+        self._lib.mlods_server_default_config(C.byref(cfg))
+        cfg.n_streams = int(n_streams)
+        cfg.max_batch_queries = int(max_batch_queries)
+        cfg.max_batch_requests = int(max_batch_requests)
+        cfg.max_pending_queries = int(max_pending_queries)
+        cfg.max_wait_us = int(max_wait_us)
+        handles = (C.c_void_p * len(self._projectors))(*[p.m_apssOctree.handle.value for p in self._projectors])
+        s = C.c_void_p(0)
+        capi.check(self._lib.mlods_server_create(handles, len(self._projectors), C.byref(cfg), C.byref(s)))
+        self._s = s
+        self._pending = {}
+
+    def submit(self, tree: int, queries, n_iterations: int = 10, kernel: Kernel | None = None) -> int:
+        q = _f32x3(queries, "queries")
+        out_p = np.empty_like(q)
+        out_n = np.empty_like(q)
+        kc = C.byref(kernel.to_c()) if kernel is not None else None
+        t = C.c_uint64(0)
+        capi.check(self._lib.mlods_server_submit(self._s, int(tree), len(q), capi.ptr(q), capi.ptr(out_p),
+                                                 capi.ptr(out_n), int(n_iterations), kc, C.byref(t)))
+        self._pending[t.value] = (q, out_p, out_n)  # keep the buffers alive until wait
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000):
+        lat = C.c_double(0)
+        rc = self._lib.mlods_server_wait(self._s, C.c_uint64(ticket), int(timeout_ms), C.byref(lat))
+        if rc == capi.MLODS_ERR_TIMEOUT:
+            raise TimeoutError(self._lib.mlods_last_error().decode(errors="replace"))
+        bufs = self._pending.pop(ticket, None)
+        capi.check(rc)
+        return bufs[1], bufs[2], lat.value
+
+    def stats(self):
+        c, b, q, qd = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        busy = C.c_double(0)
+        capi.check(self._lib.mlods_server_stats(self._s, C.byref(c), C.byref(b), C.byref(q), C.byref(qd),
+                                                C.byref(busy)))
+        return {"completed": c.value, "batches": b.value, "queries": q.value, "queued": qd.value,
+                "busy_ms": busy.value}
+
+    def close(self) -> None:
+        if getattr(self, "_s", None):
+            self._lib.mlods_server_free(self._s)
+            self._s = None
+            self._pending.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

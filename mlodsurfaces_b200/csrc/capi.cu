@@ -57,6 +57,31 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line)
     return MLODS_ERR_CUDA;
 }
 
+int validate_kernel(const mlods_kernel* k)
+{
+    if (!k) {
+        set_last_error("null kernel");
+        return MLODS_ERR_INVALID;
+    }
+    if (k->type != MLODS_GAUSSIAN && k->type != MLODS_SINGULAR && k->type != MLODS_GAUSSIAN_MULTIPLE) {
+        set_last_error("unknown kernel type %d", k->type);
+        return MLODS_ERR_INVALID;
+    }
+    if (k->n_sigmas < 0 || k->n_sigmas > MLODS_MAX_SIGMAS) {
+        set_last_error("n_sigmas=%d out of range [0, %d]", k->n_sigmas, MLODS_MAX_SIGMAS);
+        return MLODS_ERR_CAPACITY;
+    }
+    if (k->type == MLODS_GAUSSIAN_MULTIPLE && k->n_sigmas == 0) {
+        set_last_error("multi-Gaussian kernel needs at least one sigma");
+        return MLODS_ERR_INVALID;
+    }
+    if (k->type == MLODS_GAUSSIAN && !(k->sigma > 0.f)) {
+        set_last_error("Gaussian kernel needs sigma > 0");
+        return MLODS_ERR_INVALID;
+    }
+    return MLODS_OK;
+}
+
 KernelConsts make_kernel_consts(const mlods_kernel& k)
 {
     KernelConsts c;
@@ -398,26 +423,8 @@ int mlods_tree_export(mlods_tree t, int32_t* depth, int32_t* parent, int32_t* fi
 int mlods_set_kernel(mlods_tree t, const mlods_kernel* k)
 {
     CHECK_TREE(t);
-    if (!k) {
-        set_last_error("null kernel");
-        return MLODS_ERR_INVALID;
-    }
-    if (k->type != MLODS_GAUSSIAN && k->type != MLODS_SINGULAR && k->type != MLODS_GAUSSIAN_MULTIPLE) {
-        set_last_error("unknown kernel type %d", k->type);
-        return MLODS_ERR_INVALID;
-    }
-    if (k->n_sigmas < 0 || k->n_sigmas > MLODS_MAX_SIGMAS) {
-        set_last_error("n_sigmas=%d out of range [0, %d]", k->n_sigmas, MLODS_MAX_SIGMAS);
-        return MLODS_ERR_CAPACITY;
-    }
-    if (k->type == MLODS_GAUSSIAN_MULTIPLE && k->n_sigmas == 0) {
-        set_last_error("multi-Gaussian kernel needs at least one sigma");
-        return MLODS_ERR_INVALID;
-    }
-    if (k->type == MLODS_GAUSSIAN && !(k->sigma > 0.f)) {
-        set_last_error("Gaussian kernel needs sigma > 0");
-        return MLODS_ERR_INVALID;
-    }
+    const int rc = validate_kernel(k);
+    if (rc != MLODS_OK) return rc;
     t->kernel = *k;
     t->kc = make_kernel_consts(*k);
     t->kernel_set = true;
@@ -647,7 +654,47 @@ int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, con
         delete g;
         return rc;
     }
+    // unit2bbox of the box (scene.cpp:1259-1269); the grid is not shifted
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 4; ++c) g->xform[4 * r + c] = 0.f;
+        g->xform[4 * r + r] = box_max[r] - box_min[r];
+        g->xform[4 * r + 3] = box_min[r];
+    }
     *out = g;
+    return MLODS_OK;
+}
+
+int mlods_dcgrid_adaptive(mlods_tree t, int32_t max_depth, int32_t cut, void* stream, mlods_dcgrid* out)
+{
+    CHECK_TREE(t);
+    if (!out) {
+        set_last_error("dcgrid adaptive: null output");
+        return MLODS_ERR_INVALID;
+    }
+    *out = nullptr;
+    auto* g = new (std::nothrow) mlods_dcgrid_s();
+    if (!g) {
+        set_last_error("dcgrid: host allocation failed");
+        return MLODS_ERR_CAPACITY;
+    }
+    const int rc = dcgrid_adaptive(t, max_depth, cut != 0, static_cast<cudaStream_t>(stream), g->cells,
+                                   g->max_depth, g->xform, &g->n_projected);
+    if (rc != MLODS_OK) {
+        delete g;
+        return rc;
+    }
+    *out = g;
+    return MLODS_OK;
+}
+
+int mlods_dcgrid_xform(mlods_dcgrid g, float* xform, int64_t* n_projected)
+{
+    if (!g) {
+        set_last_error("null dc grid");
+        return MLODS_ERR_INVALID;
+    }
+    if (xform) std::memcpy(xform, g->xform, sizeof g->xform);
+    if (n_projected) *n_projected = g->n_projected;
     return MLODS_OK;
 }
 

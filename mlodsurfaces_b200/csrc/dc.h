@@ -1,4 +1,5 @@
-// dc.h -- dual-contouring grid (host) and corner-field / vertex evaluation (device).
+// dc.h -- dual contouring: cell grids (host), corner field / vertex
+// evaluation (device), mesh extraction and refinement.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -10,10 +11,64 @@ struct mlods_tree_s;
 
 namespace mlods
 {
+namespace dcg
+{
+// One octree cell: octree_id (sources/dual-contouring/octree.h:18-44).
+struct Cell {
+    int depth, x, y, z;
+    bool operator==(const Cell& o) const { return depth == o.depth && x == o.x && y == o.y && z == o.z; }
+};
+
+// node_comparator, octree.h:147-154: depth, then z, y, x
+inline bool cell_less(const Cell& a, const Cell& b)
+{
+    if (a.depth != b.depth) return a.depth < b.depth;
+    if (a.z != b.z) return a.z < b.z;
+    if (a.y != b.y) return a.y < b.y;
+    return a.x < b.x;
+}
+
+// octree_id::parent / ancestor_at_depth, octree.h:547-572 (division rounded
+// towards -infinity)
+inline int floor_half(int v) { return (v < 0 && (v % 2) != 0) ? v / 2 - 1 : v / 2; }
+inline Cell parent(const Cell& c) { return Cell{c.depth - 1, floor_half(c.x), floor_half(c.y), floor_half(c.z)}; }
+inline Cell ancestor_at(Cell c, int d)
+{
+    while (c.depth > d) c = parent(c);
+    return c;
+}
+// octree_id::child, octree.h:574-582
+inline Cell child(const Cell& c, int k)
+{
+    return Cell{c.depth + 1, 2 * c.x + (k & 1), 2 * c.y + ((k >> 1) & 1), 2 * c.z + ((k >> 2) & 1)};
+}
+// octree_id::neighbor, octree.h:591-602 (n = 0..26, 13 is the cell itself)
+inline Cell neighbor(const Cell& c, int n)
+{
+    const int z = n / 9, y = (n - 9 * z) / 3, x = n - 9 * z - 3 * y;
+    return Cell{c.depth, c.x + x - 1, c.y + y - 1, c.z + z - 1};
+}
+
+void remove_duplicates(std::vector<Cell>& v);
+void grade(std::vector<Cell>& nodes);
+void regularize_up(std::vector<Cell>& nodes);
+void regularize_siblings(std::vector<Cell>& nodes);
+// all 26 neighbours of the cells at `depth` (every cell when depth < 0),
+// then sorted and de-duplicated (upsample.cpp:404-414)
+void expand(std::vector<Cell>& nodes, int depth);
+void cells_to_ints(const std::vector<Cell>& nodes, std::vector<int32_t>& out, int& max_depth);
+}  // namespace dcg
+
 // Cells as (depth, x, y, z) quadruples in sorted_octree order; depth_out is the
 // deepest cell depth.
 int dcgrid_from_points(const float* pts, int64_t n, int max_depth, const float box_min[3], const float box_max[3],
                        std::vector<int32_t>& cells_out, int& depth_out);
+
+// The projection-driven grid (OctreeGenerator::generate + uniformize,
+// upsample.cpp:228-251, :262-273): cells, their depth and the 3x4 map from the
+// grid's unit frame to the tree's frame (new2bbox, scene.cpp:1311).
+int dcgrid_adaptive(mlods_tree_s* T, int max_depth, bool cut, cudaStream_t s, std::vector<int32_t>& cells_out,
+                    int& depth_out, float xform[12], int64_t* n_projected);
 
 // Field at the 8 corners of every cell (unique corners projected once) and
 // the per-cell vertex; host arrays in and out.

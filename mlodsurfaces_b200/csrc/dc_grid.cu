@@ -19,43 +19,15 @@
 
 namespace mlods
 {
-namespace
+namespace dcg
 {
-struct Cell {
-    int depth, x, y, z;
-    bool operator==(const Cell& o) const { return depth == o.depth && x == o.x && y == o.y && z == o.z; }
-};
-
-// node_comparator, octree.h:147-154
-inline bool cell_less(const Cell& a, const Cell& b)
-{
-    if (a.depth != b.depth) return a.depth < b.depth;
-    if (a.z != b.z) return a.z < b.z;
-    if (a.y != b.y) return a.y < b.y;
-    return a.x < b.x;
-}
-
-// octree_id::parent, octree.h:547-559 (division rounded towards -infinity)
-inline int floor_half(int v) { return (v < 0 && (v % 2) != 0) ? v / 2 - 1 : v / 2; }
-inline Cell parent(const Cell& c) { return Cell{c.depth - 1, floor_half(c.x), floor_half(c.y), floor_half(c.z)}; }
-inline Cell child(const Cell& c, int k)
-{
-    return Cell{c.depth + 1, 2 * c.x + (k & 1), 2 * c.y + ((k >> 1) & 1), 2 * c.z + ((k >> 2) & 1)};
-}
-// octree_id::neighbor, octree.h:591-602
-inline Cell neighbor(const Cell& c, int n)
-{
-    const int z = n / 9, y = (n - 9 * z) / 3, x = n - 9 * z - 3 * y;
-    return Cell{c.depth, c.x + x - 1, c.y + y - 1, c.z + z - 1};
-}
-
 void remove_duplicates(std::vector<Cell>& v)
 {
     std::sort(v.begin(), v.end(), cell_less);
     v.erase(std::unique(v.begin(), v.end()), v.end());
 }
 
-void remove_duplicates_reverse(std::vector<Cell>& v)
+static void remove_duplicates_reverse(std::vector<Cell>& v)
 {
     std::sort(v.rbegin(), v.rend(), cell_less);
     v.erase(std::unique(v.begin(), v.end()), v.end());
@@ -103,7 +75,34 @@ void regularize_siblings(std::vector<Cell>& nodes)
     remove_duplicates(nodes);
 }
 
-}  // namespace
+// expand, upsample.cpp:404-414
+void expand(std::vector<Cell>& nodes, int depth)
+{
+    const size_t n = nodes.size();
+    for (size_t t = 0; t < n; ++t) {
+        if (depth >= 0 && nodes[t].depth != depth) continue;
+        for (int k = 0; k < 27; ++k)
+            if (k != 13) nodes.push_back(neighbor(nodes[t], k));
+    }
+    remove_duplicates(nodes);
+}
+
+void cells_to_ints(const std::vector<Cell>& nodes, std::vector<int32_t>& out, int& max_depth)
+{
+    max_depth = 0;
+    out.resize(nodes.size() * 4);
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        out[4 * i] = nodes[i].depth;
+        out[4 * i + 1] = nodes[i].x;
+        out[4 * i + 2] = nodes[i].y;
+        out[4 * i + 3] = nodes[i].z;
+        max_depth = std::max(max_depth, nodes[i].depth);
+    }
+}
+
+}  // namespace dcg
+
+using namespace dcg;
 
 int dcgrid_from_points(const float* pts, int64_t n, int max_depth, const float box_min[3], const float box_max[3],
                        std::vector<int32_t>& cells_out, int& depth_out)
@@ -139,15 +138,7 @@ int dcgrid_from_points(const float* pts, int64_t n, int max_depth, const float b
     grade(nodes);
     regularize_up(nodes);
     regularize_siblings(nodes);
-    depth_out = 0;
-    cells_out.resize(nodes.size() * 4);
-    for (size_t i = 0; i < nodes.size(); ++i) {
-        cells_out[4 * i] = nodes[i].depth;
-        cells_out[4 * i + 1] = nodes[i].x;
-        cells_out[4 * i + 2] = nodes[i].y;
-        cells_out[4 * i + 3] = nodes[i].z;
-        depth_out = std::max(depth_out, nodes[i].depth);
-    }
+    cells_to_ints(nodes, cells_out, depth_out);
     return MLODS_OK;
 }
 

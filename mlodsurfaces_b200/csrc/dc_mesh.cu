@@ -1,0 +1,500 @@
+// dc_mesh.cu -- dual-contouring mesh extraction and refinement.
+//
+// Extraction (dual_contour::extract, dual_contouring.h:59-87, :190-229): the
+// minimal edges of the cell octree are enumerated by the recursive
+// node / face / edge procedure of minimal_edges::traverse (octree.h:400-540),
+// in the same order; an edge whose two end values (corners of the deepest of
+// its 3-4 cells) change sign gives two triangles over the cells' vertices,
+// oriented by the sign of the first end.  Vertices are numbered on first use,
+// as the reference's get_vertex does, so the index lists match it exactly.
+// Refinement (scene.cpp:1402-1452, upsample.h:55-133): the vertices are
+// projected (3 iterations), then twice smoothed, 1->4 subdivided and projected
+// again.  Integer traversal and mesh edits stay on the host; projections run
+// on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <unordered_map>
+#include <vector>
+
+#include "dc.h"
+#include "tree.cuh"
+
+struct mlods_mesh_s {
+    std::vector<float> pos;  // 3 per vertex
+    std::vector<float> nrm;  // 3 per vertex
+    std::vector<uint32_t> tri;
+};
+
+namespace mlods
+{
+namespace
+{
+using dcg::Cell;
+constexpr int kX = 0, kY = 1, kZ = 2;
+
+// (edge direction, half along it) of the 4 inner edges of a face, per face
+// direction, in the order of the reference's subedges / subedgedir tables
+// (octree.h:480-492)
+constexpr int kFaceEdges[3][4][2] = {
+    {{kY, 0}, {kY, 1}, {kZ, 0}, {kZ, 1}},
+    {{kX, 1}, {kX, 0}, {kZ, 0}, {kZ, 1}},
+    {{kY, 0}, {kY, 1}, {kX, 0}, {kX, 1}},
+};
+
+inline void perp(int e, int& p1, int& p2)
+{
+    p1 = e == kX ? kY : kX;
+    p2 = e == kZ ? kY : kZ;
+}
+
+struct Grid {
+    const int32_t* c;  // (depth, x, y, z) per cell, sorted
+    int64_t n;
+    int max_depth;
+    std::vector<int64_t> begin;  // first cell of each depth, max_depth + 2 entries
+    std::vector<int64_t> kids;   // 8 per cell, -1 for leaves
+
+    Cell cell(int64_t i) const { return Cell{c[4 * i], c[4 * i + 1], c[4 * i + 2], c[4 * i + 3]}; }
+    int64_t find(const Cell& q) const
+    {
+        if (q.depth < 0 || q.depth > max_depth) return -1;
+        int64_t lo = begin[size_t(q.depth)], hi = begin[size_t(q.depth) + 1];
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) / 2;
+            if (dcg::cell_less(cell(mid), q)) lo = mid + 1;
+            else hi = mid;
+        }
+        return (lo < begin[size_t(q.depth) + 1] && cell(lo) == q) ? lo : -1;
+    }
+};
+
+// sorted_octree relations (octree.h:227-262): every non-root cell needs its
+// parent and every inner cell exactly 8 children
+int build_grid(const int32_t* cells, int64_t n, Grid& g)
+{
+    g.c = cells;
+    g.n = n;
+    g.max_depth = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (cells[4 * i] < 0 || cells[4 * i] > 30) {
+            set_last_error("dc extract: cell %lld has depth %d", (long long)i, cells[4 * i]);
+            return MLODS_ERR_INVALID;
+        }
+        g.max_depth = std::max(g.max_depth, int(cells[4 * i]));
+        if (i > 0 && !dcg::cell_less(g.cell(i - 1), g.cell(i))) {
+            set_last_error("dc extract: cells must be sorted (depth, z, y, x) and unique (cell %lld)", (long long)i);
+            return MLODS_ERR_INVALID;
+        }
+    }
+    g.begin.assign(size_t(g.max_depth) + 2, n);
+    for (int64_t i = n - 1; i >= 0; --i) g.begin[size_t(cells[4 * i])] = i;
+    for (int d = g.max_depth; d >= 0; --d)
+        if (g.begin[size_t(d)] > g.begin[size_t(d) + 1]) g.begin[size_t(d)] = g.begin[size_t(d) + 1];
+    g.kids.assign(size_t(n) * 8, -1);
+    std::vector<uint8_t> count(size_t(n), 0);
+    for (int64_t i = 0; i < n; ++i) {
+        const Cell c = g.cell(i);
+        if (c.depth == 0) continue;
+        const Cell p = dcg::parent(c);
+        const int64_t pi = g.find(p);
+        if (pi < 0) {
+            set_last_error("dc extract: cell %lld has no parent in the grid", (long long)i);
+            return MLODS_ERR_INVALID;
+        }
+        const int k = (c.x - 2 * p.x) + 2 * (c.y - 2 * p.y) + 4 * (c.z - 2 * p.z);
+        g.kids[size_t(pi) * 8 + size_t(k)] = i;
+        ++count[size_t(pi)];
+    }
+    for (int64_t i = 0; i < n; ++i)
+        if (count[size_t(i)] != 0 && count[size_t(i)] != 8) {
+            set_last_error("dc extract: cell %lld has %d children (needs 0 or 8)", (long long)i, int(count[size_t(i)]));
+            return MLODS_ERR_INVALID;
+        }
+    return MLODS_OK;
+}
+
+struct Extractor {
+    const Grid& g;
+    const float* cf;  // 8 corner values per cell
+    std::vector<int64_t> vertex_of;
+    std::vector<int64_t> order;  // cell of each vertex, in creation order
+    std::vector<uint32_t> tri;
+
+    Extractor(const Grid& grid, const float* corner_f) : g(grid), cf(corner_f), vertex_of(size_t(grid.n), -1) {}
+
+    bool leaf(int64_t n) const { return g.kids[size_t(n) * 8] < 0; }
+    int64_t kid(int64_t n, int c) const { return leaf(n) ? n : g.kids[size_t(n) * 8 + size_t(c)]; }
+
+    uint32_t vertex(int64_t n)
+    {
+        int64_t& v = vertex_of[size_t(n)];
+        if (v < 0) {
+            v = int64_t(order.size());
+            order.push_back(n);
+        }
+        return uint32_t(v);
+    }
+
+    // on_min_edges + extract's triangle pair (dual_contouring.h:64-86, :190-229)
+    void emit(const int64_t nd[4], int e)
+    {
+        int sel = 0, sel_d = -1;
+        for (int i = 0; i < 4; ++i) {
+            const int d = g.c[4 * nd[i]];
+            if (d > sel_d) {
+                sel = i;
+                sel_d = d;
+            }
+        }
+        int p1, p2;
+        perp(e, p1, p2);
+        const int base = ((1 - (sel & 1)) << p1) | ((1 - (sel >> 1)) << p2);
+        int c0 = base, c1 = base | (1 << e);
+        if (e == kY) std::swap(c0, c1);  // the reference lists the upper end first for Y edges
+        const float f0 = cf[8 * nd[sel] + c0], f1 = cf[8 * nd[sel] + c1];
+        if (std::isnan(f0) || std::isnan(f1)) return;
+        const bool m0 = f0 < 0, m1 = f1 < 0;
+        if (m0 == m1) return;
+        static const int tris[2][3] = {{0, 1, 3}, {0, 3, 2}};
+        for (const auto& t : tris) {
+            const uint32_t v0 = vertex(nd[t[0]]), v1 = vertex(nd[t[1]]), v2 = vertex(nd[t[2]]);
+            if (v0 == v1 || v1 == v2 || v2 == v0) continue;
+            tri.push_back(v0);
+            tri.push_back(m0 ? v2 : v1);
+            tri.push_back(m0 ? v1 : v2);
+        }
+    }
+
+    // traverse_edge, octree.h:504-540
+    void edge(const int64_t nd[4], int e)
+    {
+        if (leaf(nd[0]) && leaf(nd[1]) && leaf(nd[2]) && leaf(nd[3])) {
+            emit(nd, e);
+            return;
+        }
+        int p1, p2;
+        perp(e, p1, p2);
+        for (int h = 0; h < 2; ++h) {
+            int64_t sub[4];
+            for (int s = 0; s < 4; ++s) sub[s] = kid(nd[s], (h << e) | ((1 - (s & 1)) << p1) | ((1 - (s >> 1)) << p2));
+            edge(sub, e);
+        }
+    }
+
+    // traverse_face, octree.h:457-502
+    void face(int64_t n1, int64_t n2, int d)
+    {
+        if (leaf(n1) && leaf(n2)) return;
+        int on1[4], on2[4], k1 = 0, k2 = 0;
+        for (int c = 0; c < 8; ++c) {
+            if ((c >> d) & 1) on1[k1++] = c;
+            else on2[k2++] = c;
+        }
+        for (int f = 0; f < 4; ++f) face(kid(n1, on1[f]), kid(n2, on2[f]), d);
+        for (int k = 0; k < 4; ++k) {
+            const int e = kFaceEdges[d][k][0], h = kFaceEdges[d][k][1];
+            const int fa = 3 - d - e;  // the axis normal to both
+            int p1, p2;
+            perp(e, p1, p2);
+            int64_t nd[4];
+            for (int sd = 0; sd < 2; ++sd)
+                for (int sf = 0; sf < 2; ++sf) {
+                    const int c = (h << e) | ((1 - sd) << d) | (sf << fa);
+                    const int s_p1 = p1 == d ? sd : sf, s_p2 = p2 == d ? sd : sf;
+                    nd[s_p1 + 2 * s_p2] = sd == 0 ? kid(n1, c) : kid(n2, c);
+                }
+            edge(nd, e);
+        }
+    }
+
+    // traverse_node, octree.h:423-455
+    void node(int64_t n)
+    {
+        if (leaf(n)) return;
+        const int64_t* ch = &g.kids[size_t(n) * 8];
+        for (int t = 0; t < 8; ++t) node(ch[t]);
+        for (int d = 0; d < 3; ++d)
+            for (int c = 0; c < 8; ++c)
+                if (!((c >> d) & 1)) face(ch[c], ch[c | (1 << d)], d);
+        for (int e = 0; e < 3; ++e) {
+            int p1, p2;
+            perp(e, p1, p2);
+            for (int h = 0; h < 2; ++h) {
+                int64_t nd[4];
+                for (int s = 0; s < 4; ++s) nd[s] = ch[(h << e) | ((s & 1) << p1) | ((s >> 1) << p2)];
+                edge(nd, e);
+            }
+        }
+    }
+};
+
+// 4x4 float transform applied as Eigen's Matrix4f * Vector4f (columns
+// accumulated left to right), rows 0-2 given as a 3x4 array
+inline void apply_xform(const float* m, const float* v, float* out)
+{
+    for (int r = 0; r < 3; ++r) {
+        float a = m[4 * r] * v[0];
+        a = a + m[4 * r + 1] * v[1];
+        a = a + m[4 * r + 2] * v[2];
+        out[r] = a + m[4 * r + 3];
+    }
+}
+
+}  // namespace
+
+int dc_extract(const int32_t* cells, int64_t n_cells, const float* corner_f, const float* cell_vertex,
+               mlods_mesh_s* m)
+{
+    Grid g;
+    int rc = build_grid(cells, n_cells, g);
+    if (rc != MLODS_OK) return rc;
+    m->pos.clear();
+    m->nrm.clear();
+    m->tri.clear();
+    const int64_t root = g.find(Cell{0, 0, 0, 0});
+    if (root < 0) return MLODS_OK;  // minimal_edges::traverse starts at the root only
+    Extractor ex(g, corner_f);
+    ex.node(root);
+    m->pos.resize(ex.order.size() * 3);
+    m->nrm.assign(ex.order.size() * 3, 0.f);
+    for (size_t i = 0; i < ex.order.size(); ++i)
+        for (int a = 0; a < 3; ++a) m->pos[3 * i + size_t(a)] = cell_vertex[3 * ex.order[i] + a];
+    m->tri.swap(ex.tri);
+    return MLODS_OK;
+}
+
+// mesh::smoothMesh, upsample.h:55-78
+void mesh_smooth(mlods_mesh_s* m)
+{
+    const size_t nv = m->pos.size() / 3;
+    std::vector<float> acc(nv * 3, 0.f), val(nv, 0.f);
+    const float* p = m->pos.data();
+    for (size_t t = 0; t + 2 < m->tri.size(); t += 3) {
+        const uint32_t a = m->tri[t], b = m->tri[t + 1], c = m->tri[t + 2];
+        for (int k = 0; k < 3; ++k) {
+            acc[3 * a + k] += p[3 * b + k] + p[3 * c + k];
+            acc[3 * b + k] += p[3 * a + k] + p[3 * c + k];
+            acc[3 * c + k] += p[3 * b + k] + p[3 * a + k];
+        }
+        val[a] += 2.f;
+        val[b] += 2.f;
+        val[c] += 2.f;
+    }
+    for (size_t v = 0; v < nv; ++v)
+        for (int k = 0; k < 3; ++k) m->pos[3 * v + size_t(k)] = acc[3 * v + size_t(k)] / val[v];
+}
+
+// mesh::subdivideMesh, upsample.h:80-133
+void mesh_subdivide(mlods_mesh_s* m)
+{
+    const size_t nt = m->tri.size() / 3;
+    std::unordered_map<uint64_t, uint32_t> on_edge;
+    on_edge.reserve(nt * 2);
+    auto mid = [&](uint32_t i, uint32_t j) -> uint32_t {
+        const uint64_t key = (uint64_t(std::min(i, j)) << 32) | uint64_t(std::max(i, j));
+        auto it = on_edge.find(key);
+        if (it != on_edge.end()) return it->second;
+        const uint32_t id = uint32_t(m->pos.size() / 3);
+        float q[3];
+        for (int k = 0; k < 3; ++k) q[k] = (m->pos[3 * size_t(i) + k] + m->pos[3 * size_t(j) + k]) / 2.f;
+        for (int k = 0; k < 3; ++k) m->pos.push_back(q[k]);
+        on_edge.emplace(key, id);
+        return id;
+    };
+    m->tri.reserve(nt * 12);
+    for (size_t t = 0; t < nt; ++t) {
+        const uint32_t a = m->tri[3 * t], b = m->tri[3 * t + 1], c = m->tri[3 * t + 2];
+        const uint32_t ab = mid(a, b);
+        const uint32_t bc = mid(c, b);
+        const uint32_t ca = mid(c, a);
+        m->tri[3 * t + 1] = ab;
+        m->tri[3 * t + 2] = ca;
+        const uint32_t more[9] = {ab, b, bc, ab, bc, ca, ca, bc, c};
+        m->tri.insert(m->tri.end(), more, more + 9);
+    }
+    m->nrm.resize(m->pos.size(), 0.f);  // normals.resize: new vertices get (0, 0, 0)
+}
+
+void mesh_transform(mlods_mesh_s* m, const float* xform)
+{
+    for (size_t v = 0; v < m->pos.size() / 3; ++v) {
+        float o[3];
+        apply_xform(xform, &m->pos[3 * v], o);
+        std::memcpy(&m->pos[3 * v], o, sizeof o);
+    }
+}
+
+// APSS::project of the vertices in place (scene.cpp:1422-1428)
+int mesh_project(mlods_tree_s* T, mlods_mesh_s* m, int iters, cudaStream_t s)
+{
+    const int64_t nv = int64_t(m->pos.size() / 3);
+    if (nv == 0) return MLODS_OK;
+    float* d = nullptr;
+    MLODS_CUDA(cudaMalloc(&d, size_t(nv) * 36));
+    auto done = [&](int rc) {
+        cudaFree(d);
+        return rc;
+    };
+    cudaError_t e = cudaMemcpyAsync(d, m->pos.data(), size_t(nv) * 12, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return done(cuda_fail(e, "mesh project: upload", __FILE__, __LINE__));
+    int rc = project_buffers(T, nv, d, d + 3 * nv, d + 6 * nv, iters, -1.f, s);
+    if (rc != MLODS_OK) return done(rc);
+    m->nrm.resize(m->pos.size());
+    e = cudaMemcpyAsync(m->pos.data(), d + 3 * nv, size_t(nv) * 12, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->nrm.data(), d + 6 * nv, size_t(nv) * 12, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return done(cuda_fail(e, "mesh project: download", __FILE__, __LINE__));
+    return done(MLODS_OK);
+}
+
+}  // namespace mlods
+
+using namespace mlods;
+
+extern "C" {
+
+int mlods_dc_extract(int64_t n_cells, const int32_t* cells, const float* corner_f, const float* cell_vertex,
+                     mlods_mesh* out)
+{
+    if (!out || n_cells <= 0 || !cells || !corner_f || !cell_vertex) {
+        set_last_error("dc extract: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    *out = nullptr;
+    auto* m = new (std::nothrow) mlods_mesh_s();
+    if (!m) {
+        set_last_error("dc extract: host allocation failed");
+        return MLODS_ERR_CAPACITY;
+    }
+    const int rc = dc_extract(cells, n_cells, corner_f, cell_vertex, m);
+    if (rc != MLODS_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return MLODS_OK;
+}
+
+int mlods_mesh_info(mlods_mesh m, int64_t* n_vertices, int64_t* n_triangles)
+{
+    if (!m) {
+        set_last_error("null mesh");
+        return MLODS_ERR_INVALID;
+    }
+    if (n_vertices) *n_vertices = int64_t(m->pos.size() / 3);
+    if (n_triangles) *n_triangles = int64_t(m->tri.size() / 3);
+    return MLODS_OK;
+}
+
+int mlods_mesh_get(mlods_mesh m, float* vertices, float* normals, uint32_t* indices)
+{
+    if (!m) {
+        set_last_error("null mesh");
+        return MLODS_ERR_INVALID;
+    }
+    if (vertices) std::memcpy(vertices, m->pos.data(), m->pos.size() * sizeof(float));
+    if (normals) std::memcpy(normals, m->nrm.data(), m->nrm.size() * sizeof(float));
+    if (indices) std::memcpy(indices, m->tri.data(), m->tri.size() * sizeof(uint32_t));
+    return MLODS_OK;
+}
+
+int mlods_mesh_free(mlods_mesh m)
+{
+    delete m;
+    return MLODS_OK;
+}
+
+int mlods_mesh_transform(mlods_mesh m, const float* xform)
+{
+    if (!m || !xform) {
+        set_last_error("mesh transform: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    mesh_transform(m, xform);
+    return MLODS_OK;
+}
+
+int mlods_mesh_smooth(mlods_mesh m)
+{
+    if (!m) {
+        set_last_error("null mesh");
+        return MLODS_ERR_INVALID;
+    }
+    mesh_smooth(m);
+    return MLODS_OK;
+}
+
+int mlods_mesh_subdivide(mlods_mesh m)
+{
+    if (!m) {
+        set_last_error("null mesh");
+        return MLODS_ERR_INVALID;
+    }
+    if (m->pos.size() / 3 + m->tri.size() > size_t(UINT32_MAX)) {
+        set_last_error("mesh subdivide: result would exceed 32-bit vertex indices");
+        return MLODS_ERR_CAPACITY;
+    }
+    mesh_subdivide(m);
+    return MLODS_OK;
+}
+
+int mlods_mesh_project(mlods_tree t, mlods_mesh m, int32_t n_iterations, void* stream)
+{
+    if (!t || !m || n_iterations < 0) {
+        set_last_error("mesh project: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    return mesh_project(t, m, n_iterations, static_cast<cudaStream_t>(stream));
+}
+
+int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t refine_rounds, void* stream,
+                  mlods_mesh* out)
+{
+    if (!t || !g || !out || refine_rounds < 0) {
+        set_last_error("dc mesh: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    *out = nullptr;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = int64_t(g->cells.size() / 4);
+    if (n == 0) {
+        set_last_error("dc mesh: empty grid");
+        return MLODS_ERR_INVALID;
+    }
+    std::vector<float> cf(size_t(n) * 8), vx(size_t(n) * 3);
+    std::vector<int32_t> nc(static_cast<size_t>(n));
+    int64_t nu = 0;
+    int rc = dc_evaluate(t, n, g->cells.data(), g->max_depth, g->xform, use_normals, cf.data(), vx.data(), nc.data(),
+                         &nu, s);
+    if (rc != MLODS_OK) return rc;
+    auto* m = new (std::nothrow) mlods_mesh_s();
+    if (!m) {
+        set_last_error("dc mesh: host allocation failed");
+        return MLODS_ERR_CAPACITY;
+    }
+    rc = dc_extract(g->cells.data(), n, cf.data(), vx.data(), m);
+    if (rc == MLODS_OK) {
+        mesh_transform(m, g->xform);  // scene.cpp:1400-1408
+        rc = mesh_project(t, m, 3, s);
+    }
+    for (int r = 0; rc == MLODS_OK && r < refine_rounds; ++r) {
+        mesh_smooth(m);
+        if (m->pos.size() / 3 + m->tri.size() > size_t(UINT32_MAX)) {
+            set_last_error("dc mesh: subdivision would exceed 32-bit vertex indices");
+            rc = MLODS_ERR_CAPACITY;
+            break;
+        }
+        mesh_subdivide(m);
+        rc = mesh_project(t, m, 3, s);
+    }
+    if (rc != MLODS_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return MLODS_OK;
+}
+
+}  // extern "C"

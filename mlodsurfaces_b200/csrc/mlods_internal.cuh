@@ -99,6 +99,8 @@ struct KernelConsts {
 };
 
 KernelConsts make_kernel_consts(const mlods_kernel& k);
+// Checks a kernel as mlods_set_kernel does; sets the error message.
+int validate_kernel(const mlods_kernel* k);
 
 // Weight as a function of the squared distance (Kernel::w, Kernel.cpp:64-83;
 // KernelGPU::w, GPUUtils.cu:243-257).

@@ -68,6 +68,10 @@ struct mlods_queries_s {
 struct mlods_dcgrid_s {
     std::vector<int32_t> cells;
     int max_depth = 0;
+    // rows 0-2 of the 4x4 map from the grid's unit frame to the tree's frame
+    // (new2bbox, scene.cpp:1311)
+    float xform[12] = {2.f, 0.f, 0.f, -1.f, 0.f, 2.f, 0.f, -1.f, 0.f, 0.f, 2.f, -1.f};
+    int64_t n_projected = 0;  // centre projections made while generating it
 };
 
 namespace mlods

@@ -88,3 +88,120 @@ def grid_from_points(pts, max_depth, box_min=(-1.0, -1.0, -1.0), box_max=(1.0, 1
     nodes = regularize_up(nodes)
     nodes = regularize_siblings(nodes)
     return np.array(nodes, np.int32).reshape(-1, 4)
+
+
+# ---- projection-driven grid (OctreeGenerator::generate + uniformize) ----------
+
+def expand(nodes, depth=-1):
+    """upsample.cpp:404-414: add the 26 neighbours of the cells at `depth`
+    (all cells when depth < 0), sorted and unique."""
+    out = list(nodes)
+    for c in nodes:
+        if depth >= 0 and c[0] != depth:
+            continue
+        out.extend(neighbor(c, k) for k in range(27) if k != 13)
+    return remove_duplicates(out)
+
+
+def ancestor_at(c, d):
+    while c[0] > d:
+        c = parent(c)
+    return c
+
+
+def octzone_center(cells):
+    """aabb_octree over [-1, 1]^3: cell centres in float32 (octree.h:944-955)."""
+    c = np.asarray(cells, np.int64).reshape(-1, 4)
+    w = (np.float32(2.0) / (np.int64(1) << c[:, 0]).astype(np.float32)).astype(np.float32)
+    p = c[:, 1:4].astype(np.float32)
+    lo = (np.float32(-1.0) + (w[:, None] * p).astype(np.float32)).astype(np.float32)
+    hi = (np.float32(-1.0) + (w[:, None] * (p + np.float32(1))).astype(np.float32)).astype(np.float32)
+    return ((lo + hi).astype(np.float32) / np.float32(2.0)).astype(np.float32)
+
+
+def octzone_enclosing(p, depth):
+    """aabb_octree::enclosing (octree.h:957-965)."""
+    w = np.float32(1.0) / np.float32(1 << depth)
+    t = (((np.asarray(p, np.float32) - np.float32(-1.0)).astype(np.float32) / np.float32(2.0)).astype(np.float32)
+         / w).astype(np.float32)
+    return tuple(int(v) for v in np.floor(t))
+
+
+def stable_nodes(nodes, project):
+    """find_stable_nodesGPU (upsample.cpp:304-331); project(centres) returns
+    (points, normals) of one projection step without a step limit."""
+    if not nodes:
+        return []
+    pts, nrm = project(octzone_center(nodes))
+    out = []
+    for c, p, n in zip(nodes, np.asarray(pts, np.float32), np.asarray(nrm, np.float32)):
+        l2 = np.float32(n[0] * n[0] + n[1] * n[1] + n[2] * n[2])
+        out.append((0, 0, 0, 0) if l2 < np.float32(0.5) else (c[0],) + octzone_enclosing(p, c[0]))
+    return remove_duplicates(out)
+
+
+def compute_leaves(current, max_depth, total, project):
+    """upsample.cpp:276-289."""
+    for depth in range(max_depth + 1):
+        sub = stable_nodes(current, project)
+        current = [child(c, k) for c in sub for k in range(8)]
+        current = expand(current, depth + 1)
+        total.extend(current)
+    return current
+
+
+def relative_depth(nodes, mx, mn):
+    """getRelativeDepth (upsample.cpp:146-160); mx/mn are updated in place."""
+    if not nodes:
+        return 0
+    for c in nodes:
+        a = ancestor_at(c, 0)
+        for k in range(3):
+            mn[k] = min(mn[k], a[k + 1])
+            mx[k] = max(mx[k], a[k + 1])
+    dd = 0
+    for k in range(3):
+        dd = max(dd, int(np.ceil(np.float32(np.log2(float(mx[k] - mn[k] + 1))))))
+    return dd
+
+
+def generate(max_depth, project):
+    """OctreeGenerator::generate (upsample.cpp:228-251): the collected
+    candidates (total_tree), cut to the adaptive maximum depth."""
+    depth0 = [(0, 0, 0, 0)]
+    old, total = [], []
+    max_rel = max_depth
+    mn = [2**31 - 1] * 3
+    mx = [-(2**31 - 1)] * 3
+    while depth0:
+        total.extend(depth0)
+        current = compute_leaves(depth0, max_rel, total, project)
+        max_rel = max(0, max_depth - relative_depth(current, mx, mn))
+        old.extend(depth0)
+        depth0 = remove_duplicates([ancestor_at(c, 0) for c in current])
+        depth0 = expand(depth0)
+        seen = set(old)
+        depth0 = [c for c in depth0 if c not in seen]
+    total = [ancestor_at(c, max_rel) for c in total]
+    return remove_duplicates(total)
+
+
+def uniformize(nodes, max_depth, cut=False):
+    """uniformize + retreiveCorrectRoot (upsample.cpp:262-273, :369-402):
+    (cells, new_diag, new_origin)."""
+    nodes = list(nodes) + remove_duplicates([ancestor_at(c, 0) for c in nodes])
+    d0 = [c for c in nodes if c[0] == 0]
+    mn = [min(c[k + 1] for c in d0) for k in range(3)]
+    mx = [max(c[k + 1] for c in d0) for k in range(3)]
+    dd = max(int(np.ceil(np.float32(np.log2(float(mx[k] - mn[k] + 1))))) for k in range(3))
+    diag, origin = 1.0, (0.0, 0.0, 0.0)
+    if dd > 0:
+        nodes = [(c[0] + dd, c[1] - mn[0] * (1 << c[0]), c[2] - mn[1] * (1 << c[0]), c[3] - mn[2] * (1 << c[0]))
+                 for c in nodes]
+        diag, origin = float(1 << dd), tuple(float(v) for v in mn)
+    nodes = grade(remove_duplicates(nodes))
+    nodes = regularize_up(nodes)
+    if cut:
+        nodes = [c for c in nodes if c[0] <= max_depth]
+    nodes = regularize_siblings(nodes)
+    return np.array(nodes, np.int32).reshape(-1, 4), diag, origin

@@ -1,0 +1,152 @@
+"""Projection server: requests mixed across trees, sizes and kernels give the
+same results as projecting each request alone; waits are bounded;
+admission refuses requests beyond the pending limit; closing with queued
+work neither hangs nor leaks."""
+import threading
+
+import numpy as np
+import pytest
+
+from mlodsurfaces_b200 import APSSOctree, Fastapss, ProjectionServer, synth
+from mlodsurfaces_b200 import _capi as capi
+from mlodsurfaces_b200._capi import BLEND_CPU, MlodsError
+from conftest import make_kernel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def projectors():
+    out = []
+    for i, (pts, nrm) in enumerate([synth.torus(40000, seed=61), synth.torus_knot(30000, seed=62),
+                                    synth.rbf_blobs(20000, seed=63, translate=0.0)]):
+        t = APSSOctree()
+        t.build(pts, nrm)
+        diag = synth.bbox_diag(pts)
+        f = Fastapss(t, make_kernel(["gauss", "singular", "multi"][i], diag))
+        f.setScalingProtectionSphere([3.0, 2.0, 2.5][i])
+        if i == 2:
+            f.blend_rule = BLEND_CPU
+        out.append((f, pts, diag))
+    return out
+
+
+def direct(f, q, iters, kernel=None):
+    """The request projected alone through the reference-facing protocol."""
+    if kernel is not None:
+        f.updateKernel(kernel)
+    f.copyPointsToGPU(len(q), q)
+    p = np.empty_like(q)
+    n = np.empty_like(q)
+    f.project(len(q), p, n, iters)
+    return p, n
+
+
+def make_requests(projectors, count, seed):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for j in range(count):
+        ti = int(rng.integers(0, len(projectors)))
+        f, pts, diag = projectors[ti]
+        n = int(np.exp(rng.uniform(np.log(50), np.log(20000))))
+        q = synth.perturbed_queries(pts, 0.01, seed=1000 + j)[:n]
+        iters = int(rng.integers(1, 8))
+        kernel = make_kernel(["gauss", "multi", "singular"][j % 3], diag) if j % 4 == 0 else None
+        reqs.append((ti, q, iters, kernel))
+    return reqs
+
+
+def expected(projectors, reqs):
+    out = []
+    for ti, q, iters, kernel in reqs:
+        f, pts, diag = projectors[ti]
+        p, n = direct(f, q, iters, kernel)
+        if kernel is not None:
+            restore_kernels(projectors)
+        out.append((p, n))
+    return out
+
+
+def restore_kernels(projectors):
+    for i, (f, pts, diag) in enumerate(projectors):
+        f.updateKernel(make_kernel(["gauss", "singular", "multi"][i], diag))
+
+
+def test_mixed_requests_equal_projection_alone(projectors):
+    reqs = make_requests(projectors, 40, seed=5)
+    want = expected(projectors, reqs)
+    restore_kernels(projectors)
+    srv = ProjectionServer([f for f, _, _ in projectors], n_streams=2, max_batch_queries=60000)
+    try:
+        tickets = [srv.submit(ti, q, iters, kernel) for ti, q, iters, kernel in reqs]
+        for t, (wp, wn) in zip(tickets, want):
+            p, n, lat = srv.wait(t, timeout_ms=60000)
+            assert np.array_equal(p, wp) and np.array_equal(n, wn)
+            assert lat > 0
+        st = srv.stats()
+        assert st["completed"] == len(reqs) and st["queued"] == 0
+        assert st["batches"] < len(reqs)  # requests were batched together
+    finally:
+        srv.close()
+
+
+def test_concurrent_submitters(projectors):
+    reqs = make_requests(projectors, 24, seed=9)
+    want = expected(projectors, reqs)
+    restore_kernels(projectors)
+    srv = ProjectionServer([f for f, _, _ in projectors], n_streams=3)
+    results = {}
+    errors = []
+
+    def client(idx):
+        try:
+            for j in idx:
+                ti, q, iters, kernel = reqs[j]
+                t = srv.submit(ti, q, iters, kernel)
+                results[j] = srv.wait(t, timeout_ms=60000)
+        except Exception as e:  # noqa: BLE001
+            errors.append(e)
+
+    threads = [threading.Thread(target=client, args=(range(k, len(reqs), 4),)) for k in range(4)]
+    try:
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join(timeout=120)
+        assert not errors and len(results) == len(reqs)
+        for j, (wp, wn) in enumerate(want):
+            assert np.array_equal(results[j][0], wp) and np.array_equal(results[j][1], wn)
+    finally:
+        srv.close()
+
+
+def test_bounded_wait_admission_and_errors(projectors):
+    f, pts, diag = projectors[0]
+    srv = ProjectionServer([f], n_streams=1, max_pending_queries=300000)
+    try:
+        q = synth.perturbed_queries(pts, 0.01, seed=77)
+        big = np.concatenate([q] * 7)[:280000]
+        t = srv.submit(0, big, 10)
+        with pytest.raises(TimeoutError):
+            srv.wait(t, timeout_ms=0)
+        p, n, _ = srv.wait(t, timeout_ms=120000)  # the ticket is still valid after a timeout
+        assert np.isfinite(p).all()
+        with pytest.raises(MlodsError) as e:
+            srv.submit(0, np.concatenate([q] * 8)[:300001], 1)  # beyond max_pending_queries
+        assert e.value.code == capi.MLODS_ERR_CAPACITY
+        with pytest.raises(MlodsError):
+            srv.wait(987654321)  # unknown ticket
+        with pytest.raises(MlodsError):
+            srv.submit(5, q[:10], 1)  # no such tree
+    finally:
+        srv.close()
+
+
+def test_close_with_queued_work_returns(projectors):
+    f, pts, diag = projectors[1]
+    srv = ProjectionServer([f], n_streams=1)
+    q = synth.perturbed_queries(pts, 0.01, seed=78)
+    for _ in range(20):
+        srv.submit(0, q, 10)
+    srv.close()  # cancels what is queued, finishes the running batch, joins
+    srv.close()
