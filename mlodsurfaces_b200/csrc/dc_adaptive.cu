@@ -1,4 +1,4 @@
-// dc_adaptive.cu -- the projection-driven dual-contouring grid.
+// dc_adaptive.cu -- the projection-driven dual-contouring grid, on the device.
 //
 // OctreeGenerator::generate (upsample.cpp:228-251) refines cells level by
 // level: the centre of every candidate cell is projected once onto the
@@ -10,8 +10,16 @@
 // every level's candidates are collected.  uniformize (:262-273) then shifts
 // the collection under one root (retreiveCorrectRoot / union_nodes,
 // :369-402), grades, completes ancestors and siblings and optionally cuts at
-// the maximum depth.  The projections run on the device (one launch per
-// level); the integer set work stays on the host, as the reference's does.
+// the maximum depth.
+//
+// The reference does the set work with std::sort / std::unique over octree_id
+// vectors on one host thread.  Here a cell is a 64-bit key whose unsigned
+// order is node_comparator's (depth, then z, y, x), every step generates keys
+// with one kernel and a radix sort + unique makes the set; only the few
+// depth-0 cells are handled on the host.  Two steps are regrouped without
+// changing the result: the 26-neighbour expansion of the 8 children of a cell
+// is the 4x4x4 block around them, generated directly; grade runs level by
+// level from the deepest, which is the order the reference's loop visits.
 #include <algorithm>
 #include <cfloat>
 #include <climits>
@@ -19,6 +27,7 @@
 #include <vector>
 
 #include "dc.h"
+#include "primitives.cuh"
 #include "tree.cuh"
 
 namespace mlods
@@ -26,211 +35,641 @@ namespace mlods
 namespace
 {
 using dcg::Cell;
+
+// ---- cell keys: 4 bits depth | 20 bits z | 20 bits y | 20 bits x (biased)
+constexpr int kCoordBits = 20;
+constexpr int kBias = 1 << (kCoordBits - 1);
+constexpr uint64_t kCoordMask = (uint64_t(1) << kCoordBits) - 1;
+constexpr int kMaxKeyDepth = 15;
 // bound on the depth-0 cells explored (the [-1, 1]^3 zone is one of them; a
 // surface normalised into it reaches its 26 neighbours at most)
 constexpr size_t kMaxRootCells = 4096;
 
-// aabb_octree over [-1, 1]^3 (upsample.cpp:307-310): centre of a cell,
-// octree.h:944-955, float arithmetic
-inline void octzone_center(const Cell& c, float out[3])
+__host__ __device__ inline bool encodable(int d, int x, int y, int z)
 {
-    const float w = 2.0f / float(1 << c.depth);
-    const int p[3] = {c.x, c.y, c.z};
-    for (int a = 0; a < 3; ++a) {
-        const float lo = -1.0f + w * float(p[a]);
-        const float hi = -1.0f + w * float(p[a] + 1);
-        out[a] = (lo + hi) / 2.0f;
-    }
+    return d >= 0 && d <= kMaxKeyDepth && x >= -kBias && x < kBias && y >= -kBias && y < kBias && z >= -kBias &&
+           z < kBias;
 }
-
-// float -> int as x86 truncation does for out-of-range values (INT_MIN)
-inline int floor_to_int(float v)
+__host__ __device__ inline uint64_t make_key(int d, int x, int y, int z)
 {
-    const float f = std::floor(v);
-    if (!(f >= -2147483648.0f && f < 2147483648.0f)) return INT_MIN;
-    return int(f);
+    return (uint64_t(d) << 60) | (uint64_t(z + kBias) << 40) | (uint64_t(y + kBias) << 20) | uint64_t(x + kBias);
 }
-
-// aabb_octree::enclosing, octree.h:957-965
-inline Cell octzone_enclosing(const float p[3], int depth)
+__host__ __device__ inline int key_depth(uint64_t k) { return int(k >> 60); }
+__host__ __device__ inline int key_x(uint64_t k) { return int(k & kCoordMask) - kBias; }
+__host__ __device__ inline int key_y(uint64_t k) { return int((k >> 20) & kCoordMask) - kBias; }
+__host__ __device__ inline int key_z(uint64_t k) { return int((k >> 40) & kCoordMask) - kBias; }
+__host__ __device__ inline int fl_half(int v) { return (v < 0 && (v % 2) != 0) ? v / 2 - 1 : v / 2; }
+__host__ __device__ inline uint64_t key_parent(uint64_t k)
 {
-    const float w = 1.0f / float(1 << depth);
-    int c[3];
-    for (int a = 0; a < 3; ++a) c[a] = floor_to_int((p[a] - -1.0f) / 2.0f / w);
-    return Cell{depth, c[0], c[1], c[2]};
+    return make_key(key_depth(k) - 1, fl_half(key_x(k)), fl_half(key_y(k)), fl_half(key_z(k)));
 }
+__host__ __device__ inline uint64_t key_ancestor(uint64_t k, int d)
+{
+    while (key_depth(k) > d) k = key_parent(k);
+    return k;
+}
+inline Cell key_cell(uint64_t k) { return Cell{key_depth(k), key_x(k), key_y(k), key_z(k)}; }
 
-struct Projector {
-    mlods_tree_s* T;
-    cudaStream_t s;
-    float* d_buf = nullptr;
-    size_t cap = 0;
-    int64_t projected = 0;
-    ~Projector() { cudaFree(d_buf); }
+constexpr unsigned kThreads = 256;
+inline unsigned blocks_for(int64_t n) { return unsigned((n + kThreads - 1) / kThreads); }
 
-    // One projection step of the cell centres, no step limit
-    // (find_stable_nodesGPU, upsample.cpp:304-331): the enclosing cell at the
-    // same depth, or the root when the projection failed; sorted, unique.
-    int stable(const std::vector<Cell>& nodes, std::vector<Cell>& out)
+// A set of cells on the device: sorted unique keys plus scratch of the same
+// capacity, grown on demand.
+struct CellSet {
+    uint64_t* a = nullptr;  // the keys
+    uint64_t* b = nullptr;  // scratch keys
+    uint32_t* flags = nullptr;
+    uint32_t* excl = nullptr;
+    uint32_t* d_total = nullptr;
+    void* tmp = nullptr;
+    size_t cap = 0, tmp_cap = 0;
+    int64_t n = 0;
+    ~CellSet()
     {
-        out.clear();
-        const size_t n = nodes.size();
-        if (n == 0) return MLODS_OK;
-        if (cap < n) {
-            cudaFree(d_buf);
-            d_buf = nullptr;
-            cap = 0;
-            MLODS_CUDA(cudaMalloc(&d_buf, n * 9 * sizeof(float)));
-            cap = n;
-        }
-        std::vector<float> h(n * 3), hn(n * 3);
-        for (size_t i = 0; i < n; ++i) octzone_center(nodes[i], &h[3 * i]);
-        float* d_q = d_buf;
-        float* d_p = d_buf + 3 * n;
-        float* d_n = d_buf + 6 * n;
-        MLODS_CUDA(cudaMemcpyAsync(d_q, h.data(), n * 12, cudaMemcpyHostToDevice, s));
-        const int rc = project_buffers(T, int64_t(n), d_q, d_p, d_n, 1, FLT_MAX, s);
-        if (rc != MLODS_OK) return rc;
-        MLODS_CUDA(cudaMemcpyAsync(h.data(), d_p, n * 12, cudaMemcpyDeviceToHost, s));
-        MLODS_CUDA(cudaMemcpyAsync(hn.data(), d_n, n * 12, cudaMemcpyDeviceToHost, s));
-        MLODS_CUDA(cudaStreamSynchronize(s));
-        projected += int64_t(n);
-        out.resize(n);
-        for (size_t i = 0; i < n; ++i) {
-            const float* v = &hn[3 * i];
-            const float l2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-            out[i] = l2 < 0.5f ? Cell{0, 0, 0, 0} : octzone_enclosing(&h[3 * i], nodes[i].depth);
-        }
-        dcg::remove_duplicates(out);
-        return MLODS_OK;
+        cudaFree(a);
+        cudaFree(b);
+        cudaFree(flags);
+        cudaFree(excl);
+        cudaFree(d_total);
+        cudaFree(tmp);
     }
 };
 
-void append(std::vector<Cell>& v, const std::vector<Cell>& a) { v.insert(v.end(), a.begin(), a.end()); }
-
-// compute_leaves, upsample.cpp:276-289
-int compute_leaves(Projector& P, std::vector<Cell> current, int max_depth, std::vector<Cell>& total,
-                   std::vector<Cell>& out)
+int reserve(CellSet& c, int64_t need, bool keep, cudaStream_t s)
 {
-    std::vector<Cell> sub;
-    for (int depth = 0; depth < max_depth + 1; ++depth) {
-        const int rc = P.stable(current, sub);
-        if (rc != MLODS_OK) return rc;
-        current.resize(sub.size() * 8);
-        for (size_t i = 0; i < sub.size(); ++i)
-            for (int k = 0; k < 8; ++k) current[8 * i + size_t(k)] = dcg::child(sub[i], k);
-        dcg::expand(current, depth + 1);
-        append(total, current);
+    if (size_t(need) <= c.cap) return MLODS_OK;
+    const size_t cap = std::max<size_t>(size_t(need), c.cap + c.cap / 2);
+    uint64_t *a = nullptr, *b = nullptr;
+    uint32_t *f = nullptr, *e = nullptr;
+    MLODS_CUDA(cudaMalloc(&a, cap * 8));
+    cudaError_t err = cudaMalloc(&b, cap * 8);
+    if (err == cudaSuccess) err = cudaMalloc(&f, cap * 4);
+    if (err == cudaSuccess) err = cudaMalloc(&e, cap * 4);
+    if (err == cudaSuccess && !c.d_total) err = cudaMalloc(&c.d_total, 256);
+    if (err == cudaSuccess && keep && c.n > 0) err = cudaMemcpyAsync(a, c.a, size_t(c.n) * 8, cudaMemcpyDeviceToDevice, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) {
+        cudaFree(a);
+        cudaFree(b);
+        cudaFree(f);
+        cudaFree(e);
+        return cuda_fail(err, "dc cells: grow", __FILE__, __LINE__);
     }
-    out.swap(current);
+    cudaFree(c.a);
+    cudaFree(c.b);
+    cudaFree(c.flags);
+    cudaFree(c.excl);
+    c.a = a;
+    c.b = b;
+    c.flags = f;
+    c.excl = e;
+    c.cap = cap;
+    const size_t tb = std::max(radix_temp_bytes(int64_t(cap)), scan_temp_bytes(int64_t(cap)));
+    if (tb > c.tmp_cap) {
+        cudaFree(c.tmp);
+        c.tmp = nullptr;
+        c.tmp_cap = 0;
+        MLODS_CUDA(cudaMalloc(&c.tmp, tb));
+        c.tmp_cap = tb;
+    }
     return MLODS_OK;
 }
 
-// getRelativeDepth, upsample.cpp:146-160 (min/max persist across calls)
-int relative_depth(const std::vector<Cell>& nodes, int mx[3], int mn[3])
+__global__ void unique_flags_kernel(const uint64_t* __restrict__ k, int64_t n, uint32_t* __restrict__ f)
 {
-    if (nodes.empty()) return 0;
-    for (const Cell& n : nodes) {
-        const Cell a = dcg::ancestor_at(n, 0);
-        const int p[3] = {a.x, a.y, a.z};
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = std::min(mn[k], p[k]);
-            mx[k] = std::max(mx[k], p[k]);
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) f[i] = (i == 0 || k[i] != k[i - 1]) ? 1u : 0u;
+}
+
+__global__ void compact_kernel(const uint64_t* __restrict__ k, const uint32_t* __restrict__ f,
+                               const uint32_t* __restrict__ e, int64_t n, uint64_t* __restrict__ out)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n && f[i]) out[e[i]] = k[i];
+}
+
+// Sorts c.a[0, c.n) and removes duplicates in place.
+int sort_unique(CellSet& c, cudaStream_t s)
+{
+    if (c.n <= 1) return MLODS_OK;
+    bool alt = false;
+    MLODS_CUDA(radix_sort_pairs_u64(c.a, nullptr, c.b, nullptr, c.n, 64, &alt, c.tmp, s));
+    if (alt) std::swap(c.a, c.b);
+    unique_flags_kernel<<<blocks_for(c.n), kThreads, 0, s>>>(c.a, c.n, c.flags);
+    note_launch();
+    MLODS_CUDA(cudaGetLastError());
+    MLODS_CUDA(exclusive_scan_u32(c.flags, c.excl, c.n, c.d_total, c.tmp, s));
+    compact_kernel<<<blocks_for(c.n), kThreads, 0, s>>>(c.a, c.flags, c.excl, c.n, c.b);
+    note_launch();
+    MLODS_CUDA(cudaGetLastError());
+    uint32_t total = 0;
+    MLODS_CUDA(cudaMemcpyAsync(&total, c.d_total, 4, cudaMemcpyDeviceToHost, s));
+    MLODS_CUDA(cudaStreamSynchronize(s));
+    std::swap(c.a, c.b);
+    c.n = int64_t(total);
+    return MLODS_OK;
+}
+
+// Appends n keys from device memory.
+int append(CellSet& c, const uint64_t* d_keys, int64_t n, cudaStream_t s)
+{
+    if (n <= 0) return MLODS_OK;
+    int rc = reserve(c, c.n + n, true, s);
+    if (rc != MLODS_OK) return rc;
+    MLODS_CUDA(cudaMemcpyAsync(c.a + c.n, d_keys, size_t(n) * 8, cudaMemcpyDeviceToDevice, s));
+    c.n += n;
+    return MLODS_OK;
+}
+
+int upload(CellSet& c, const std::vector<uint64_t>& keys, cudaStream_t s)
+{
+    c.n = 0;
+    int rc = reserve(c, int64_t(keys.size()), false, s);
+    if (rc != MLODS_OK) return rc;
+    if (!keys.empty()) MLODS_CUDA(cudaMemcpyAsync(c.a, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice, s));
+    MLODS_CUDA(cudaStreamSynchronize(s));
+    c.n = int64_t(keys.size());
+    return MLODS_OK;
+}
+
+int download(const CellSet& c, std::vector<uint64_t>& keys, cudaStream_t s)
+{
+    keys.resize(size_t(c.n));
+    if (c.n) MLODS_CUDA(cudaMemcpyAsync(keys.data(), c.a, size_t(c.n) * 8, cudaMemcpyDeviceToHost, s));
+    MLODS_CUDA(cudaStreamSynchronize(s));
+    return MLODS_OK;
+}
+
+// ---- kernels of the generator
+
+// aabb_octree over [-1, 1]^3: cell centre, float arithmetic (octree.h:944-955)
+__global__ void centres_kernel(const uint64_t* __restrict__ k, int64_t n, float* __restrict__ out)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t key = k[i];
+    const float w = __fdiv_rn(2.0f, float(1 << key_depth(key)));
+    const int p[3] = {key_x(key), key_y(key), key_z(key)};
+    for (int a = 0; a < 3; ++a) {
+        const float lo = __fadd_rn(-1.0f, __fmul_rn(w, float(p[a])));
+        const float hi = __fadd_rn(-1.0f, __fmul_rn(w, float(p[a] + 1)));
+        out[3 * i + a] = __fdiv_rn(__fadd_rn(lo, hi), 2.0f);
+    }
+}
+
+// find_stable_nodesGPU's per-cell step: the cell at the same depth enclosing
+// the projected centre (aabb_octree::enclosing, octree.h:957-965), or the
+// root when the projection failed (|n|^2 < 0.5) or lands outside the key range
+__global__ void enclosing_kernel(const uint64_t* __restrict__ k, int64_t n, const float* __restrict__ p,
+                                 const float* __restrict__ nv, uint64_t* __restrict__ out)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int d = key_depth(k[i]);
+    const float n0 = nv[3 * i], n1 = nv[3 * i + 1], n2 = nv[3 * i + 2];
+    const float l2 = __fadd_rn(__fadd_rn(__fmul_rn(n0, n0), __fmul_rn(n1, n1)), __fmul_rn(n2, n2));
+    uint64_t r = make_key(0, 0, 0, 0);
+    if (!(l2 < 0.5f)) {
+        const float w = __fdiv_rn(1.0f, float(1 << d));
+        int c[3];
+        bool ok = true;
+        for (int a = 0; a < 3; ++a) {
+            const float t = floorf(__fdiv_rn(__fdiv_rn(__fsub_rn(p[3 * i + a], -1.0f), 2.0f), w));
+            ok = ok && t >= float(-kBias) && t < float(kBias);
+            c[a] = ok ? int(t) : 0;
         }
+        if (ok) r = make_key(d, c[0], c[1], c[2]);
     }
-    int dd = 0;
-    for (int k = 0; k < 3; ++k) {
-        const int ext = mx[k] - mn[k] + 1;
-        dd = std::max(dd, int(std::ceil(float(std::log2(double(ext))))));  // int extent: log2 in double
+    out[i] = r;
+}
+
+// compute_leaves' children + expand(depth + 1): a kept cell at the level
+// depth gives the 4x4x4 block around its children (the union of their
+// 27-neighbourhoods); a root kept for a failed projection deeper down gives
+// its 8 children only (they are not at depth + 1, so not expanded)
+__global__ void children_block_kernel(const uint64_t* __restrict__ k, int64_t n, int depth,
+                                      uint64_t* __restrict__ out, const int64_t* __restrict__ out_off)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t key = k[i];
+    const int d = key_depth(key);
+    const int x = 2 * key_x(key), y = 2 * key_y(key), z = 2 * key_z(key);
+    uint64_t* o = out + out_off[i];
+    if (d == depth) {
+        int m = 0;
+        for (int dz = -1; dz <= 2; ++dz)
+            for (int dy = -1; dy <= 2; ++dy)
+                for (int dx = -1; dx <= 2; ++dx) o[m++] = make_key(d + 1, x + dx, y + dy, z + dz);
+    } else {
+        for (int c = 0; c < 8; ++c) o[c] = make_key(d + 1, x + (c & 1), y + ((c >> 1) & 1), z + ((c >> 2) & 1));
     }
-    return dd;
 }
 
-std::vector<Cell> depth0_ancestors(std::vector<Cell> nodes)
+__global__ void block_sizes_kernel(const uint64_t* __restrict__ k, int64_t n, int depth, int64_t* __restrict__ sz)
 {
-    for (Cell& n : nodes) n = dcg::ancestor_at(n, 0);
-    dcg::remove_duplicates(nodes);
-    return nodes;
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) sz[i] = key_depth(k[i]) == depth ? 64 : 8;
 }
 
-// onlySetDepthNodes, upsample.cpp:162-172
-void only_set_depth(std::vector<Cell>& nodes, int depth)
+__global__ void ancestor_kernel(const uint64_t* __restrict__ k, int64_t n, int depth, uint64_t* __restrict__ out)
 {
-    for (Cell& n : nodes)
-        if (n.depth > depth) n = dcg::ancestor_at(n, depth);
-    dcg::remove_duplicates(nodes);
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = key_ancestor(k[i], depth);
 }
 
-// OctreeGenerator::generate, upsample.cpp:228-251; returns the collected
-// candidates (the reference's total_tree) cut to the adaptive maximum depth
-int generate(Projector& P, int max_depth, std::vector<Cell>& total)
+// min / max of the depth-0 ancestors' positions (getRelativeDepth, union_nodes)
+__global__ void root_box_kernel(const uint64_t* __restrict__ k, int64_t n, int only_depth0, int* __restrict__ mm)
 {
-    std::vector<Cell> depth0 = {Cell{0, 0, 0, 0}}, old_depth0, current;
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (only_depth0 && key_depth(k[i]) != 0) return;
+    const uint64_t a = key_ancestor(k[i], 0);
+    const int p[3] = {key_x(a), key_y(a), key_z(a)};
+    for (int c = 0; c < 3; ++c) {
+        atomicMin(mm + c, p[c]);
+        atomicMax(mm + 3 + c, p[c]);
+    }
+}
+
+// union_nodes' shift: pos -= min * 2^depth, depth += dd
+__global__ void shift_kernel(uint64_t* __restrict__ k, int64_t n, int mx, int my, int mz, int dd, int* bad)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t key = k[i];
+    const int d = key_depth(key);
+    const int s = 1 << d;
+    const int x = key_x(key) - mx * s, y = key_y(key) - my * s, z = key_z(key) - mz * s;
+    if (!encodable(d + dd, x, y, z)) {
+        atomicExch(bad, 1);
+        return;
+    }
+    k[i] = make_key(d + dd, x, y, z);
+}
+
+// grade's step for the cells of one depth: parents of the 8 corner neighbours
+// (neighbour ids 0, 2, 6, 8, 18, 20, 24, 26, upsample.cpp:69)
+__global__ void grade_kernel(const uint64_t* __restrict__ k, int64_t n, uint64_t* __restrict__ out)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t key = k[i];
+    const int d = key_depth(key), x = key_x(key), y = key_y(key), z = key_z(key);
+    for (int c = 0; c < 8; ++c) {
+        const int dx = (c & 1) ? 1 : -1, dy = (c & 2) ? 1 : -1, dz = (c & 4) ? 1 : -1;
+        out[8 * i + c] = make_key(d - 1, fl_half(x + dx), fl_half(y + dy), fl_half(z + dz));
+    }
+}
+
+__global__ void parent_kernel(const uint64_t* __restrict__ k, int64_t n, uint64_t* __restrict__ out)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = key_parent(k[i]);
+}
+
+// regularize_siblings: the 8 children of every non-root cell's parent; a
+// depth-0 cell contributes the root (the default octree_id), upsample.cpp:48-65
+__global__ void siblings_kernel(const uint64_t* __restrict__ k, int64_t n, uint64_t* __restrict__ out)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t key = k[i];
+    if (key_depth(key) <= 0) {
+        for (int c = 0; c < 8; ++c) out[8 * i + c] = make_key(0, 0, 0, 0);
+        return;
+    }
+    const uint64_t p = key_parent(key);
+    const int d = key_depth(key), x = 2 * key_x(p), y = 2 * key_y(p), z = 2 * key_z(p);
+    for (int c = 0; c < 8; ++c) out[8 * i + c] = make_key(d, x + (c & 1), y + ((c >> 1) & 1), z + ((c >> 2) & 1));
+}
+
+__global__ void depth_hist_kernel(const uint64_t* __restrict__ k, int64_t n, unsigned long long* __restrict__ h)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(h + key_depth(k[i]), 1ull);
+}
+
+// ---- host orchestration
+
+struct Gen {
+    mlods_tree_s* T;
+    cudaStream_t s;
+    int64_t projected = 0;
+    float* d_proj = nullptr;  // 9 floats per cell (centre, projection, normal)
+    size_t proj_cap = 0;
+    int64_t* d_off = nullptr;
+    size_t off_cap = 0;
+    int* d_mm = nullptr;
+    unsigned long long* d_hist = nullptr;
+    ~Gen()
+    {
+        cudaFree(d_proj);
+        cudaFree(d_off);
+        cudaFree(d_mm);
+        cudaFree(d_hist);
+    }
+
+    // first key of each depth of a sorted set (17 entries)
+    int depth_ranges(const CellSet& c, int64_t begin[17])
+    {
+        if (!d_hist) MLODS_CUDA(cudaMalloc(&d_hist, 16 * sizeof(unsigned long long)));
+        MLODS_CUDA(cudaMemsetAsync(d_hist, 0, 16 * sizeof(unsigned long long), s));
+        if (c.n) {
+            depth_hist_kernel<<<blocks_for(c.n), kThreads, 0, s>>>(c.a, c.n, d_hist);
+            note_launch();
+            MLODS_CUDA(cudaGetLastError());
+        }
+        unsigned long long h[16];
+        MLODS_CUDA(cudaMemcpyAsync(h, d_hist, sizeof h, cudaMemcpyDeviceToHost, s));
+        MLODS_CUDA(cudaStreamSynchronize(s));
+        begin[0] = 0;
+        for (int d = 0; d < 16; ++d) begin[d + 1] = begin[d] + int64_t(h[d]);
+        return MLODS_OK;
+    }
+
+    // find_stable_nodesGPU: out = sorted unique enclosing cells of the
+    // projected centres of `cur`
+    int stable(const CellSet& cur, CellSet& out)
+    {
+        out.n = 0;
+        if (cur.n == 0) return MLODS_OK;
+        const int64_t n = cur.n;
+        if (proj_cap < size_t(n)) {
+            cudaFree(d_proj);
+            d_proj = nullptr;
+            proj_cap = 0;
+            MLODS_CUDA(cudaMalloc(&d_proj, size_t(n) * 36));
+            proj_cap = size_t(n);
+        }
+        float* c = d_proj;
+        float* p = d_proj + 3 * n;
+        float* nv = d_proj + 6 * n;
+        centres_kernel<<<blocks_for(n), kThreads, 0, s>>>(cur.a, n, c);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+        const int rc = project_buffers(T, n, c, p, nv, 1, FLT_MAX, s);
+        if (rc != MLODS_OK) return rc;
+        projected += n;
+        int r2 = reserve(out, n, false, s);
+        if (r2 != MLODS_OK) return r2;
+        enclosing_kernel<<<blocks_for(n), kThreads, 0, s>>>(cur.a, n, p, nv, out.a);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+        out.n = n;
+        return sort_unique(out, s);
+    }
+
+    // children + 26-neighbour expansion of the kept cells of level `depth`
+    int children(const CellSet& sub, int depth, CellSet& out)
+    {
+        out.n = 0;
+        const int64_t n = sub.n;
+        if (n == 0) return MLODS_OK;
+        if (off_cap < size_t(n) + 1) {
+            cudaFree(d_off);
+            d_off = nullptr;
+            off_cap = 0;
+            MLODS_CUDA(cudaMalloc(&d_off, (size_t(n) + 1) * 8));
+            off_cap = size_t(n) + 1;
+        }
+        block_sizes_kernel<<<blocks_for(n), kThreads, 0, s>>>(sub.a, n, depth, d_off);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+        // offsets on the host: sub is at most a few million cells
+        std::vector<int64_t> h(size_t(n) + 1);
+        MLODS_CUDA(cudaMemcpyAsync(h.data(), d_off, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
+        MLODS_CUDA(cudaStreamSynchronize(s));
+        int64_t acc = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const int64_t v = h[size_t(i)];
+            h[size_t(i)] = acc;
+            acc += v;
+        }
+        MLODS_CUDA(cudaMemcpyAsync(d_off, h.data(), size_t(n) * 8, cudaMemcpyHostToDevice, s));
+        int rc = reserve(out, acc, false, s);
+        if (rc != MLODS_OK) return rc;
+        children_block_kernel<<<blocks_for(n), kThreads, 0, s>>>(sub.a, n, depth, out.a, d_off);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+        MLODS_CUDA(cudaStreamSynchronize(s));
+        out.n = acc;
+        return sort_unique(out, s);
+    }
+
+    int root_box(const CellSet& c, bool only_depth0, int mn[3], int mx[3], bool* any)
+    {
+        if (!d_mm) MLODS_CUDA(cudaMalloc(&d_mm, 8 * sizeof(int)));
+        const int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+        MLODS_CUDA(cudaMemcpyAsync(d_mm, init, sizeof init, cudaMemcpyHostToDevice, s));
+        if (c.n) {
+            root_box_kernel<<<blocks_for(c.n), kThreads, 0, s>>>(c.a, c.n, only_depth0 ? 1 : 0, d_mm);
+            note_launch();
+            MLODS_CUDA(cudaGetLastError());
+        }
+        int h[6];
+        MLODS_CUDA(cudaMemcpyAsync(h, d_mm, sizeof h, cudaMemcpyDeviceToHost, s));
+        MLODS_CUDA(cudaStreamSynchronize(s));
+        *any = h[0] != INT_MAX;
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = h[k];
+            mx[k] = h[3 + k];
+        }
+        return MLODS_OK;
+    }
+
+    // keys at `depth` of a sorted set -> launch(keys, n, out) writes per_key
+    // keys each; they are added to the set, which is sorted again
+    template <typename Launch>
+    int grow_level(CellSet& set, int depth, int per_key, CellSet& scratch, Launch launch)
+    {
+        int64_t begin[17];
+        int rc = depth_ranges(set, begin);
+        if (rc != MLODS_OK) return rc;
+        const int64_t n = begin[depth + 1] - begin[depth];
+        if (n == 0) return MLODS_OK;
+        rc = reserve(scratch, n * per_key, false, s);
+        if (rc != MLODS_OK) return rc;
+        launch(set.a + begin[depth], n, scratch.a);
+        MLODS_CUDA(cudaGetLastError());
+        rc = append(set, scratch.a, n * per_key, s);
+        if (rc != MLODS_OK) return rc;
+        return sort_unique(set, s);
+    }
+};
+
+int log2_ceil_extent(int ext) { return int(std::ceil(float(std::log2(double(ext))))); }
+
+// OctreeGenerator::generate: the collected candidates, cut to the adaptive
+// maximum depth, sorted and unique, in `total`
+int generate(Gen& G, int max_depth, CellSet& total)
+{
+    cudaStream_t s = G.s;
+    std::vector<uint64_t> depth0 = {make_key(0, 0, 0, 0)};
+    std::vector<uint64_t> old_depth0;
     int max_rel = max_depth;
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {-INT_MAX, -INT_MAX, -INT_MAX};
-    total.clear();
+    CellSet cur, sub;
+    total.n = 0;
     while (!depth0.empty()) {
-        append(total, depth0);
-        const int rc = compute_leaves(P, depth0, max_rel, total, current);
+        int rc = upload(cur, depth0, s);
         if (rc != MLODS_OK) return rc;
-        max_rel = std::max(0, max_depth - relative_depth(current, mx, mn));
-        append(old_depth0, depth0);
-        if (old_depth0.size() > kMaxRootCells) {
+        rc = append(total, cur.a, cur.n, s);
+        if (rc != MLODS_OK) return rc;
+        for (int depth = 0; depth < max_rel + 1; ++depth) {  // compute_leaves
+            if (depth + 1 > kMaxKeyDepth) {
+                set_last_error("dc adaptive grid: depth %d beyond the supported %d", depth + 1, kMaxKeyDepth);
+                return MLODS_ERR_CAPACITY;
+            }
+            rc = G.stable(cur, sub);
+            if (rc == MLODS_OK) rc = G.children(sub, depth, cur);
+            if (rc == MLODS_OK) rc = append(total, cur.a, cur.n, s);
+            if (rc != MLODS_OK) return rc;
+        }
+        // getRelativeDepth with the running min / max
+        int cmn[3], cmx[3];
+        bool any = false;
+        rc = G.root_box(cur, false, cmn, cmx, &any);
+        if (rc != MLODS_OK) return rc;
+        int rd = 0;
+        if (any) {
+            for (int k = 0; k < 3; ++k) {
+                mn[k] = std::min(mn[k], cmn[k]);
+                mx[k] = std::max(mx[k], cmx[k]);
+            }
+            for (int k = 0; k < 3; ++k) rd = std::max(rd, log2_ceil_extent(mx[k] - mn[k] + 1));
+        }
+        max_rel = std::max(0, max_depth - rd);
+        old_depth0.insert(old_depth0.end(), depth0.begin(), depth0.end());
+        // depth0_ancestors(current), expand(-1), minus the cells already explored
+        CellSet anc;
+        rc = reserve(anc, cur.n, false, s);
+        if (rc != MLODS_OK) return rc;
+        if (cur.n) {
+            ancestor_kernel<<<blocks_for(cur.n), kThreads, 0, s>>>(cur.a, cur.n, 0, anc.a);
+            note_launch();
+            MLODS_CUDA(cudaGetLastError());
+        }
+        anc.n = cur.n;
+        rc = sort_unique(anc, s);
+        std::vector<uint64_t> a0;
+        if (rc == MLODS_OK) rc = download(anc, a0, s);
+        if (rc != MLODS_OK) return rc;
+        std::vector<Cell> next;
+        for (uint64_t k : a0) next.push_back(key_cell(k));
+        dcg::expand(next, -1);
+        std::vector<uint64_t> seen = old_depth0;
+        std::sort(seen.begin(), seen.end());
+        depth0.clear();
+        for (const Cell& c : next) {
+            if (!encodable(c.depth, c.x, c.y, c.z)) continue;
+            const uint64_t k = make_key(c.depth, c.x, c.y, c.z);
+            if (!std::binary_search(seen.begin(), seen.end(), k)) depth0.push_back(k);
+        }
+        if (old_depth0.size() + depth0.size() > kMaxRootCells) {
             set_last_error("dc adaptive grid: the surface spans more than %zu unit cells", kMaxRootCells);
             return MLODS_ERR_CAPACITY;
         }
-        depth0 = depth0_ancestors(current);
-        dcg::expand(depth0, -1);
-        // vector_difference_inplace, upsample.cpp:103-112
-        std::vector<Cell> seen = old_depth0;
-        dcg::remove_duplicates(seen);
-        depth0.erase(std::remove_if(depth0.begin(), depth0.end(),
-                                    [&](const Cell& c) {
-                                        return std::binary_search(seen.begin(), seen.end(), c, dcg::cell_less);
-                                    }),
-                     depth0.end());
     }
-    only_set_depth(total, max_rel);
-    return MLODS_OK;
+    // onlySetDepthNodes(total_tree, max_rel)
+    CellSet tmp;
+    int rc = reserve(tmp, total.n, false, s);
+    if (rc != MLODS_OK) return rc;
+    if (total.n) {
+        ancestor_kernel<<<blocks_for(total.n), kThreads, 0, s>>>(total.a, total.n, max_rel, tmp.a);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+        MLODS_CUDA(cudaMemcpyAsync(total.a, tmp.a, size_t(total.n) * 8, cudaMemcpyDeviceToDevice, s));
+    }
+    return sort_unique(total, s);
 }
 
-// union_nodes + retreiveCorrectRoot, upsample.cpp:369-402
-void correct_root(std::vector<Cell>& nodes, float new_diag[3], float new_origin[3])
+// uniformize (upsample.cpp:262-273) on the device
+int uniformize(Gen& G, CellSet& nodes, int max_depth, bool cut, float nd[3], float no[3])
 {
-    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {-INT_MAX, -INT_MAX, -INT_MAX};
-    bool has0 = false;
-    for (const Cell& n : nodes) {
-        if (n.depth != 0) continue;
-        const int p[3] = {n.x, n.y, n.z};
-        for (int k = 0; k < 3; ++k) {
-            mn[k] = std::min(mn[k], p[k]);
-            mx[k] = std::max(mx[k], p[k]);
-        }
-        has0 = true;
+    cudaStream_t s = G.s;
+    CellSet scratch;
+    // nodes + depth0_ancestors(nodes)
+    int rc = reserve(scratch, nodes.n, false, s);
+    if (rc != MLODS_OK) return rc;
+    if (nodes.n) {
+        ancestor_kernel<<<blocks_for(nodes.n), kThreads, 0, s>>>(nodes.a, nodes.n, 0, scratch.a);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
     }
+    rc = append(nodes, scratch.a, nodes.n, s);
+    if (rc == MLODS_OK) rc = sort_unique(nodes, s);
+    if (rc != MLODS_OK) return rc;
+    // retreiveCorrectRoot / union_nodes
+    int mn[3], mx[3];
+    bool any = false;
+    rc = G.root_box(nodes, true, mn, mx, &any);
+    if (rc != MLODS_OK) return rc;
     int dd = 0;
-    if (has0)
-        for (int k = 0; k < 3; ++k) dd = std::max(dd, int(std::ceil(float(std::log2(double(mx[k] - mn[k] + 1))))));
-    if (!has0 || dd == 0) {
-        // the reference returns depth -1 here and then evaluates 1 << -1; a
-        // single depth-0 cell needs no shift, so keep the unit frame
-        for (int k = 0; k < 3; ++k) {
-            new_diag[k] = 1.0f;
-            new_origin[k] = 0.0f;
-        }
-        return;
-    }
-    for (Cell& n : nodes) {
-        const int s = 1 << n.depth;
-        n.x -= mn[0] * s;
-        n.y -= mn[1] * s;
-        n.z -= mn[2] * s;
-        n.depth += dd;
-    }
+    if (any)
+        for (int k = 0; k < 3; ++k) dd = std::max(dd, log2_ceil_extent(mx[k] - mn[k] + 1));
     for (int k = 0; k < 3; ++k) {
-        new_origin[k] = float(mn[k]);  // unit_octree::bounds(octree_id(0, min)).min()
-        new_diag[k] = float(1 << dd);
+        nd[k] = 1.0f;
+        no[k] = 0.0f;
     }
+    if (any && dd > 0) {
+        int* d_bad = G.d_mm + 6;
+        MLODS_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+        shift_kernel<<<blocks_for(nodes.n), kThreads, 0, s>>>(nodes.a, nodes.n, mn[0], mn[1], mn[2], dd, d_bad);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+        int bad = 0;
+        MLODS_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, s));
+        MLODS_CUDA(cudaStreamSynchronize(s));
+        if (bad) {
+            set_last_error("dc adaptive grid: the shifted grid exceeds the supported depth or extent");
+            return MLODS_ERR_CAPACITY;
+        }
+        rc = sort_unique(nodes, s);  // the shift keeps the order within a depth only
+        if (rc != MLODS_OK) return rc;
+        for (int k = 0; k < 3; ++k) {
+            no[k] = float(mn[k]);
+            nd[k] = float(1 << dd);
+        }
+    }
+    int64_t begin[17];
+    rc = G.depth_ranges(nodes, begin);
+    if (rc != MLODS_OK) return rc;
+    int deepest = 0;
+    for (int d = 0; d < 16; ++d)
+        if (begin[d + 1] > begin[d]) deepest = d;
+    // grade, deepest level first (the order of the reference's loop)
+    for (int d = deepest; d >= 1; --d) {
+        rc = G.grow_level(nodes, d, 8, scratch, [&](const uint64_t* k, int64_t n, uint64_t* out) {
+            grade_kernel<<<blocks_for(n), kThreads, 0, s>>>(k, n, out);
+            note_launch();
+        });
+        if (rc != MLODS_OK) return rc;
+    }
+    // regularize_up: every ancestor
+    for (int d = deepest; d >= 1; --d) {
+        rc = G.grow_level(nodes, d, 1, scratch, [&](const uint64_t* k, int64_t n, uint64_t* out) {
+            parent_kernel<<<blocks_for(n), kThreads, 0, s>>>(k, n, out);
+            note_launch();
+        });
+        if (rc != MLODS_OK) return rc;
+    }
+    if (cut) {
+        rc = G.depth_ranges(nodes, begin);
+        if (rc != MLODS_OK) return rc;
+        nodes.n = begin[std::min(max_depth, 15) + 1];  // sorted by depth: keep the prefix
+    }
+    // regularize_siblings
+    rc = reserve(scratch, nodes.n * 8, false, s);
+    if (rc != MLODS_OK) return rc;
+    if (nodes.n) {
+        siblings_kernel<<<blocks_for(nodes.n), kThreads, 0, s>>>(nodes.a, nodes.n, scratch.a);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+    }
+    rc = append(nodes, scratch.a, nodes.n * 8, s);
+    if (rc != MLODS_OK) return rc;
+    return sort_unique(nodes, s);
 }
 
 }  // namespace
@@ -238,8 +677,8 @@ void correct_root(std::vector<Cell>& nodes, float new_diag[3], float new_origin[
 int dcgrid_adaptive(mlods_tree_s* T, int max_depth, bool cut, cudaStream_t s, std::vector<int32_t>& cells_out,
                     int& depth_out, float xform[12], int64_t* n_projected)
 {
-    if (max_depth < 0 || max_depth > 14) {
-        set_last_error("dc adaptive grid: max_depth=%d out of range [0, 14]", max_depth);
+    if (max_depth < 0 || max_depth > 12) {
+        set_last_error("dc adaptive grid: max_depth=%d out of range [0, 12]", max_depth);
         return MLODS_ERR_INVALID;
     }
     if (!T->kernel_set) {
@@ -250,22 +689,21 @@ int dcgrid_adaptive(mlods_tree_s* T, int max_depth, bool cut, cudaStream_t s, st
     // global) projection even when the octree is in kNN / ball mode
     const int saved_mode = T->params.mode;
     if (saved_mode == MLODS_MODE_KNN || saved_mode == MLODS_MODE_BALL) T->params.mode = MLODS_MODE_MLOD;
-    Projector P{T, s};
-    std::vector<Cell> nodes;
-    const int rc = generate(P, max_depth, nodes);
+    Gen G{T, s};
+    CellSet nodes;
+    int rc = generate(G, max_depth, nodes);
     T->params.mode = saved_mode;
     if (rc != MLODS_OK) return rc;
-    if (n_projected) *n_projected = P.projected;
-    // uniformize, upsample.cpp:262-273
-    append(nodes, depth0_ancestors(nodes));
+    if (n_projected) *n_projected = G.projected;
     float nd[3], no[3];
-    correct_root(nodes, nd, no);
-    dcg::grade(nodes);
-    dcg::regularize_up(nodes);
-    if (cut) nodes.erase(std::remove_if(nodes.begin(), nodes.end(), [&](const Cell& c) { return c.depth > max_depth; }),
-                         nodes.end());
-    dcg::regularize_siblings(nodes);
-    dcg::cells_to_ints(nodes, cells_out, depth_out);
+    rc = uniformize(G, nodes, max_depth, cut, nd, no);
+    if (rc != MLODS_OK) return rc;
+    std::vector<uint64_t> keys;
+    rc = download(nodes, keys, s);
+    if (rc != MLODS_OK) return rc;
+    std::vector<Cell> cells(keys.size());
+    for (size_t i = 0; i < keys.size(); ++i) cells[i] = key_cell(keys[i]);
+    dcg::cells_to_ints(cells, cells_out, depth_out);
     // new2bbox = unit2bbox * sortedOctreeToUnit (scene.cpp:1259-1311), box [-1, 1]^3
     for (int r = 0; r < 3; ++r) {
         for (int c = 0; c < 4; ++c) xform[4 * r + c] = 0.f;

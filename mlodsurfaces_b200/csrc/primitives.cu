@@ -125,7 +125,7 @@ __global__ void radix_scatter_kernel(const uint64_t* __restrict__ keys, const ui
         const int64_t i = base + int64_t(k) * kSortThreads + threadIdx.x;
         const bool valid = i < n;
         const uint64_t key = valid ? keys[i] : 0ull;
-        const uint32_t val = valid ? vals[i] : 0u;
+        const uint32_t val = (valid && vals) ? vals[i] : 0u;  // vals == nullptr: keys only
         const uint32_t d = valid ? uint32_t((key >> shift) & 255u) : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t rank = __popc(peers & lt_mask);
@@ -148,7 +148,7 @@ __global__ void radix_scatter_kernel(const uint64_t* __restrict__ keys, const ui
         }
         if (valid) {
             keys_out[pos] = key;
-            vals_out[pos] = val;
+            if (vals_out) vals_out[pos] = val;
         }
         __syncthreads();
     }

@@ -18,7 +18,8 @@ cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, uin
 // Stable sort of (key, value) pairs by key bits [0, nbits), least significant
 // digit first, 8 bits per pass.  Keys/values are ping-ponged between the two
 // buffers; on return *result_in_alt tells which buffer holds the result.
-// temp must hold radix_temp_bytes(n) bytes.
+// temp must hold radix_temp_bytes(n) bytes.  vals and vals_alt may both be
+// nullptr to sort keys alone.
 size_t radix_temp_bytes(int64_t n);
 cudaError_t radix_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt, int64_t n,
                                  int nbits, bool* result_in_alt, void* temp, cudaStream_t s);

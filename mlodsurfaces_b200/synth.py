@@ -61,14 +61,40 @@ def _blob_field(x, c, rho2):
     return f, g.sum(1)
 
 
+def _newton_torch(x, c, rho2, tau, device):
+    """The Newton projection of rbf_blobs on a torch device (float64)."""
+    import torch
+
+    xt = torch.from_numpy(x).to(device)
+    ct = torch.from_numpy(c).to(device)
+    rt = torch.from_numpy(rho2).to(device)
+
+    def field(v):
+        d = v[:, None, :] - ct[None, :, :]
+        e = torch.exp(-(d * d).sum(-1) / rt[None, :])
+        return e.sum(1), ((-2.0 * e / rt[None, :])[:, :, None] * d).sum(1)
+
+    for _ in range(30):
+        f, g = field(xt)
+        gg = (g * g).sum(1).clamp_min(1e-30)
+        step = ((f - tau) / gg)[:, None] * g
+        done = (f - tau).abs() <= 1e-13
+        xt = torch.where(done[:, None], xt, xt - step)
+        if bool(done.all()):
+            break
+    f, g = field(xt)
+    return xt.cpu().numpy(), f.cpu().numpy(), g.cpu().numpy()
+
+
 def rbf_blobs(n: int, n_blobs: int = 12, noise: float = 0.003, seed: int = 2, tau: float = 0.5,
-              translate: float = 1e3, batch: int = 1 << 18):
+              translate: float = 1e3, batch: int = 1 << 18, device=None):
     """Samples of the level set sum_j exp(-|x-c_j|^2/rho_j^2) = tau.
 
     Centres ~ U[-1, 1]^3, radii ~ U[0.2, 0.5].  Candidates start on the
     single-blob spheres and are Newton-projected onto the union's level set;
     normals are the normalised negative gradient (outward).  After noise the
-    cloud is moved by translate * diag along (1, 1, 1)/sqrt(3).
+    cloud is moved by translate * diag along (1, 1, 1)/sqrt(3).  With a torch
+    `device` the Newton iterations run there (same candidates and noise).
     """
     rng = np.random.default_rng(seed)
     c = rng.uniform(-1.0, 1.0, (n_blobs, 3))
@@ -83,15 +109,18 @@ def rbf_blobs(n: int, n_blobs: int = 12, noise: float = 0.003, seed: int = 2, ta
         u = rng.normal(size=(m, 3))
         u /= np.linalg.norm(u, axis=1, keepdims=True)
         x = c[j] + (rho[j] * s)[:, None] * u
-        act = np.arange(m)
-        for _ in range(30):
-            f, g = _blob_field(x[act], c, rho2)
-            gg = (g * g).sum(1)
-            x[act] = x[act] - ((f - tau) / np.maximum(gg, 1e-30))[:, None] * g
-            act = act[np.abs(f - tau) > 1e-13]
-            if len(act) == 0:
-                break
-        f, g = _blob_field(x, c, rho2)
+        if device is not None:
+            x, f, g = _newton_torch(x, c, rho2, tau, device)
+        else:
+            act = np.arange(m)
+            for _ in range(30):
+                f, g = _blob_field(x[act], c, rho2)
+                gg = (g * g).sum(1)
+                x[act] = x[act] - ((f - tau) / np.maximum(gg, 1e-30))[:, None] * g
+                act = act[np.abs(f - tau) > 1e-13]
+                if len(act) == 0:
+                    break
+            f, g = _blob_field(x, c, rho2)
         gn = np.linalg.norm(g, axis=1)
         ok = (np.abs(f - tau) < 1e-9) & (gn > 1e-6) & np.all(np.abs(x) < 4.0, axis=1)
         pts.append(x[ok])
