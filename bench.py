@@ -47,11 +47,14 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--check-queries", type=int, default=2048, help="queries checked against the FP64 oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["precision", "torus", "dc", "batch"], default="precision",
+    ap.add_argument("--workload", choices=["precision", "torus", "dc", "batch", "serve"], default="precision",
                     help="precision: 2M-point RBF surface, MLoD projection (default); torus: 100k-point torus, "
                          "CPU-path semantics; dc: 5M-point torus knot, adaptive depth-9 dual contouring; "
                          "batch: 64 resident clouds (about 40M points) in one launch")
     ap.add_argument("--clouds", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=0.0, help="serve: request arrivals per second (0 = 70%% of "
+                                                               "the measured capacity)")
+    ap.add_argument("--serve-seconds", type=float, default=20.0)
     ap.add_argument("--dc-depth", type=int, default=9)
     return ap.parse_args()
 
@@ -311,6 +314,34 @@ def run_ours(args, rank, world, local_rank):
     total_ms_max = max_over_ranks([float(sum(step_ms))], world, dev)[0]
     value = job_throughput(world, len(q), args.steps, total_ms_max)
 
+    # ---- the same steps with exact convergence (outputs bit-identical to the
+    # full iteration count: a query stops once its float iterate repeats)
+    conv = None
+    if world == 1:
+        from mlodsurfaces_b200._capi import CONVERGE_EXACT, CONVERGE_OFF
+
+        ref_out = d_p.clone()
+        f.converge = CONVERGE_EXACT
+        f._sync_params()
+        step()
+        torch.cuda.synchronize(dev)
+        conv_ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            conv_ms.append(e0.elapsed_time(e1))
+        same = bool(torch.equal(d_p, ref_out))
+        f.converge = CONVERGE_OFF
+        f._sync_params()
+        conv = {"value": len(q) * args.steps / (sum(conv_ms) / 1e3), "unit": UNIT,
+                "ms_per_step": statistics.mean(conv_ms), "outputs_bit_identical": same,
+                "note": "MLODS_CONVERGE_EXACT: a query stops when its float iterate repeats"}
+
     # ---- end to end through the public C ABI with host buffers (Fastapss protocol)
     h_q = torch.from_numpy(q).pin_memory()
     h_p = torch.empty_like(h_q).pin_memory()
@@ -368,6 +399,7 @@ def run_ours(args, rank, world, local_rank):
                              f" visits per query-iteration); peak {peak_kind}; traffic = DRAM bytes per launch from "
                              f"ncu: the node arrays are read from DRAM about once, later visits hit L1/L2"},
         "kernel_ms": kms,
+        "converge_exact": conv,
         "traversal": {"visits_per_query_iteration": mean_visits / len(q) / args.iters,
                       "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),
                       "max_stack_ranges": max_stack},
@@ -433,6 +465,26 @@ def run_dc(args):
     mesh = f.dc_mesh(grid)
     mesh_ms = 1e3 * (time.perf_counter() - t0)
     v, _, tri = mesh.arrays()
+    # the same pipeline from its parts, timed per stage
+    from mlodsurfaces_b200 import Mesh
+
+    parts = {}
+
+    def timed(name, fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        parts[name] = parts.get(name, 0.0) + 1e3 * (time.perf_counter() - t)
+        return out
+
+    m2 = timed("extract", lambda: Mesh.extract(grid.cells, cf, vx))
+    timed("transform", lambda: m2.transform(grid.xform))
+    timed("project", lambda: m2.project(f, 3))
+    for _ in range(2):
+        timed("smooth", m2.smooth)
+        timed("subdivide", m2.subdivide)
+        timed("project", lambda: m2.project(f, 3))
     value = n_unique * len(step_ms) / (sum(step_ms) / 1e3)
     visits = st["node_visits"]
     kms = statistics.mean(proj_ms)
@@ -457,7 +509,8 @@ def run_dc(args):
                    "corner_projections_saved": f"{8 * n_cells} corner slots -> {n_unique} unique",
                    "l2": "inputs larger than L2 (tree + corner buffers)"},
         "stages_ms": {"tree_build": build_ms, "adaptive_grid": grid_ms, "corner_field": statistics.mean(step_ms),
-                      "corner_projection_kernel": kms, "mesh_pipeline": mesh_ms},
+                      "corner_projection_kernel": kms, "mesh_pipeline": mesh_ms,
+                      "mesh_parts": {k: round(v_, 1) for k, v_ in parts.items()}},
         "mesh": {"vertices": int(len(v)), "triangles": int(len(tri))},
         "e2e": {"value": value, "unit": "corners/s", "h2d_bytes_per_step": int(grid.cells.nbytes),
                 "d2h_bytes_per_step": int(cf.nbytes + vx.nbytes + nc.nbytes),
@@ -629,6 +682,152 @@ def run_batch(args):
     }
 
 
+def run_serve(args):
+    """Serving workload: 8 resident clouds of 0.5-8M points, Poisson request
+    arrivals, request sizes log-uniform in [1e3, 1e6] queries, each request
+    with a weight kernel drawn from the three families; latency is measured
+    from submit to results in host memory."""
+    import threading
+
+    import torch
+
+    from mlodsurfaces_b200 import APSSOctree, Fastapss, Kernel, ProjectionServer, synth
+
+    rng = np.random.default_rng(21)
+    dev = "cuda"
+    clouds = []
+    for i in range(8):
+        n = int(np.exp(rng.uniform(np.log(5e5), np.log(8e6))))
+        if i % 3 == 0:
+            pts, nrm = synth.torus(n, seed=300 + i)
+        elif i % 3 == 1:
+            pts, nrm = synth.rbf_blobs(n, seed=300 + i, translate=0.0, device=dev)
+        else:
+            pts, nrm = synth.torus_knot(n, seed=300 + i)
+        pts = synth.make_tie_free(pts)
+        clouds.append((pts, nrm, synth.bbox_diag(pts)))
+    projectors = []
+    for pts, nrm, diag in clouds:
+        t = APSSOctree()
+        t.build(pts, nrm)
+        k = Kernel()
+        k.type = Kernel.GAUSSIAN
+        k.sigma = 0.02 * diag
+        f = Fastapss(t, k)
+        f.setScalingProtectionSphere(2.0)
+        projectors.append(f)
+    pools = [synth.perturbed_queries(pts, 0.01, seed=400 + i)[:1_000_000] for i, (pts, _, _) in enumerate(clouds)]
+
+    def request(r):
+        ci = int(r.integers(0, len(clouds)))
+        n = min(int(np.exp(r.uniform(np.log(1e3), np.log(1e6)))), len(pools[ci]))
+        start = int(r.integers(0, len(pools[ci]) - n + 1))
+        diag = clouds[ci][2]
+        k = Kernel()
+        kind = int(r.integers(0, 3))
+        if kind == 0:
+            k.type = Kernel.GAUSSIAN
+            k.sigma = float(r.uniform(0.01, 0.03)) * diag
+        elif kind == 1:
+            k.type = Kernel.GAUSSIAN_MULTIPLE
+            k.sigmas = [0.01 * diag * 2.0**j for j in range(int(r.integers(2, 5)))]
+        else:
+            k.type = Kernel.SINGULAR
+            k.exponent = 4.0
+            k.constant_shift = 1e-3
+        return ci, pools[ci][start:start + n], k
+
+    srv = ProjectionServer(projectors, n_streams=2)
+    iters = args.iters
+    # capacity: a closed loop of back-to-back requests
+    r0 = np.random.default_rng(5)
+    warm = [request(r0) for _ in range(24)]
+    t0 = time.perf_counter()
+    tickets = [srv.submit(ci, q, iters, k) for ci, q, k in warm]
+    for t in tickets:
+        srv.wait(t, timeout_ms=600000)
+    cap_s = time.perf_counter() - t0
+    capacity_rps = len(warm) / cap_s
+    rate = args.rate if args.rate > 0 else 0.7 * capacity_rps
+    # open loop: Poisson arrivals for serve_seconds
+    r1 = np.random.default_rng(6)
+    reqs = []
+    t_next = 0.0
+    while t_next < args.serve_seconds:
+        reqs.append((t_next, request(r1)))
+        t_next += float(r1.exponential(1.0 / rate))
+    lat, done_q = [], [0]
+    lock = threading.Lock()
+    pending = []
+
+    def collector():
+        i = 0
+        while True:
+            with lock:
+                if i >= len(pending):
+                    if collector.stop:
+                        return
+                    item = None
+                else:
+                    item = pending[i]
+            if item is None:
+                time.sleep(0.0005)
+                continue
+            t, n = item
+            _, _, ms = srv.wait(t, timeout_ms=600000)
+            lat.append(ms)
+            done_q[0] += n
+            i += 1
+
+    collector.stop = False
+    th = threading.Thread(target=collector)
+    th.start()
+    clocks = ClockSampler(0)
+    clocks.start()
+    start = time.perf_counter()
+    for at, (ci, q, k) in reqs:
+        now = time.perf_counter() - start
+        if at > now:
+            time.sleep(at - now)
+        t = srv.submit(ci, q, iters, k)
+        with lock:
+            pending.append((t, len(q)))
+    with lock:
+        collector.stop = True
+    th.join()
+    elapsed = time.perf_counter() - start
+    clk = clocks.stop()
+    stats = srv.stats()
+    srv.close()
+    total_q = done_q[0]
+    return {
+        "metric": "served queries/s and request latency p50/p99 (8 resident clouds, Poisson arrivals)",
+        "value": total_q / elapsed,
+        "unit": "queries/s",
+        "n_gpus": 1,
+        "steps": len(reqs),
+        "warmup": len(warm),
+        "ms_per_step": float(np.mean(lat)),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (f64 sphere solve)",
+        "data": "synthetic: seeded tori, RBF-blob surfaces and torus knots, 0.5-8M points each",
+        "config": {"workload": "serving: 8 resident clouds, Poisson arrivals, request sizes log-uniform "
+                               "in [1e3, 1e6], per-request kernels",
+                   "n_points": int(sum(len(c[0]) for c in clouds)), "iterations": iters, "n_streams": 2,
+                   "offered_rate_rps": rate, "closed_loop_capacity_rps": capacity_rps,
+                   "seconds": args.serve_seconds},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(np.max(lat)), "per": "request, submit to results in host memory"},
+        "e2e": {"value": total_q / elapsed, "unit": "queries/s", "h2d_bytes_per_step": int(12 * total_q / len(reqs)),
+                "d2h_bytes_per_step": int(24 * total_q / len(reqs)),
+                "path": "mlods_server_submit / mlods_server_wait (host arrays)"},
+        "server": stats,
+        "clocks": clk,
+    }
+
+
 def run_reference(args, rank):
     """Reference arm: the reference's own CPU implementation (oracle/_ref,
     APSSOctree::projectCPU under OpenMP) on the same workload, each step a
@@ -693,6 +892,10 @@ def main():
     if args.workload == "batch":
         if rank == 0:
             print(json.dumps(run_batch(args)), flush=True)
+        return
+    if args.workload == "serve":
+        if rank == 0:
+            print(json.dumps(run_serve(args)), flush=True)
         return
     if world > 1:
         import datetime

@@ -347,6 +347,53 @@ int mlods_server_stats(mlods_server s, int64_t* completed, int64_t* batches, int
                        double* busy_ms);
 int mlods_server_free(mlods_server s);
 
+/* ---- point-set and parameter files (Pn.cpp:102-290, scene.cpp:1183-1250) --
+ * mlods_cloud_load reads a .pn (raw float32 x y z nx ny nz records) or .ply
+ * file (the vertex element's x, y, z and, when present, nx, ny, nz; ascii or
+ * binary, any scalar type) and, with do_normalize, applies Pn::normalize:
+ * positions become (p - offset) / norme with offset the mean point and norme
+ * the largest coordinate of the box widened by 0.5% of its diagonal.
+ * mlods_cloud_save writes p * norme + offset (offset may be NULL) as a
+ * binary little-endian .ply (normals optional) or a .pn (normals required),
+ * as Pn::save does.  mlods_cloud_normalize applies Pn::normalize to an
+ * array.  The .params functions read and write the reference's parameter
+ * file, a packed 134-byte sequence of the fields below in this order. */
+typedef struct mlods_cloud_s* mlods_cloud;
+int mlods_cloud_load(const char* path, int32_t do_normalize, mlods_cloud* out);
+int mlods_cloud_info(mlods_cloud c, int64_t* n_points, int32_t* has_normals, float* offset, float* norme);
+int mlods_cloud_get(mlods_cloud c, float* pts, float* nrm);
+int mlods_cloud_free(mlods_cloud c);
+int mlods_cloud_save(const char* path, const float* pts, const float* nrm, int64_t n, const float* offset,
+                     float norme);
+int mlods_cloud_normalize(const float* pts, int64_t n, float* out_pts, float* offset, float* norme);
+
+#define MLODS_PARAMS_FILE_BYTES 134
+typedef struct mlods_scene_params {
+    float cam_quat[4];          /* viewer camera (not used by the projection) */
+    float cam_translation[3];
+    float cam_dist;
+    float sigma;                /* Kernel::sigma, in units of the box radius */
+    float fixed_sigmas[5];      /* Kernel::fixedSigmas */
+    float beginning_sigma;      /* Kernel::beginningSigma */
+    float factor;               /* Kernel::factor */
+    float constant_shift;       /* Kernel::constant_shift */
+    float exponent;             /* Kernel::exponent */
+    float cutoff;               /* scalingProtectionSphere */
+    uint32_t n_computed_sigmas; /* Kernel::nbOfComputedSigmas */
+    uint32_t max_iterations;    /* projection iterations */
+    uint32_t max_depth;         /* DC / upsampling octree depth */
+    uint32_t min_depth;         /* MLoD minimum depth */
+    uint32_t fast_method;       /* 1: Fastapss (MLoD), 0: GlobalAPSS */
+    int32_t kernel_type;        /* MLODS_GAUSSIAN / _SINGULAR / _GAUSSIAN_MULTIPLE */
+    uint8_t computed_sigma;     /* 1: sigmas from beginning_sigma * factor^i, 0: fixed_sigmas */
+    uint8_t cut;                /* uniformize's cut */
+    uint32_t n_points;          /* queries per upsampling round */
+    uint32_t max_upsamples;
+    float offset[6];
+} mlods_scene_params;
+int mlods_params_file_load(const char* path, mlods_scene_params* p);
+int mlods_params_file_save(const char* path, const mlods_scene_params* p);
+
 /* Number of kernels this library has launched in this process (diagnostics). */
 int64_t mlods_kernel_launches(void);
 

@@ -7,6 +7,6 @@ mirror of the reference's C++ projection API (``Kernel``, ``APSSOctree``,
 ``APSS``/``Fastapss``) plus seeded synthetic inputs (``synth``).
 """
 from .apss import APSS, APSSOctree, DCGrid, Fastapss, FastapssBatch, GlobalAPSS, Kernel, Mesh, ProjectionServer, unit2bbox  # noqa: F401
-from . import synth  # noqa: F401
+from . import io, synth  # noqa: F401
 
-__all__ = ["APSS", "APSSOctree", "DCGrid", "Fastapss", "FastapssBatch", "GlobalAPSS", "Kernel", "Mesh", "ProjectionServer", "synth", "unit2bbox"]
+__all__ = ["APSS", "APSSOctree", "DCGrid", "Fastapss", "FastapssBatch", "GlobalAPSS", "Kernel", "Mesh", "ProjectionServer", "io", "synth", "unit2bbox"]

@@ -40,6 +40,7 @@ CONVERGE_EXACT = 1
 CONVERGE_TOL = 2
 
 NOALLOC_MAX_QUERIES = 524288
+PARAMS_FILE_BYTES = 134
 
 
 class mlods_kernel(C.Structure):
@@ -65,6 +66,32 @@ class mlods_params(C.Structure):
         ("prune_tol", C.c_float),
         ("converge", C.c_int32),
         ("converge_tol", C.c_float),
+    ]
+
+
+class mlods_scene_params(C.Structure):
+    _fields_ = [
+        ("cam_quat", C.c_float * 4),
+        ("cam_translation", C.c_float * 3),
+        ("cam_dist", C.c_float),
+        ("sigma", C.c_float),
+        ("fixed_sigmas", C.c_float * 5),
+        ("beginning_sigma", C.c_float),
+        ("factor", C.c_float),
+        ("constant_shift", C.c_float),
+        ("exponent", C.c_float),
+        ("cutoff", C.c_float),
+        ("n_computed_sigmas", C.c_uint32),
+        ("max_iterations", C.c_uint32),
+        ("max_depth", C.c_uint32),
+        ("min_depth", C.c_uint32),
+        ("fast_method", C.c_uint32),
+        ("kernel_type", C.c_int32),
+        ("computed_sigma", C.c_uint8),
+        ("cut", C.c_uint8),
+        ("n_points", C.c_uint32),
+        ("max_upsamples", C.c_uint32),
+        ("offset", C.c_float * 6),
     ]
 
 
@@ -158,6 +185,14 @@ SIGNATURES = {
     "mlods_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int32, C.POINTER(C.c_double)]),
     "mlods_server_stats": (C.c_int, [_P, _I64, _I64, _I64, _I64, C.POINTER(C.c_double)]),
     "mlods_server_free": (C.c_int, [_P]),
+    "mlods_cloud_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_P)]),
+    "mlods_cloud_info": (C.c_int, [_P, _I64, _I32, _P, C.POINTER(C.c_float)]),
+    "mlods_cloud_get": (C.c_int, [_P, _P, _P]),
+    "mlods_cloud_free": (C.c_int, [_P]),
+    "mlods_cloud_save": (C.c_int, [C.c_char_p, _P, _P, C.c_int64, _P, C.c_float]),
+    "mlods_cloud_normalize": (C.c_int, [_P, C.c_int64, _P, _P, C.POINTER(C.c_float)]),
+    "mlods_params_file_load": (C.c_int, [C.c_char_p, C.POINTER(mlods_scene_params)]),
+    "mlods_params_file_save": (C.c_int, [C.c_char_p, C.POINTER(mlods_scene_params)]),
 }
 
 _lib = None

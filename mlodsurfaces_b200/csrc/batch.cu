@@ -23,7 +23,10 @@ struct mlods_batch_s {
     mlods::CloudArgs* d_clouds = nullptr;
     int64_t* d_offsets = nullptr;
     mlods::BatchFrame* d_frames = nullptr;
-    int64_t* d_stats = nullptr;  // same layout as a tree's stats block
+    int64_t* d_rank_slot = nullptr;
+    int32_t* d_rank_cloud = nullptr;
+    int64_t* d_stats = nullptr;  // stats block (8 int64) then one work counter per group
+    std::vector<mlods::BatchGroup> groups;
     void* d_order_buf = nullptr;
     size_t order_bytes = 0;
     std::vector<mlods::CloudArgs> h_clouds;  // last uploaded
@@ -54,6 +57,7 @@ namespace mlods
 namespace
 {
 inline size_t up256(size_t v) { return (v + 255) / 256 * 256; }
+constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + kMaxBatchGroups * sizeof(unsigned int);
 
 void drop_graph(mlods_batch_s* b)
 {
@@ -69,23 +73,24 @@ void drop_graph(mlods_batch_s* b)
 int enqueue(mlods_batch_s* b, const float* d_q, int64_t total, bool timed, cudaStream_t s)
 {
     const int n = int(b->trees.size());
-    MLODS_CUDA(cudaMemsetAsync(b->d_stats, 0, 8 * sizeof(int64_t), s));
-    uint32_t* order = nullptr;
-    if (b->reorder && total > 1) {
-        order = static_cast<uint32_t*>(b->d_order_buf);
-        void* tmp = static_cast<char*>(b->d_order_buf) + up256(size_t(total) * 4);
-        MLODS_CUDA(compute_batch_order(d_q, total, b->d_offsets, n, b->d_frames, order, tmp, s));
-    }
+    MLODS_CUDA(cudaMemsetAsync(b->d_stats, 0, kStatsBytes, s));
+    // the order groups the clouds by kernel specialisation (always needed),
+    // with Morton order inside each cloud when reorder is on
+    uint32_t* order = static_cast<uint32_t*>(b->d_order_buf);
+    void* tmp = static_cast<char*>(b->d_order_buf) + up256(size_t(total) * 4);
+    MLODS_CUDA(compute_batch_order(d_q, total, b->d_offsets, n, b->d_frames, b->reorder != 0, order, tmp, s));
     BatchArgs a;
     a.clouds = b->d_clouds;
     a.q_offsets = b->d_offsets;
     a.n_clouds = n;
     a.total = total;
     a.order = order;
-    a.counter = reinterpret_cast<unsigned int*>(b->d_stats + 3);
+    a.rank_slot = b->d_rank_slot;
+    a.rank_cloud = b->d_rank_cloud;
+    a.counters = reinterpret_cast<unsigned int*>(b->d_stats + 8);
     a.stats = b->d_stats;
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev0, s));
-    MLODS_CUDA(launch_mlod_batch(a, sm_count_for_current_device(), b->grid_pct, s));
+    MLODS_CUDA(launch_mlod_batch(a, b->groups, sm_count_for_current_device(), b->grid_pct, s));
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev1, s));
     if (timed) b->ran = true;
     return MLODS_OK;
@@ -127,7 +132,15 @@ int batch_prepare(mlods_batch_s* b, const int64_t* offsets, const float* d_q, fl
                         -1.f, T->params.blend_rule);
         float ext = 0.f;
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
-        frames[size_t(i)] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f, 0.f};
+        frames[size_t(i)] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f, 0u};
+    }
+    std::vector<BatchGroup> groups;
+    std::vector<int64_t> rank_slot(static_cast<size_t>(n) + 1);
+    std::vector<int32_t> rank_cloud(static_cast<size_t>(n));
+    plan_batch_groups(clouds.data(), offsets, n, frames.data(), rank_slot.data(), rank_cloud.data(), groups);
+    if (int(groups.size()) > kMaxBatchGroups) {
+        set_last_error("batch: %zu kernel specialisations exceed the %d supported", groups.size(), kMaxBatchGroups);
+        return MLODS_ERR_CAPACITY;
     }
     const bool same = b->h_clouds.size() == clouds.size() && b->h_offsets.size() == size_t(n + 1) &&
                       std::memcmp(b->h_clouds.data(), clouds.data(), clouds.size() * sizeof(CloudArgs)) == 0 &&
@@ -139,9 +152,14 @@ int batch_prepare(mlods_batch_s* b, const int64_t* offsets, const float* d_q, fl
         MLODS_CUDA(cudaMemcpyAsync(b->d_offsets, offsets, size_t(n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaMemcpyAsync(b->d_frames, frames.data(), frames.size() * sizeof(BatchFrame),
                                    cudaMemcpyHostToDevice, s));
+        MLODS_CUDA(cudaMemcpyAsync(b->d_rank_slot, rank_slot.data(), rank_slot.size() * sizeof(int64_t),
+                                   cudaMemcpyHostToDevice, s));
+        MLODS_CUDA(cudaMemcpyAsync(b->d_rank_cloud, rank_cloud.data(), rank_cloud.size() * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
         b->h_clouds = clouds;
         b->h_offsets.assign(offsets, offsets + n + 1);
+        b->groups = groups;
     }
     const size_t need = up256(size_t(total) * 4) + query_order_temp_bytes(total);
     if (b->order_bytes < need) {
@@ -227,7 +245,9 @@ int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* ou
     cudaError_t e = cudaMalloc(&b->d_clouds, size_t(n_trees) * sizeof(CloudArgs));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_offsets, size_t(n_trees + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_frames, size_t(n_trees) * sizeof(BatchFrame));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_stats, 8 * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_rank_slot, size_t(n_trees + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_rank_cloud, size_t(n_trees) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_stats, kStatsBytes);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
     if (e != cudaSuccess) {
@@ -245,6 +265,8 @@ int mlods_batch_free(mlods_batch b)
     cudaFree(b->d_clouds);
     cudaFree(b->d_offsets);
     cudaFree(b->d_frames);
+    cudaFree(b->d_rank_slot);
+    cudaFree(b->d_rank_cloud);
     cudaFree(b->d_stats);
     cudaFree(b->d_order_buf);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);

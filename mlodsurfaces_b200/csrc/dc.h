@@ -70,6 +70,19 @@ int dcgrid_from_points(const float* pts, int64_t n, int max_depth, const float b
 int dcgrid_adaptive(mlods_tree_s* T, int max_depth, bool cut, cudaStream_t s, std::vector<int32_t>& cells_out,
                     int& depth_out, float xform[12], int64_t* n_projected);
 
+// A triangle mesh in device memory and the refinement steps on it
+// (mesh_dev.cu); each returns an MLODS_* status.
+struct DeviceMesh;
+DeviceMesh* dmesh_create();
+void dmesh_destroy(DeviceMesh* m);
+int dmesh_upload(DeviceMesh& m, const float* pos, int64_t nv, const uint32_t* tri, int64_t nt, cudaStream_t s);
+int dmesh_download(const DeviceMesh& m, std::vector<float>& pos, std::vector<float>& nrm, std::vector<uint32_t>& tri,
+                   cudaStream_t s);
+int dmesh_transform(DeviceMesh& m, const float* xform, cudaStream_t s);
+int dmesh_project(mlods_tree_s* T, DeviceMesh& m, int iters, cudaStream_t s);
+int dmesh_smooth(DeviceMesh& m, cudaStream_t s);
+int dmesh_subdivide(DeviceMesh& m, cudaStream_t s);
+
 // Field at the 8 corners of every cell (unique corners projected once) and
 // the per-cell vertex; host arrays in and out.
 int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,

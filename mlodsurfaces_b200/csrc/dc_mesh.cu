@@ -12,9 +12,11 @@
 // again.  Integer traversal and mesh edits stay on the host; projections run
 // on the device.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -54,7 +56,7 @@ struct Grid {
     int64_t n;
     int max_depth;
     std::vector<int64_t> begin;  // first cell of each depth, max_depth + 2 entries
-    std::vector<int64_t> kids;   // 8 per cell, -1 for leaves
+    std::vector<int32_t> kids;   // 8 per cell, -1 for leaves
 
     Cell cell(int64_t i) const { return Cell{c[4 * i], c[4 * i + 1], c[4 * i + 2], c[4 * i + 3]}; }
     int64_t find(const Cell& q) const
@@ -92,40 +94,175 @@ int build_grid(const int32_t* cells, int64_t n, Grid& g)
     for (int64_t i = n - 1; i >= 0; --i) g.begin[size_t(cells[4 * i])] = i;
     for (int d = g.max_depth; d >= 0; --d)
         if (g.begin[size_t(d)] > g.begin[size_t(d) + 1]) g.begin[size_t(d)] = g.begin[size_t(d) + 1];
-    g.kids.assign(size_t(n) * 8, -1);
-    std::vector<uint8_t> count(size_t(n), 0);
-    for (int64_t i = 0; i < n; ++i) {
-        const Cell c = g.cell(i);
-        if (c.depth == 0) continue;
-        const Cell p = dcg::parent(c);
-        const int64_t pi = g.find(p);
-        if (pi < 0) {
-            set_last_error("dc extract: cell %lld has no parent in the grid", (long long)i);
-            return MLODS_ERR_INVALID;
-        }
-        const int k = (c.x - 2 * p.x) + 2 * (c.y - 2 * p.y) + 4 * (c.z - 2 * p.z);
-        g.kids[size_t(pi) * 8 + size_t(k)] = i;
-        ++count[size_t(pi)];
+    if (n >= (int64_t(1) << 31)) {
+        set_last_error("dc extract: %lld cells exceed 32-bit cell indices", (long long)n);
+        return MLODS_ERR_CAPACITY;
     }
-    for (int64_t i = 0; i < n; ++i)
-        if (count[size_t(i)] != 0 && count[size_t(i)] != 8) {
-            set_last_error("dc extract: cell %lld has %d children (needs 0 or 8)", (long long)i, int(count[size_t(i)]));
+    g.kids.assign(size_t(n) * 8, -1);
+    // parent lookups on host threads: every cell writes one distinct slot of
+    // its parent, so the writes do not overlap
+    const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::atomic<int64_t> orphan{-1};
+    auto link = [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            const Cell c = g.cell(i);
+            if (c.depth == 0) continue;
+            const Cell p = dcg::parent(c);
+            const int64_t pi = g.find(p);
+            if (pi < 0) {
+                orphan.store(i);
+                continue;
+            }
+            const int k = (c.x - 2 * p.x) + 2 * (c.y - 2 * p.y) + 4 * (c.z - 2 * p.z);
+            g.kids[size_t(pi) * 8 + size_t(k)] = int32_t(i);
+        }
+    };
+    std::vector<std::thread> pool;
+    const int64_t step = (n + hw - 1) / hw;
+    for (unsigned t = 1; t < hw && int64_t(t) * step < n; ++t)
+        pool.emplace_back(link, int64_t(t) * step, std::min(n, int64_t(t + 1) * step));
+    link(0, std::min(n, step));
+    for (std::thread& th : pool) th.join();
+    if (orphan.load() >= 0) {
+        set_last_error("dc extract: cell %lld has no parent in the grid", (long long)orphan.load());
+        return MLODS_ERR_INVALID;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        int cnt = 0;
+        for (int k = 0; k < 8; ++k) cnt += g.kids[size_t(i) * 8 + size_t(k)] >= 0;
+        if (cnt != 0 && cnt != 8) {
+            set_last_error("dc extract: cell %lld has %d children (needs 0 or 8)", (long long)i, cnt);
             return MLODS_ERR_INVALID;
         }
+    }
     return MLODS_OK;
 }
 
-struct Extractor {
+// One call of the reference's recursive enumeration: traverse_node (kind 0,
+// one cell), traverse_face (kind 1, two cells, direction d) or traverse_edge
+// (kind 2, four cells, direction d).
+struct Call {
+    int kind, dir;
+    int64_t n[4];
+};
+
+// A sign-changing minimal edge: its four cells (slot order) and whether its
+// triangles are flipped.
+struct Crossing {
+    int32_t n[4];
+    int32_t flip;
+};
+
+struct Walker {
     const Grid& g;
     const float* cf;  // 8 corner values per cell
+
+    bool leaf(int64_t n) const { return g.kids[size_t(n) * 8] < 0; }
+    int64_t kid(int64_t n, int c) const { return leaf(n) ? n : g.kids[size_t(n) * 8 + size_t(c)]; }
+    bool minimal(const Call& c) const
+    {
+        return c.kind == 2 && leaf(c.n[0]) && leaf(c.n[1]) && leaf(c.n[2]) && leaf(c.n[3]);
+    }
+
+    // The calls a call makes, in the reference's order (octree.h:423-540).
+    template <typename F>
+    void children(const Call& c, F f) const
+    {
+        if (c.kind == 0) {  // traverse_node
+            if (leaf(c.n[0])) return;
+            const int32_t* ch = &g.kids[size_t(c.n[0]) * 8];
+            for (int t = 0; t < 8; ++t) f(Call{0, 0, {ch[t], 0, 0, 0}});
+            for (int d = 0; d < 3; ++d)
+                for (int k = 0; k < 8; ++k)
+                    if (!((k >> d) & 1)) f(Call{1, d, {ch[k], ch[k | (1 << d)], 0, 0}});
+            for (int e = 0; e < 3; ++e) {
+                int p1, p2;
+                perp(e, p1, p2);
+                for (int h = 0; h < 2; ++h) {
+                    Call x{2, e, {0, 0, 0, 0}};
+                    for (int s = 0; s < 4; ++s) x.n[s] = ch[(h << e) | ((s & 1) << p1) | ((s >> 1) << p2)];
+                    f(x);
+                }
+            }
+        } else if (c.kind == 1) {  // traverse_face
+            const int d = c.dir;
+            const int64_t n1 = c.n[0], n2 = c.n[1];
+            if (leaf(n1) && leaf(n2)) return;
+            int on1[4], on2[4], k1 = 0, k2 = 0;
+            for (int k = 0; k < 8; ++k) {
+                if ((k >> d) & 1) on1[k1++] = k;
+                else on2[k2++] = k;
+            }
+            for (int q = 0; q < 4; ++q) f(Call{1, d, {kid(n1, on1[q]), kid(n2, on2[q]), 0, 0}});
+            for (int k = 0; k < 4; ++k) {
+                const int e = kFaceEdges[d][k][0], h = kFaceEdges[d][k][1];
+                const int fa = 3 - d - e;  // the axis normal to both
+                int p1, p2;
+                perp(e, p1, p2);
+                Call x{2, e, {0, 0, 0, 0}};
+                for (int sd = 0; sd < 2; ++sd)
+                    for (int sf = 0; sf < 2; ++sf) {
+                        const int kk = (h << e) | ((1 - sd) << d) | (sf << fa);
+                        const int s1 = p1 == d ? sd : sf, s2 = p2 == d ? sd : sf;
+                        x.n[s1 + 2 * s2] = sd == 0 ? kid(n1, kk) : kid(n2, kk);
+                    }
+                f(x);
+            }
+        } else {  // traverse_edge
+            if (minimal(c)) return;
+            int p1, p2;
+            perp(c.dir, p1, p2);
+            for (int h = 0; h < 2; ++h) {
+                Call x{2, c.dir, {0, 0, 0, 0}};
+                for (int s = 0; s < 4; ++s)
+                    x.n[s] = kid(c.n[s], (h << c.dir) | ((1 - (s & 1)) << p1) | ((1 - (s >> 1)) << p2));
+                f(x);
+            }
+        }
+    }
+
+    // on_min_edges' test (dual_contouring.h:196-228): the edge's end values
+    // are corners of the deepest of its cells (the first one on ties)
+    void test(const Call& c, std::vector<Crossing>& out) const
+    {
+        int sel = 0, sel_d = -1;
+        for (int i = 0; i < 4; ++i) {
+            const int d = g.c[4 * c.n[i]];
+            if (d > sel_d) {
+                sel = i;
+                sel_d = d;
+            }
+        }
+        int p1, p2;
+        perp(c.dir, p1, p2);
+        const int base = ((1 - (sel & 1)) << p1) | ((1 - (sel >> 1)) << p2);
+        int c0 = base, c1 = base | (1 << c.dir);
+        if (c.dir == kY) std::swap(c0, c1);  // the reference lists the upper end first for Y edges
+        const float f0 = cf[8 * c.n[sel] + c0], f1 = cf[8 * c.n[sel] + c1];
+        if (std::isnan(f0) || std::isnan(f1)) return;
+        const bool m0 = f0 < 0, m1 = f1 < 0;
+        if (m0 == m1) return;
+        out.push_back(Crossing{{int32_t(c.n[0]), int32_t(c.n[1]), int32_t(c.n[2]), int32_t(c.n[3])}, m0 ? 1 : 0});
+    }
+
+    void run(const Call& c, std::vector<Crossing>& out) const
+    {
+        if (minimal(c)) {
+            test(c, out);
+            return;
+        }
+        children(c, [&](const Call& x) { run(x, out); });
+    }
+};
+
+// extract's triangle pair per crossing and first-use vertex numbering
+// (dual_contouring.h:64-86), in enumeration order
+struct Numbering {
     std::vector<int64_t> vertex_of;
     std::vector<int64_t> order;  // cell of each vertex, in creation order
     std::vector<uint32_t> tri;
 
-    Extractor(const Grid& grid, const float* corner_f) : g(grid), cf(corner_f), vertex_of(size_t(grid.n), -1) {}
-
-    bool leaf(int64_t n) const { return g.kids[size_t(n) * 8] < 0; }
-    int64_t kid(int64_t n, int c) const { return leaf(n) ? n : g.kids[size_t(n) * 8 + size_t(c)]; }
+    explicit Numbering(int64_t n_cells) : vertex_of(size_t(n_cells), -1) {}
 
     uint32_t vertex(int64_t n)
     {
@@ -137,95 +274,15 @@ struct Extractor {
         return uint32_t(v);
     }
 
-    // on_min_edges + extract's triangle pair (dual_contouring.h:64-86, :190-229)
-    void emit(const int64_t nd[4], int e)
+    void add(const Crossing& x)
     {
-        int sel = 0, sel_d = -1;
-        for (int i = 0; i < 4; ++i) {
-            const int d = g.c[4 * nd[i]];
-            if (d > sel_d) {
-                sel = i;
-                sel_d = d;
-            }
-        }
-        int p1, p2;
-        perp(e, p1, p2);
-        const int base = ((1 - (sel & 1)) << p1) | ((1 - (sel >> 1)) << p2);
-        int c0 = base, c1 = base | (1 << e);
-        if (e == kY) std::swap(c0, c1);  // the reference lists the upper end first for Y edges
-        const float f0 = cf[8 * nd[sel] + c0], f1 = cf[8 * nd[sel] + c1];
-        if (std::isnan(f0) || std::isnan(f1)) return;
-        const bool m0 = f0 < 0, m1 = f1 < 0;
-        if (m0 == m1) return;
         static const int tris[2][3] = {{0, 1, 3}, {0, 3, 2}};
         for (const auto& t : tris) {
-            const uint32_t v0 = vertex(nd[t[0]]), v1 = vertex(nd[t[1]]), v2 = vertex(nd[t[2]]);
+            const uint32_t v0 = vertex(x.n[t[0]]), v1 = vertex(x.n[t[1]]), v2 = vertex(x.n[t[2]]);
             if (v0 == v1 || v1 == v2 || v2 == v0) continue;
             tri.push_back(v0);
-            tri.push_back(m0 ? v2 : v1);
-            tri.push_back(m0 ? v1 : v2);
-        }
-    }
-
-    // traverse_edge, octree.h:504-540
-    void edge(const int64_t nd[4], int e)
-    {
-        if (leaf(nd[0]) && leaf(nd[1]) && leaf(nd[2]) && leaf(nd[3])) {
-            emit(nd, e);
-            return;
-        }
-        int p1, p2;
-        perp(e, p1, p2);
-        for (int h = 0; h < 2; ++h) {
-            int64_t sub[4];
-            for (int s = 0; s < 4; ++s) sub[s] = kid(nd[s], (h << e) | ((1 - (s & 1)) << p1) | ((1 - (s >> 1)) << p2));
-            edge(sub, e);
-        }
-    }
-
-    // traverse_face, octree.h:457-502
-    void face(int64_t n1, int64_t n2, int d)
-    {
-        if (leaf(n1) && leaf(n2)) return;
-        int on1[4], on2[4], k1 = 0, k2 = 0;
-        for (int c = 0; c < 8; ++c) {
-            if ((c >> d) & 1) on1[k1++] = c;
-            else on2[k2++] = c;
-        }
-        for (int f = 0; f < 4; ++f) face(kid(n1, on1[f]), kid(n2, on2[f]), d);
-        for (int k = 0; k < 4; ++k) {
-            const int e = kFaceEdges[d][k][0], h = kFaceEdges[d][k][1];
-            const int fa = 3 - d - e;  // the axis normal to both
-            int p1, p2;
-            perp(e, p1, p2);
-            int64_t nd[4];
-            for (int sd = 0; sd < 2; ++sd)
-                for (int sf = 0; sf < 2; ++sf) {
-                    const int c = (h << e) | ((1 - sd) << d) | (sf << fa);
-                    const int s_p1 = p1 == d ? sd : sf, s_p2 = p2 == d ? sd : sf;
-                    nd[s_p1 + 2 * s_p2] = sd == 0 ? kid(n1, c) : kid(n2, c);
-                }
-            edge(nd, e);
-        }
-    }
-
-    // traverse_node, octree.h:423-455
-    void node(int64_t n)
-    {
-        if (leaf(n)) return;
-        const int64_t* ch = &g.kids[size_t(n) * 8];
-        for (int t = 0; t < 8; ++t) node(ch[t]);
-        for (int d = 0; d < 3; ++d)
-            for (int c = 0; c < 8; ++c)
-                if (!((c >> d) & 1)) face(ch[c], ch[c | (1 << d)], d);
-        for (int e = 0; e < 3; ++e) {
-            int p1, p2;
-            perp(e, p1, p2);
-            for (int h = 0; h < 2; ++h) {
-                int64_t nd[4];
-                for (int s = 0; s < 4; ++s) nd[s] = ch[(h << e) | ((s & 1) << p1) | ((s >> 1) << p2)];
-                edge(nd, e);
-            }
+            tri.push_back(x.flip ? v2 : v1);
+            tri.push_back(x.flip ? v1 : v2);
         }
     }
 };
@@ -255,13 +312,44 @@ int dc_extract(const int32_t* cells, int64_t n_cells, const float* corner_f, con
     m->tri.clear();
     const int64_t root = g.find(Cell{0, 0, 0, 0});
     if (root < 0) return MLODS_OK;  // minimal_edges::traverse starts at the root only
-    Extractor ex(g, corner_f);
-    ex.node(root);
-    m->pos.resize(ex.order.size() * 3);
-    m->nrm.assign(ex.order.size() * 3, 0.f);
-    for (size_t i = 0; i < ex.order.size(); ++i)
-        for (int a = 0; a < 3; ++a) m->pos[3 * i + size_t(a)] = cell_vertex[3 * ex.order[i] + a];
-    m->tri.swap(ex.tri);
+    if (n_cells >= (int64_t(1) << 31)) {
+        set_last_error("dc extract: %lld cells exceed 32-bit cell indices", (long long)n_cells);
+        return MLODS_ERR_CAPACITY;
+    }
+    const Walker w{g, corner_f};
+    // the top of the recursion as an ordered list of independent calls
+    const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<Call> tasks = {Call{0, 0, {root, 0, 0, 0}}};
+    for (int round = 0; round < 8 && tasks.size() < size_t(16 * hw); ++round) {
+        std::vector<Call> next;
+        bool grew = false;
+        for (const Call& c : tasks) {
+            size_t before = next.size();
+            if (!w.minimal(c)) w.children(c, [&](const Call& x) { next.push_back(x); });
+            if (next.size() == before && w.minimal(c)) next.push_back(c);  // a minimal edge stays a task
+            grew = grew || next.size() != before + 1;
+        }
+        tasks.swap(next);
+        if (!grew) break;
+    }
+    // the calls run on host threads; their crossings concatenate in task order
+    std::vector<std::vector<Crossing>> found(tasks.size());
+    std::atomic<size_t> next_task{0};
+    auto worker = [&]() {
+        for (size_t t; (t = next_task.fetch_add(1)) < tasks.size();) w.run(tasks[t], found[t]);
+    };
+    std::vector<std::thread> pool;
+    for (unsigned i = 1; i < hw && i < tasks.size(); ++i) pool.emplace_back(worker);
+    worker();
+    for (std::thread& th : pool) th.join();
+    Numbering num(n_cells);
+    for (const auto& list : found)
+        for (const Crossing& x : list) num.add(x);
+    m->pos.resize(num.order.size() * 3);
+    m->nrm.assign(num.order.size() * 3, 0.f);
+    for (size_t i = 0; i < num.order.size(); ++i)
+        for (int a = 0; a < 3; ++a) m->pos[3 * i + size_t(a)] = cell_vertex[3 * num.order[i] + a];
+    m->tri.swap(num.tri);
     return MLODS_OK;
 }
 
@@ -475,20 +563,26 @@ int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t ref
         return MLODS_ERR_CAPACITY;
     }
     rc = dc_extract(g->cells.data(), n, cf.data(), vx.data(), m);
+    // the refinement loop stays in device memory (mesh_dev.cu)
+    DeviceMesh* dmp = rc == MLODS_OK ? dmesh_create() : nullptr;
+    if (rc == MLODS_OK && !dmp) {
+        set_last_error("dc mesh: host allocation failed");
+        rc = MLODS_ERR_CAPACITY;
+    }
     if (rc == MLODS_OK) {
-        mesh_transform(m, g->xform);  // scene.cpp:1400-1408
-        rc = mesh_project(t, m, 3, s);
-    }
-    for (int r = 0; rc == MLODS_OK && r < refine_rounds; ++r) {
-        mesh_smooth(m);
-        if (m->pos.size() / 3 + m->tri.size() > size_t(UINT32_MAX)) {
-            set_last_error("dc mesh: subdivision would exceed 32-bit vertex indices");
-            rc = MLODS_ERR_CAPACITY;
-            break;
+        DeviceMesh& dm = *dmp;
+        rc = dmesh_upload(dm, m->pos.data(), int64_t(m->pos.size() / 3), m->tri.data(), int64_t(m->tri.size() / 3),
+                          s);
+        if (rc == MLODS_OK) rc = dmesh_transform(dm, g->xform, s);  // scene.cpp:1400-1408
+        if (rc == MLODS_OK) rc = dmesh_project(t, dm, 3, s);
+        for (int r = 0; rc == MLODS_OK && r < refine_rounds; ++r) {
+            rc = dmesh_smooth(dm, s);
+            if (rc == MLODS_OK) rc = dmesh_subdivide(dm, s);
+            if (rc == MLODS_OK) rc = dmesh_project(t, dm, 3, s);
         }
-        mesh_subdivide(m);
-        rc = mesh_project(t, m, 3, s);
+        if (rc == MLODS_OK) rc = dmesh_download(dm, m->pos, m->nrm, m->tri, s);
     }
+    dmesh_destroy(dmp);
     if (rc != MLODS_OK) {
         delete m;
         return rc;

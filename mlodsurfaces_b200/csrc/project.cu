@@ -384,40 +384,59 @@ __global__ void __launch_bounds__(kProjectThreads, kProjectMinBlocks) mlod_proje
     flush_stats(a.stats, visits, rounds, max_top, overflows, iterations);
 }
 
-// Many trees, one launch.  Query slot s (in processing order) belongs to the
-// cloud whose [q_offsets[c], q_offsets[c+1]) holds it; order[s] is the global
-// index of the query in the concatenated buffers.  The weight kernel and the
-// blend rule are read per query (uniform across the warp), so one
-// instantiation serves every cloud.
-template <int CAP>
-__global__ void __launch_bounds__(kProjectThreads, kProjectMinBlocks) mlod_batch_kernel(BatchArgs b)
+// Many trees, one launch per kernel specialisation.  The warps of a launch
+// take slots of their group's range; the query at slot s is order[s] in the
+// concatenated buffers and belongs to the cloud whose offset range holds it.
+// A warp copies its cloud's arguments to shared memory when the cloud
+// changes (consecutive slots mostly share one), so the walk reads them as
+// cheaply as the single-tree kernel reads its parameters.
+template <int KTYPE, int NSIG, int RULE, int CAP>
+__global__ void __launch_bounds__(kProjectThreads, kBatchMinBlocks)
+    mlod_batch_kernel(BatchArgs b, int64_t slot_begin, int64_t slot_end, unsigned int* counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31;
-    WarpStack<CAP>& st = reinterpret_cast<WarpStack<CAP>*>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpStack<CAP>& st = reinterpret_cast<WarpStack<CAP>*>(smem_raw)[warp];
+    CloudArgs* cache = reinterpret_cast<CloudArgs*>(smem_raw + (kProjectThreads / 32) * sizeof(WarpStack<CAP>)) + warp;
+    int cached = -1;
+    int64_t c_lo = 0, c_hi = 0, c_base = 0;  // slot range and first global index of the cached cloud
     int64_t visits = 0, rounds = 0, overflows = 0, iterations = 0;
     int max_top = 0;
     for (;;) {
         unsigned int qs = 0;
-        if (lane == 0) qs = atomicAdd(b.counter, 1u);
+        if (lane == 0) qs = atomicAdd(counter, 1u);
         qs = __shfl_sync(kFull, qs, 0);
-        if (int64_t(qs) >= b.total) break;
-        // cloud of this slot (binary search over the offsets)
-        int lo = 0, hi = b.n_clouds;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (int64_t(qs) >= __ldg(b.q_offsets + mid)) lo = mid; else hi = mid;
+        const int64_t slot = slot_begin + int64_t(qs);
+        if (slot >= slot_end) break;
+        const int64_t g = int64_t(__ldg(b.order + slot));
+        if (slot < c_lo || slot >= c_hi) {
+            // the cloud owning this slot: binary search over the rank table
+            int lo = 0, hi = b.n_clouds;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (slot >= __ldg(b.rank_slot + mid)) lo = mid; else hi = mid;
+            }
+            const int cl = __ldg(b.rank_cloud + lo);
+            c_lo = __ldg(b.rank_slot + lo);
+            c_hi = __ldg(b.rank_slot + lo + 1);
+            c_base = __ldg(b.q_offsets + cl);
+            if (cl != cached) {
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(b.clouds + cl);
+                uint32_t* dst = reinterpret_cast<uint32_t*>(cache);
+                for (int w = lane; w < int(sizeof(CloudArgs) / 4); w += 32) dst[w] = __ldg(src + w);
+                cached = cl;
+                __syncwarp();
+            }
         }
-        const CloudArgs& c = b.clouds[lo];
-        const uint32_t g = b.order ? b.order[qs] : qs;
-        const uint32_t qi = uint32_t(int64_t(g) - b.q_offsets[lo]);
+        const uint32_t qi = uint32_t(g - c_base);
         WalkStats ws;
-        project_query<-1, 0, -1, CAP>(c, qi, st, ws);
+        project_query<KTYPE, NSIG, RULE, CAP>(*cache, qi, st, ws);
         visits += ws.visits;
         rounds += ws.rounds;
         iterations += ws.iterations;
         max_top = max(max_top, ws.max_top);
         overflows += ws.overflow ? 1 : 0;
+        __syncwarp();  // every lane is done with the cached arguments
     }
     flush_stats(b.stats, visits, rounds, max_top, overflows, iterations);
 }
@@ -486,8 +505,8 @@ __global__ void query_codes_kernel(const float* __restrict__ q, int64_t n, doubl
 }
 
 __global__ void batch_codes_kernel(const float* __restrict__ q, int64_t n, const int64_t* __restrict__ q_offsets,
-                                   int n_clouds, const BatchFrame* __restrict__ frames, uint64_t* __restrict__ keys,
-                                   uint32_t* __restrict__ idx)
+                                   int n_clouds, const BatchFrame* __restrict__ frames, int morton,
+                                   uint64_t* __restrict__ keys, uint32_t* __restrict__ idx)
 {
     int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -504,10 +523,10 @@ __global__ void batch_codes_kernel(const float* __restrict__ q, int64_t n, const
         u = fminf(fmaxf(u, 0.f), 0.99999994f);
         c[k] = uint32_t(u * 1024.f);
     }
-    uint64_t code = uint64_t(lo);
+    uint64_t code = uint64_t(fr.rank);
     for (int b = 9; b >= 0; --b)
         code = (code << 3) | ((c[0] >> b) & 1u) | (((c[1] >> b) & 1u) << 1) | (((c[2] >> b) & 1u) << 2);
-    keys[i] = code;
+    keys[i] = morton ? code : (uint64_t(fr.rank) << 30);
     idx[i] = uint32_t(i);
 }
 
@@ -526,6 +545,50 @@ __global__ void reorganize_kernel(float* __restrict__ q, const uint32_t* __restr
 
 inline size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 
+template <int KTYPE, int NSIG, int RULE>
+cudaError_t launch_batch_typed(const BatchArgs& b, const BatchGroup& g, unsigned int* counter, int sm_count,
+                               int grid_scale_pct, cudaStream_t s)
+{
+    constexpr int CAP = kProjectStackCap;
+    auto kern = mlod_batch_kernel<KTYPE, NSIG, RULE, CAP>;
+    const size_t smem = size_t(kProjectThreads / 32) * (sizeof(WarpStack<CAP>) + sizeof(CloudArgs));
+    cudaError_t e = cudaSuccess;
+    int64_t grid = persistent_grid(kern, smem, g.slot_end - g.slot_begin, sm_count, &e);
+    if (e != cudaSuccess) return e;
+    if (grid_scale_pct > 0 && grid_scale_pct < 100) grid = std::max<int64_t>(1, grid * grid_scale_pct / 100);
+    kern<<<unsigned(grid), kProjectThreads, smem, s>>>(b, g.slot_begin, g.slot_end, counter);
+    note_launch();
+    return cudaGetLastError();
+}
+
+template <int RULE>
+cudaError_t launch_batch_rule(const BatchArgs& b, const BatchGroup& g, unsigned int* counter, int sm_count,
+                              int pct, cudaStream_t s)
+{
+    if (g.ktype == MLODS_GAUSSIAN) return launch_batch_typed<MLODS_GAUSSIAN, 0, RULE>(b, g, counter, sm_count, pct, s);
+    if (g.ktype == MLODS_SINGULAR) return launch_batch_typed<MLODS_SINGULAR, 0, RULE>(b, g, counter, sm_count, pct, s);
+    switch (g.nsig) {
+    case 2: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 2, RULE>(b, g, counter, sm_count, pct, s);
+    case 3: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 3, RULE>(b, g, counter, sm_count, pct, s);
+    case 4: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 4, RULE>(b, g, counter, sm_count, pct, s);
+    case 5: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 5, RULE>(b, g, counter, sm_count, pct, s);
+    case 6: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 6, RULE>(b, g, counter, sm_count, pct, s);
+    case 8: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 8, RULE>(b, g, counter, sm_count, pct, s);
+    default: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 0, RULE>(b, g, counter, sm_count, pct, s);
+    }
+}
+
+// the specialisation a cloud's kernel runs with: multi-Gaussian kernels with
+// 2-6 or 8 terms have their own instantiation, other counts share one
+inline int spec_nsig(const KernelConsts& kc)
+{
+    if (kc.type != MLODS_GAUSSIAN_MULTIPLE) return 0;
+    switch (kc.nsig) {
+    case 2: case 3: case 4: case 5: case 6: case 8: return kc.nsig;
+    default: return 0;
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_invalid, uint32_t end_valid,
@@ -542,18 +605,54 @@ cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int s
     return launch_rule<MLODS_BLEND_CPU>(a, ktype, sm_count, s);
 }
 
-cudaError_t launch_mlod_batch(const BatchArgs& b, int sm_count, int grid_scale_pct, cudaStream_t s)
+void plan_batch_groups(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, BatchFrame* frames,
+                       int64_t* rank_slot, int32_t* rank_cloud, std::vector<BatchGroup>& groups)
 {
-    constexpr int CAP = kProjectStackCap;
-    auto kern = mlod_batch_kernel<CAP>;
-    const size_t smem = size_t(kProjectThreads / 32) * sizeof(WarpStack<CAP>);
-    cudaError_t e = cudaSuccess;
-    int64_t grid = persistent_grid(kern, smem, b.total, sm_count, &e);
-    if (e != cudaSuccess) return e;
-    if (grid_scale_pct > 0 && grid_scale_pct < 100) grid = std::max<int64_t>(1, grid * grid_scale_pct / 100);
-    kern<<<unsigned(grid), kProjectThreads, smem, s>>>(b);
-    note_launch();
-    return cudaGetLastError();
+    auto key = [&](int i) {
+        const CloudArgs& c = clouds[i];
+        return (c.rule == MLODS_BLEND_GPU ? 0 : 1) * 1024 + c.kc.type * 32 + spec_nsig(c.kc);
+    };
+    std::vector<int> idx(static_cast<size_t>(n_clouds));
+    for (int i = 0; i < n_clouds; ++i) idx[size_t(i)] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key(a) < key(b); });
+    groups.clear();
+    int64_t slot = 0;
+    for (int r = 0; r < n_clouds; ++r) {
+        const int i = idx[size_t(r)];
+        frames[i].rank = uint32_t(r);
+        rank_slot[r] = slot;
+        rank_cloud[r] = i;
+        const int64_t n = q_offsets[i + 1] - q_offsets[i];
+        if (groups.empty() || key(idx[size_t(r - 1)]) != key(i)) {
+            BatchGroup g;
+            g.ktype = clouds[i].kc.type;
+            g.nsig = spec_nsig(clouds[i].kc);
+            g.rule = clouds[i].rule;
+            g.slot_begin = g.slot_end = slot;
+            groups.push_back(g);
+        }
+        slot += n;
+        groups.back().slot_end = slot;
+    }
+    rank_slot[n_clouds] = slot;
+    groups.erase(std::remove_if(groups.begin(), groups.end(),
+                                [](const BatchGroup& g) { return g.slot_end == g.slot_begin; }),
+                 groups.end());
+}
+
+cudaError_t launch_mlod_batch(const BatchArgs& b, const std::vector<BatchGroup>& groups, int sm_count,
+                              int grid_scale_pct, cudaStream_t s)
+{
+    if (int(groups.size()) > kMaxBatchGroups) return cudaErrorInvalidValue;
+    for (size_t k = 0; k < groups.size(); ++k) {
+        const BatchGroup& g = groups[k];
+        unsigned int* counter = b.counters + k;
+        const cudaError_t e = g.rule == MLODS_BLEND_GPU
+                                  ? launch_batch_rule<MLODS_BLEND_GPU>(b, g, counter, sm_count, grid_scale_pct, s)
+                                  : launch_batch_rule<MLODS_BLEND_CPU>(b, g, counter, sm_count, grid_scale_pct, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 size_t query_order_temp_bytes(int64_t n)
@@ -583,14 +682,16 @@ cudaError_t compute_query_order(const float* d_q, int64_t n, const double origin
 }
 
 cudaError_t compute_batch_order(const float* d_q, int64_t n, const int64_t* d_q_offsets, int n_clouds,
-                                const BatchFrame* d_frames, uint32_t* d_order, void* temp, cudaStream_t s)
+                                const BatchFrame* d_frames, bool morton, uint32_t* d_order, void* temp,
+                                cudaStream_t s)
 {
     char* t = static_cast<char*>(temp);
     uint64_t* k0 = reinterpret_cast<uint64_t*>(t);
     uint64_t* k1 = reinterpret_cast<uint64_t*>(t + up256(size_t(n) * 8));
     uint32_t* v1 = reinterpret_cast<uint32_t*>(t + 2 * up256(size_t(n) * 8));
     void* rt = t + 2 * up256(size_t(n) * 8) + up256(size_t(n) * 4);
-    batch_codes_kernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(d_q, n, d_q_offsets, n_clouds, d_frames, k0, d_order);
+    batch_codes_kernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(d_q, n, d_q_offsets, n_clouds, d_frames,
+                                                                 morton ? 1 : 0, k0, d_order);
     note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "mlods_internal.cuh"
 
 namespace mlods
@@ -12,12 +14,16 @@ namespace mlods
 #ifndef MLODS_PROJECT_MIN_BLOCKS
 #define MLODS_PROJECT_MIN_BLOCKS 10
 #endif
+#ifndef MLODS_BATCH_MIN_BLOCKS
+#define MLODS_BATCH_MIN_BLOCKS 8
+#endif
 #ifndef MLODS_PROJECT_STACK_CAP
 #define MLODS_PROJECT_STACK_CAP 160
 #endif
 constexpr int kProjectThreads = 128;                          // 4 warps per block, one query per warp at a time
 constexpr int kProjectMinBlocks = MLODS_PROJECT_MIN_BLOCKS;  // 10 -> 40 warps per SM, <= 48 registers
 constexpr int kProjectStackCap = MLODS_PROJECT_STACK_CAP;    // sibling ranges per warp (28 bytes each)
+constexpr int kBatchMinBlocks = MLODS_BATCH_MIN_BLOCKS;      // the batch kernel keeps more registers (64)
 
 // One tree and its projection settings, plus the query buffers it serves.
 struct CloudArgs {
@@ -46,26 +52,48 @@ struct ProjectArgs {
 
 // Many trees in one launch: clouds[c] serves the global query range
 // [q_offsets[c], q_offsets[c+1]) of the concatenated buffers (each cloud's
-// q_in/out_p/out_n point at the start of its own range).
+// q_in/out_p/out_n point at the start of its own range).  order[slot] is the
+// global index of the query processed at each slot; clouds that share a
+// kernel specialisation occupy consecutive slots, and each such group runs
+// as one launch of its specialised kernel over its slot range.
 struct BatchArgs {
     const CloudArgs* clouds;
     const int64_t* q_offsets;  // n_clouds + 1 entries
     int n_clouds;
     int64_t total;
-    const uint32_t* order;     // processing order over all queries (grouped by cloud), or nullptr
-    unsigned int* counter;
-    int64_t* stats;
+    const uint32_t* order;     // slot -> global query index (grouped, Morton order inside each cloud)
+    const int64_t* rank_slot;  // n_clouds + 1 entries: first slot of the cloud of each rank
+    const int32_t* rank_cloud; // n_clouds entries: cloud of each rank
+    unsigned int* counters;    // one work counter per group, zero before launch
+    int64_t* stats;            // [0] visits, [1] max stack, [2] overflows, [4] rounds, [5] iterations
 };
 
-// Per-cloud frame used to key queries in Morton order.
+constexpr int kMaxBatchGroups = 32;
+
+// One kernel specialisation of a batch and its slot range.
+struct BatchGroup {
+    int ktype, nsig, rule;
+    int64_t slot_begin, slot_end;
+};
+
+// Per-cloud frame used to key queries: the group-ordered rank of the cloud
+// and its Morton frame.
 struct BatchFrame {
     double o0, o1, o2;
     float inv_ext;
-    float pad;
+    uint32_t rank;
 };
 
+// Ranks the clouds so that those of one kernel specialisation (weight type,
+// number of sigmas, blend rule) are consecutive and fills frames[i].rank,
+// rank_slot (n_clouds + 1 entries) and rank_cloud (n_clouds); groups receive
+// the slot ranges.  Host only.
+void plan_batch_groups(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, BatchFrame* frames,
+                       int64_t* rank_slot, int32_t* rank_cloud, std::vector<BatchGroup>& groups);
+
 cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int sm_count, cudaStream_t s);
-cudaError_t launch_mlod_batch(const BatchArgs& b, int sm_count, int grid_scale_pct, cudaStream_t s);
+cudaError_t launch_mlod_batch(const BatchArgs& b, const std::vector<BatchGroup>& groups, int sm_count,
+                              int grid_scale_pct, cudaStream_t s);
 
 // Swaps query points invalid[i] and end_valid-1-i (GPUUtils.cu:413-424).
 cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_invalid, uint32_t end_valid,
@@ -77,8 +105,10 @@ cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_i
 size_t query_order_temp_bytes(int64_t n);
 cudaError_t compute_query_order(const float* d_q, int64_t n, const double origin[3], float extent, uint32_t* d_order,
                                 void* temp, cudaStream_t s);
-// Same for a batch: grouped by cloud, Morton order inside each cloud.
+// Same for a batch: grouped by cloud rank, Morton order inside each cloud
+// (input order when morton is false).
 cudaError_t compute_batch_order(const float* d_q, int64_t n, const int64_t* d_q_offsets, int n_clouds,
-                                const BatchFrame* d_frames, uint32_t* d_order, void* temp, cudaStream_t s);
+                                const BatchFrame* d_frames, bool morton, uint32_t* d_order, void* temp,
+                                cudaStream_t s);
 
 }  // namespace mlods

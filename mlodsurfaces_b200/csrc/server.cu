@@ -53,9 +53,13 @@ struct Worker {
     mlods::CloudArgs* h_clouds = nullptr;  // pinned
     int64_t* h_offsets = nullptr;
     mlods::BatchFrame* h_frames = nullptr;
+    int64_t* h_rank_slot = nullptr;
+    int32_t* h_rank_cloud = nullptr;
     mlods::CloudArgs* d_clouds = nullptr;
     int64_t* d_offsets = nullptr;
     mlods::BatchFrame* d_frames = nullptr;
+    int64_t* d_rank_slot = nullptr;
+    int32_t* d_rank_cloud = nullptr;
     size_t cloud_cap = 0;
     int64_t* d_stats = nullptr;
     void* d_order = nullptr;  // query order and its sort buffers
@@ -86,6 +90,7 @@ namespace mlods
 namespace
 {
 inline size_t al256(size_t v) { return (v + 255) / 256 * 256; }
+constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + kMaxBatchGroups * sizeof(unsigned int);
 
 int grow_pinned(void** p, size_t bytes)
 {
@@ -123,6 +128,10 @@ int ensure_capacity(Worker& w, int64_t total, size_t n_req)
         if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_clouds), cap * sizeof(CloudArgs));
         if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_offsets), (cap + 1) * sizeof(int64_t));
         if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_frames), cap * sizeof(BatchFrame));
+        if (rc == MLODS_OK) rc = grow_pinned(reinterpret_cast<void**>(&w.h_rank_slot), (cap + 1) * sizeof(int64_t));
+        if (rc == MLODS_OK) rc = grow_pinned(reinterpret_cast<void**>(&w.h_rank_cloud), cap * sizeof(int32_t));
+        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_rank_slot), (cap + 1) * sizeof(int64_t));
+        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_rank_cloud), cap * sizeof(int32_t));
         if (rc != MLODS_OK) return rc;
         w.cloud_cap = cap;
     }
@@ -153,32 +162,36 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Request*>& batch)
         if (r->own_kernel) c.kc = r->kc;
         float ext = 0.f;
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
-        w.h_frames[i] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f, 0.f};
+        w.h_frames[i] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f, 0u};
         w.h_offsets[i] = off;
         off += r->n;
     }
     w.h_offsets[batch.size()] = total;
     const size_t nc = batch.size();
+    std::vector<BatchGroup> groups;
+    plan_batch_groups(w.h_clouds, w.h_offsets, int(nc), w.h_frames, w.h_rank_slot, w.h_rank_cloud, groups);
     MLODS_CUDA(cudaMemcpyAsync(dq, hq, size_t(total) * 12, cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_clouds, w.h_clouds, nc * sizeof(CloudArgs), cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_offsets, w.h_offsets, (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_frames, w.h_frames, nc * sizeof(BatchFrame), cudaMemcpyHostToDevice, w.s));
-    MLODS_CUDA(cudaMemsetAsync(w.d_stats, 0, 8 * sizeof(int64_t), w.s));
-    uint32_t* order = nullptr;
-    if (total > 1) {
-        order = static_cast<uint32_t*>(w.d_order);
-        char* tmp = static_cast<char*>(w.d_order) + al256(size_t(total) * 4);
-        MLODS_CUDA(compute_batch_order(dq, total, w.d_offsets, int(nc), w.d_frames, order, tmp, w.s));
-    }
+    MLODS_CUDA(cudaMemcpyAsync(w.d_rank_slot, w.h_rank_slot, (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                               w.s));
+    MLODS_CUDA(cudaMemcpyAsync(w.d_rank_cloud, w.h_rank_cloud, nc * sizeof(int32_t), cudaMemcpyHostToDevice, w.s));
+    MLODS_CUDA(cudaMemsetAsync(w.d_stats, 0, kStatsBytes, w.s));
+    uint32_t* order = static_cast<uint32_t*>(w.d_order);
+    char* tmp = static_cast<char*>(w.d_order) + al256(size_t(total) * 4);
+    MLODS_CUDA(compute_batch_order(dq, total, w.d_offsets, int(nc), w.d_frames, true, order, tmp, w.s));
     BatchArgs a;
     a.clouds = w.d_clouds;
     a.q_offsets = w.d_offsets;
     a.n_clouds = int(nc);
     a.total = total;
     a.order = order;
-    a.counter = reinterpret_cast<unsigned int*>(w.d_stats + 3);
+    a.rank_slot = w.d_rank_slot;
+    a.rank_cloud = w.d_rank_cloud;
+    a.counters = reinterpret_cast<unsigned int*>(w.d_stats + 8);
     a.stats = w.d_stats;
-    MLODS_CUDA(launch_mlod_batch(a, sm_count_for_current_device(), 100, w.s));
+    MLODS_CUDA(launch_mlod_batch(a, groups, sm_count_for_current_device(), 100, w.s));
     MLODS_CUDA(cudaMemcpyAsync(hp, dp, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s));
     MLODS_CUDA(cudaMemcpyAsync(hn, dn, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s));
     MLODS_CUDA(cudaStreamSynchronize(w.s));
@@ -243,6 +256,10 @@ void destroy_worker(Worker* w)
     cudaFreeHost(w->h_clouds);
     cudaFreeHost(w->h_offsets);
     cudaFreeHost(w->h_frames);
+    cudaFreeHost(w->h_rank_slot);
+    cudaFreeHost(w->h_rank_cloud);
+    cudaFree(w->d_rank_slot);
+    cudaFree(w->d_rank_cloud);
     cudaFree(w->d_buf);
     cudaFree(w->d_clouds);
     cudaFree(w->d_offsets);
@@ -329,7 +346,7 @@ int mlods_server_create(const mlods_tree* trees, int32_t n_trees, const mlods_se
     for (int i = 0; i < c.n_streams; ++i) {
         auto* w = new (std::nothrow) Worker();
         cudaError_t e = w ? cudaStreamCreateWithFlags(&w->s, cudaStreamNonBlocking) : cudaErrorMemoryAllocation;
-        if (e == cudaSuccess) e = cudaMalloc(&w->d_stats, 8 * sizeof(int64_t));
+        if (e == cudaSuccess) e = cudaMalloc(&w->d_stats, kStatsBytes);
         if (e != cudaSuccess) {
             destroy_worker(w);
             stop_server(S);
