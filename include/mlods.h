@@ -367,6 +367,16 @@ int mlods_cloud_save(const char* path, const float* pts, const float* nrm, int64
                      float norme);
 int mlods_cloud_normalize(const float* pts, int64_t n, float* out_pts, float* offset, float* norme);
 
+/* Pn::order (Pn.cpp:388-440): perm receives the point indices sorted by
+ * their Morton code on a grid^3 lattice over the points' cube (grid 64 in
+ * the reference); equal codes keep their input order.
+ * Pn::initialize(n, pointSetToFit, factor) (Pn.cpp:324-357): n_out queries,
+ * each an input point moved inside the disk of radius meanGap of its tangent
+ * plane, with the point's normal; seeded (the reference's draws are not). */
+int mlods_cloud_morton_order(const float* pts, int64_t n, int32_t grid, uint32_t* perm);
+int mlods_cloud_sample_around(const float* pts, const float* nrm, int64_t n_pts, int64_t n_out, float factor,
+                              uint64_t seed, float* out_pts, float* out_nrm);
+
 #define MLODS_PARAMS_FILE_BYTES 134
 typedef struct mlods_scene_params {
     float cam_quat[4];          /* viewer camera (not used by the projection) */

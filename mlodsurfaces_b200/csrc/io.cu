@@ -15,6 +15,7 @@
 #include <cstring>
 #include <fstream>
 #include <new>
+#include <random>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -449,6 +450,97 @@ int mlods_cloud_normalize(const float* pts, int64_t n, float* out_pts, float* of
     std::memcpy(out_pts, c.pos.data(), c.pos.size() * sizeof(float));
     if (offset) std::memcpy(offset, c.offset, sizeof c.offset);
     if (norme) *norme = c.norme;
+    return MLODS_OK;
+}
+
+// Pn::order (Pn.cpp:388-440): Morton codes of the points on a grid^3 lattice
+// over the cube [min, max]^3 of the box's extreme coordinates (x to bits
+// 1, 4, 7..., y to 0, 3, 6..., z to 2, 5, 8...), points sorted by code.  The
+// reference's std::sort leaves equal codes in unspecified order; here they
+// keep their input order (counting sort).
+int mlods_cloud_morton_order(const float* pts, int64_t n, int32_t grid, uint32_t* perm)
+{
+    if (!pts || !perm || n < 0 || n >= (int64_t(1) << 32) || grid < 1 || grid > 1024) {
+        set_last_error("cloud morton order: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    if (n == 0) return MLODS_OK;
+    float mn[3], mx[3];
+    for (int a = 0; a < 3; ++a) mn[a] = mx[a] = pts[a];
+    for (int64_t i = 1; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            const float v = pts[3 * i + a];
+            if (v < mn[a]) mn[a] = v;
+            if (v > mx[a]) mx[a] = v;
+        }
+    const float lo = std::min(std::min(mn[0], mn[1]), mn[2]);
+    const float hi = std::max(std::max(mx[0], mx[1]), mx[2]);
+    const float norme = hi - lo;
+    int bits = 0;
+    while ((1 << bits) < grid) ++bits;
+    std::vector<uint32_t> code(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t c[3];
+        for (int a = 0; a < 3; ++a) {
+            const float t = std::floor((pts[3 * i + a] - lo) / norme * float(grid));
+            c[a] = (t > 0.f) ? std::min(uint32_t(t), uint32_t(grid - 1)) : 0u;  // glm::clamp to [0, grid-1]
+        }
+        uint32_t m = 0;
+        for (int b = 0; b < bits && 3 * b + 2 < 32; ++b)
+            m |= ((c[1] >> b) & 1u) << (3 * b) | ((c[0] >> b) & 1u) << (3 * b + 1) | ((c[2] >> b) & 1u) << (3 * b + 2);
+        code[size_t(i)] = m;
+    }
+    const size_t ncodes = size_t(1) << std::min(30, 3 * bits);
+    std::vector<uint32_t> start(ncodes + 1, 0);
+    for (uint32_t m : code) ++start[m + 1];
+    for (size_t k = 0; k < ncodes; ++k) start[k + 1] += start[k];
+    for (int64_t i = 0; i < n; ++i) perm[start[code[size_t(i)]]++] = uint32_t(i);
+    return MLODS_OK;
+}
+
+// Pn::initialize(n, pointSetToFit, factor) (Pn.cpp:324-357): n queries, each
+// a random input point moved by a random vector of the disk of radius
+// meanGap in its tangent plane (meanGap = 2 * cbrt(pi / n_points) * factor,
+// Pn::computeMeanGap, Pn.cpp:170-176).  The reference draws from rand() and
+// a std::random_device seed; here one seeded std::mt19937 does.
+int mlods_cloud_sample_around(const float* pts, const float* nrm, int64_t n_pts, int64_t n_out, float factor,
+                              uint64_t seed, float* out_pts, float* out_nrm)
+{
+    if (!pts || !nrm || n_pts <= 0 || n_out < 0 || !out_pts) {
+        set_last_error("cloud sample: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    const float r = 0.5f;
+    const float surface = 4.f * float(M_PI) * r * r;
+    const float gap = (std::cbrt(surface / float(n_pts)) * 2.f) * factor;
+    std::mt19937_64 mt(seed);
+    std::uniform_int_distribution<int64_t> pick(0, n_pts - 1);
+    std::uniform_real_distribution<float> unit(0.f, 1.f);
+    auto cross = [](const float* a, const float* b, float* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    auto normalize3 = [](float* v) {
+        const float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int a = 0; a < 3; ++a) v[a] /= l;
+    };
+    for (int64_t i = 0; i < n_out; ++i) {
+        const int64_t k = pick(mt);
+        const float* p = pts + 3 * k;
+        const float* nv = nrm + 3 * k;
+        static const float ez[3] = {0.f, 0.f, 1.f}, ey[3] = {0.f, 1.f, 0.f};
+        float e1[3], e2[3];
+        cross(nv, nv[2] != 0.f ? ez : ey, e1);  // dot(n, (0, 0, 1)) != 0
+        normalize3(e1);
+        cross(nv, e1, e2);
+        normalize3(e2);
+        const float rr = gap * std::sqrt(unit(mt));
+        const float th = unit(mt) * 2.f * float(M_PI);
+        for (int a = 0; a < 3; ++a) out_pts[3 * i + a] = p[a] + (rr * std::cos(th) * e1[a] + rr * std::sin(th) * e2[a]);
+        if (out_nrm)
+            for (int a = 0; a < 3; ++a) out_nrm[3 * i + a] = nv[a];
+    }
     return MLODS_OK;
 }
 

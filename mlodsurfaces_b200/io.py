@@ -65,6 +65,29 @@ def normalize(points):
     return out, off, float(norme.value)
 
 
+def morton_order(points, grid: int = 64) -> np.ndarray:
+    """Pn::order: the permutation that sorts the points by Morton code on a
+    grid^3 lattice (ties keep their input order)."""
+    lib = capi.load()
+    p = np.ascontiguousarray(np.asarray(points, np.float32).reshape(-1, 3))
+    perm = np.empty(len(p), np.uint32)
+    capi.check(lib.mlods_cloud_morton_order(capi.ptr(p), len(p), int(grid), capi.ptr(perm)))
+    return perm
+
+
+def sample_around(points, normals, n: int, factor: float = 1.0, seed: int = 0):
+    """Pn::initialize(n, pointSetToFit, factor): n queries near the points
+    (random tangent-disk offsets of radius meanGap), with their normals."""
+    lib = capi.load()
+    p = np.ascontiguousarray(np.asarray(points, np.float32).reshape(-1, 3))
+    nv = np.ascontiguousarray(np.asarray(normals, np.float32).reshape(-1, 3))
+    out_p = np.empty((int(n), 3), np.float32)
+    out_n = np.empty((int(n), 3), np.float32)
+    capi.check(lib.mlods_cloud_sample_around(capi.ptr(p), capi.ptr(nv), len(p), int(n), float(factor),
+                                             C.c_uint64(seed), capi.ptr(out_p), capi.ptr(out_n)))
+    return out_p, out_n
+
+
 _ARRAYS = {"cam_quat": 4, "cam_translation": 3, "fixed_sigmas": 5, "offset": 6}
 
 

@@ -141,3 +141,37 @@ def test_reference_params_files(tmp_path):
     with pytest.raises(MlodsError):
         (tmp_path / "short.params").write_bytes(b"\0" * 100)
         io.load_params(tmp_path / "short.params")
+
+
+def morton_restated(p, grid=64):
+    """Pn::order's codes (Pn.cpp:388-440) and a stable sort."""
+    p = np.asarray(p, np.float32)
+    lo = np.float32(min(p[:, 0].min(), p[:, 1].min(), p[:, 2].min()))
+    hi = np.float32(max(p[:, 0].max(), p[:, 1].max(), p[:, 2].max()))
+    norme = np.float32(hi - lo)
+    t = np.floor((((p - lo).astype(np.float32) / norme).astype(np.float32) * np.float32(grid)).astype(np.float32))
+    c = np.clip(t, 0, grid - 1).astype(np.uint64)
+    code = np.zeros(len(p), np.uint64)
+    for b in range(6):
+        code |= ((c[:, 1] >> b) & 1) << (3 * b) | ((c[:, 0] >> b) & 1) << (3 * b + 1) | ((c[:, 2] >> b) & 1) << (3 * b + 2)
+    return np.argsort(code, kind="stable")
+
+
+def test_morton_order_matches_restatement():
+    pts, _ = synth.torus(20000, seed=8)
+    perm = io.morton_order(pts)
+    assert np.array_equal(perm.astype(np.int64), morton_restated(pts))
+    assert sorted(perm.tolist()) == list(range(len(pts)))
+
+
+def test_sample_around_stays_on_tangent_disks():
+    pts, nrm = synth.torus(5000, seed=9)
+    q, qn = io.sample_around(pts, nrm, 3000, factor=1.0, seed=3)
+    gap = 2.0 * np.cbrt(np.pi / len(pts))
+    # every query is within meanGap of some input point, in that point's tangent plane
+    from scipy.spatial import cKDTree
+    d, k = cKDTree(pts).query(q)
+    assert d.max() <= gap * 1.0001
+    q2, _ = io.sample_around(pts, nrm, 3000, factor=1.0, seed=3)
+    assert np.array_equal(q, q2)  # seeded
+    assert np.allclose(np.linalg.norm(qn, axis=1), 1.0, atol=1e-5)
