@@ -55,6 +55,7 @@ def parse_args():
     ap.add_argument("--rate", type=float, default=0.0, help="serve: request arrivals per second (0 = 70%% of "
                                                                "the measured capacity)")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-batch", type=int, default=1 << 18, help="serve: largest batch in queries")
     ap.add_argument("--dc-depth", type=int, default=9)
     return ap.parse_args()
 
@@ -465,6 +466,7 @@ def run_dc(args):
     mesh = f.dc_mesh(grid)
     mesh_ms = 1e3 * (time.perf_counter() - t0)
     v, _, tri = mesh.arrays()
+    inside = mesh.stage_ms()
     # the same pipeline from its parts, timed per stage
     from mlodsurfaces_b200 import Mesh
 
@@ -510,7 +512,8 @@ def run_dc(args):
                    "l2": "inputs larger than L2 (tree + corner buffers)"},
         "stages_ms": {"tree_build": build_ms, "adaptive_grid": grid_ms, "corner_field": statistics.mean(step_ms),
                       "corner_projection_kernel": kms, "mesh_pipeline": mesh_ms,
-                      "mesh_parts": {k: round(v_, 1) for k, v_ in parts.items()}},
+                      "mesh_stages": {k: round(v_, 1) for k, v_ in inside.items()},
+                      "mesh_parts_host_path": {k: round(v_, 1) for k, v_ in parts.items()}},
         "mesh": {"vertices": int(len(v)), "triangles": int(len(tri))},
         "e2e": {"value": value, "unit": "corners/s", "h2d_bytes_per_step": int(grid.cells.nbytes),
                 "d2h_bytes_per_step": int(cf.nbytes + vx.nbytes + nc.nbytes),
@@ -737,7 +740,9 @@ def run_serve(args):
             k.constant_shift = 1e-3
         return ci, pools[ci][start:start + n], k
 
-    srv = ProjectionServer(projectors, n_streams=2)
+    # small batches keep a request's wait short, large ones amortise the
+    # per-batch work; a request larger than the cap runs alone
+    srv = ProjectionServer(projectors, n_streams=2, max_batch_queries=args.serve_batch)
     iters = args.iters
     # capacity: a closed loop of back-to-back requests
     r0 = np.random.default_rng(5)
@@ -816,6 +821,7 @@ def run_serve(args):
         "config": {"workload": "serving: 8 resident clouds, Poisson arrivals, request sizes log-uniform "
                                "in [1e3, 1e6], per-request kernels",
                    "n_points": int(sum(len(c[0]) for c in clouds)), "iterations": iters, "n_streams": 2,
+                   "max_batch_queries": args.serve_batch,
                    "offered_rate_rps": rate, "closed_loop_capacity_rps": capacity_rps,
                    "seconds": args.serve_seconds},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),

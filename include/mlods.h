@@ -251,6 +251,10 @@ int mlods_mesh_smooth(mlods_mesh m);
 int mlods_mesh_subdivide(mlods_mesh m);
 int mlods_mesh_project(mlods_tree t, mlods_mesh m, int32_t n_iterations, void* stream);
 int mlods_mesh_free(mlods_mesh m);
+/* Host wall time (ms) of mlods_dc_mesh's 7 stages: corner field, extraction,
+ * upload + transform, projections, smoothing, subdivision, download (zeros
+ * for meshes built otherwise). */
+int mlods_mesh_stage_ms(mlods_mesh m, double* ms);
 int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t refine_rounds, void* stream,
                   mlods_mesh* out);
 

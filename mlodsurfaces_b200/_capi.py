@@ -177,6 +177,7 @@ SIGNATURES = {
     "mlods_mesh_subdivide": (C.c_int, [_P]),
     "mlods_mesh_project": (C.c_int, [_P, _P, C.c_int32, _P]),
     "mlods_mesh_free": (C.c_int, [_P]),
+    "mlods_mesh_stage_ms": (C.c_int, [_P, _P]),
     "mlods_dc_mesh": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P, C.POINTER(_P)]),
     "mlods_server_default_config": (None, [C.POINTER(mlods_server_config)]),
     "mlods_server_create": (C.c_int, [_P, C.c_int32, C.POINTER(mlods_server_config), C.POINTER(_P)]),

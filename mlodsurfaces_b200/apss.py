@@ -340,6 +340,13 @@ class Mesh:
         """(vertices (n, 3), normals (n, 3), triangles (m, 3) uint32)."""
         return _mesh_arrays(self._lib, self._m)
 
+    def stage_ms(self) -> dict:
+        """Host time of the pipeline stages of APSS.dc_mesh (ms)."""
+        ms = np.zeros(7, np.float64)
+        capi.check(self._lib.mlods_mesh_stage_ms(self._m, capi.ptr(ms)))
+        names = ("corner_field", "extract", "upload", "project", "smooth", "subdivide", "download")
+        return {k: float(v) for k, v in zip(names, ms)}
+
     def transform(self, xform) -> None:
         x = np.ascontiguousarray(np.asarray(xform, np.float32).reshape(3, 4))
         capi.check(self._lib.mlods_mesh_transform(self._m, capi.ptr(x)))

@@ -232,10 +232,11 @@ inline size_t al(size_t v) { return (v + 255) / 256 * 256; }
 
 }  // namespace
 
-int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
-                int use_normals, float* corner_f, float* vertex, int32_t* n_cross, int64_t* n_unique, cudaStream_t s)
+int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
+                    int use_normals, DcField& out, cudaStream_t s)
 {
-    if (n_cells <= 0 || !cells || !xform || !corner_f || !vertex || !n_cross) {
+    dc_field_free(out);
+    if (n_cells <= 0 || !cells || !xform) {
         set_last_error("dc evaluate: bad arguments");
         return MLODS_ERR_INVALID;
     }
@@ -269,6 +270,7 @@ int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_
              al(size_t(n_cells) * 16);
     char* base = nullptr;
     MLODS_CUDA(cudaMalloc(&base, bytes));
+    out.base = base;
     size_t off = 0;
     auto take = [&](size_t b) {
         char* p = base + off;
@@ -290,9 +292,8 @@ int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_
     float* d_cn = use_normals ? reinterpret_cast<float*>(take(size_t(nc8) * 12)) : nullptr;
     float* d_vert = reinterpret_cast<float*>(take(size_t(n_cells) * 12));
     int32_t* d_ncross = reinterpret_cast<int32_t*>(d_vert + 3 * n_cells);
-
     auto fail = [&](cudaError_t e, const char* what) {
-        cudaFree(base);
+        dc_field_free(out);
         return cuda_fail(e, what, __FILE__, __LINE__);
     };
 #define DC_CHECK(call, what)                            \
@@ -329,7 +330,7 @@ int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_
     // one projection step of every unique corner (scene.cpp:1382-1386)
     int rc = project_buffers(T, U, cpos, cproj, cnrm, 1, -1.f, s);
     if (rc != MLODS_OK) {
-        cudaFree(base);
+        dc_field_free(out);
         return rc;
     }
     field_kernel<<<grid_for(U), kThreads, 0, s>>>(cpos, cproj, cnrm, U, cf);
@@ -341,13 +342,40 @@ int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_
     vertex_kernel<<<grid_for(n_cells), kThreads, 0, s>>>(d_cells, n_cells, max_depth, d_cf, d_cn, d_vert, d_ncross);
     note_launch();
     DC_CHECK(cudaGetLastError(), "vertex");
-    DC_CHECK(cudaMemcpyAsync(corner_f, d_cf, size_t(nc8) * 4, cudaMemcpyDeviceToHost, s), "download field");
-    DC_CHECK(cudaMemcpyAsync(vertex, d_vert, size_t(n_cells) * 12, cudaMemcpyDeviceToHost, s), "download vertex");
-    DC_CHECK(cudaMemcpyAsync(n_cross, d_ncross, size_t(n_cells) * 4, cudaMemcpyDeviceToHost, s), "download counts");
     DC_CHECK(cudaStreamSynchronize(s), "sync dc");
 #undef DC_CHECK
-    cudaFree(base);
-    if (n_unique) *n_unique = U;
+    out.cells = d_cells;
+    out.cf = d_cf;
+    out.vert = d_vert;
+    out.ncross = d_ncross;
+    out.n = n_cells;
+    out.n_unique = U;
+    return MLODS_OK;
+}
+
+void dc_field_free(DcField& f)
+{
+    cudaFree(f.base);
+    f = DcField{};
+}
+
+int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
+                int use_normals, float* corner_f, float* vertex, int32_t* n_cross, int64_t* n_unique, cudaStream_t s)
+{
+    if (!corner_f || !vertex || !n_cross) {
+        set_last_error("dc evaluate: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    DcField f;
+    int rc = dc_field_device(T, n_cells, cells, max_depth, xform, use_normals, f, s);
+    if (rc != MLODS_OK) return rc;
+    cudaError_t e = cudaMemcpyAsync(corner_f, f.cf, size_t(n_cells) * 32, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vertex, f.vert, size_t(n_cells) * 12, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(n_cross, f.ncross, size_t(n_cells) * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (n_unique) *n_unique = f.n_unique;
+    dc_field_free(f);
+    if (e != cudaSuccess) return cuda_fail(e, "dc evaluate: download", __FILE__, __LINE__);
     return MLODS_OK;
 }
 

@@ -83,6 +83,31 @@ int dmesh_project(mlods_tree_s* T, DeviceMesh& m, int iters, cudaStream_t s);
 int dmesh_smooth(DeviceMesh& m, cudaStream_t s);
 int dmesh_subdivide(DeviceMesh& m, cudaStream_t s);
 
+// The corner field of a grid kept in device memory: cells (int4), 8 corner
+// values, vertex and crossing count per cell, in one allocation.
+struct DcField {
+    void* base = nullptr;
+    const int4* cells = nullptr;
+    float* cf = nullptr;
+    float* vert = nullptr;
+    int32_t* ncross = nullptr;
+    int64_t n = 0, n_unique = 0;
+};
+int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
+                    int use_normals, DcField& out, cudaStream_t s);
+void dc_field_free(DcField& f);
+
+// Extraction on the device (dc_extract_dev.cu) from a device field; the mesh
+// goes to `out` (unit-frame vertices).  *used_device is false when the grid
+// is too deep for the device path (the caller then extracts on the host).
+int dc_extract_device(const int4* d_cells, int64_t n_cells, const int64_t* h_depth_begin, int max_depth,
+                      const float* d_cf, const float* d_cell_vertex, DeviceMesh& out, bool* used_device,
+                      cudaStream_t s);
+int dmesh_reserve(DeviceMesh& m, int64_t nv, int64_t nt);
+float* dmesh_pos(DeviceMesh& m);
+float* dmesh_nrm(DeviceMesh& m);
+uint32_t* dmesh_tri(DeviceMesh& m);
+
 // Field at the 8 corners of every cell (unique corners projected once) and
 // the per-cell vertex; host arrays in and out.
 int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,

@@ -248,7 +248,7 @@ __global__ void enclosing_kernel(const uint64_t* __restrict__ k, int64_t n, cons
 // 27-neighbourhoods); a root kept for a failed projection deeper down gives
 // its 8 children only (they are not at depth + 1, so not expanded)
 __global__ void children_block_kernel(const uint64_t* __restrict__ k, int64_t n, int depth,
-                                      uint64_t* __restrict__ out, const int64_t* __restrict__ out_off)
+                                      uint64_t* __restrict__ out, const uint32_t* __restrict__ out_off)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -266,10 +266,10 @@ __global__ void children_block_kernel(const uint64_t* __restrict__ k, int64_t n,
     }
 }
 
-__global__ void block_sizes_kernel(const uint64_t* __restrict__ k, int64_t n, int depth, int64_t* __restrict__ sz)
+__global__ void block_sizes_kernel(const uint64_t* __restrict__ k, int64_t n, int depth, uint32_t* __restrict__ sz)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) sz[i] = key_depth(k[i]) == depth ? 64 : 8;
+    if (i < n) sz[i] = key_depth(k[i]) == depth ? 64u : 8u;
 }
 
 __global__ void ancestor_kernel(const uint64_t* __restrict__ k, int64_t n, int depth, uint64_t* __restrict__ out)
@@ -358,14 +358,17 @@ struct Gen {
     int64_t projected = 0;
     float* d_proj = nullptr;  // 9 floats per cell (centre, projection, normal)
     size_t proj_cap = 0;
-    int64_t* d_off = nullptr;
+    uint32_t* d_off = nullptr;  // block sizes, then their exclusive scan (+ total)
     size_t off_cap = 0;
+    void* d_scan = nullptr;
+    size_t scan_cap = 0;
     int* d_mm = nullptr;
     unsigned long long* d_hist = nullptr;
     ~Gen()
     {
         cudaFree(d_proj);
         cudaFree(d_off);
+        cudaFree(d_scan);
         cudaFree(d_mm);
         cudaFree(d_hist);
     }
@@ -430,23 +433,28 @@ struct Gen {
             cudaFree(d_off);
             d_off = nullptr;
             off_cap = 0;
-            MLODS_CUDA(cudaMalloc(&d_off, (size_t(n) + 1) * 8));
+            MLODS_CUDA(cudaMalloc(&d_off, (size_t(n) + 1) * 4));
             off_cap = size_t(n) + 1;
+        }
+        if (scan_cap < scan_temp_bytes(n)) {
+            cudaFree(d_scan);
+            d_scan = nullptr;
+            scan_cap = 0;
+            MLODS_CUDA(cudaMalloc(&d_scan, scan_temp_bytes(n)));
+            scan_cap = scan_temp_bytes(n);
+        }
+        if (n > (int64_t(1) << 25)) {  // 64 keys each must stay within 32-bit offsets
+            set_last_error("dc adaptive grid: %lld kept cells in one level exceed the supported 2^25", (long long)n);
+            return MLODS_ERR_CAPACITY;
         }
         block_sizes_kernel<<<blocks_for(n), kThreads, 0, s>>>(sub.a, n, depth, d_off);
         note_launch();
         MLODS_CUDA(cudaGetLastError());
-        // offsets on the host: sub is at most a few million cells
-        std::vector<int64_t> h(size_t(n) + 1);
-        MLODS_CUDA(cudaMemcpyAsync(h.data(), d_off, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
+        MLODS_CUDA(exclusive_scan_u32(d_off, d_off, n, d_off + n, d_scan, s));
+        uint32_t total32 = 0;
+        MLODS_CUDA(cudaMemcpyAsync(&total32, d_off + n, 4, cudaMemcpyDeviceToHost, s));
         MLODS_CUDA(cudaStreamSynchronize(s));
-        int64_t acc = 0;
-        for (int64_t i = 0; i < n; ++i) {
-            const int64_t v = h[size_t(i)];
-            h[size_t(i)] = acc;
-            acc += v;
-        }
-        MLODS_CUDA(cudaMemcpyAsync(d_off, h.data(), size_t(n) * 8, cudaMemcpyHostToDevice, s));
+        const int64_t acc = int64_t(total32);
         int rc = reserve(out, acc, false, s);
         if (rc != MLODS_OK) return rc;
         children_block_kernel<<<blocks_for(n), kThreads, 0, s>>>(sub.a, n, depth, out.a, d_off);

@@ -13,6 +13,7 @@
 // on the device.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -27,6 +28,9 @@ struct mlods_mesh_s {
     std::vector<float> pos;  // 3 per vertex
     std::vector<float> nrm;  // 3 per vertex
     std::vector<uint32_t> tri;
+    // host wall time of mlods_dc_mesh's stages (ms): corner field, extraction,
+    // upload + transform, projections, smoothing, subdivision, download
+    double stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace mlods
@@ -488,6 +492,16 @@ int mlods_mesh_get(mlods_mesh m, float* vertices, float* normals, uint32_t* indi
     return MLODS_OK;
 }
 
+int mlods_mesh_stage_ms(mlods_mesh m, double* ms)
+{
+    if (!m || !ms) {
+        set_last_error("mesh stage times: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    std::memcpy(ms, m->stage_ms, sizeof m->stage_ms);
+    return MLODS_OK;
+}
+
 int mlods_mesh_free(mlods_mesh m)
 {
     delete m;
@@ -551,37 +565,62 @@ int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t ref
         set_last_error("dc mesh: empty grid");
         return MLODS_ERR_INVALID;
     }
-    std::vector<float> cf(size_t(n) * 8), vx(size_t(n) * 3);
-    std::vector<int32_t> nc(static_cast<size_t>(n));
-    int64_t nu = 0;
-    int rc = dc_evaluate(t, n, g->cells.data(), g->max_depth, g->xform, use_normals, cf.data(), vx.data(), nc.data(),
-                         &nu, s);
-    if (rc != MLODS_OK) return rc;
+    using clk = std::chrono::steady_clock;
+    auto since = [](clk::time_point t0) { return std::chrono::duration<double, std::milli>(clk::now() - t0).count(); };
     auto* m = new (std::nothrow) mlods_mesh_s();
-    if (!m) {
+    DeviceMesh* dmp = dmesh_create();
+    if (!m || !dmp) {
+        delete m;
+        dmesh_destroy(dmp);
         set_last_error("dc mesh: host allocation failed");
         return MLODS_ERR_CAPACITY;
     }
-    rc = dc_extract(g->cells.data(), n, cf.data(), vx.data(), m);
-    // the refinement loop stays in device memory (mesh_dev.cu)
-    DeviceMesh* dmp = rc == MLODS_OK ? dmesh_create() : nullptr;
-    if (rc == MLODS_OK && !dmp) {
-        set_last_error("dc mesh: host allocation failed");
-        rc = MLODS_ERR_CAPACITY;
-    }
+    DeviceMesh& dm = *dmp;
+    // corner field in device memory
+    auto t0 = clk::now();
+    DcField field;
+    int rc = dc_field_device(t, n, g->cells.data(), g->max_depth, g->xform, use_normals, field, s);
+    m->stage_ms[0] = since(t0);
+    // extraction: on the device when the grid allows, else on the host
+    t0 = clk::now();
+    bool on_device = false;
     if (rc == MLODS_OK) {
-        DeviceMesh& dm = *dmp;
-        rc = dmesh_upload(dm, m->pos.data(), int64_t(m->pos.size() / 3), m->tri.data(), int64_t(m->tri.size() / 3),
-                          s);
-        if (rc == MLODS_OK) rc = dmesh_transform(dm, g->xform, s);  // scene.cpp:1400-1408
-        if (rc == MLODS_OK) rc = dmesh_project(t, dm, 3, s);
-        for (int r = 0; rc == MLODS_OK && r < refine_rounds; ++r) {
-            rc = dmesh_smooth(dm, s);
-            if (rc == MLODS_OK) rc = dmesh_subdivide(dm, s);
-            if (rc == MLODS_OK) rc = dmesh_project(t, dm, 3, s);
-        }
-        if (rc == MLODS_OK) rc = dmesh_download(dm, m->pos, m->nrm, m->tri, s);
+        std::vector<int64_t> begin(size_t(g->max_depth) + 2, n);
+        for (int64_t i = n - 1; i >= 0; --i) begin[size_t(g->cells[4 * size_t(i)])] = i;
+        for (int d = g->max_depth; d >= 0; --d) begin[size_t(d)] = std::min(begin[size_t(d)], begin[size_t(d) + 1]);
+        rc = dc_extract_device(field.cells, n, begin.data(), g->max_depth, field.cf, field.vert, dm, &on_device, s);
     }
+    if (rc == MLODS_OK && !on_device) {
+        std::vector<float> cf(size_t(n) * 8), vx(size_t(n) * 3);
+        cudaError_t e = cudaMemcpyAsync(cf.data(), field.cf, cf.size() * 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(vx.data(), field.vert, vx.size() * 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        rc = e == cudaSuccess ? dc_extract(g->cells.data(), n, cf.data(), vx.data(), m)
+                              : cuda_fail(e, "dc mesh: field download", __FILE__, __LINE__);
+        if (rc == MLODS_OK)
+            rc = dmesh_upload(dm, m->pos.data(), int64_t(m->pos.size() / 3), m->tri.data(),
+                              int64_t(m->tri.size() / 3), s);
+    }
+    dc_field_free(field);
+    m->stage_ms[1] = since(t0);
+    // the refinement loop stays in device memory (mesh_dev.cu); each stage
+    // ends synchronised, so its host time is its device time plus launches
+    auto stage = [&](int k, auto fn) {
+        if (rc != MLODS_OK) return;
+        const auto ts = clk::now();
+        rc = fn();
+        if (rc == MLODS_OK && cudaStreamSynchronize(s) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "dc mesh stage", __FILE__, __LINE__);
+        m->stage_ms[k] += since(ts);
+    };
+    stage(2, [&] { return dmesh_transform(dm, g->xform, s); });  // scene.cpp:1400-1408
+    stage(3, [&] { return dmesh_project(t, dm, 3, s); });
+    for (int r = 0; rc == MLODS_OK && r < refine_rounds; ++r) {
+        stage(4, [&] { return dmesh_smooth(dm, s); });
+        stage(5, [&] { return dmesh_subdivide(dm, s); });
+        stage(3, [&] { return dmesh_project(t, dm, 3, s); });
+    }
+    stage(6, [&] { return dmesh_download(dm, m->pos, m->nrm, m->tri, s); });
     dmesh_destroy(dmp);
     if (rc != MLODS_OK) {
         delete m;

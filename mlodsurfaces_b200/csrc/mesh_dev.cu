@@ -197,6 +197,20 @@ struct DeviceMesh {
 };
 
 DeviceMesh* dmesh_create() { return new (std::nothrow) DeviceMesh(); }
+
+int dmesh_reserve(DeviceMesh& m, int64_t nv, int64_t nt)
+{
+    int rc = m.pos.need(size_t(std::max<int64_t>(nv, 1)) * 12);
+    if (rc == MLODS_OK) rc = m.nrm.need(size_t(std::max<int64_t>(nv, 1)) * 12);
+    if (rc == MLODS_OK) rc = m.tri.need(size_t(std::max<int64_t>(nt, 1)) * 12);
+    if (rc != MLODS_OK) return rc;
+    m.nv = nv;
+    m.nt = nt;
+    return MLODS_OK;
+}
+float* dmesh_pos(DeviceMesh& m) { return static_cast<float*>(m.pos.p); }
+float* dmesh_nrm(DeviceMesh& m) { return static_cast<float*>(m.nrm.p); }
+uint32_t* dmesh_tri(DeviceMesh& m) { return static_cast<uint32_t*>(m.tri.p); }
 void dmesh_destroy(DeviceMesh* m) { delete m; }
 
 int dmesh_upload(DeviceMesh& m, const float* pos, int64_t nv, const uint32_t* tri, int64_t nt, cudaStream_t s)

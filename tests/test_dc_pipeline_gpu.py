@@ -76,6 +76,27 @@ def unpaired_fraction(t):
     return bad / max(1, len(directed))
 
 
+def test_dc_mesh_on_adaptive_grid_equals_parts(torus_apss):
+    """The device extraction on a shifted, projection-driven grid equals the
+    host extraction of the same field."""
+    pts, nrm, diag, k, f = torus_apss
+    g = DCGrid.adaptive(f, 5)
+    mesh = f.dc_mesh(g, refine_rounds=1)
+    v, n, t = mesh.arrays()
+    cf, vx, nc, _ = f.dc_evaluate(g.cells, g.max_depth, g.xform)
+    m = Mesh.extract(g.cells, cf, vx)
+    m.transform(g.xform)
+    m.project(f, 3)
+    m.smooth()
+    m.subdivide()
+    m.project(f, 3)
+    pv, pn, pt = m.arrays()
+    assert len(t) > 1000
+    assert np.array_equal(t, pt) and np.array_equal(v, pv) and np.array_equal(n, pn)
+    st = mesh.stage_ms()
+    assert st["extract"] > 0 and st["project"] > 0
+
+
 def test_dc_mesh_pipeline(torus_apss):
     pts, nrm, diag, k, f = torus_apss
     g = DCGrid(pts, 5)
