@@ -47,8 +47,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--check-queries", type=int, default=2048, help="queries checked against the FP64 oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["precision", "torus", "dc", "batch", "serve"], default="precision",
-                    help="precision: 2M-point RBF surface, MLoD projection (default); torus: 100k-point torus, "
+    ap.add_argument("--workload", choices=["precision", "knn", "torus", "dc", "batch", "serve"], default="precision",
+                    help="precision: 2M-point RBF surface, MLoD projection (default); knn: the same data, kNN=32 "
+                         "APSS; torus: 100k-point torus, "
                          "CPU-path semantics; dc: 5M-point torus knot, adaptive depth-9 dual contouring; "
                          "batch: 64 resident clouds (about 40M points) in one launch")
     ap.add_argument("--clouds", type=int, default=64)
@@ -68,6 +69,11 @@ SPECS = {
                   "rule_desc": "GPU (Fastapss)",
                   "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag; queries = points + "
                           "N(0, 0.01 diag)"},
+    "knn": {"desc": "precision data, APSS over the 32 nearest neighbours (kNN mode)",
+            "kernel_desc": "multi-Gaussian sigma1=0.01*diag factor 2 x4", "cutoff": 3.0, "rule": 0, "knn": 32,
+            "rule_desc": "kNN APSS (APSSOctree::projectAPSSCPU semantics)",
+            "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag; queries = points + "
+                    "N(0, 0.01 diag)"},
     "torus": {"desc": "torus: 100k-point torus, single Gaussian, CPU-path semantics",
               "kernel_desc": "Gaussian sigma=0.02*diag", "cutoff": 3.0, "rule": 1,
               "rule_desc": "CPU (APSSOctree::projectCPU)",
@@ -207,6 +213,12 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def synth_radius(pts) -> float:
+    """Half the diagonal of the points' tight box (the tree's root radius)."""
+    p = np.asarray(pts, np.float32)
+    return float(np.linalg.norm(p.max(0).astype(np.float64) - p.min(0).astype(np.float64)) / 2)
+
+
 def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out):
     """CPU baseline leg: the reference's own CPU path (oracle/_ref) timed on a
     bounded query sample with every host thread, and the GPU outputs checked
@@ -222,21 +234,29 @@ def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out):
         build_s = time.time() - t0
         sel = rng.choice(len(q), 256, replace=False)
         cutoff = SPECS[args.workload]["cutoff"]
-        _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores)
+        kk = SPECS[args.workload].get("knn", 0)
+        mode = {"mode": 2, "k": kk} if kk else {}
+        _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores, **mode)
         per_q = max(s0 / 256, 1e-7)
         ns = int(min(len(q), max(256, args.cpu_seconds / per_q)))
         sel = rng.choice(len(q), ns, replace=False)
-        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores)
+        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores, **mode)
         out["cpu_baseline"] = {"value": ns / secs, "unit": UNIT, "cores": cores, "kind": "reference",
                                "sample": f"{ns} random queries of the workload, {args.iters} iterations, "
-                                         f"APSSOctree::projectCPU under OpenMP; tree build {build_s:.1f} s "
-                                         f"single-threaded, not included"}
+                                         f"APSSOctree::{'projectAPSSCPU (kNN)' if kk else 'projectCPU'} under "
+                                         f"OpenMP; tree build {build_s:.1f} s single-threaded, not included"}
         del rt
     # accuracy of the GPU result against the FP64 oracle
-    ot = oracle.OracleTree(pts, nrm, 12)
-    sel = rng.choice(len(q), min(args.check_queries, len(q)), replace=False)
-    x64, _ = ot.project_mlod(q[sel], args.iters, kernel, rule=SPECS[args.workload]["rule"],
-                             cutoff=SPECS[args.workload]["cutoff"])
+    kk = SPECS[args.workload].get("knn", 0)
+    if kk:  # brute-force FP64 kNN APSS: a smaller sample
+        sel = rng.choice(len(q), min(args.check_queries, 256, len(q)), replace=False)
+        x64, _ = oracle.project_apss(pts, nrm, q[sel], args.iters, kernel, 0, k=kk,
+                                     step_max=synth_radius(pts))
+    else:
+        ot = oracle.OracleTree(pts, nrm, 12)
+        sel = rng.choice(len(q), min(args.check_queries, len(q)), replace=False)
+        x64, _ = ot.project_mlod(q[sel], args.iters, kernel, rule=SPECS[args.workload]["rule"],
+                                 cutoff=SPECS[args.workload]["cutoff"])
     x = gpu_out[sel].astype(np.float64)
     err = np.linalg.norm(x - x64, axis=1) / diag
     half_ulp = np.abs(np.spacing(x64.astype(np.float32)).astype(np.float64)) / 2
@@ -264,6 +284,8 @@ def run_ours(args, rank, world, local_rank):
     tree.build(pts, nrm)
     inf = tree.info()
     tree_mb = inf.device_bytes / 2**20
+    if spec.get("knn"):
+        tree.knnMode(True, spec["knn"])
     f = Fastapss(tree, kernel, len(q))
     f.setScalingProtectionSphere(spec["cutoff"])
     f.blend_rule = spec["rule"]
@@ -318,7 +340,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- the same steps with exact convergence (outputs bit-identical to the
     # full iteration count: a query stops once its float iterate repeats)
     conv = None
-    if world == 1:
+    if world == 1 and not spec.get("knn"):
         from mlodsurfaces_b200._capi import CONVERGE_EXACT, CONVERGE_OFF
 
         ref_out = d_p.clone()
@@ -370,6 +392,13 @@ def run_ours(args, rank, world, local_rank):
     # ---- roofline of the projection kernel (algorithmic bytes per launch)
     mean_visits = statistics.mean(visits)
     bytes_per_launch = len(q) * (12 + 24) + 64 * mean_visits
+    roof_note = (f"algorithmic bytes = 36 per query + 64 per node visit ({mean_visits / len(q) / args.iters:.0f}"
+                 f" visits per query-iteration); traffic = DRAM bytes per launch from ncu: the node arrays are read "
+                 f"from DRAM about once, later visits hit L1/L2")
+    if spec.get("knn"):  # the k neighbours' positions and normals, every iteration
+        bytes_per_launch = len(q) * (12 + 24) + len(q) * args.iters * spec["knn"] * 24
+        roof_note = (f"algorithmic bytes = 36 per query + {spec['knn']} neighbours x 24 bytes per query-iteration "
+                     f"(the octree walk of the gather is not counted)")
     kms = statistics.mean(kern_ms)
     achieved = bytes_per_launch / (kms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
@@ -396,14 +425,13 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": PROFILED_TRAFFIC.get((args.workload, n_points_for(args), args.iters)),
-                     "note": f"algorithmic bytes = 36 per query + 64 per node visit ({mean_visits / len(q) / args.iters:.0f}"
-                             f" visits per query-iteration); peak {peak_kind}; traffic = DRAM bytes per launch from "
-                             f"ncu: the node arrays are read from DRAM about once, later visits hit L1/L2"},
+                     "note": f"{roof_note}; peak {peak_kind}"},
         "kernel_ms": kms,
         "converge_exact": conv,
-        "traversal": {"visits_per_query_iteration": mean_visits / len(q) / args.iters,
-                      "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),
-                      "max_stack_ranges": max_stack},
+        "traversal": None if spec.get("knn") else {
+            "visits_per_query_iteration": mean_visits / len(q) / args.iters,
+            "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),
+            "max_stack_ranges": max_stack},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -842,25 +870,27 @@ def run_reference(args, rank):
 
     if not oracle.ref_available():
         return {"impl": "reference", "unavailable": "reference CPU shim oracle/_ref/libmlods_ref.so not built"}
-    spec = SPECS[args.workload if args.workload in SPECS else "precision"]
-    pts, nrm, q, diag, kernel = workload(n_points_for(args), rank, args.workload if args.workload in SPECS
-                                         else "precision")
+    wl = args.workload if args.workload in SPECS else "precision"
+    spec = SPECS[wl]
+    pts, nrm, q, diag, kernel = workload(n_points_for(args), rank, wl)
+    knn_mode = {"mode": 2, "k": spec["knn"]} if spec.get("knn") else {}
     cores = os.cpu_count() or 1
     rt = oracle.RefTree(pts, nrm, 12)
     rng = np.random.default_rng(7)
     sel = rng.choice(len(q), 256, replace=False)
-    _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=spec["cutoff"], nthreads=cores)
+    _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=spec["cutoff"], nthreads=cores, **knn_mode)
     per_q = max(s0 / 256, 1e-7)
     budget = 150.0 / max(args.steps + args.warmup, 1)
     ns = int(min(len(q), max(256, budget / per_q)))
     times = []
     for i in range(args.warmup + args.steps):
         sel = rng.choice(len(q), ns, replace=False)
-        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=spec["cutoff"], nthreads=cores)
+        _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=spec["cutoff"], nthreads=cores, **knn_mode)
         if i >= args.warmup:
             times.append(secs)
     value = ns * len(times) / sum(times)
-    sample = f"{ns} random queries per step, {args.iters} iterations, APSSOctree::projectCPU under OpenMP"
+    fn = "projectAPSSCPU (kNN)" if spec.get("knn") else "projectCPU"
+    sample = f"{ns} random queries per step, {args.iters} iterations, APSSOctree::{fn} under OpenMP"
     return {
         "impl": "reference",
         "metric": METRIC,

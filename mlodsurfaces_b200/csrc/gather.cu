@@ -26,7 +26,16 @@ namespace
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kGCount = 0x7FFFFFFFu;
 constexpr uint32_t kGPoints = 1u << 31;  // entry is a range of sorted point positions
-constexpr int kGatherCap = 128;          // stack entries per warp
+constexpr int kGatherCap = 256;          // stack entries per warp
+// A range entry holds at most 8 nodes, each pushing at most one entry, so a
+// depth-first walk below any entry adds at most 7 entries per level for the
+// 12 node levels and the point level, plus one: 92.  The walk pops as many
+// entries as fill the warp while the stack has room for one such walk after
+// a full batch (32 pushes), and only the top entry beyond that, so the
+// stack stays below kGatherCap.
+constexpr int kDfsReserve = 7 * (kMaxTreeDepth + 1) + 1;
+constexpr int kBatchPopLimit = kGatherCap - kDfsReserve - 32;
+static_assert(kBatchPopLimit > 0, "gather stack too small for a depth-first walk");
 
 struct GStack {
     uint32_t first[kGatherCap];
@@ -281,7 +290,8 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
                     c = int(e_cnt & kGCount);
                 }
                 const int incl = warp_incl_scan_i(c);
-                const uint32_t fit = __ballot_sync(kFull, lane < top && incl <= 32);
+                const int pop_lanes = top > kBatchPopLimit ? 1 : top;  // depth-first near the cap
+                const uint32_t fit = __ballot_sync(kFull, lane < pop_lanes && incl <= 32);
                 int npop = __popc(fit);
                 const bool partial = npop == 0;
                 int total;

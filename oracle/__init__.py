@@ -268,6 +268,12 @@ def refgpu() -> C.CDLL:
         lib.refgpu_project.restype = C.c_double
         lib.refgpu_project.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, _P, _P]
         lib.refgpu_free.argtypes = [_P]
+        lib.refgpu_global_create.restype = _P
+        lib.refgpu_global_create.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                             _P, C.c_int]
+        lib.refgpu_global_project.restype = C.c_double
+        lib.refgpu_global_project.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_float, _P, _P]
+        lib.refgpu_global_free.argtypes = [_P]
         _refgpu = lib
     return _refgpu
 
@@ -301,6 +307,34 @@ class RefGpu:
         on = np.empty((len(q), 3), np.float32)
         ms = refgpu().refgpu_project(self._h, _ptr(q), len(q), int(calls), int(iters_per_call), float(step_max),
                                      _ptr(op), _ptr(on))
+        if ms < 0:
+            raise ValueError("query count out of the reference's launch range")
+        return op, on, ms
+
+
+class RefGpuGlobal:
+    """The reference's own GlobalAPSS (GPU, all points per query)."""
+
+    def __init__(self, pts, nrm, kernel, max_depth=12):
+        self.pts = _f32(pts)
+        self.nrm = _f32(nrm)
+        sig = np.ascontiguousarray(np.asarray(kernel.sigmas if len(kernel.sigmas) else [0.0], np.float32))
+        self._h = refgpu().refgpu_global_create(_ptr(self.pts), _ptr(self.nrm), len(self.pts), int(max_depth),
+                                                int(kernel.type), float(kernel.sigma), float(kernel.exponent),
+                                                float(kernel.constant_shift), _ptr(sig), len(kernel.sigmas))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            refgpu().refgpu_global_free(self._h)
+            self._h = None
+
+    def project(self, q, calls=10, step_max=-1.0):
+        """(points, normals, device milliseconds of `calls` one-step calls)."""
+        q = _f32(q)
+        op = np.empty((len(q), 3), np.float32)
+        on = np.empty((len(q), 3), np.float32)
+        ms = refgpu().refgpu_global_project(self._h, _ptr(q), len(q), int(calls), float(step_max), _ptr(op),
+                                            _ptr(on))
         if ms < 0:
             raise ValueError("query count out of the reference's launch range")
         return op, on, ms

@@ -26,6 +26,12 @@ struct RefGpu {
     Fastapss* apss = nullptr;
     Kernel kernel;
 };
+
+struct RefGlobal {
+    APSSOctree* tree = nullptr;
+    GlobalAPSS* apss = nullptr;
+    Kernel kernel;
+};
 }  // namespace
 
 extern "C" {
@@ -100,6 +106,71 @@ double refgpu_project(void* h, const float* q, int64_t n, int calls, int iters_p
 void refgpu_free(void* h)
 {
     auto* r = static_cast<RefGpu*>(h);
+    if (!r) return;
+    delete r->apss;
+    delete r->tree;
+    delete r;
+}
+
+// The reference's GlobalAPSS (GlobalAPSS.cu:95-258): every query sums over
+// all points, one projection step per project() call, and each call copies
+// the points and normals back to the host (GlobalAPSS.cu:231-232).
+void* refgpu_global_create(const float* pts, const float* nrm, int64_t n, int max_depth, int ktype, float sigma,
+                           float exponent, float shift, const float* sigmas, int nsig)
+{
+    std::vector<glm::vec3> p(n), nn(n);
+    for (int64_t i = 0; i < n; ++i) {
+        p[i] = glm::vec3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+        nn[i] = glm::vec3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
+    }
+    auto* r = new RefGlobal();
+    r->tree = new APSSOctree();
+    r->tree->build(p, nn, true, unsigned(max_depth), 1);
+    r->kernel.type = ktype == 0 ? Kernel::GAUSSIAN : (ktype == 1 ? Kernel::SINGULAR : Kernel::GAUSSIAN_MULTIPLE);
+    r->kernel.sigma = sigma;
+    r->kernel.exponent = exponent;
+    r->kernel.constant_shift = shift;
+    r->kernel.sigmas.assign(sigmas, sigmas + nsig);
+    r->apss = new GlobalAPSS(r->tree);
+    r->apss->copyToGPU(r->kernel, unsigned(n));
+    return r;
+}
+
+// Uploads n queries and runs `calls` GlobalAPSS::project calls of one step
+// each (the reference's call pattern: scene.cpp:929-933).  Returns the
+// device milliseconds of the calls (CUDA events on the default stream), or a
+// negative value if n is out of the reference's launch range.
+double refgpu_global_project(void* h, const float* q, int64_t n, int calls, float step_max, float* out_p,
+                             float* out_n)
+{
+    if (n <= 0 || n > int64_t(65535) * 128) return -1.0;
+    auto* r = static_cast<RefGlobal*>(h);
+    std::vector<glm::vec3> qq(n), op(n), on(n);
+    for (int64_t i = 0; i < n; ++i) qq[i] = glm::vec3(q[3 * i], q[3 * i + 1], q[3 * i + 2]);
+    r->apss->copyPointsToGPU(unsigned(n), qq.data());
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, 0);
+    for (int c = 0; c < calls; ++c) r->apss->project(unsigned(n), op.data(), on.data(), 1u, r->kernel, step_max);
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (int64_t i = 0; i < n; ++i) {
+        out_p[3 * i] = op[i].x; out_p[3 * i + 1] = op[i].y; out_p[3 * i + 2] = op[i].z;
+        out_n[3 * i] = on[i].x; out_n[3 * i + 1] = on[i].y; out_n[3 * i + 2] = on[i].z;
+    }
+    r->apss->erasePointsFromGPU();
+    return double(ms);
+}
+
+void refgpu_global_free(void* h)
+{
+    auto* r = static_cast<RefGlobal*>(h);
     if (!r) return;
     delete r->apss;
     delete r->tree;

@@ -129,3 +129,31 @@ def test_global_apss_matches_oracle_and_reference(golden):
     o64, _ = oracle.OracleTree(golden["pts"], golden["nrm"], 12).project_global(q, 2, k)
     assert rel_err(op, o64, diag).max() < TOL_DIAG
     assert rel_err(op, golden["global_gauss_p"], diag).max() < TOL_DIAG
+
+
+def test_knn_walk_on_a_large_cloud_never_overflows():
+    """2M points on the translated RBF surface, k = 32, all 2M queries: the
+    walk turns depth-first near its stack capacity, so no query is dropped,
+    and sampled results match brute force and the FP64 restatement."""
+    pts, nrm = synth.rbf_blobs(2_000_000, seed=2)
+    pts = synth.make_tie_free(pts)
+    q = synth.perturbed_queries(pts, 0.01, seed=3)
+    diag = synth.bbox_diag(pts)
+    k = make_kernel("multi", diag)
+    t = tree_of(pts, nrm)
+    t.knnMode(True, 32)
+    f = Fastapss(t, k, len(q))
+    f.copyPointsToGPU(len(q), q)
+    op = np.empty((len(q), 3), np.float32)
+    on = np.empty((len(q), 3), np.float32)
+    f.project(len(q), op, on, 3, k)
+    assert f.last_stats()["overflows"] == 0
+    sel = np.random.default_rng(5).choice(len(q), 48, replace=False)
+    o64, _ = oracle.project_apss(pts, nrm, q[sel], 3, k, mode=0, k=32, step_max=t.radius())
+    # the cloud sits 1e3 diagonals from the origin: a float32 output is only
+    # good to half a unit in the last place there (about 3e-5 diag), so the
+    # tolerance applies beyond that rounding
+    half_ulp = np.abs(np.spacing(o64.astype(np.float32)).astype(np.float64)) / 2
+    excess = np.linalg.norm(np.maximum(np.abs(op[sel].astype(np.float64) - o64) - half_ulp, 0.0), axis=1) / diag
+    assert excess.max() < TOL_DIAG
+    assert_knn_sets(pts, q[sel], 32, t)
