@@ -47,9 +47,10 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--check-queries", type=int, default=2048, help="queries checked against the FP64 oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["precision", "knn", "torus", "dc", "batch", "serve"], default="precision",
+    ap.add_argument("--workload", choices=["precision", "knn", "global", "torus", "dc", "batch", "serve"],
+                    default="precision",
                     help="precision: 2M-point RBF surface, MLoD projection (default); knn: the same data, kNN=32 "
-                         "APSS; torus: 100k-point torus, "
+                         "APSS; global: 200k points of it, global APSS; torus: 100k-point torus, "
                          "CPU-path semantics; dc: 5M-point torus knot, adaptive depth-9 dual contouring; "
                          "batch: 64 resident clouds (about 40M points) in one launch")
     ap.add_argument("--clouds", type=int, default=64)
@@ -74,6 +75,11 @@ SPECS = {
             "rule_desc": "kNN APSS (APSSOctree::projectAPSSCPU semantics)",
             "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag; queries = points + "
                     "N(0, 0.01 diag)"},
+    "global": {"desc": "precision data at 200k points, global APSS (every point weighs in every query)",
+               "kernel_desc": "multi-Gaussian sigma1=0.01*diag factor 2 x4", "cutoff": 3.0, "rule": 0, "global": True,
+               "rule_desc": "global APSS (GlobalAPSS / APSSOctree::projectCPU without the tree)",
+               "data": "synthetic: seeded 12-blob RBF implicit surface, translated 1e3*diag; queries = points + "
+                       "N(0, 0.01 diag)"},
     "torus": {"desc": "torus: 100k-point torus, single Gaussian, CPU-path semantics",
               "kernel_desc": "Gaussian sigma=0.02*diag", "cutoff": 3.0, "rule": 1,
               "rule_desc": "CPU (APSSOctree::projectCPU)",
@@ -105,6 +111,8 @@ def workload(n_points: int, rank: int, kind: str = "precision"):
 def n_points_for(args):
     if args.workload == "torus" and args.n_points == 2_000_000:
         return 100_000
+    if args.workload == "global" and args.n_points == 2_000_000:
+        return 200_000
     return args.n_points
 
 
@@ -213,6 +221,14 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def cpu_path_name(kind: str) -> str:
+    if SPECS.get(kind, {}).get("knn"):
+        return "projectAPSSCPU (kNN)"
+    if SPECS.get(kind, {}).get("global"):
+        return "projectCPU (global, fast=false)"
+    return "projectCPU"
+
+
 def synth_radius(pts) -> float:
     """Half the diagonal of the points' tight box (the tree's root radius)."""
     p = np.asarray(pts, np.float32)
@@ -235,7 +251,7 @@ def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out):
         sel = rng.choice(len(q), 256, replace=False)
         cutoff = SPECS[args.workload]["cutoff"]
         kk = SPECS[args.workload].get("knn", 0)
-        mode = {"mode": 2, "k": kk} if kk else {}
+        mode = {"mode": 2, "k": kk} if kk else ({"mode": 1} if SPECS[args.workload].get("global") else {})
         _, _, s0 = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores, **mode)
         per_q = max(s0 / 256, 1e-7)
         ns = int(min(len(q), max(256, args.cpu_seconds / per_q)))
@@ -243,12 +259,16 @@ def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out):
         _, _, secs = rt.project(q[sel], args.iters, kernel, cutoff=cutoff, nthreads=cores, **mode)
         out["cpu_baseline"] = {"value": ns / secs, "unit": UNIT, "cores": cores, "kind": "reference",
                                "sample": f"{ns} random queries of the workload, {args.iters} iterations, "
-                                         f"APSSOctree::{'projectAPSSCPU (kNN)' if kk else 'projectCPU'} under "
+                                         f"APSSOctree::{cpu_path_name(args.workload)} under "
                                          f"OpenMP; tree build {build_s:.1f} s single-threaded, not included"}
         del rt
     # accuracy of the GPU result against the FP64 oracle
     kk = SPECS[args.workload].get("knn", 0)
-    if kk:  # brute-force FP64 kNN APSS: a smaller sample
+    if SPECS[args.workload].get("global"):  # FP64 all-points sums: a smaller sample
+        ot = oracle.OracleTree(pts, nrm, 12)
+        sel = rng.choice(len(q), min(args.check_queries, 128, len(q)), replace=False)
+        x64, _ = ot.project_global(q[sel], args.iters, kernel)
+    elif kk:  # brute-force FP64 kNN APSS: a smaller sample
         sel = rng.choice(len(q), min(args.check_queries, 256, len(q)), replace=False)
         x64, _ = oracle.project_apss(pts, nrm, q[sel], args.iters, kernel, 0, k=kk,
                                      step_max=synth_radius(pts))
@@ -273,7 +293,7 @@ def run_ours(args, rank, world, local_rank):
 
     import torch
 
-    from mlodsurfaces_b200 import APSSOctree, Fastapss
+    from mlodsurfaces_b200 import APSSOctree, Fastapss, GlobalAPSS
     from mlodsurfaces_b200 import _capi as capi
 
     torch.cuda.set_device(local_rank)
@@ -286,7 +306,7 @@ def run_ours(args, rank, world, local_rank):
     tree_mb = inf.device_bytes / 2**20
     if spec.get("knn"):
         tree.knnMode(True, spec["knn"])
-    f = Fastapss(tree, kernel, len(q))
+    f = (GlobalAPSS if spec.get("global") else Fastapss)(tree, kernel, len(q))
     f.setScalingProtectionSphere(spec["cutoff"])
     f.blend_rule = spec["rule"]
     lib = capi.load()
@@ -340,7 +360,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- the same steps with exact convergence (outputs bit-identical to the
     # full iteration count: a query stops once its float iterate repeats)
     conv = None
-    if world == 1 and not spec.get("knn"):
+    if world == 1 and not spec.get("knn") and not spec.get("global"):
         from mlodsurfaces_b200._capi import CONVERGE_EXACT, CONVERGE_OFF
 
         ref_out = d_p.clone()
@@ -402,6 +422,19 @@ def run_ours(args, rank, world, local_rank):
     kms = statistics.mean(kern_ms)
     achieved = bytes_per_launch / (kms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": PROFILED_TRAFFIC.get((args.workload, n_points_for(args), args.iters)),
+                "note": f"{roof_note}; peak {peak_kind}"}
+    if spec.get("global"):  # every pair evaluates len(sigmas) exponentials on the special-function units
+        nsig = len(kernel.sigmas)
+        ex2 = float(len(q)) * len(pts) * args.iters * nsig / (kms / 1e3) / 1e9
+        mhz = clk.get("sm_mhz") or 1965.0
+        peak_ex2 = 148 * 16 * mhz / 1e3
+        roofline = {"bound": "sfu", "achieved": ex2, "peak": peak_ex2, "unit": "Gex2/s", "frac": ex2 / peak_ex2,
+                    "traffic": None,
+                    "note": f"{len(q)} queries x {len(pts)} points x {args.iters} iterations x {nsig} exp2 per launch; "
+                            f"peak = 148 SMs x 16 exp2 per SM per clock (nominal) at the median sampled SM clock; "
+                            f"the points stream from L2 through shared memory (HBM is not the bound)"}
 
     result = {
         "metric": METRIC,
@@ -423,12 +456,10 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(h_p.numel() * 4 + h_n.numel() * 4),
                 "path": "mlods_queries_upload + mlods_project (host pinned in/out)"},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": PROFILED_TRAFFIC.get((args.workload, n_points_for(args), args.iters)),
-                     "note": f"{roof_note}; peak {peak_kind}"},
+        "roofline": roofline,
         "kernel_ms": kms,
         "converge_exact": conv,
-        "traversal": None if spec.get("knn") else {
+        "traversal": None if spec.get("knn") or spec.get("global") else {
             "visits_per_query_iteration": mean_visits / len(q) / args.iters,
             "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),
             "max_stack_ranges": max_stack},
@@ -873,7 +904,7 @@ def run_reference(args, rank):
     wl = args.workload if args.workload in SPECS else "precision"
     spec = SPECS[wl]
     pts, nrm, q, diag, kernel = workload(n_points_for(args), rank, wl)
-    knn_mode = {"mode": 2, "k": spec["knn"]} if spec.get("knn") else {}
+    knn_mode = {"mode": 2, "k": spec["knn"]} if spec.get("knn") else ({"mode": 1} if spec.get("global") else {})
     cores = os.cpu_count() or 1
     rt = oracle.RefTree(pts, nrm, 12)
     rng = np.random.default_rng(7)
@@ -889,8 +920,7 @@ def run_reference(args, rank):
         if i >= args.warmup:
             times.append(secs)
     value = ns * len(times) / sum(times)
-    fn = "projectAPSSCPU (kNN)" if spec.get("knn") else "projectCPU"
-    sample = f"{ns} random queries per step, {args.iters} iterations, APSSOctree::{fn} under OpenMP"
+    sample = f"{ns} random queries per step, {args.iters} iterations, APSSOctree::{cpu_path_name(wl)} under OpenMP"
     return {
         "impl": "reference",
         "metric": METRIC,

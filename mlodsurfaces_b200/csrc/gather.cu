@@ -479,32 +479,63 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
 // ---------------------------------------------------------------- global APSS
 
 constexpr int kGlobalThreads = 128;
-constexpr int kGlobalTile = 512;
+constexpr int kGlobalTile = 256;  // points per shared-memory tile
+constexpr int kGlobalQpt = 2;     // queries per thread: each point read from shared memory serves two
 
-// One thread per query; every point of the cloud contributes
+// Weight of the CPU path (Kernel::w, Kernel.cpp:51-76) with the number of
+// multi-Gaussian terms fixed at compile time when NSIG > 0.
+template <int KTYPE, int NSIG>
+__device__ __forceinline__ float global_weight(const KernelConsts& kc, float d2)
+{
+    float w;
+    if (KTYPE == MLODS_GAUSSIAN_MULTIPLE && NSIG > 0) {
+        w = 0.f;
+#pragma unroll
+        for (int i = 0; i < NSIG; ++i) w = fmaf(exp2f(d2 * kc.ms_scale[i]), kc.ms_w[i], w);
+    } else {
+        w = kernel_weight<KTYPE>(kc, d2);
+    }
+    if (KTYPE == MLODS_GAUSSIAN_MULTIPLE && w == 0.f) w = kc.shift;  // Kernel.cpp:70-74
+    return w;
+}
+
+// kGlobalQpt queries per thread; every point of the cloud contributes
 // w(p_i, q) a_i {1, n_i, p_i, p_i.n_i, |p_i|^2} (APSSOctree::APSSStats,
 // CPUUtils.cpp:515-528).  Points stream through shared memory in tiles;
 // per-tile float partial sums are accumulated in double.
-template <int KTYPE>
+template <int KTYPE, int NSIG>
 __global__ void __launch_bounds__(kGlobalThreads) global_apss_kernel(GlobalArgs a)
 {
+    constexpr int Q = kGlobalQpt;
     __shared__ float4 s_p[kGlobalTile];
     __shared__ float4 s_n[kGlobalTile];
-    const int64_t qi = int64_t(blockIdx.x) * kGlobalThreads + threadIdx.x;
-    const bool valid = qi < a.nq;
-    double xd[3] = {0, 0, 0};
-    float q0[3] = {0, 0, 0};
-    if (valid) {
+    const int64_t q_first = int64_t(blockIdx.x) * kGlobalThreads * Q + threadIdx.x;
+    double xd[Q][3];
+    float nrm[Q][3];
+    bool valid[Q], failed[Q];
+#pragma unroll
+    for (int u = 0; u < Q; ++u) {
+        const int64_t qi = q_first + int64_t(u) * kGlobalThreads;
+        valid[u] = qi < a.nq;
+        failed[u] = false;
+        const double o[3] = {a.o0, a.o1, a.o2};
+#pragma unroll
         for (int c = 0; c < 3; ++c) {
-            q0[c] = a.q_in[3 * qi + c];
-            xd[c] = double(q0[c]) - (c == 0 ? a.o0 : (c == 1 ? a.o1 : a.o2));
+            xd[u][c] = valid[u] ? double(a.q_in[3 * qi + c]) - o[c] : 0.0;
+            nrm[u][c] = 0.f;
         }
     }
-    float nrm[3] = {0.f, 0.f, 0.f};
-    bool failed = false;
     for (int it = 0; it < a.n_iter; ++it) {
-        const float lx = float(xd[0]), ly = float(xd[1]), lz = float(xd[2]);
-        double tot[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        float lx[Q], ly[Q], lz[Q];
+        double tot[Q][9];
+#pragma unroll
+        for (int u = 0; u < Q; ++u) {
+            lx[u] = float(xd[u][0]);
+            ly[u] = float(xd[u][1]);
+            lz[u] = float(xd[u][2]);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) tot[u][c] = 0.0;
+        }
         for (int64_t base = 0; base < a.n_pts; base += kGlobalTile) {
             __syncthreads();
             for (int j = threadIdx.x; j < kGlobalTile; j += kGlobalThreads) {
@@ -515,51 +546,70 @@ __global__ void __launch_bounds__(kGlobalThreads) global_apss_kernel(GlobalArgs 
                     const float ar = __ldg(a.area + __float_as_uint(p.w));
                     s_p[j] = make_float4(p.x, p.y, p.z, ar);
                     s_n[j] = nn;
-                } else {
+                } else {  // zero area: no contribution
                     s_p[j] = make_float4(0.f, 0.f, 0.f, 0.f);
                     s_n[j] = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
             }
             __syncthreads();
-            float acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            float acc[Q][9];
+#pragma unroll
+            for (int u = 0; u < Q; ++u)
+#pragma unroll
+                for (int c = 0; c < 9; ++c) acc[u][c] = 0.f;
+#pragma unroll 2
             for (int j = 0; j < kGlobalTile; ++j) {
                 const float4 p = s_p[j];
                 const float4 nn = s_n[j];
-                const float dx = p.x - lx, dy = p.y - ly, dz = p.z - lz;
-                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const float w = kernel_weight<KTYPE>(a.kc, dd) * p.w;
-                acc[0] += w;
-                acc[1] = fmaf(w, nn.x, acc[1]);
-                acc[2] = fmaf(w, nn.y, acc[2]);
-                acc[3] = fmaf(w, nn.z, acc[3]);
-                acc[4] = fmaf(w, dx, acc[4]);
-                acc[5] = fmaf(w, dy, acc[5]);
-                acc[6] = fmaf(w, dz, acc[6]);
-                acc[7] = fmaf(w, fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z)), acc[7]);
-                acc[8] = fmaf(w, dd, acc[8]);
+#pragma unroll
+                for (int u = 0; u < Q; ++u) {
+                    const float dx = p.x - lx[u], dy = p.y - ly[u], dz = p.z - lz[u];
+                    const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float w = global_weight<KTYPE, NSIG>(a.kc, dd) * p.w;
+                    acc[u][0] += w;
+                    acc[u][1] = fmaf(w, nn.x, acc[u][1]);
+                    acc[u][2] = fmaf(w, nn.y, acc[u][2]);
+                    acc[u][3] = fmaf(w, nn.z, acc[u][3]);
+                    acc[u][4] = fmaf(w, dx, acc[u][4]);
+                    acc[u][5] = fmaf(w, dy, acc[u][5]);
+                    acc[u][6] = fmaf(w, dz, acc[u][6]);
+                    acc[u][7] = fmaf(w, fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z)), acc[u][7]);
+                    acc[u][8] = fmaf(w, dd, acc[u][8]);
+                }
             }
-            for (int c = 0; c < 9; ++c) tot[c] += double(acc[c]);
+#pragma unroll
+            for (int u = 0; u < Q; ++u)
+#pragma unroll
+                for (int c = 0; c < 9; ++c) tot[u][c] += double(acc[u][c]);
         }
-        if (!valid || failed) continue;
-        float s[9];
-        for (int c = 0; c < 9; ++c) s[c] = float(tot[c]);
-        double x[3];
-        if (!fit_cpu(s, double(a.step_max), x, nrm)) {
-            nrm[0] = nrm[1] = nrm[2] = 0.f;
-            failed = true;
-            continue;
+#pragma unroll
+        for (int u = 0; u < Q; ++u) {
+            if (!valid[u] || failed[u]) continue;
+            float s[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) s[c] = float(tot[u][c]);
+            double x[3];
+            if (!fit_cpu(s, double(a.step_max), x, nrm[u])) {
+                // NaN: the iterate stays, normal 0 (CPUUtils.cpp:770-776)
+                nrm[u][0] = nrm[u][1] = nrm[u][2] = 0.f;
+                failed[u] = true;
+                continue;
+            }
+            xd[u][0] = double(lx[u]) + x[0];
+            xd[u][1] = double(ly[u]) + x[1];
+            xd[u][2] = double(lz[u]) + x[2];
         }
-        xd[0] = double(lx) + x[0];
-        xd[1] = double(ly) + x[1];
-        xd[2] = double(lz) + x[2];
     }
-    if (valid) {
-        a.out_p[3 * qi] = float(xd[0] + a.o0);
-        a.out_p[3 * qi + 1] = float(xd[1] + a.o1);
-        a.out_p[3 * qi + 2] = float(xd[2] + a.o2);
-        a.out_n[3 * qi] = nrm[0];
-        a.out_n[3 * qi + 1] = nrm[1];
-        a.out_n[3 * qi + 2] = nrm[2];
+#pragma unroll
+    for (int u = 0; u < Q; ++u) {
+        if (!valid[u]) continue;
+        const int64_t qi = q_first + int64_t(u) * kGlobalThreads;
+        a.out_p[3 * qi] = float(xd[u][0] + a.o0);
+        a.out_p[3 * qi + 1] = float(xd[u][1] + a.o1);
+        a.out_p[3 * qi + 2] = float(xd[u][2] + a.o2);
+        a.out_n[3 * qi] = nrm[u][0];
+        a.out_n[3 * qi + 1] = nrm[u][1];
+        a.out_n[3 * qi + 2] = nrm[u][2];
     }
 }
 
@@ -601,11 +651,22 @@ cudaError_t launch_gather(const GatherArgs& a, int mode, int ktype, int sm_count
 
 cudaError_t launch_global_apss(const GlobalArgs& a, int ktype, cudaStream_t s)
 {
-    const unsigned grid = unsigned((a.nq + kGlobalThreads - 1) / kGlobalThreads);
+    const int64_t per_block = int64_t(kGlobalThreads) * kGlobalQpt;
+    const unsigned grid = unsigned((a.nq + per_block - 1) / per_block);
     switch (ktype) {
-    case MLODS_GAUSSIAN: global_apss_kernel<MLODS_GAUSSIAN><<<grid, kGlobalThreads, 0, s>>>(a); break;
-    case MLODS_SINGULAR: global_apss_kernel<MLODS_SINGULAR><<<grid, kGlobalThreads, 0, s>>>(a); break;
-    default: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE><<<grid, kGlobalThreads, 0, s>>>(a); break;
+    case MLODS_GAUSSIAN: global_apss_kernel<MLODS_GAUSSIAN, 0><<<grid, kGlobalThreads, 0, s>>>(a); break;
+    case MLODS_SINGULAR: global_apss_kernel<MLODS_SINGULAR, 0><<<grid, kGlobalThreads, 0, s>>>(a); break;
+    default:
+        switch (a.kc.nsig) {
+        case 1: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 1><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        case 2: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 2><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        case 3: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 3><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        case 4: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 4><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        case 5: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 5><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        case 6: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 6><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        case 8: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 8><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        default: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 0><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        }
     }
     note_launch();
     return cudaGetLastError();
