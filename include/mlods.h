@@ -381,6 +381,17 @@ int mlods_cloud_morton_order(const float* pts, int64_t n, int32_t grid, uint32_t
 int mlods_cloud_sample_around(const float* pts, const float* nrm, int64_t n_pts, int64_t n_out, float factor,
                               uint64_t seed, float* out_pts, float* out_nrm);
 
+/* scene::generateFromOctree (scene.cpp:733-756), on the device: n_out points,
+ * each in a cell drawn uniformly from d_cells (n_cells rows of int32
+ * {depth, x, y, z} of the [-1, 1]^3 octree, 16-byte aligned), at the cell
+ * centre plus an offset uniform in [-0.5, 0.5)^3 times 4 / 2^depth; the
+ * normal is the point itself (d_out_nrm may be NULL).  Draws are a
+ * counter-based hash of (seed, index), so a seed fixes the output.  A row
+ * whose depth is outside [0, 30] yields a NaN point.  Asynchronous on
+ * `stream`. */
+int mlods_sample_cells_device(const int32_t* d_cells, int64_t n_cells, int64_t n_out, uint64_t seed,
+                              float* d_out_pts, float* d_out_nrm, void* stream);
+
 #define MLODS_PARAMS_FILE_BYTES 134
 typedef struct mlods_scene_params {
     float cam_quat[4];          /* viewer camera (not used by the projection) */

@@ -194,6 +194,7 @@ SIGNATURES = {
     "mlods_cloud_normalize": (C.c_int, [_P, C.c_int64, _P, _P, C.POINTER(C.c_float)]),
     "mlods_cloud_morton_order": (C.c_int, [_P, C.c_int64, C.c_int32, _P]),
     "mlods_cloud_sample_around": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_float, C.c_uint64, _P, _P]),
+    "mlods_sample_cells_device": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_uint64, _P, _P, _P]),
     "mlods_params_file_load": (C.c_int, [C.c_char_p, C.POINTER(mlods_scene_params)]),
     "mlods_params_file_save": (C.c_int, [C.c_char_p, C.POINTER(mlods_scene_params)]),
 }

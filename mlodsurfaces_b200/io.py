@@ -88,6 +88,27 @@ def sample_around(points, normals, n: int, factor: float = 1.0, seed: int = 0):
     return out_p, out_n
 
 
+def sample_cells(cells, n: int, seed: int = 0, device=None, stream=None):
+    """scene::generateFromOctree (scene.cpp:733-756) on the device: n points
+    in cells {depth, x, y, z} of the [-1, 1]^3 octree drawn uniformly, each at
+    its cell centre plus a uniform offset in [-2, 2)^3 / 2^depth; the normals
+    are the points.  Returns two (n, 3) float32 CUDA tensors.  Asynchronous on
+    `stream` (default: torch's current stream)."""
+    import torch
+
+    lib = capi.load()
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    c = torch.as_tensor(np.ascontiguousarray(np.asarray(cells, np.int32).reshape(-1, 4))) \
+        if not isinstance(cells, torch.Tensor) else cells.to(torch.int32).reshape(-1, 4).contiguous()
+    c = c.to(dev)
+    out_p = torch.empty((int(n), 3), dtype=torch.float32, device=dev)
+    out_n = torch.empty((int(n), 3), dtype=torch.float32, device=dev)
+    s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+    capi.check(lib.mlods_sample_cells_device(capi.ptr(c), int(c.shape[0]), int(n), C.c_uint64(seed),
+                                             capi.ptr(out_p), capi.ptr(out_n), C.c_void_p(s)))
+    return out_p, out_n
+
+
 _ARRAYS = {"cam_quat": 4, "cam_translation": 3, "fixed_sigmas": 5, "offset": 6}
 
 
