@@ -524,8 +524,16 @@ def run_dc(args):
     t0 = time.perf_counter()
     mesh = f.dc_mesh(grid)
     mesh_ms = 1e3 * (time.perf_counter() - t0)
-    v, _, tri = mesh.arrays()
     inside = mesh.stage_ms()
+    t0 = time.perf_counter()
+    v, _, tri = mesh.arrays()  # the mesh stays on the device until copied out
+    inside["download"] = 1e3 * (time.perf_counter() - t0)
+    mesh_ms += inside["download"]
+    for i in range(2):  # into page-locked memory: the first call allocates it, the second reuses it
+        t0 = time.perf_counter()
+        hv = mesh.arrays(pinned=True)
+        inside["download_pinned" if i else "download_pinned_first"] = 1e3 * (time.perf_counter() - t0)
+        del hv
     # the same pipeline from its parts, timed per stage
     from mlodsurfaces_b200 import Mesh
 

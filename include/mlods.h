@@ -240,20 +240,27 @@ int mlods_dc_evaluate(mlods_tree t, int64_t n_cells, const int32_t* cells, int32
  * (positions and normals).  mlods_dc_mesh runs the whole reference pipeline
  * on a grid: corner field, extraction, transform to the tree's frame,
  * projection (3 iterations), then refine_rounds x (smooth, subdivide,
- * project 3 iterations); the reference uses 2 rounds. */
+ * project 3 iterations); the reference uses 2 rounds.
+ * A mesh from mlods_dc_extract lives in host memory; one from mlods_dc_mesh
+ * stays in device memory: the mesh functions then run on the device (the
+ * same results in the same order), mlods_mesh_get copies it into the
+ * caller's buffers (pinned buffers copy fastest), and
+ * mlods_mesh_device_arrays gives its device arrays (float3 positions and
+ * normals, uint3 triangles), valid until the mesh is changed or freed. */
 typedef struct mlods_mesh_s* mlods_mesh;
 int mlods_dc_extract(int64_t n_cells, const int32_t* cells, const float* corner_f, const float* cell_vertex,
                      mlods_mesh* out);
 int mlods_mesh_info(mlods_mesh m, int64_t* n_vertices, int64_t* n_triangles);
 int mlods_mesh_get(mlods_mesh m, float* vertices, float* normals, uint32_t* indices);
+int mlods_mesh_device_arrays(mlods_mesh m, const float** vertices, const float** normals, const uint32_t** indices);
 int mlods_mesh_transform(mlods_mesh m, const float* xform);
 int mlods_mesh_smooth(mlods_mesh m);
 int mlods_mesh_subdivide(mlods_mesh m);
 int mlods_mesh_project(mlods_tree t, mlods_mesh m, int32_t n_iterations, void* stream);
 int mlods_mesh_free(mlods_mesh m);
 /* Host wall time (ms) of mlods_dc_mesh's 7 stages: corner field, extraction,
- * upload + transform, projections, smoothing, subdivision, download (zeros
- * for meshes built otherwise). */
+ * upload + transform, projections, smoothing, subdivision, download (0: the
+ * mesh stays in device memory); zeros for meshes built otherwise. */
 int mlods_mesh_stage_ms(mlods_mesh m, double* ms);
 int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t refine_rounds, void* stream,
                   mlods_mesh* out);

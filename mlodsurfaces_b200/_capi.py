@@ -172,6 +172,7 @@ SIGNATURES = {
     "mlods_dc_extract": (C.c_int, [C.c_int64, _P, _P, _P, C.POINTER(_P)]),
     "mlods_mesh_info": (C.c_int, [_P, _I64, _I64]),
     "mlods_mesh_get": (C.c_int, [_P, _P, _P, _P]),
+    "mlods_mesh_device_arrays": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "mlods_mesh_transform": (C.c_int, [_P, _P]),
     "mlods_mesh_smooth": (C.c_int, [_P]),
     "mlods_mesh_subdivide": (C.c_int, [_P]),

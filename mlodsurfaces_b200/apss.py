@@ -302,15 +302,31 @@ class DCGrid:
             pass
 
 
-def _mesh_arrays(lib, m):
+def _mesh_arrays(lib, m, pinned: bool = False):
     nv = C.c_int64(0)
     nt = C.c_int64(0)
     capi.check(lib.mlods_mesh_info(m, C.byref(nv), C.byref(nt)))
-    v = np.empty((nv.value, 3), np.float32)
-    n = np.empty((nv.value, 3), np.float32)
-    t = np.empty((nt.value, 3), np.uint32)
+    if pinned:  # page-locked host memory: the device-to-host copy runs at link speed
+        import torch
+
+        v = torch.empty((nv.value, 3), dtype=torch.float32, pin_memory=True).numpy()
+        n = torch.empty((nv.value, 3), dtype=torch.float32, pin_memory=True).numpy()
+        t = torch.empty((nt.value, 3), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    else:
+        v = np.empty((nv.value, 3), np.float32)
+        n = np.empty((nv.value, 3), np.float32)
+        t = np.empty((nt.value, 3), np.uint32)
     capi.check(lib.mlods_mesh_get(m, capi.ptr(v), capi.ptr(n), capi.ptr(t)))
     return v, n, t
+
+
+class _DeviceView:
+    """__cuda_array_interface__ of an array owned by the library."""
+
+    def __init__(self, ptr: int, shape, typestr: str, owner):
+        self._owner = owner  # keeps the mesh alive while the view exists
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None, "stream": None}
 
 
 class Mesh:
@@ -336,9 +352,30 @@ class Mesh:
         capi.check(lib.mlods_dc_extract(len(cells), capi.ptr(cells), capi.ptr(cf), capi.ptr(vx), C.byref(m)))
         return cls(m)
 
-    def arrays(self):
-        """(vertices (n, 3), normals (n, 3), triangles (m, 3) uint32)."""
-        return _mesh_arrays(self._lib, self._m)
+    def arrays(self, pinned: bool = False):
+        """(vertices (n, 3), normals (n, 3), triangles (m, 3) uint32) as host
+        arrays; pinned=True copies into page-locked memory."""
+        return _mesh_arrays(self._lib, self._m, pinned)
+
+    def device_arrays(self):
+        """The mesh of APSS.dc_mesh in device memory, without a copy: torch
+        CUDA tensors (vertices (n, 3) float32, normals (n, 3) float32,
+        triangles (m, 3) int32 holding the uint32 indices), valid while this
+        mesh is alive and unchanged."""
+        import torch
+
+        nv = C.c_int64(0)
+        nt = C.c_int64(0)
+        capi.check(self._lib.mlods_mesh_info(self._m, C.byref(nv), C.byref(nt)))
+        pv, pn, pt = C.c_void_p(0), C.c_void_p(0), C.c_void_p(0)
+        capi.check(self._lib.mlods_mesh_device_arrays(self._m, C.byref(pv), C.byref(pn), C.byref(pt)))
+        out = []
+        for p, shape, ts in ((pv, (nv.value, 3), "<f4"), (pn, (nv.value, 3), "<f4"), (pt, (nt.value, 3), "<i4")):
+            if shape[0] == 0:
+                out.append(torch.empty(shape, dtype=torch.float32 if ts == "<f4" else torch.int32, device="cuda"))
+            else:
+                out.append(torch.as_tensor(_DeviceView(p.value, shape, ts, self), device="cuda"))
+        return tuple(out)
 
     def stage_ms(self) -> dict:
         """Host time of the pipeline stages of APSS.dc_mesh (ms)."""

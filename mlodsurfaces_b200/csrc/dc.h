@@ -104,6 +104,10 @@ int dc_extract_device(const int4* d_cells, int64_t n_cells, const int64_t* h_dep
                       const float* d_cf, const float* d_cell_vertex, DeviceMesh& out, bool* used_device,
                       cudaStream_t s);
 int dmesh_reserve(DeviceMesh& m, int64_t nv, int64_t nt);
+int64_t dmesh_nv(const DeviceMesh& m);
+int64_t dmesh_nt(const DeviceMesh& m);
+// Copies the mesh into caller buffers (any may be null) and waits for it.
+int dmesh_get(const DeviceMesh& m, float* pos, float* nrm, uint32_t* tri, cudaStream_t s);
 float* dmesh_pos(DeviceMesh& m);
 float* dmesh_nrm(DeviceMesh& m);
 uint32_t* dmesh_tri(DeviceMesh& m);

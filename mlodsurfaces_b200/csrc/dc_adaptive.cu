@@ -344,10 +344,26 @@ __global__ void siblings_kernel(const uint64_t* __restrict__ k, int64_t n, uint6
     for (int c = 0; c < 8; ++c) out[8 * i + c] = make_key(d, x + (c & 1), y + ((c >> 1) & 1), z + ((c >> 2) & 1));
 }
 
-__global__ void depth_hist_kernel(const uint64_t* __restrict__ k, int64_t n, unsigned long long* __restrict__ h)
+// First position of each depth in a sorted key set (the depth is the top 4
+// bits of the key): one binary search per depth, thread d, d in [0, 16].
+__global__ void depth_bounds_kernel(const uint64_t* __restrict__ k, int64_t n, long long* __restrict__ begin)
 {
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) atomicAdd(h + key_depth(k[i]), 1ull);
+    const int d = threadIdx.x;
+    if (d > 16) return;
+    if (d == 16) {
+        begin[16] = n;
+        return;
+    }
+    const uint64_t want = uint64_t(d) << 60;
+    int64_t lo = 0, hi = n;  // first key >= want
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo) / 2;
+        if (k[mid] < want)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    begin[d] = lo;
 }
 
 // ---- host orchestration
@@ -363,31 +379,31 @@ struct Gen {
     void* d_scan = nullptr;
     size_t scan_cap = 0;
     int* d_mm = nullptr;
-    unsigned long long* d_hist = nullptr;
+    long long* d_begin = nullptr;
     ~Gen()
     {
         cudaFree(d_proj);
         cudaFree(d_off);
         cudaFree(d_scan);
         cudaFree(d_mm);
-        cudaFree(d_hist);
+        cudaFree(d_begin);
     }
 
     // first key of each depth of a sorted set (17 entries)
     int depth_ranges(const CellSet& c, int64_t begin[17])
     {
-        if (!d_hist) MLODS_CUDA(cudaMalloc(&d_hist, 16 * sizeof(unsigned long long)));
-        MLODS_CUDA(cudaMemsetAsync(d_hist, 0, 16 * sizeof(unsigned long long), s));
-        if (c.n) {
-            depth_hist_kernel<<<blocks_for(c.n), kThreads, 0, s>>>(c.a, c.n, d_hist);
-            note_launch();
-            MLODS_CUDA(cudaGetLastError());
+        if (c.n == 0) {
+            for (int d = 0; d < 17; ++d) begin[d] = 0;
+            return MLODS_OK;
         }
-        unsigned long long h[16];
-        MLODS_CUDA(cudaMemcpyAsync(h, d_hist, sizeof h, cudaMemcpyDeviceToHost, s));
+        if (!d_begin) MLODS_CUDA(cudaMalloc(&d_begin, 17 * sizeof(long long)));
+        depth_bounds_kernel<<<1, 32, 0, s>>>(c.a, c.n, d_begin);
+        note_launch();
+        MLODS_CUDA(cudaGetLastError());
+        long long h[17];
+        MLODS_CUDA(cudaMemcpyAsync(h, d_begin, sizeof h, cudaMemcpyDeviceToHost, s));
         MLODS_CUDA(cudaStreamSynchronize(s));
-        begin[0] = 0;
-        for (int d = 0; d < 16; ++d) begin[d + 1] = begin[d] + int64_t(h[d]);
+        for (int d = 0; d < 17; ++d) begin[d] = int64_t(h[d]);
         return MLODS_OK;
     }
 

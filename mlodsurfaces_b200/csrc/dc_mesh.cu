@@ -24,13 +24,24 @@
 #include "dc.h"
 #include "tree.cuh"
 
+// A mesh lives either in device memory (`dev`, the result of mlods_dc_mesh:
+// the mesh functions then run on the device and mlods_mesh_get copies it
+// out) or in the host vectors (the result of mlods_dc_extract).
 struct mlods_mesh_s {
     std::vector<float> pos;  // 3 per vertex
     std::vector<float> nrm;  // 3 per vertex
     std::vector<uint32_t> tri;
+    mlods::DeviceMesh* dev = nullptr;
     // host wall time of mlods_dc_mesh's stages (ms): corner field, extraction,
-    // upload + transform, projections, smoothing, subdivision, download
+    // upload + transform, projections, smoothing, subdivision, download (0:
+    // the mesh stays in device memory)
     double stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    mlods_mesh_s() = default;
+    mlods_mesh_s(const mlods_mesh_s&) = delete;
+    mlods_mesh_s& operator=(const mlods_mesh_s&) = delete;
+    ~mlods_mesh_s() { mlods::dmesh_destroy(dev); }
+    int64_t nv() const { return dev ? mlods::dmesh_nv(*dev) : int64_t(pos.size() / 3); }
+    int64_t nt() const { return dev ? mlods::dmesh_nt(*dev) : int64_t(tri.size() / 3); }
 };
 
 namespace mlods
@@ -475,8 +486,8 @@ int mlods_mesh_info(mlods_mesh m, int64_t* n_vertices, int64_t* n_triangles)
         set_last_error("null mesh");
         return MLODS_ERR_INVALID;
     }
-    if (n_vertices) *n_vertices = int64_t(m->pos.size() / 3);
-    if (n_triangles) *n_triangles = int64_t(m->tri.size() / 3);
+    if (n_vertices) *n_vertices = m->nv();
+    if (n_triangles) *n_triangles = m->nt();
     return MLODS_OK;
 }
 
@@ -486,9 +497,26 @@ int mlods_mesh_get(mlods_mesh m, float* vertices, float* normals, uint32_t* indi
         set_last_error("null mesh");
         return MLODS_ERR_INVALID;
     }
+    if (m->dev) return dmesh_get(*m->dev, vertices, normals, indices, nullptr);
     if (vertices) std::memcpy(vertices, m->pos.data(), m->pos.size() * sizeof(float));
     if (normals) std::memcpy(normals, m->nrm.data(), m->nrm.size() * sizeof(float));
     if (indices) std::memcpy(indices, m->tri.data(), m->tri.size() * sizeof(uint32_t));
+    return MLODS_OK;
+}
+
+int mlods_mesh_device_arrays(mlods_mesh m, const float** vertices, const float** normals, const uint32_t** indices)
+{
+    if (!m) {
+        set_last_error("null mesh");
+        return MLODS_ERR_INVALID;
+    }
+    if (!m->dev) {
+        set_last_error("mesh device arrays: the mesh is in host memory");
+        return MLODS_ERR_INVALID;
+    }
+    if (vertices) *vertices = dmesh_pos(*m->dev);
+    if (normals) *normals = dmesh_nrm(*m->dev);
+    if (indices) *indices = dmesh_tri(*m->dev);
     return MLODS_OK;
 }
 
@@ -514,6 +542,7 @@ int mlods_mesh_transform(mlods_mesh m, const float* xform)
         set_last_error("mesh transform: bad arguments");
         return MLODS_ERR_INVALID;
     }
+    if (m->dev) return dmesh_transform(*m->dev, xform, nullptr);
     mesh_transform(m, xform);
     return MLODS_OK;
 }
@@ -523,6 +552,12 @@ int mlods_mesh_smooth(mlods_mesh m)
     if (!m) {
         set_last_error("null mesh");
         return MLODS_ERR_INVALID;
+    }
+    if (m->dev) {
+        const int rc = dmesh_smooth(*m->dev, nullptr);
+        if (rc != MLODS_OK) return rc;
+        MLODS_CUDA(cudaStreamSynchronize(nullptr));
+        return MLODS_OK;
     }
     mesh_smooth(m);
     return MLODS_OK;
@@ -534,9 +569,15 @@ int mlods_mesh_subdivide(mlods_mesh m)
         set_last_error("null mesh");
         return MLODS_ERR_INVALID;
     }
-    if (m->pos.size() / 3 + m->tri.size() > size_t(UINT32_MAX)) {
+    if (uint64_t(m->nv()) + 3 * uint64_t(m->nt()) > uint64_t(UINT32_MAX)) {
         set_last_error("mesh subdivide: result would exceed 32-bit vertex indices");
         return MLODS_ERR_CAPACITY;
+    }
+    if (m->dev) {
+        const int rc = dmesh_subdivide(*m->dev, nullptr);
+        if (rc != MLODS_OK) return rc;
+        MLODS_CUDA(cudaStreamSynchronize(nullptr));
+        return MLODS_OK;
     }
     mesh_subdivide(m);
     return MLODS_OK;
@@ -548,7 +589,14 @@ int mlods_mesh_project(mlods_tree t, mlods_mesh m, int32_t n_iterations, void* s
         set_last_error("mesh project: bad arguments");
         return MLODS_ERR_INVALID;
     }
-    return mesh_project(t, m, n_iterations, static_cast<cudaStream_t>(stream));
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (m->dev) {
+        const int rc = dmesh_project(t, *m->dev, n_iterations, s);
+        if (rc != MLODS_OK) return rc;
+        MLODS_CUDA(cudaStreamSynchronize(s));
+        return MLODS_OK;
+    }
+    return mesh_project(t, m, n_iterations, s);
 }
 
 int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t refine_rounds, void* stream,
@@ -600,6 +648,11 @@ int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t ref
         if (rc == MLODS_OK)
             rc = dmesh_upload(dm, m->pos.data(), int64_t(m->pos.size() / 3), m->tri.data(),
                               int64_t(m->tri.size() / 3), s);
+        if (rc == MLODS_OK && cudaStreamSynchronize(s) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "dc mesh: upload", __FILE__, __LINE__);
+        std::vector<float>().swap(m->pos);  // the device copy is the mesh from here on
+        std::vector<float>().swap(m->nrm);
+        std::vector<uint32_t>().swap(m->tri);
     }
     dc_field_free(field);
     m->stage_ms[1] = since(t0);
@@ -620,8 +673,7 @@ int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t ref
         stage(5, [&] { return dmesh_subdivide(dm, s); });
         stage(3, [&] { return dmesh_project(t, dm, 3, s); });
     }
-    stage(6, [&] { return dmesh_download(dm, m->pos, m->nrm, m->tri, s); });
-    dmesh_destroy(dmp);
+    m->dev = dmp;  // the mesh stays in device memory; mlods_mesh_get copies it out
     if (rc != MLODS_OK) {
         delete m;
         return rc;

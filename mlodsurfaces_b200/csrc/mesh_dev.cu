@@ -212,6 +212,17 @@ float* dmesh_pos(DeviceMesh& m) { return static_cast<float*>(m.pos.p); }
 float* dmesh_nrm(DeviceMesh& m) { return static_cast<float*>(m.nrm.p); }
 uint32_t* dmesh_tri(DeviceMesh& m) { return static_cast<uint32_t*>(m.tri.p); }
 void dmesh_destroy(DeviceMesh* m) { delete m; }
+int64_t dmesh_nv(const DeviceMesh& m) { return m.nv; }
+int64_t dmesh_nt(const DeviceMesh& m) { return m.nt; }
+
+int dmesh_get(const DeviceMesh& m, float* pos, float* nrm, uint32_t* tri, cudaStream_t s)
+{
+    if (m.nv && pos) MLODS_CUDA(cudaMemcpyAsync(pos, m.pos.p, size_t(m.nv) * 12, cudaMemcpyDeviceToHost, s));
+    if (m.nv && nrm) MLODS_CUDA(cudaMemcpyAsync(nrm, m.nrm.p, size_t(m.nv) * 12, cudaMemcpyDeviceToHost, s));
+    if (m.nt && tri) MLODS_CUDA(cudaMemcpyAsync(tri, m.tri.p, size_t(m.nt) * 12, cudaMemcpyDeviceToHost, s));
+    MLODS_CUDA(cudaStreamSynchronize(s));
+    return MLODS_OK;
+}
 
 int dmesh_upload(DeviceMesh& m, const float* pos, int64_t nv, const uint32_t* tri, int64_t nt, cudaStream_t s)
 {

@@ -97,6 +97,45 @@ def test_dc_mesh_on_adaptive_grid_equals_parts(torus_apss):
     assert st["extract"] > 0 and st["project"] > 0
 
 
+def test_device_resident_mesh(torus_apss):
+    """A dc_mesh result stays in device memory: the mesh functions run there
+    (one refinement round by hand equals refine_rounds=1), and the host copy,
+    the pinned host copy and the device views agree."""
+    pts, nrm, diag, k, f = torus_apss
+    g = DCGrid.adaptive(f, 5)
+    want = f.dc_mesh(g, refine_rounds=1).arrays()
+    m = f.dc_mesh(g, refine_rounds=0)
+    assert m.stage_ms()["download"] == 0.0
+    m.smooth()
+    m.subdivide()
+    m.project(f, 3)
+    got = m.arrays()
+    pinned = m.arrays(pinned=True)
+    dv, dn, dt = m.device_arrays()
+    for a, b in zip(want, got):
+        assert np.array_equal(a, b)
+    for a, b in zip(got, pinned):
+        assert np.array_equal(a, b)
+    assert np.array_equal(dv.cpu().numpy(), got[0]) and np.array_equal(dn.cpu().numpy(), got[1])
+    assert np.array_equal(dt.cpu().numpy().view(np.uint32), got[2])
+    # a moved transform on the device equals the same map applied to the copy
+    xf = np.array([[2, 0, 0, 0.5], [0, 1, 0, -0.25], [0, 0, 0.5, 1]], np.float32)
+    m.transform(xf)
+    v2 = m.arrays()[0]
+    ref = got[0] @ xf[:, :3].T + xf[:, 3]
+    assert np.allclose(v2, ref, rtol=0, atol=1e-6)
+
+
+def test_host_mesh_has_no_device_arrays(torus_apss):
+    pts, nrm, diag, k, f = torus_apss
+    g = DCGrid(pts, 4)
+    cf, vx, nc, _ = f.dc_evaluate(g.cells, g.max_depth, g.xform)
+    m = Mesh.extract(g.cells, cf, vx)
+    from mlodsurfaces_b200._capi import MlodsError
+    with pytest.raises(MlodsError):
+        m.device_arrays()
+
+
 def test_dc_mesh_pipeline(torus_apss):
     pts, nrm, diag, k, f = torus_apss
     g = DCGrid(pts, 5)
