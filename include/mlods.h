@@ -226,6 +226,12 @@ int mlods_dcgrid_xform(mlods_dcgrid g, float* xform, int64_t* n_projected);
 int mlods_dc_evaluate(mlods_tree t, int64_t n_cells, const int32_t* cells, int32_t max_depth, const float* xform,
                       int32_t use_normals, float* corner_f, float* vertex, int32_t* n_cross,
                       int64_t* n_unique_corners, void* stream);
+/* The same with the cells and the three outputs in device memory (xform stays
+ * a host array): nothing crosses the host link but the 12-float map and the
+ * unique-corner count.  Returns when the outputs are written. */
+int mlods_dc_evaluate_device(mlods_tree t, int64_t n_cells, const int32_t* d_cells, int32_t max_depth,
+                             const float* xform, int32_t use_normals, float* d_corner_f, float* d_vertex,
+                             int32_t* d_n_cross, int64_t* n_unique_corners, void* stream);
 
 /* ---- mesh extraction and refinement (dual_contouring.h:59-87, scene.cpp:1396-1452) ----
  * mlods_dc_extract builds the dual-contouring mesh of a grid (cells sorted as

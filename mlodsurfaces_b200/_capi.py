@@ -161,6 +161,7 @@ SIGNATURES = {
     "mlods_dcgrid_cells": (C.c_int, [_P, _P]),
     "mlods_dcgrid_free": (C.c_int, [_P]),
     "mlods_dc_evaluate": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, C.c_int32, _P, _P, _P, _I64, _P]),
+    "mlods_dc_evaluate_device": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, C.c_int32, _P, _P, _P, _I64, _P]),
     "mlods_batch_create": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
     "mlods_batch_free": (C.c_int, [_P]),
     "mlods_batch_project": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, _P]),

@@ -543,6 +543,28 @@ class APSS:
                                                capi.ptr(nc), C.byref(nu), C.c_void_p(0)))
         return cf, vx, nc, nu.value
 
+    def dc_evaluate_device(self, d_cells, max_depth: int, xform=None, use_normals: bool = False, stream=None):
+        """dc_evaluate with the cells (an (n, 4) int32 CUDA tensor) and the
+        results in device memory: (corner_f (n, 8), vertex (n, 3), n_cross
+        (n,) as CUDA tensors, number of unique corners projected)."""
+        import torch
+
+        self._sync_params()
+        cells = d_cells.reshape(-1, 4)
+        if cells.dtype != torch.int32 or not cells.is_cuda or not cells.is_contiguous():
+            raise ValueError("cells must be a contiguous int32 CUDA tensor of shape (n, 4)")
+        xf = np.ascontiguousarray(unit2bbox() if xform is None else np.asarray(xform, np.float32).reshape(3, 4))
+        n = cells.shape[0]
+        cf = torch.empty((n, 8), dtype=torch.float32, device=cells.device)
+        vx = torch.empty((n, 3), dtype=torch.float32, device=cells.device)
+        nc = torch.empty((n,), dtype=torch.int32, device=cells.device)
+        nu = C.c_int64(0)
+        s = stream if stream is not None else torch.cuda.current_stream(cells.device).cuda_stream
+        capi.check(self._lib.mlods_dc_evaluate_device(self.m_apssOctree.handle, n, capi.ptr(cells), int(max_depth),
+                                                      capi.ptr(xf), 1 if use_normals else 0, capi.ptr(cf),
+                                                      capi.ptr(vx), capi.ptr(nc), C.byref(nu), C.c_void_p(s)))
+        return cf, vx, nc, nu.value
+
     def dc_mesh(self, grid: DCGrid, use_normals: bool = False, refine_rounds: int = 2, stream=None) -> Mesh:
         """scene::computeDualContouring's mesh (scene.cpp:1346-1452): corner
         field, extraction, transform to the tree's frame, projection, then

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "dc.h"
@@ -31,6 +32,42 @@ int sm_count_for_current_device()
     if (dev < 64) cache[dev] = v;
     return v;
 }
+
+// Stream-ordered scratch from a memory pool owned by the library (one per
+// device), which keeps up to 8 GiB of freed scratch for reuse, so per-call
+// buffers of a few GB cost neither a cudaMalloc nor a synchronising cudaFree.
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s)
+{
+    static cudaMemPool_t pools[64] = {};
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 64) return cudaMallocAsync(p, bytes, s);
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&pools[dev], &props);
+            if (e != cudaSuccess) {
+                pools[dev] = nullptr;
+                return e;
+            }
+            uint64_t keep = uint64_t(8) << 30;
+            e = cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) return e;
+        }
+        pool = pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
+cudaError_t scratch_free(void* p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) : cudaSuccess; }
 
 namespace
 {
@@ -734,8 +771,21 @@ int mlods_dc_evaluate(mlods_tree t, int64_t n_cells, const int32_t* cells, int32
         set_last_error("dc evaluate: no kernel set (call mlods_set_kernel first)");
         return MLODS_ERR_STATE;
     }
-    return dc_evaluate(t, n_cells, cells, max_depth, xform, use_normals, corner_f, vertex, n_cross, n_unique_corners,
-                       static_cast<cudaStream_t>(stream));
+    return dc_evaluate(t, n_cells, cells, false, max_depth, xform, use_normals, corner_f, vertex, n_cross,
+                       n_unique_corners, static_cast<cudaStream_t>(stream));
+}
+
+int mlods_dc_evaluate_device(mlods_tree t, int64_t n_cells, const int32_t* d_cells, int32_t max_depth,
+                             const float* xform, int32_t use_normals, float* d_corner_f, float* d_vertex,
+                             int32_t* d_n_cross, int64_t* n_unique_corners, void* stream)
+{
+    CHECK_TREE(t);
+    if (!t->kernel_set) {
+        set_last_error("dc evaluate: no kernel set (call mlods_set_kernel first)");
+        return MLODS_ERR_STATE;
+    }
+    return dc_evaluate(t, n_cells, d_cells, true, max_depth, xform, use_normals, d_corner_f, d_vertex, d_n_cross,
+                       n_unique_corners, static_cast<cudaStream_t>(stream));
 }
 
 int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_t* max_stack, int64_t* overflows,

@@ -56,6 +56,31 @@ __global__ void corner_keys_kernel(const int4* __restrict__ cells, int64_t n_cel
     vals[i] = uint32_t(i);
 }
 
+// Cell checks: depth in [0, max_depth] and the cell's lattice box inside the
+// key range.  err |= 1 (depth) or 2 (lattice); bad = lowest failing cell.
+__global__ void check_cells_kernel(const int4* __restrict__ cells, int64_t n_cells, Lattice L,
+                                   uint32_t* __restrict__ err, unsigned long long* __restrict__ bad)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n_cells) return;
+    const int4 c = cells[i];
+    uint32_t e = 0;
+    if (c.x < 0 || c.x > L.max_depth) {
+        e = 1u;
+    } else {
+        const int64_t delta = int64_t(1) << (L.max_depth - c.x);
+        const int v[3] = {c.y, c.z, c.w};
+        for (int a = 0; a < 3; ++a) {
+            const int64_t l0 = int64_t(v[a]) * delta, l1 = (int64_t(v[a]) + 1) * delta;
+            if (l0 < -L.bias || l1 >= L.bias) e = 2u;
+        }
+    }
+    if (e) {
+        atomicOr(err, e);
+        atomicMin(bad, (unsigned long long)i);
+    }
+}
+
 __global__ void unique_flags_kernel(const uint64_t* __restrict__ keys, int64_t n, uint32_t* __restrict__ flags)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -232,8 +257,8 @@ inline size_t al(size_t v) { return (v + 255) / 256 * 256; }
 
 }  // namespace
 
-int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
-                    int use_normals, DcField& out, cudaStream_t s)
+int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, bool cells_on_device, int max_depth,
+                    const float* xform, int use_normals, DcField& out, cudaStream_t s)
 {
     dc_field_free(out);
     if (n_cells <= 0 || !cells || !xform) {
@@ -248,29 +273,14 @@ int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int 
     L.max_depth = max_depth;
     L.bits = max_depth + 4;
     L.bias = int64_t(1) << (max_depth + 2);
-    for (int64_t i = 0; i < n_cells; ++i) {
-        const int d = cells[4 * i];
-        if (d < 0 || d > max_depth) {
-            set_last_error("dc evaluate: cell %lld has depth %d outside [0, %d]", (long long)i, d, max_depth);
-            return MLODS_ERR_INVALID;
-        }
-        const int64_t delta = int64_t(1) << (max_depth - d);
-        for (int a = 1; a < 4; ++a) {
-            const int64_t l0 = int64_t(cells[4 * i + a]) * delta, l1 = (int64_t(cells[4 * i + a]) + 1) * delta;
-            if (l0 < -L.bias || l1 >= L.bias) {
-                set_last_error("dc evaluate: cell %lld lies outside the supported lattice", (long long)i);
-                return MLODS_ERR_CAPACITY;
-            }
-        }
-    }
     const int64_t nc8 = n_cells * 8;
     size_t bytes = al(size_t(n_cells) * 16) + 2 * al(size_t(nc8) * 8) + 2 * al(size_t(nc8) * 4) +
-                   2 * al(size_t(nc8) * 4) + al(64) + std::max(radix_temp_bytes(nc8), scan_temp_bytes(nc8));
-    bytes += al(size_t(nc8) * 4 * 10) + al(size_t(nc8) * 4) + (use_normals ? al(size_t(nc8) * 12) : 0) +
-             al(size_t(n_cells) * 16);
+                   2 * al(size_t(nc8) * 4) + al(128) + std::max(radix_temp_bytes(nc8), scan_temp_bytes(nc8));
+    bytes += al(size_t(nc8) * 4) + (use_normals ? al(size_t(nc8) * 12) : 0) + al(size_t(n_cells) * 16);
     char* base = nullptr;
-    MLODS_CUDA(cudaMalloc(&base, bytes));
+    MLODS_CUDA(scratch_alloc(reinterpret_cast<void**>(&base), bytes, s));
     out.base = base;
+    out.stream = s;
     size_t off = 0;
     auto take = [&](size_t b) {
         char* p = base + off;
@@ -284,10 +294,11 @@ int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int 
     uint32_t* v1 = reinterpret_cast<uint32_t*>(take(size_t(nc8) * 4));
     uint32_t* flags = reinterpret_cast<uint32_t*>(take(size_t(nc8) * 4));
     uint32_t* excl = reinterpret_cast<uint32_t*>(take(size_t(nc8) * 4));
-    uint32_t* d_total = reinterpret_cast<uint32_t*>(take(64));
+    uint32_t* d_total = reinterpret_cast<uint32_t*>(take(128));  // unique count, cell errors, first bad cell, xform
+    uint32_t* d_err = d_total + 1;
+    unsigned long long* d_bad = reinterpret_cast<unsigned long long*>(d_total + 2);
     float* d_xf = reinterpret_cast<float*>(d_total + 4);
     void* tmp = take(std::max(radix_temp_bytes(nc8), scan_temp_bytes(nc8)));
-    float* pos = reinterpret_cast<float*>(take(size_t(nc8) * 4 * 10));  // up to nc8 unique corners x (3 pos + 3 proj + 3 nrm + f)
     float* d_cf = reinterpret_cast<float*>(take(size_t(nc8) * 4));
     float* d_cn = use_normals ? reinterpret_cast<float*>(take(size_t(nc8) * 12)) : nullptr;
     float* d_vert = reinterpret_cast<float*>(take(size_t(n_cells) * 12));
@@ -302,8 +313,15 @@ int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int 
         if (_e != cudaSuccess) return fail(_e, what);   \
     } while (0)
 
-    DC_CHECK(cudaMemcpyAsync(d_cells, cells, size_t(n_cells) * 16, cudaMemcpyHostToDevice, s), "upload cells");
+    DC_CHECK(cudaMemcpyAsync(d_cells, cells, size_t(n_cells) * 16,
+                             cells_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
+             "upload cells");
     DC_CHECK(cudaMemcpyAsync(d_xf, xform, 12 * sizeof(float), cudaMemcpyHostToDevice, s), "upload xform");
+    DC_CHECK(cudaMemsetAsync(d_err, 0, 4, s), "clear cell errors");
+    DC_CHECK(cudaMemsetAsync(d_bad, 0xff, 8, s), "clear first bad cell");
+    check_cells_kernel<<<grid_for(n_cells), kThreads, 0, s>>>(d_cells, n_cells, L, d_err, d_bad);
+    note_launch();
+    DC_CHECK(cudaGetLastError(), "check cells");
     corner_keys_kernel<<<grid_for(nc8), kThreads, 0, s>>>(d_cells, n_cells, L, k0, v0);
     note_launch();
     DC_CHECK(cudaGetLastError(), "corner keys");
@@ -315,10 +333,24 @@ int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int 
     note_launch();
     DC_CHECK(cudaGetLastError(), "unique flags");
     DC_CHECK(exclusive_scan_u32(flags, excl, nc8, d_total, tmp, s), "unique scan");
-    uint32_t h_u = 0;
-    DC_CHECK(cudaMemcpyAsync(&h_u, d_total, 4, cudaMemcpyDeviceToHost, s), "read unique count");
+    uint32_t h_head[4] = {0, 0, 0, 0};  // unique count, cell errors, first bad cell
+    DC_CHECK(cudaMemcpyAsync(h_head, d_total, 16, cudaMemcpyDeviceToHost, s), "read unique count");
     DC_CHECK(cudaStreamSynchronize(s), "sync unique count");
-    const int64_t U = h_u;
+    if (h_head[1]) {
+        unsigned long long bad = 0;
+        std::memcpy(&bad, h_head + 2, 8);
+        dc_field_free(out);
+        if (h_head[1] & 1u) {
+            set_last_error("dc evaluate: cell %llu has a depth outside [0, %d]", bad, max_depth);
+            return MLODS_ERR_INVALID;
+        }
+        set_last_error("dc evaluate: cell %llu lies outside the supported lattice", bad);
+        return MLODS_ERR_CAPACITY;
+    }
+    const int64_t U = h_head[0];
+    // U unique corners x (3 position + 3 projection + 3 normal + field)
+    DC_CHECK(scratch_alloc(&out.base2, size_t(std::max<int64_t>(U, 1)) * 40, s), "unique corner buffers");
+    float* pos = static_cast<float*>(out.base2);
     float* cpos = pos;
     float* cproj = pos + 3 * U;
     float* cnrm = pos + 6 * U;
@@ -342,6 +374,8 @@ int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int 
     vertex_kernel<<<grid_for(n_cells), kThreads, 0, s>>>(d_cells, n_cells, max_depth, d_cf, d_cn, d_vert, d_ncross);
     note_launch();
     DC_CHECK(cudaGetLastError(), "vertex");
+    DC_CHECK(scratch_free(out.base2, s), "free unique corner buffers");  // stream-ordered: after the scatter
+    out.base2 = nullptr;
     DC_CHECK(cudaStreamSynchronize(s), "sync dc");
 #undef DC_CHECK
     out.cells = d_cells;
@@ -355,23 +389,26 @@ int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int 
 
 void dc_field_free(DcField& f)
 {
-    cudaFree(f.base);
+    scratch_free(f.base, f.stream);
+    scratch_free(f.base2, f.stream);
     f = DcField{};
 }
 
-int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
-                int use_normals, float* corner_f, float* vertex, int32_t* n_cross, int64_t* n_unique, cudaStream_t s)
+int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, bool cells_on_device, int max_depth,
+                const float* xform, int use_normals, float* corner_f, float* vertex, int32_t* n_cross,
+                int64_t* n_unique, cudaStream_t s)
 {
     if (!corner_f || !vertex || !n_cross) {
         set_last_error("dc evaluate: bad arguments");
         return MLODS_ERR_INVALID;
     }
     DcField f;
-    int rc = dc_field_device(T, n_cells, cells, max_depth, xform, use_normals, f, s);
+    int rc = dc_field_device(T, n_cells, cells, cells_on_device, max_depth, xform, use_normals, f, s);
     if (rc != MLODS_OK) return rc;
-    cudaError_t e = cudaMemcpyAsync(corner_f, f.cf, size_t(n_cells) * 32, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(vertex, f.vert, size_t(n_cells) * 12, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(n_cross, f.ncross, size_t(n_cells) * 4, cudaMemcpyDeviceToHost, s);
+    // cudaMemcpyDefault: host or device outputs, told apart by address (unified addressing)
+    cudaError_t e = cudaMemcpyAsync(corner_f, f.cf, size_t(n_cells) * 32, cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vertex, f.vert, size_t(n_cells) * 12, cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(n_cross, f.ncross, size_t(n_cells) * 4, cudaMemcpyDefault, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (n_unique) *n_unique = f.n_unique;
     dc_field_free(f);

@@ -86,15 +86,17 @@ int dmesh_subdivide(DeviceMesh& m, cudaStream_t s);
 // The corner field of a grid kept in device memory: cells (int4), 8 corner
 // values, vertex and crossing count per cell, in one allocation.
 struct DcField {
-    void* base = nullptr;
+    void* base = nullptr;   // scratch of the library pool, freed in stream order
+    void* base2 = nullptr;  // unique-corner buffers
+    cudaStream_t stream = nullptr;
     const int4* cells = nullptr;
     float* cf = nullptr;
     float* vert = nullptr;
     int32_t* ncross = nullptr;
     int64_t n = 0, n_unique = 0;
 };
-int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
-                    int use_normals, DcField& out, cudaStream_t s);
+int dc_field_device(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, bool cells_on_device, int max_depth,
+                    const float* xform, int use_normals, DcField& out, cudaStream_t s);
 void dc_field_free(DcField& f);
 
 // Extraction on the device (dc_extract_dev.cu) from a device field; the mesh
@@ -113,7 +115,9 @@ float* dmesh_nrm(DeviceMesh& m);
 uint32_t* dmesh_tri(DeviceMesh& m);
 
 // Field at the 8 corners of every cell (unique corners projected once) and
-// the per-cell vertex; host arrays in and out.
-int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, int max_depth, const float* xform,
-                int use_normals, float* corner_f, float* vertex, int32_t* n_cross, int64_t* n_unique, cudaStream_t s);
+// the per-cell vertex; cells in host or device memory, outputs in host or
+// device memory (told apart by address).
+int dc_evaluate(mlods_tree_s* T, int64_t n_cells, const int32_t* cells, bool cells_on_device, int max_depth,
+                const float* xform, int use_normals, float* corner_f, float* vertex, int32_t* n_cross,
+                int64_t* n_unique, cudaStream_t s);
 }  // namespace mlods

@@ -627,7 +627,7 @@ int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t ref
     // corner field in device memory
     auto t0 = clk::now();
     DcField field;
-    int rc = dc_field_device(t, n, g->cells.data(), g->max_depth, g->xform, use_normals, field, s);
+    int rc = dc_field_device(t, n, g->cells.data(), false, g->max_depth, g->xform, use_normals, field, s);
     m->stage_ms[0] = since(t0);
     // extraction: on the device when the grid allows, else on the host
     t0 = clk::now();

@@ -124,6 +124,9 @@ void note_launch(int n = 1);
 int64_t launches_so_far();
 // Multiprocessor count of the current device (cached per device).
 int sm_count_for_current_device();
+// Stream-ordered scratch memory from the library's pool on the current device.
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+cudaError_t scratch_free(void* p, cudaStream_t s);
 
 // Error-reporting helpers (host).
 void set_last_error(const char* fmt, ...);

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import shutil
 import subprocess
 from pathlib import Path
 
@@ -33,6 +34,8 @@ def build(with_ref: bool = True) -> None:
     targets = ["oracle"]
     if with_ref and (REF_ROOT / "sources" / "apss").is_dir():
         targets.append("ref")
+        if shutil.which("nvcc"):  # the reference's own GPU path, for the GPU-side pins
+            targets.append("refgpu")
     subprocess.run(["make", "-s", "-C", str(HERE), f"REF_ROOT={REF_ROOT}"] + targets, check=True)
 
 

@@ -92,3 +92,34 @@ def test_qef_with_normals_stays_in_its_cell(dc_setup):
     eps = 1e-6
     assert np.isfinite(vx).all()
     assert ((vx[act] >= lo[act] - eps) & (vx[act] <= lo[act] + width[act, None] + eps)).all()
+
+
+def test_device_buffers_give_the_host_results(dc_setup):
+    """mlods_dc_evaluate_device: cells and results in device memory, the
+    same values as the host-buffer call, on two calls in a row (the second
+    reuses the library's pooled scratch)."""
+    import torch
+
+    from mlodsurfaces_b200._capi import MlodsError
+
+    pts, nrm, diag, k, f, g = dc_setup
+    want = f.dc_evaluate(g.cells, g.max_depth)
+    d_cells = torch.from_numpy(np.ascontiguousarray(g.cells, np.int32)).cuda()
+    for _ in range(2):
+        cf, vx, nc, nu = f.dc_evaluate_device(d_cells, g.max_depth)
+        torch.cuda.synchronize()
+        assert nu == want[3]
+        assert np.array_equal(cf.cpu().numpy(), want[0], equal_nan=True)
+        assert np.array_equal(vx.cpu().numpy(), want[1]) and np.array_equal(nc.cpu().numpy(), want[2])
+    # cells deeper than max_depth or off the lattice are refused on the device path too
+    bad = d_cells.clone()
+    bad[7, 0] = g.max_depth + 1
+    with pytest.raises(MlodsError):
+        f.dc_evaluate_device(bad, g.max_depth)
+    bad = d_cells.clone()
+    bad[3, 1] = 1 << 30
+    with pytest.raises(MlodsError):
+        f.dc_evaluate_device(bad, g.max_depth)
+    # and the host path still works after a refusal
+    again = f.dc_evaluate(g.cells, g.max_depth)
+    assert np.array_equal(again[0], want[0], equal_nan=True)
