@@ -499,10 +499,88 @@ __device__ __forceinline__ float global_weight(const KernelConsts& kc, float d2)
     return w;
 }
 
-// kGlobalQpt queries per thread; every point of the cloud contributes
-// w(p_i, q) a_i {1, n_i, p_i, p_i.n_i, |p_i|^2} (APSSOctree::APSSStats,
-// CPUUtils.cpp:515-528).  Points stream through shared memory in tiles;
-// per-tile float partial sums are accumulated in double.
+// Sums over the points [p_begin, p_end) for kGlobalQpt queries per thread
+// (local-frame float positions lx, ly, lz): every point contributes
+// w(p_i, q) a_i {1, n_i, p_i - q, (p_i - q).n_i, |p_i - q|^2}
+// (APSSOctree::APSSStats, CPUUtils.cpp:515-528).  Points stream through
+// shared memory in tiles; per-tile float partial sums are added to `tot` in
+// double.  Every thread of the block calls it (it synchronises the block).
+template <int KTYPE, int NSIG>
+__device__ __forceinline__ void global_pair_sums(const GlobalArgs& a, int64_t p_begin, int64_t p_end,
+                                                 const float (&lx)[kGlobalQpt], const float (&ly)[kGlobalQpt],
+                                                 const float (&lz)[kGlobalQpt], double (&tot)[kGlobalQpt][9],
+                                                 float4* s_p, float4* s_n)
+{
+    constexpr int Q = kGlobalQpt;
+    for (int64_t base = p_begin; base < p_end; base += kGlobalTile) {
+        __syncthreads();
+        for (int j = threadIdx.x; j < kGlobalTile; j += kGlobalThreads) {
+            const int64_t g = base + j;
+            if (g < p_end) {
+                const float4 p = __ldg(a.spts + g);
+                const float4 nn = __ldg(a.snrm + g);
+                const float ar = __ldg(a.area + __float_as_uint(p.w));
+                s_p[j] = make_float4(p.x, p.y, p.z, ar);
+                s_n[j] = nn;
+            } else {  // zero area: no contribution
+                s_p[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                s_n[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        __syncthreads();
+        float acc[Q][9];
+#pragma unroll
+        for (int u = 0; u < Q; ++u)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) acc[u][c] = 0.f;
+#pragma unroll 2
+        for (int j = 0; j < kGlobalTile; ++j) {
+            const float4 p = s_p[j];
+            const float4 nn = s_n[j];
+#pragma unroll
+            for (int u = 0; u < Q; ++u) {
+                const float dx = p.x - lx[u], dy = p.y - ly[u], dz = p.z - lz[u];
+                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float w = global_weight<KTYPE, NSIG>(a.kc, dd) * p.w;
+                acc[u][0] += w;
+                acc[u][1] = fmaf(w, nn.x, acc[u][1]);
+                acc[u][2] = fmaf(w, nn.y, acc[u][2]);
+                acc[u][3] = fmaf(w, nn.z, acc[u][3]);
+                acc[u][4] = fmaf(w, dx, acc[u][4]);
+                acc[u][5] = fmaf(w, dy, acc[u][5]);
+                acc[u][6] = fmaf(w, dz, acc[u][6]);
+                acc[u][7] = fmaf(w, fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z)), acc[u][7]);
+                acc[u][8] = fmaf(w, dd, acc[u][8]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < Q; ++u)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) tot[u][c] += double(acc[u][c]);
+    }
+}
+
+// One fit step of a query from its sums: false (iterate kept, normal 0) when
+// the fit is NaN (CPUUtils.cpp:770-776).
+__device__ __forceinline__ bool global_step(const GlobalArgs& a, const double (&tot)[9], float lx, float ly, float lz,
+                                            double xd[3], float nrm[3])
+{
+    float s[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) s[c] = float(tot[c]);
+    double x[3];
+    if (!fit_cpu(s, double(a.step_max), x, nrm)) {
+        nrm[0] = nrm[1] = nrm[2] = 0.f;
+        return false;
+    }
+    xd[0] = double(lx) + x[0];
+    xd[1] = double(ly) + x[1];
+    xd[2] = double(lz) + x[2];
+    return true;
+}
+
+// All iterations of kGlobalQpt queries per thread in one launch, every point
+// per iteration: the form for query counts that fill the GPU.
 template <int KTYPE, int NSIG>
 __global__ void __launch_bounds__(kGlobalThreads) global_apss_kernel(GlobalArgs a)
 {
@@ -536,68 +614,11 @@ __global__ void __launch_bounds__(kGlobalThreads) global_apss_kernel(GlobalArgs 
 #pragma unroll
             for (int c = 0; c < 9; ++c) tot[u][c] = 0.0;
         }
-        for (int64_t base = 0; base < a.n_pts; base += kGlobalTile) {
-            __syncthreads();
-            for (int j = threadIdx.x; j < kGlobalTile; j += kGlobalThreads) {
-                const int64_t g = base + j;
-                if (g < a.n_pts) {
-                    const float4 p = __ldg(a.spts + g);
-                    const float4 nn = __ldg(a.snrm + g);
-                    const float ar = __ldg(a.area + __float_as_uint(p.w));
-                    s_p[j] = make_float4(p.x, p.y, p.z, ar);
-                    s_n[j] = nn;
-                } else {  // zero area: no contribution
-                    s_p[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    s_n[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
-            __syncthreads();
-            float acc[Q][9];
-#pragma unroll
-            for (int u = 0; u < Q; ++u)
-#pragma unroll
-                for (int c = 0; c < 9; ++c) acc[u][c] = 0.f;
-#pragma unroll 2
-            for (int j = 0; j < kGlobalTile; ++j) {
-                const float4 p = s_p[j];
-                const float4 nn = s_n[j];
-#pragma unroll
-                for (int u = 0; u < Q; ++u) {
-                    const float dx = p.x - lx[u], dy = p.y - ly[u], dz = p.z - lz[u];
-                    const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    const float w = global_weight<KTYPE, NSIG>(a.kc, dd) * p.w;
-                    acc[u][0] += w;
-                    acc[u][1] = fmaf(w, nn.x, acc[u][1]);
-                    acc[u][2] = fmaf(w, nn.y, acc[u][2]);
-                    acc[u][3] = fmaf(w, nn.z, acc[u][3]);
-                    acc[u][4] = fmaf(w, dx, acc[u][4]);
-                    acc[u][5] = fmaf(w, dy, acc[u][5]);
-                    acc[u][6] = fmaf(w, dz, acc[u][6]);
-                    acc[u][7] = fmaf(w, fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z)), acc[u][7]);
-                    acc[u][8] = fmaf(w, dd, acc[u][8]);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < Q; ++u)
-#pragma unroll
-                for (int c = 0; c < 9; ++c) tot[u][c] += double(acc[u][c]);
-        }
+        global_pair_sums<KTYPE, NSIG>(a, 0, a.n_pts, lx, ly, lz, tot, s_p, s_n);
 #pragma unroll
         for (int u = 0; u < Q; ++u) {
             if (!valid[u] || failed[u]) continue;
-            float s[9];
-#pragma unroll
-            for (int c = 0; c < 9; ++c) s[c] = float(tot[u][c]);
-            double x[3];
-            if (!fit_cpu(s, double(a.step_max), x, nrm[u])) {
-                // NaN: the iterate stays, normal 0 (CPUUtils.cpp:770-776)
-                nrm[u][0] = nrm[u][1] = nrm[u][2] = 0.f;
-                failed[u] = true;
-                continue;
-            }
-            xd[u][0] = double(lx[u]) + x[0];
-            xd[u][1] = double(ly[u]) + x[1];
-            xd[u][2] = double(lz[u]) + x[2];
+            if (!global_step(a, tot[u], lx[u], ly[u], lz[u], xd[u], nrm[u])) failed[u] = true;
         }
     }
 #pragma unroll
@@ -611,6 +632,143 @@ __global__ void __launch_bounds__(kGlobalThreads) global_apss_kernel(GlobalArgs 
         a.out_n[3 * qi + 1] = nrm[u][1];
         a.out_n[3 * qi + 2] = nrm[u][2];
     }
+}
+
+// The split form, for query counts too small to fill the GPU: the points are
+// cut into `chunks` ranges, block (x, y) sums query tile x against range y
+// and writes its double sums to part[(y * nq + q) * 9 + c]; then one thread
+// per query adds the ranges in order, fits, and moves the iterate.  One such
+// pair of launches per iteration.
+struct GlobalSplit {
+    double* part;     // chunks * nq * 9
+    double* xd;       // nq * 3, the iterate in the local frame
+    float* nrm;       // nq * 3
+    uint32_t* failed; // nq
+    int chunks;
+    int64_t chunk_pts;
+};
+
+__global__ void global_split_init_kernel(GlobalArgs a, GlobalSplit g)
+{
+    const int64_t qi = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (qi >= a.nq) return;
+    const double o[3] = {a.o0, a.o1, a.o2};
+    for (int c = 0; c < 3; ++c) {
+        g.xd[3 * qi + c] = double(a.q_in[3 * qi + c]) - o[c];
+        g.nrm[3 * qi + c] = 0.f;
+    }
+    g.failed[qi] = 0u;
+}
+
+template <int KTYPE, int NSIG>
+__global__ void __launch_bounds__(kGlobalThreads) global_split_sums_kernel(GlobalArgs a, GlobalSplit g)
+{
+    constexpr int Q = kGlobalQpt;
+    __shared__ float4 s_p[kGlobalTile];
+    __shared__ float4 s_n[kGlobalTile];
+    const int64_t q_first = int64_t(blockIdx.x) * kGlobalThreads * Q + threadIdx.x;
+    const int64_t p_begin = int64_t(blockIdx.y) * g.chunk_pts;
+    const int64_t p_end = p_begin + g.chunk_pts < a.n_pts ? p_begin + g.chunk_pts : a.n_pts;
+    float lx[Q], ly[Q], lz[Q];
+    double tot[Q][9];
+#pragma unroll
+    for (int u = 0; u < Q; ++u) {
+        const int64_t qi = q_first + int64_t(u) * kGlobalThreads;
+        const bool valid = qi < a.nq;
+        lx[u] = valid ? float(g.xd[3 * qi]) : 0.f;
+        ly[u] = valid ? float(g.xd[3 * qi + 1]) : 0.f;
+        lz[u] = valid ? float(g.xd[3 * qi + 2]) : 0.f;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) tot[u][c] = 0.0;
+    }
+    global_pair_sums<KTYPE, NSIG>(a, p_begin, p_end, lx, ly, lz, tot, s_p, s_n);
+#pragma unroll
+    for (int u = 0; u < Q; ++u) {
+        const int64_t qi = q_first + int64_t(u) * kGlobalThreads;
+        if (qi >= a.nq) continue;
+        double* dst = g.part + (int64_t(blockIdx.y) * a.nq + qi) * 9;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) dst[c] = tot[u][c];
+    }
+}
+
+__global__ void global_split_step_kernel(GlobalArgs a, GlobalSplit g, bool last)
+{
+    const int64_t qi = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (qi >= a.nq) return;
+    double xd[3] = {g.xd[3 * qi], g.xd[3 * qi + 1], g.xd[3 * qi + 2]};
+    float nrm[3] = {g.nrm[3 * qi], g.nrm[3 * qi + 1], g.nrm[3 * qi + 2]};
+    if (!g.failed[qi]) {
+        double tot[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < g.chunks; ++k) {
+            const double* src = g.part + (int64_t(k) * a.nq + qi) * 9;
+#pragma unroll
+            for (int c = 0; c < 9; ++c) tot[c] += src[c];
+        }
+        const float lx = float(xd[0]), ly = float(xd[1]), lz = float(xd[2]);
+        if (!global_step(a, tot, lx, ly, lz, xd, nrm)) g.failed[qi] = 1u;
+        for (int c = 0; c < 3; ++c) {
+            g.xd[3 * qi + c] = xd[c];
+            g.nrm[3 * qi + c] = nrm[c];
+        }
+    }
+    if (last) {
+        a.out_p[3 * qi] = float(xd[0] + a.o0);
+        a.out_p[3 * qi + 1] = float(xd[1] + a.o1);
+        a.out_p[3 * qi + 2] = float(xd[2] + a.o2);
+        a.out_n[3 * qi] = nrm[0];
+        a.out_n[3 * qi + 1] = nrm[1];
+        a.out_n[3 * qi + 2] = nrm[2];
+    }
+}
+
+// Launches the global projection of one kernel specialisation: the fused
+// kernel when the query tiles fill the GPU about four times over, else the
+// split form over as many point ranges as bring it there.
+template <int KTYPE, int NSIG>
+cudaError_t launch_global_typed(const GlobalArgs& a, int sm_count, cudaStream_t s)
+{
+    const int64_t per_block = int64_t(kGlobalThreads) * kGlobalQpt;
+    const int64_t qblocks = (a.nq + per_block - 1) / per_block;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, global_apss_kernel<KTYPE, NSIG>,
+                                                                  kGlobalThreads, 0);
+    if (e != cudaSuccess) return e;
+    const int64_t target = 4 * int64_t(per_sm < 1 ? 1 : per_sm) * sm_count;
+    int64_t chunks = (target + qblocks - 1) / qblocks;
+    const int64_t max_chunks = a.n_pts / (8 * kGlobalTile);  // ranges of at least 2048 points
+    if (chunks > max_chunks) chunks = max_chunks;
+    if (chunks > 64) chunks = 64;
+    if (chunks <= 1 || a.n_iter < 1) {
+        global_apss_kernel<KTYPE, NSIG><<<unsigned(qblocks), kGlobalThreads, 0, s>>>(a);
+        note_launch();
+        return cudaGetLastError();
+    }
+    GlobalSplit g;
+    g.chunks = int(chunks);
+    g.chunk_pts = (a.n_pts + chunks - 1) / chunks;
+    const size_t part_bytes = size_t(chunks) * size_t(a.nq) * 9 * sizeof(double);
+    const size_t state_bytes = size_t(a.nq) * (3 * sizeof(double) + 3 * sizeof(float) + sizeof(uint32_t));
+    void* mem = nullptr;
+    e = scratch_alloc(&mem, part_bytes + state_bytes + 256, s);
+    if (e != cudaSuccess) return e;
+    char* m = static_cast<char*>(mem);
+    g.part = reinterpret_cast<double*>(m);
+    g.xd = reinterpret_cast<double*>(m + part_bytes);
+    g.nrm = reinterpret_cast<float*>(m + part_bytes + size_t(a.nq) * 3 * sizeof(double));
+    g.failed = reinterpret_cast<uint32_t*>(m + part_bytes + size_t(a.nq) * (3 * sizeof(double) + 3 * sizeof(float)));
+    const unsigned q_threads = 256;
+    const unsigned q_grid = unsigned((a.nq + q_threads - 1) / q_threads);
+    global_split_init_kernel<<<q_grid, q_threads, 0, s>>>(a, g);
+    note_launch();
+    for (int it = 0; it < a.n_iter && e == cudaSuccess; ++it) {
+        global_split_sums_kernel<KTYPE, NSIG><<<dim3(unsigned(qblocks), unsigned(chunks)), kGlobalThreads, 0, s>>>(a, g);
+        global_split_step_kernel<<<q_grid, q_threads, 0, s>>>(a, g, it + 1 == a.n_iter);
+        note_launch(2);
+        e = cudaGetLastError();
+    }
+    const cudaError_t ef = scratch_free(mem, s);
+    return e != cudaSuccess ? e : ef;
 }
 
 template <int KTYPE, int MODE>
@@ -651,25 +809,22 @@ cudaError_t launch_gather(const GatherArgs& a, int mode, int ktype, int sm_count
 
 cudaError_t launch_global_apss(const GlobalArgs& a, int ktype, cudaStream_t s)
 {
-    const int64_t per_block = int64_t(kGlobalThreads) * kGlobalQpt;
-    const unsigned grid = unsigned((a.nq + per_block - 1) / per_block);
+    const int sm = sm_count_for_current_device();
     switch (ktype) {
-    case MLODS_GAUSSIAN: global_apss_kernel<MLODS_GAUSSIAN, 0><<<grid, kGlobalThreads, 0, s>>>(a); break;
-    case MLODS_SINGULAR: global_apss_kernel<MLODS_SINGULAR, 0><<<grid, kGlobalThreads, 0, s>>>(a); break;
+    case MLODS_GAUSSIAN: return launch_global_typed<MLODS_GAUSSIAN, 0>(a, sm, s);
+    case MLODS_SINGULAR: return launch_global_typed<MLODS_SINGULAR, 0>(a, sm, s);
     default:
         switch (a.kc.nsig) {
-        case 1: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 1><<<grid, kGlobalThreads, 0, s>>>(a); break;
-        case 2: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 2><<<grid, kGlobalThreads, 0, s>>>(a); break;
-        case 3: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 3><<<grid, kGlobalThreads, 0, s>>>(a); break;
-        case 4: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 4><<<grid, kGlobalThreads, 0, s>>>(a); break;
-        case 5: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 5><<<grid, kGlobalThreads, 0, s>>>(a); break;
-        case 6: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 6><<<grid, kGlobalThreads, 0, s>>>(a); break;
-        case 8: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 8><<<grid, kGlobalThreads, 0, s>>>(a); break;
-        default: global_apss_kernel<MLODS_GAUSSIAN_MULTIPLE, 0><<<grid, kGlobalThreads, 0, s>>>(a); break;
+        case 1: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 1>(a, sm, s);
+        case 2: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 2>(a, sm, s);
+        case 3: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 3>(a, sm, s);
+        case 4: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 4>(a, sm, s);
+        case 5: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 5>(a, sm, s);
+        case 6: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 6>(a, sm, s);
+        case 8: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 8>(a, sm, s);
+        default: return launch_global_typed<MLODS_GAUSSIAN_MULTIPLE, 0>(a, sm, s);
         }
     }
-    note_launch();
-    return cudaGetLastError();
 }
 
 }  // namespace mlods

@@ -157,3 +157,36 @@ def test_knn_walk_on_a_large_cloud_never_overflows():
     excess = np.linalg.norm(np.maximum(np.abs(op[sel].astype(np.float64) - o64) - half_ulp, 0.0), axis=1) / diag
     assert excess.max() < TOL_DIAG
     assert_knn_sets(pts, q[sel], 32, t)
+
+
+def test_global_apss_split_and_fused_forms():
+    """Few queries take the split form (point ranges summed by separate
+    blocks, then added in order), many queries the one-launch form; both
+    match the FP64 restatement and each other."""
+    pts, nrm = synth.torus(20000, seed=91)
+    diag = synth.bbox_diag(pts)
+    k = make_kernel("multi", diag)
+    q = synth.perturbed_queries(np.tile(pts, (31, 1)), 0.01, seed=92)  # 620k queries: the one-launch form
+    t = tree_of(pts, nrm)
+    g = GlobalAPSS(t, k)
+    import torch
+
+    d_q = torch.from_numpy(q).cuda()
+    d_p = torch.empty_like(d_q)
+    d_n = torch.empty_like(d_q)
+    g.project_device(d_q, d_p, d_n, 2)
+    full = d_p.cpu().numpy()
+    few = q[:300]
+    d_q2 = torch.from_numpy(np.ascontiguousarray(few)).cuda()
+    d_p2 = torch.empty_like(d_q2)
+    d_n2 = torch.empty_like(d_q2)
+    g.project_device(d_q2, d_p2, d_n2, 2)
+    split = d_p2.cpu().numpy()
+    ot = oracle.OracleTree(pts, nrm, 12)
+    o64, _ = ot.project_global(few[:64], 2, k)
+    assert rel_err(split[:64], o64, diag).max() < TOL_DIAG
+    assert rel_err(full[:64], o64, diag).max() < TOL_DIAG
+    assert rel_err(split, full[:300], diag).max() < TOL_DIAG
+    sel = np.random.default_rng(3).choice(len(q), 64, replace=False)
+    o64b, _ = ot.project_global(q[sel], 2, k)
+    assert rel_err(full[sel], o64b, diag).max() < TOL_DIAG
