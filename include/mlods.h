@@ -279,6 +279,10 @@ int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t ref
  * the launching stream).  Any pointer may be NULL.  Synchronises. */
 int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_t* max_stack, int64_t* overflows,
                      float* kernel_ms);
+/* Iterations the last MLoD projection on this tree ran, summed over its
+ * queries: n x n_iterations, fewer under a convergence mode (each query
+ * counts the iterations it evaluated).  Extension; synchronises. */
+int mlods_last_iterations(mlods_tree t, int64_t* iterations);
 
 /* ---- batched projection over many resident trees (extension) ---------------
  * No counterpart in the reference, which projects one tree per launch

@@ -154,6 +154,7 @@ SIGNATURES = {
     "mlods_queries_reorganize": (C.c_int, [_P, C.c_int64, _P, C.c_uint32, _P]),
     "mlods_project_host": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, C.c_int32, _P]),
     "mlods_last_stats": (C.c_int, [_P, _I64, _I64, _I32, _I64, C.POINTER(C.c_float)]),
+    "mlods_last_iterations": (C.c_int, [_P, _I64]),
     "mlods_kernel_launches": (C.c_int64, []),
     "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),
     "mlods_dcgrid_from_points": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, C.POINTER(_P)]),

@@ -583,8 +583,10 @@ class APSS:
         ms = C.c_float(0)
         capi.check(self._lib.mlods_last_stats(self.m_apssOctree.handle, C.byref(v), C.byref(r), C.byref(m),
                                               C.byref(o), C.byref(ms)))
+        it = C.c_int64(0)
+        capi.check(self._lib.mlods_last_iterations(self.m_apssOctree.handle, C.byref(it)))
         return {"node_visits": v.value, "rounds": r.value, "max_stack": m.value, "overflows": o.value,
-                "kernel_ms": ms.value}
+                "kernel_ms": ms.value, "iterations": it.value}
 
     # -- options, GPUUtils.h:40-43
     def setScalingProtectionSphere(self, val: float) -> None:

@@ -807,6 +807,19 @@ int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_
     return MLODS_OK;
 }
 
+int mlods_last_iterations(mlods_tree t, int64_t* iterations)
+{
+    CHECK_TREE(t);
+    if (!iterations) {
+        set_last_error("last iterations: null output");
+        return MLODS_ERR_INVALID;
+    }
+    int64_t h[6] = {0, 0, 0, 0, 0, 0};
+    if (t->d_stats) MLODS_CUDA(cudaMemcpy(h, t->d_stats, sizeof h, cudaMemcpyDeviceToHost));
+    *iterations = h[5];
+    return MLODS_OK;
+}
+
 int64_t mlods_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 }  // extern "C"

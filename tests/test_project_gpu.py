@@ -147,6 +147,9 @@ def test_tolerance_convergence_stays_within_tolerance(torus20k):
     assert rel_err(b, rp, diag).max() < TOL_DIAG
     _, _, sa, _ = run_gpu(pts, nrm, q, k, iters=10)
     assert sb["node_visits"] < sa["node_visits"]
+    # every query counts the iterations it evaluated
+    assert sa["iterations"] == 10 * len(q)
+    assert len(q) <= sb["iterations"] < sa["iterations"]
 
 
 def test_in_place_protocol_continues_from_last_positions(torus20k):
