@@ -753,21 +753,30 @@ def run_batch(args):
         visits.append(st["node_visits"])
     launches = lib.mlods_kernel_launches() - launches0
     clk = clocks.stop()
-    # the same work as one launch per cloud (the reference's one-object-per-call form)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    # the same work as one launch per cloud (the reference's one-object-per-call
+    # form), warmed up and timed like the batch, and its outputs compared
+    batch_p, batch_n = d_p.clone(), d_n.clone()
     off = 0
     views = []
     for c in counts:
         views.append((d_q[off:off + c], d_p[off:off + c], d_n[off:off + c]))
         off += c
-    e0.record(stream)
     for f, (vq, vp, vn) in zip(projectors, views):
         f.project_device(vq, vp, vn, iters)
-    e1.record(stream)
-    e1.synchronize()
-    per_cloud_ms = e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    same = bool(torch.equal(d_p, batch_p) and torch.equal(d_n, batch_n))
+    per_cloud = []
+    for _ in range(max(args.steps, 1)):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for f, (vq, vp, vn) in zip(projectors, views):
+            f.project_device(vq, vp, vn, iters)
+        e1.record(stream)
+        e1.synchronize()
+        per_cloud.append(e0.elapsed_time(e1))
+    per_cloud_ms = statistics.mean(per_cloud)
     ms = statistics.mean(step_ms)
     value = total / (ms / 1e3)
     kms = statistics.mean(kern_ms)
@@ -794,6 +803,7 @@ def run_batch(args):
                              f"{st['grid_pct']}% of the persistent size",
                    "l2": "L2 flushed (256 MB write) before every timed step"},
         "one_launch_per_cloud_ms": per_cloud_ms,
+        "outputs_equal_one_launch_per_cloud": same,
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "note": f"batch kernel; 36 B per query + 64 B per node visit; peak {peak_kind}"},
@@ -865,8 +875,7 @@ def run_serve(args):
     warm = [request(r0) for _ in range(24)]
     t0 = time.perf_counter()
     tickets = [srv.submit(ci, q, iters, k) for ci, q, k in warm]
-    for t in tickets:
-        srv.wait(t, timeout_ms=600000)
+    warm_out = [srv.wait(t, timeout_ms=600000)[:2] for t in tickets]
     cap_s = time.perf_counter() - t0
     capacity_rps = len(warm) / cap_s
     rate = args.rate if args.rate > 0 else 0.7 * capacity_rps
@@ -921,6 +930,17 @@ def run_serve(args):
     stats = srv.stats()
     srv.close()
     total_q = done_q[0]
+    # served results against each request projected alone (the reference-facing
+    # protocol with the request's kernel): bit-identical
+    same = True
+    for (ci, q, k), (p_srv, n_srv) in list(zip(warm, warm_out))[:6]:
+        f = projectors[ci]
+        f.updateKernel(k)
+        f.copyPointsToGPU(len(q), q)
+        p_one = np.empty_like(q)
+        n_one = np.empty_like(q)
+        f.project(len(q), p_one, n_one, iters)
+        same = same and bool(np.array_equal(p_one, p_srv) and np.array_equal(n_one, n_srv))
     return {
         "metric": "served queries/s and request latency p50/p99 (8 resident clouds, Poisson arrivals)",
         "value": total_q / elapsed,
@@ -946,6 +966,7 @@ def run_serve(args):
                 "d2h_bytes_per_step": int(24 * total_q / len(reqs)),
                 "path": "mlods_server_submit / mlods_server_wait (host arrays)"},
         "server": stats,
+        "outputs_equal_alone": same,
         "clocks": clk,
     }
 

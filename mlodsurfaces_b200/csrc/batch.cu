@@ -137,7 +137,8 @@ int batch_prepare(mlods_batch_s* b, const int64_t* offsets, const float* d_q, fl
     std::vector<BatchGroup> groups;
     std::vector<int64_t> rank_slot(static_cast<size_t>(n) + 1);
     std::vector<int32_t> rank_cloud(static_cast<size_t>(n));
-    plan_batch_groups(clouds.data(), offsets, n, frames.data(), rank_slot.data(), rank_cloud.data(), groups);
+    plan_batch_groups(clouds.data(), offsets, n, frames.data(), rank_slot.data(), rank_cloud.data(), groups,
+                      batch_solo_min_queries(sm_count_for_current_device()));
     if (int(groups.size()) > kMaxBatchGroups) {
         set_last_error("batch: %zu kernel specialisations exceed the %d supported", groups.size(), kMaxBatchGroups);
         return MLODS_ERR_CAPACITY;

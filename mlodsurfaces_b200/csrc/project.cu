@@ -605,16 +605,34 @@ cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int s
     return launch_rule<MLODS_BLEND_CPU>(a, ktype, sm_count, s);
 }
 
+int64_t batch_solo_min_queries(int sm_count)
+{
+    return 8 * int64_t(kProjectMinBlocks) * (kProjectThreads / 32) * sm_count;
+}
+
 void plan_batch_groups(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, BatchFrame* frames,
-                       int64_t* rank_slot, int32_t* rank_cloud, std::vector<BatchGroup>& groups)
+                       int64_t* rank_slot, int32_t* rank_cloud, std::vector<BatchGroup>& groups, int64_t solo_min)
 {
     auto key = [&](int i) {
         const CloudArgs& c = clouds[i];
         return (c.rule == MLODS_BLEND_GPU ? 0 : 1) * 1024 + c.kc.type * 32 + spec_nsig(c.kc);
     };
+    auto count = [&](int i) { return q_offsets[i + 1] - q_offsets[i]; };
+    // the largest clouds (at least solo_min queries) run on their own
+    std::vector<char> solo(static_cast<size_t>(n_clouds), 0);
+    if (solo_min > 0) {
+        std::vector<int> by_size;
+        for (int i = 0; i < n_clouds; ++i)
+            if (count(i) >= solo_min) by_size.push_back(i);
+        std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) { return count(a) > count(b); });
+        for (size_t k = 0; k < by_size.size() && k < size_t(kMaxSoloClouds); ++k) solo[size_t(by_size[k])] = 1;
+    }
     std::vector<int> idx(static_cast<size_t>(n_clouds));
     for (int i = 0; i < n_clouds; ++i) idx[size_t(i)] = i;
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return key(a) < key(b); });
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+        if (key(a) != key(b)) return key(a) < key(b);
+        return solo[size_t(a)] > solo[size_t(b)];
+    });
     groups.clear();
     int64_t slot = 0;
     for (int r = 0; r < n_clouds; ++r) {
@@ -622,13 +640,22 @@ void plan_batch_groups(const CloudArgs* clouds, const int64_t* q_offsets, int n_
         frames[i].rank = uint32_t(r);
         rank_slot[r] = slot;
         rank_cloud[r] = i;
-        const int64_t n = q_offsets[i + 1] - q_offsets[i];
-        if (groups.empty() || key(idx[size_t(r - 1)]) != key(i)) {
+        const int64_t n = count(i);
+        const bool own = solo[size_t(i)] != 0;
+        if (own || groups.empty() || groups.back().solo >= 0 || key(idx[size_t(r - 1)]) != key(i)) {
             BatchGroup g;
             g.ktype = clouds[i].kc.type;
             g.nsig = spec_nsig(clouds[i].kc);
             g.rule = clouds[i].rule;
             g.slot_begin = g.slot_end = slot;
+            if (own) {
+                g.solo = i;
+                g.solo_args = clouds[i];
+                const int64_t o = q_offsets[i];
+                g.solo_args.q_in = clouds[i].q_in - 3 * o;
+                g.solo_args.out_p = clouds[i].out_p - 3 * o;
+                g.solo_args.out_n = clouds[i].out_n - 3 * o;
+            }
             groups.push_back(g);
         }
         slot += n;
@@ -647,6 +674,17 @@ cudaError_t launch_mlod_batch(const BatchArgs& b, const std::vector<BatchGroup>&
     for (size_t k = 0; k < groups.size(); ++k) {
         const BatchGroup& g = groups[k];
         unsigned int* counter = b.counters + k;
+        if (g.solo >= 0) {
+            ProjectArgs a;
+            a.cloud = g.solo_args;
+            a.order = b.order + g.slot_begin;
+            a.nq = g.slot_end - g.slot_begin;
+            a.counter = counter;
+            a.stats = b.stats;
+            const cudaError_t e = launch_mlod_project(a, g.ktype, g.rule, sm_count, s);
+            if (e != cudaSuccess) return e;
+            continue;
+        }
         const cudaError_t e = g.rule == MLODS_BLEND_GPU
                                   ? launch_batch_rule<MLODS_BLEND_GPU>(b, g, counter, sm_count, grid_scale_pct, s)
                                   : launch_batch_rule<MLODS_BLEND_CPU>(b, g, counter, sm_count, grid_scale_pct, s);

@@ -68,12 +68,19 @@ struct BatchArgs {
     int64_t* stats;            // [0] visits, [1] max stack, [2] overflows, [4] rounds, [5] iterations
 };
 
-constexpr int kMaxBatchGroups = 32;
+constexpr int kMaxBatchGroups = 256;
+constexpr int kMaxSoloClouds = 128;  // clouds launched on their own, at most
 
-// One kernel specialisation of a batch and its slot range.
+// One launch of a batch and its slot range: either a kernel specialisation
+// shared by several clouds (solo < 0), run by the batched kernel, or one
+// large cloud (solo = its index) run by the single-tree kernel with the
+// cloud's arguments in the constant bank; solo_args then addresses the whole
+// concatenated buffers, so that the global indices of `order` apply.
 struct BatchGroup {
     int ktype, nsig, rule;
     int64_t slot_begin, slot_end;
+    int solo = -1;
+    CloudArgs solo_args;
 };
 
 // Per-cloud frame used to key queries: the group-ordered rank of the cloud
@@ -88,8 +95,14 @@ struct BatchFrame {
 // number of sigmas, blend rule) are consecutive and fills frames[i].rank,
 // rank_slot (n_clouds + 1 entries) and rank_cloud (n_clouds); groups receive
 // the slot ranges.  Host only.
+// Clouds with at least solo_min queries (0: none) get their own launch,
+// up to kMaxSoloClouds of them, largest first.
 void plan_batch_groups(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, BatchFrame* frames,
-                       int64_t* rank_slot, int32_t* rank_cloud, std::vector<BatchGroup>& groups);
+                       int64_t* rank_slot, int32_t* rank_cloud, std::vector<BatchGroup>& groups,
+                       int64_t solo_min);
+// Query count from which a cloud of a batch runs in a launch of its own:
+// eight queries per resident warp of the single-tree kernel.
+int64_t batch_solo_min_queries(int sm_count);
 
 cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int sm_count, cudaStream_t s);
 cudaError_t launch_mlod_batch(const BatchArgs& b, const std::vector<BatchGroup>& groups, int sm_count,

@@ -169,7 +169,12 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Request*>& batch)
     w.h_offsets[batch.size()] = total;
     const size_t nc = batch.size();
     std::vector<BatchGroup> groups;
-    plan_batch_groups(w.h_clouds, w.h_offsets, int(nc), w.h_frames, w.h_rank_slot, w.h_rank_cloud, groups);
+    plan_batch_groups(w.h_clouds, w.h_offsets, int(nc), w.h_frames, w.h_rank_slot, w.h_rank_cloud, groups,
+                      batch_solo_min_queries(sm_count_for_current_device()));
+    if (int(groups.size()) > kMaxBatchGroups) {
+        set_last_error("server: %zu launches exceed the %d supported", groups.size(), kMaxBatchGroups);
+        return MLODS_ERR_CAPACITY;
+    }
     MLODS_CUDA(cudaMemcpyAsync(dq, hq, size_t(total) * 12, cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_clouds, w.h_clouds, nc * sizeof(CloudArgs), cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_offsets, w.h_offsets, (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, w.s));
