@@ -287,7 +287,9 @@ int mlods_last_iterations(mlods_tree t, int64_t* iterations);
 /* ---- batched projection over many resident trees (extension) ---------------
  * No counterpart in the reference, which projects one tree per launch
  * (Fastapss::project, Fastapss.cu:439-455).  A batch holds a fixed list of
- * trees; mlods_batch_project projects, in ONE persistent kernel launch, the
+ * trees; mlods_batch_project projects, in a few persistent kernel launches on
+ * one stream (one per kernel specialisation shared by the smaller trees, one
+ * per tree with at least 8 queries per resident warp), the
  * device query buffer d_q (float xyz, concatenated per tree: tree i owns
  * queries [offsets[i], offsets[i+1]), offsets is a HOST array of n_trees + 1
  * entries starting at 0) onto their trees, writing d_out_pts/d_out_nrm in the

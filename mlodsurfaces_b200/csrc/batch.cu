@@ -1,10 +1,12 @@
-// batch.cu -- many resident trees projected in one persistent launch.
+// batch.cu -- many resident trees projected by a few persistent launches.
 //
 // No counterpart in the reference (one tree, one launch per call).  The batch
 // keeps per-tree launch arguments on the device, orders all queries by
-// (tree, Morton code) with one radix sort, and runs mlod_batch_kernel, whose
-// warps pull queries from a shared counter across trees so that trees of very
-// different sizes load-balance inside one launch.  With use_graph the
+// (tree, Morton code) with one radix sort, and runs, per kernel
+// specialisation, mlod_batch_kernel over the smaller trees, whose warps pull
+// queries from a shared counter across trees so that trees of very different
+// sizes load-balance inside one launch; each large tree runs the single-tree
+// kernel over its own slot range.  With use_graph the
 // memset/order/kernel sequence is captured once in a CUDA graph and replayed
 // while the buffers and sizes stay the same.  A small autotuner picks the
 // query order (Morton or input order) and the grid size by timing.
