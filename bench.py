@@ -52,7 +52,7 @@ def parse_args():
                     help="precision: 2M-point RBF surface, MLoD projection (default); knn: the same data, kNN=32 "
                          "APSS; global: 200k points of it, global APSS; torus: 100k-point torus, "
                          "CPU-path semantics; dc: 5M-point torus knot, adaptive depth-9 dual contouring; "
-                         "batch: 64 resident clouds (about 40M points) in one launch")
+                         "batch: 64 resident clouds (about 40M points) in one graph launch")
     ap.add_argument("--clouds", type=int, default=64)
     ap.add_argument("--rate", type=float, default=0.0, help="serve: request arrivals per second (0 = 70%% of "
                                                                "the measured capacity)")
@@ -784,7 +784,7 @@ def run_batch(args):
     peak, peak_kind = measured_peak_hbm()
     st = b.last_stats()
     return {
-        "metric": "queries projected/s, 64 resident clouds in one launch",
+        "metric": "queries projected/s, 64 resident clouds in one graph launch",
         "value": value,
         "unit": "queries/s",
         "n_gpus": 1,
@@ -796,7 +796,7 @@ def run_batch(args):
         "vs_baseline": None,
         "dtype": "f32 (f64 sphere solve)",
         "data": "synthetic: seeded tori and RBF-blob surfaces, sizes log-uniform in [1e4, 4e6], random scales",
-        "config": {"workload": f"batched: {args.clouds} clouds, {n_points} points, one launch per step",
+        "config": {"workload": f"batched: {args.clouds} clouds, {n_points} points, one graph launch per step",
                    "n_points": n_points, "n_queries": total, "iterations": iters, "cutoff": 2.0,
                    "kernels": "Gaussian / multi-Gaussian / rational drawn per cloud", "tree_depths": "7..10",
                    "launch": f"CUDA graph, query order {'Morton' if st['reorder'] else 'input'}, grid "
