@@ -193,7 +193,7 @@ class ClockSampler:
 # (2M points, 2M queries, 10 iterations), from a single-pass ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum: see
 # profiles/mlod_project_kernel_precision_2M_launches.md.
-PROFILED_TRAFFIC = {("precision", 2_000_000, 10): 465.77e6 + 130.46e6}
+PROFILED_TRAFFIC = {("precision", 2_000_000, 10): 515.25e6 + 168.89e6}
 
 
 def max_over_ranks(values, world: int, device):
