@@ -664,55 +664,83 @@ def run_dc(args):
     return res
 
 
-def batch_clouds(n_clouds: int, seed: int = 5):
-    """64 clouds, sizes log-uniform in [1e4, 4e6], each a torus or an RBF-blob
-    surface with its own scale and offset, a weight kernel drawn uniformly
-    and a tree depth in 7..10; queries = points + N(0, 0.01 diag)."""
+def batch_cloud_specs(n_clouds: int, seed: int = 5):
+    """Parameters of the batched workload's clouds: sizes log-uniform in
+    [1e4, 4e6], each a torus or an RBF-blob surface with its own scale and
+    offset, a weight kernel type drawn uniformly and a tree depth in 7..10."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_clouds):
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(4e6))))
+        r = float(rng.uniform(0.2, 0.45)) if i % 2 == 0 else None
+        scale = float(np.exp(rng.uniform(np.log(0.01), np.log(100.0))))
+        offset = rng.uniform(-10 * scale, 10 * scale, 3)
+        kind = int(rng.integers(0, 3))
+        depth = int(rng.integers(7, 11))
+        specs.append({"i": i, "n": n, "r": r, "scale": scale, "offset": offset, "kind": kind, "depth": depth})
+    return specs
+
+
+def make_batch_cloud(spec):
+    """One cloud of the batched workload: (points, normals, queries = points +
+    N(0, 0.01 diag), diag, kernel, tree depth)."""
     import torch
 
     from mlodsurfaces_b200 import Kernel, synth
 
-    rng = np.random.default_rng(seed)
-    dev = "cuda" if torch.cuda.is_available() else None
-    out = []
-    for i in range(n_clouds):
-        n = int(np.exp(rng.uniform(np.log(1e4), np.log(4e6))))
-        if i % 2 == 0:
-            pts, nrm = synth.torus(n, r=float(rng.uniform(0.2, 0.45)), seed=100 + i)
-        else:
-            pts, nrm = synth.rbf_blobs(n, seed=100 + i, translate=0.0, device=dev)
-        scale = float(np.exp(rng.uniform(np.log(0.01), np.log(100.0))))
-        pts = (pts.astype(np.float64) * scale + rng.uniform(-10 * scale, 10 * scale, 3)).astype(np.float32)
-        pts = synth.make_tie_free(pts)
-        diag = synth.bbox_diag(pts)
-        q = synth.perturbed_queries(pts, 0.01, seed=200 + i)
-        k = Kernel()
-        kind = int(rng.integers(0, 3))
-        if kind == 0:
-            k.type = Kernel.GAUSSIAN
-            k.sigma = 0.02 * diag
-        elif kind == 1:
-            k.type = Kernel.GAUSSIAN_MULTIPLE
-            k.sigmas = [0.01 * diag * 2.0**j for j in range(4)]
-        else:
-            k.type = Kernel.SINGULAR
-            k.exponent = 4.0
-            k.constant_shift = 1e-3
-        out.append((pts, nrm, q, diag, k, int(rng.integers(7, 11))))
-    return out
+    i, n = spec["i"], spec["n"]
+    if i % 2 == 0:
+        pts, nrm = synth.torus(n, r=spec["r"], seed=100 + i)
+    else:
+        pts, nrm = synth.rbf_blobs(n, seed=100 + i, translate=0.0,
+                                   device="cuda" if torch.cuda.is_available() else None)
+    pts = (pts.astype(np.float64) * spec["scale"] + spec["offset"]).astype(np.float32)
+    pts = synth.make_tie_free(pts)
+    diag = synth.bbox_diag(pts)
+    q = synth.perturbed_queries(pts, 0.01, seed=200 + i)
+    k = Kernel()
+    if spec["kind"] == 0:
+        k.type = Kernel.GAUSSIAN
+        k.sigma = 0.02 * diag
+    elif spec["kind"] == 1:
+        k.type = Kernel.GAUSSIAN_MULTIPLE
+        k.sigmas = [0.01 * diag * 2.0**j for j in range(4)]
+    else:
+        k.type = Kernel.SINGULAR
+        k.exponent = 4.0
+        k.constant_shift = 1e-3
+    return pts, nrm, q, diag, k, spec["depth"]
 
 
-def run_batch(args):
+def batch_placement(specs, world: int, iters: int) -> list[int]:
+    """Rank of every cloud of the batched workload: whole clouds per GPU,
+    balanced by queries x iterations within 150 GB per GPU."""
+    from mlodsurfaces_b200 import shard
+
+    work = [s["n"] * iters for s in specs]
+    nbytes = [shard.cloud_bytes(s["n"], s["n"]) for s in specs]
+    return shard.assign_clouds(work, nbytes, world, capacity=150 * 10**9)
+
+
+def run_batch(args, rank: int = 0, world: int = 1):
     """Batched workload: every cloud's tree resident, all queries projected
-    in one persistent launch (graph-captured, launch shape tuned), against
-    the same work as one launch per cloud."""
+    by one graph launch per step (launch shape tuned), against the same work
+    as one launch per cloud.  Under torchrun each rank holds whole clouds
+    (placed by work within its memory) and the step time is the slowest
+    rank's; the work is fixed as the ranks grow (strong scaling)."""
     import torch
 
     from mlodsurfaces_b200 import APSSOctree, Fastapss, FastapssBatch
     from mlodsurfaces_b200 import _capi as capi
 
     lib = capi.load()
-    clouds = batch_clouds(args.clouds)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    specs = batch_cloud_specs(args.clouds)
+    place = batch_placement(specs, world, args.iters) if world > 1 else [0] * len(specs)
+    mine = [s for s, r in zip(specs, place) if r == rank]
+    all_queries = int(sum(s["n"] for s in specs))
+    all_points = all_queries
+    clouds = [make_batch_cloud(s) for s in mine]
     projectors, qs = [], []
     for pts, nrm, q, diag, k, depth in clouds:
         t = APSSOctree()
@@ -721,6 +749,8 @@ def run_batch(args):
         f.setScalingProtectionSphere(2.0)
         projectors.append(f)
         qs.append(q)
+    if not clouds:
+        raise RuntimeError(f"rank {rank} holds no cloud: use fewer GPUs than the {len(specs)} clouds")
     counts = [len(q) for q in qs]
     total = int(sum(counts))
     n_points = int(sum(len(c[0]) for c in clouds))
@@ -734,7 +764,9 @@ def run_batch(args):
     for _ in range(max(args.warmup, 0)):
         b.project_device(counts, d_q, d_p, d_n, iters, use_graph=True)
     torch.cuda.synchronize()
-    clocks = ClockSampler(0)
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     launches0 = lib.mlods_kernel_launches()
     step_ms, kern_ms, visits = [], [], []
@@ -752,6 +784,8 @@ def run_batch(args):
         kern_ms.append(st["kernel_ms"])
         visits.append(st["node_visits"])
     launches = lib.mlods_kernel_launches() - launches0
+    if world > 1:
+        torch.distributed.barrier()
     clk = clocks.stop()
     # the same work as one launch per cloud (the reference's one-object-per-call
     # form), warmed up and timed like the batch, and its outputs compared
@@ -776,9 +810,13 @@ def run_batch(args):
         e1.record(stream)
         e1.synchronize()
         per_cloud.append(e0.elapsed_time(e1))
-    per_cloud_ms = statistics.mean(per_cloud)
-    ms = statistics.mean(step_ms)
-    value = total / (ms / 1e3)
+    # the job lasts as long as its slowest rank; every rank's outputs must match
+    step_max, per_cloud_max, differ = max_over_ranks([sum(step_ms), sum(per_cloud), 0.0 if same else 1.0],
+                                                     world, dev)
+    same = differ == 0.0
+    per_cloud_ms = per_cloud_max / len(per_cloud)
+    ms = step_max / len(step_ms)
+    value = all_queries / (ms / 1e3)
     kms = statistics.mean(kern_ms)
     achieved = (total * 36 + 64 * statistics.mean(visits)) / (kms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
@@ -787,17 +825,19 @@ def run_batch(args):
         "metric": "queries projected/s, 64 resident clouds in one graph launch",
         "value": value,
         "unit": "queries/s",
-        "n_gpus": 1,
+        "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": ms,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32 (f64 sphere solve)",
         "data": "synthetic: seeded tori and RBF-blob surfaces, sizes log-uniform in [1e4, 4e6], random scales",
-        "config": {"workload": f"batched: {args.clouds} clouds, {n_points} points, one graph launch per step",
-                   "n_points": n_points, "n_queries": total, "iterations": iters, "cutoff": 2.0,
+        "config": {"workload": f"batched: {args.clouds} clouds, {all_points} points, one graph launch per step",
+                   "n_points": all_points, "n_queries": all_queries, "iterations": iters, "cutoff": 2.0,
+                   "parallelism": (f"whole clouds per GPU, {world} GPUs (rank 0: {len(clouds)} clouds, "
+                                   f"{n_points} points)") if world > 1 else "1 GPU",
                    "kernels": "Gaussian / multi-Gaussian / rational drawn per cloud", "tree_depths": "7..10",
                    "launch": f"CUDA graph, query order {'Morton' if st['reorder'] else 'input'}, grid "
                              f"{st['grid_pct']}% of the persistent size",
@@ -806,7 +846,8 @@ def run_batch(args):
         "outputs_equal_one_launch_per_cloud": same,
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "note": f"batch kernel; 36 B per query + 64 B per node visit; peak {peak_kind}"},
+                     "traffic": None, "note": f"rank 0's batch launches; 36 B per query + 64 B per node visit; "
+                                              f"peak {peak_kind}"},
         "clocks": clk,
     }
 
@@ -1034,8 +1075,23 @@ def main():
             print(json.dumps(run_dc(args)), flush=True)
         return
     if args.workload == "batch":
-        if rank == 0:
-            print(json.dumps(run_batch(args)), flush=True)
+        if world > 1:
+            import datetime
+
+            import torch
+
+            torch.cuda.set_device(local_rank)
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                                 device_id=torch.device("cuda", local_rank))
+        try:
+            res = run_batch(args, rank, world)
+            if rank == 0:
+                print(json.dumps(res), flush=True)
+        finally:
+            if world > 1:
+                import torch
+
+                torch.distributed.destroy_process_group()
         return
     if args.workload == "serve":
         if rank == 0:
