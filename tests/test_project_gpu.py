@@ -197,3 +197,36 @@ def test_protocol_errors(torus20k):
     with pytest.raises(MlodsError):
         f.project(11, None, None, 1)  # more than uploaded
     f.project(10, None, None, 1)
+
+
+TINY = {
+    "one point": [[0.1, 0.2, 0.3]],
+    "two points": [[0, 0, 0], [1, 0.5, 0.25]],
+    "three points": [[0, 0, 0], [1, 0, 0], [0, 1, 0]],
+    "coincident points": [[0.3, 0.3, 0.3]] * 3,
+}
+
+
+@pytest.mark.parametrize("name", list(TINY))
+@pytest.mark.parametrize("rule", [BLEND_GPU, BLEND_CPU])
+def test_tiny_clouds(name, rule):
+    """Clouds of one to three points: a degenerate fit fails in band (the
+    query stays, normal zero) exactly where the oracle's does, otherwise the
+    projection matches it.  Coincident points build a multi-point leaf (the
+    reference draws a random side for them, CPUUtils.cpp:299-308)."""
+    pts = np.array(TINY[name], np.float32)
+    nrm = np.tile(np.array([[0, 0, 1]], np.float32), (len(pts), 1))
+    q = np.array([[0.2, 0.1, 0.5], [0.5, 0.5, -0.3], [0.1, 0.2, 0.3]], np.float32)
+    from mlodsurfaces_b200 import Kernel
+
+    k = Kernel()
+    k.type = Kernel.GAUSSIAN
+    k.sigma = 0.5
+    op, on, _, _ = run_gpu(pts, nrm, q, k, iters=3, cutoff=2.0, rule=rule)
+    x64, n64 = oracle.OracleTree(pts, nrm, 12).project_mlod(q, 3, k, rule=rule, cutoff=2.0)
+    failed64 = np.all(n64 == 0, axis=1)
+    failed = np.all(on == 0, axis=1)
+    assert np.array_equal(failed, failed64)
+    assert np.array_equal(op[failed], q[failed])
+    scale = max(float(np.ptp(pts, axis=0).max()), 1.0)
+    assert np.abs(op[~failed] - x64[~failed]).max(initial=0.0) < TOL_DIAG * scale
