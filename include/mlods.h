@@ -198,6 +198,12 @@ int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_i
 typedef struct mlods_dcgrid_s* mlods_dcgrid;
 int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, const float* box_min,
                              const float* box_max, mlods_dcgrid* out);
+/* The same grid with its set work on the device (keys, radix sort, unique,
+ * the grade and regularize steps level by level); pts may be in host or
+ * device memory.  Falls back to the host code for max_depth > 15 or points
+ * whose cells lie beyond 2^19 cells from the box.  Synchronous on `stream`. */
+int mlods_dcgrid_from_points_device(const float* pts, int64_t n, int32_t max_depth, const float* box_min,
+                                    const float* box_max, void* stream, mlods_dcgrid* out);
 int mlods_dcgrid_info(mlods_dcgrid g, int64_t* n_cells, int32_t* max_depth);
 int mlods_dcgrid_cells(mlods_dcgrid g, int32_t* cells);  /* 4 int32 per cell */
 int mlods_dcgrid_free(mlods_dcgrid g);

@@ -246,6 +246,15 @@ class APSSOctree:
         return out
 
 
+def _cuda_available() -> bool:
+    try:
+        import torch
+
+        return bool(torch.cuda.is_available())
+    except Exception:
+        return False
+
+
 class DCGrid:
     """Dual-contouring cell grid.  ``cells`` is an int32 (n, 4) array of
     (depth, x, y, z) in sorted_octree order, ``max_depth`` the deepest level
@@ -254,21 +263,36 @@ class DCGrid:
 
     ``DCGrid(points, max_depth)`` is the grid on the input points
     (OctreeGenerator::generateFromPoints + uniformizeFromPoints,
-    upsample.cpp:128-144, :253-260; the ``-b`` mode);
+    upsample.cpp:128-144, :253-260; the ``-b`` mode), its set work on the
+    GPU when one is present (``device=None``), else on the host; points may
+    be a CUDA tensor;
     ``DCGrid.adaptive(apss, max_depth)`` the projection-driven grid of the
     default mode (OctreeGenerator::generate + uniformize, upsample.cpp:228-273).
     """
 
     def __init__(self, points=None, max_depth: int = 0, box_min=(-1.0, -1.0, -1.0), box_max=(1.0, 1.0, 1.0),
-                 _handle=None):
+                 _handle=None, device: bool | None = None, stream=None):
         self._lib = capi.load()
         if _handle is None:
-            pts = _f32x3(points, "points")
+            on_gpu = getattr(points, "is_cuda", False)
+            if device is None:
+                device = on_gpu or _cuda_available()
+            if on_gpu:
+                pts = points.detach().to(dtype=__import__("torch").float32).reshape(-1, 3).contiguous()
+                if not device:
+                    pts = pts.cpu().numpy()
+            else:
+                pts = _f32x3(points, "points")
             bmin = np.asarray(box_min, np.float32)
             bmax = np.asarray(box_max, np.float32)
             g = C.c_void_p(0)
-            capi.check(self._lib.mlods_dcgrid_from_points(capi.ptr(pts), len(pts), int(max_depth), capi.ptr(bmin),
-                                                          capi.ptr(bmax), C.byref(g)))
+            if device:
+                capi.check(self._lib.mlods_dcgrid_from_points_device(capi.ptr(pts), len(pts), int(max_depth),
+                                                                     capi.ptr(bmin), capi.ptr(bmax),
+                                                                     C.c_void_p(stream or 0), C.byref(g)))
+            else:
+                capi.check(self._lib.mlods_dcgrid_from_points(capi.ptr(pts), len(pts), int(max_depth),
+                                                              capi.ptr(bmin), capi.ptr(bmax), C.byref(g)))
         else:
             g = _handle
         self._g = g

@@ -673,8 +673,8 @@ int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_i
     return MLODS_OK;
 }
 
-int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, const float* box_min,
-                             const float* box_max, mlods_dcgrid* out)
+static int dcgrid_points(const float* pts, int64_t n, int32_t max_depth, const float* box_min, const float* box_max,
+                         bool device, cudaStream_t s, mlods_dcgrid* out)
 {
     if (!out || !box_min || !box_max) {
         set_last_error("dcgrid: null argument");
@@ -686,7 +686,19 @@ int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, con
         set_last_error("dcgrid: host allocation failed");
         return MLODS_ERR_CAPACITY;
     }
-    const int rc = dcgrid_from_points(pts, n, max_depth, box_min, box_max, g->cells, g->max_depth);
+    bool handled = false;
+    int rc = MLODS_OK;
+    if (device) rc = dcgrid_from_points_device(pts, n, max_depth, box_min, box_max, s, g->cells, g->max_depth, &handled);
+    if (rc == MLODS_OK && !handled) {
+        if (device && pts && n > 0) {  // the host version reads host memory
+            std::vector<float> h(size_t(n) * 3);
+            cudaError_t e = cudaMemcpy(h.data(), pts, h.size() * sizeof(float), cudaMemcpyDefault);
+            rc = e == cudaSuccess ? dcgrid_from_points(h.data(), n, max_depth, box_min, box_max, g->cells, g->max_depth)
+                                  : cuda_fail(e, "dcgrid: points download", __FILE__, __LINE__);
+        } else {
+            rc = dcgrid_from_points(pts, n, max_depth, box_min, box_max, g->cells, g->max_depth);
+        }
+    }
     if (rc != MLODS_OK) {
         delete g;
         return rc;
@@ -699,6 +711,18 @@ int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, con
     }
     *out = g;
     return MLODS_OK;
+}
+
+int mlods_dcgrid_from_points(const float* pts, int64_t n, int32_t max_depth, const float* box_min,
+                             const float* box_max, mlods_dcgrid* out)
+{
+    return dcgrid_points(pts, n, max_depth, box_min, box_max, false, nullptr, out);
+}
+
+int mlods_dcgrid_from_points_device(const float* pts, int64_t n, int32_t max_depth, const float* box_min,
+                                    const float* box_max, void* stream, mlods_dcgrid* out)
+{
+    return dcgrid_points(pts, n, max_depth, box_min, box_max, true, static_cast<cudaStream_t>(stream), out);
 }
 
 int mlods_dcgrid_adaptive(mlods_tree t, int32_t max_depth, int32_t cut, void* stream, mlods_dcgrid* out)

@@ -64,6 +64,12 @@ void cells_to_ints(const std::vector<Cell>& nodes, std::vector<int32_t>& out, in
 int dcgrid_from_points(const float* pts, int64_t n, int max_depth, const float box_min[3], const float box_max[3],
                        std::vector<int32_t>& cells_out, int& depth_out);
 
+// dcgrid_from_points with the set work on the device; *handled is false when
+// the inputs need the host version (depth or coordinates beyond the keys).
+int dcgrid_from_points_device(const float* pts, int64_t n, int max_depth, const float box_min[3],
+                              const float box_max[3], cudaStream_t s, std::vector<int32_t>& cells_out, int& depth_out,
+                              bool* handled);
+
 // The projection-driven grid (OctreeGenerator::generate + uniformize,
 // upsample.cpp:228-251, :262-273): cells, their depth and the 3x4 map from the
 // grid's unit frame to the tree's frame (new2bbox, scene.cpp:1311).

@@ -346,6 +346,31 @@ __global__ void siblings_kernel(const uint64_t* __restrict__ k, int64_t n, uint6
 
 // First position of each depth in a sorted key set (the depth is the top 4
 // bits of the key): one binary search per depth, thread d, d in [0, 16].
+// aabb_octree::enclosing at `depth` of every point (octree.h:957-965):
+// P = (p - min) / diag / w, floored, in float as the host does; a point whose
+// cell has no key sets *bad.
+__global__ void enclosing_points_kernel(const float* __restrict__ p, int64_t n, int depth, float3 bmin, float3 diag,
+                                        float w, uint64_t* __restrict__ out, int* __restrict__ bad)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float lo[3] = {bmin.x, bmin.y, bmin.z}, dg[3] = {diag.x, diag.y, diag.z};
+    int c[3];
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+        const float t = __fdiv_rn(__fdiv_rn(__fsub_rn(p[3 * i + a], lo[a]), dg[a]), w);
+        const float f = floorf(t);
+        if (!(f >= -float(kBias) && f < float(kBias))) {  // NaN too
+            ok = false;
+            c[a] = 0;
+        } else {
+            c[a] = int(f);
+        }
+    }
+    if (!ok) atomicOr(bad, 1);
+    out[i] = make_key(depth, c[0], c[1], c[2]);
+}
+
 __global__ void depth_bounds_kernel(const uint64_t* __restrict__ k, int64_t n, long long* __restrict__ begin)
 {
     const int d = threadIdx.x;
@@ -608,6 +633,8 @@ int generate(Gen& G, int max_depth, CellSet& total)
     return sort_unique(total, s);
 }
 
+int grade_up_siblings(Gen& G, CellSet& nodes, int cut_depth, CellSet& scratch);
+
 // uniformize (upsample.cpp:262-273) on the device
 int uniformize(Gen& G, CellSet& nodes, int max_depth, bool cut, float nd[3], float no[3])
 {
@@ -656,8 +683,16 @@ int uniformize(Gen& G, CellSet& nodes, int max_depth, bool cut, float nd[3], flo
             nd[k] = float(1 << dd);
         }
     }
+    return grade_up_siblings(G, nodes, cut ? max_depth : -1, scratch);
+}
+
+// grade, regularize_up, the optional cut and regularize_siblings
+// (upsample.cpp:40-93, :253-273) on a sorted unique set
+int grade_up_siblings(Gen& G, CellSet& nodes, int cut_depth, CellSet& scratch)
+{
+    cudaStream_t s = G.s;
     int64_t begin[17];
-    rc = G.depth_ranges(nodes, begin);
+    int rc = G.depth_ranges(nodes, begin);
     if (rc != MLODS_OK) return rc;
     int deepest = 0;
     for (int d = 0; d < 16; ++d)
@@ -678,10 +713,10 @@ int uniformize(Gen& G, CellSet& nodes, int max_depth, bool cut, float nd[3], flo
         });
         if (rc != MLODS_OK) return rc;
     }
-    if (cut) {
+    if (cut_depth >= 0) {
         rc = G.depth_ranges(nodes, begin);
         if (rc != MLODS_OK) return rc;
-        nodes.n = begin[std::min(max_depth, 15) + 1];  // sorted by depth: keep the prefix
+        nodes.n = begin[std::min(cut_depth, 15) + 1];  // sorted by depth: keep the prefix
     }
     // regularize_siblings
     rc = reserve(scratch, nodes.n * 8, false, s);
@@ -697,6 +732,50 @@ int uniformize(Gen& G, CellSet& nodes, int max_depth, bool cut, float nd[3], flo
 }
 
 }  // namespace
+
+int dcgrid_from_points_device(const float* pts, int64_t n, int max_depth, const float box_min[3],
+                              const float box_max[3], cudaStream_t s, std::vector<int32_t>& cells_out, int& depth_out,
+                              bool* handled)
+{
+    *handled = false;
+    if (n <= 0 || !pts || max_depth < 0 || max_depth > kMaxKeyDepth) return MLODS_OK;  // the host path decides
+    float3 lo = make_float3(box_min[0], box_min[1], box_min[2]);
+    float3 dg = make_float3(box_max[0] - box_min[0], box_max[1] - box_min[1], box_max[2] - box_min[2]);
+    if (!(dg.x > 0.f && dg.y > 0.f && dg.z > 0.f)) return MLODS_OK;
+    Gen G{nullptr, s};
+    CellSet nodes, scratch;
+    int rc = reserve(nodes, n, false, s);
+    if (rc != MLODS_OK) return rc;
+    float* d_pts = nullptr;
+    MLODS_CUDA(scratch_alloc(reinterpret_cast<void**>(&d_pts), size_t(n) * 12 + 256, s));
+    int* d_bad = reinterpret_cast<int*>(reinterpret_cast<char*>(d_pts) + ((size_t(n) * 12 + 15) / 16) * 16);
+    cudaError_t e = cudaMemcpyAsync(d_pts, pts, size_t(n) * 12, cudaMemcpyDefault, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), s);
+    if (e == cudaSuccess) {
+        const float w = 1.0f / float(1 << max_depth);
+        enclosing_points_kernel<<<blocks_for(n), kThreads, 0, s>>>(d_pts, n, max_depth, lo, dg, w, nodes.a, d_bad);
+        note_launch();
+        e = cudaGetLastError();
+    }
+    int bad = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    scratch_free(d_pts, s);
+    if (e != cudaSuccess) return cuda_fail(e, "dc grid from points", __FILE__, __LINE__);
+    if (bad) return MLODS_OK;  // points off the key range: the host path
+    nodes.n = n;
+    rc = sort_unique(nodes, s);  // remove_duplicates
+    if (rc == MLODS_OK) rc = grade_up_siblings(G, nodes, -1, scratch);  // uniformizeFromPoints
+    if (rc != MLODS_OK) return rc;
+    std::vector<uint64_t> keys;
+    rc = download(nodes, keys, s);
+    if (rc != MLODS_OK) return rc;
+    std::vector<Cell> cells(keys.size());
+    for (size_t i = 0; i < keys.size(); ++i) cells[i] = key_cell(keys[i]);
+    dcg::cells_to_ints(cells, cells_out, depth_out);
+    *handled = true;
+    return MLODS_OK;
+}
 
 int dcgrid_adaptive(mlods_tree_s* T, int max_depth, bool cut, cudaStream_t s, std::vector<int32_t>& cells_out,
                     int& depth_out, float xform[12], int64_t* n_projected)
