@@ -348,12 +348,17 @@ int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float* d_q, floa
  * (optionally with their own weight kernel) and returns a ticket at once;
  * worker threads, one per CUDA stream, take everything queued whenever they
  * are free (up to max_batch_queries / max_batch_requests, optionally waiting
- * max_wait_us for more) and project it with one launch of the multi-tree
- * kernel; results are written to out_pts / out_nrm (either may be NULL),
+ * max_wait_us for more) and project it with the batched launches (grouped
+ * small requests, large requests on their own); results are written to
+ * out_pts / out_nrm (either may be NULL),
  * identical to mlods_project_host on the same tree and kernel.  The query and
  * output arrays must stay valid until the ticket is waited for.
  * Admission: a submit that would leave more than max_pending_queries queued
- * returns MLODS_ERR_CAPACITY.  mlods_server_wait blocks at most timeout_ms
+ * returns MLODS_ERR_CAPACITY.  The bounds are the server's memory footprint:
+ * a batch in flight holds 36 bytes of device buffers and 36 bytes of pinned
+ * staging per query (plus its sort scratch), so device memory stays within
+ * n_streams x max_batch_queries x 36 bytes beside the resident trees, and
+ * queued work within max_pending_queries.  mlods_server_wait blocks at most timeout_ms
  * (MLODS_ERR_TIMEOUT after that; wait again later), returns the request's
  * status and its latency from submit to results on the host, and retires the
  * ticket.  mlods_server_free cancels queued requests, lets running batches
