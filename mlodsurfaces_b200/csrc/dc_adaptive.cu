@@ -75,6 +75,17 @@ inline unsigned blocks_for(int64_t n) { return unsigned((n + kThreads - 1) / kTh
 
 // A set of cells on the device: sorted unique keys plus scratch of the same
 // capacity, grown on demand.
+// Device buffers of the generator come from the library's stream-ordered
+// pool: every step runs on one stream, so a buffer freed there is reused by
+// later steps without a cudaMalloc or a synchronising cudaFree.
+template <typename T>
+cudaError_t pool_alloc(T** p, size_t bytes, cudaStream_t s)
+{
+    return scratch_alloc(reinterpret_cast<void**>(p), bytes, s);
+}
+
+// A set of cells on the device: sorted unique keys plus scratch of the same
+// capacity, grown on demand, on one stream.
 struct CellSet {
     uint64_t* a = nullptr;  // the keys
     uint64_t* b = nullptr;  // scratch keys
@@ -84,41 +95,46 @@ struct CellSet {
     void* tmp = nullptr;
     size_t cap = 0, tmp_cap = 0;
     int64_t n = 0;
+    cudaStream_t s = nullptr;
+    CellSet() = default;
+    CellSet(const CellSet&) = delete;
+    CellSet& operator=(const CellSet&) = delete;
     ~CellSet()
     {
-        cudaFree(a);
-        cudaFree(b);
-        cudaFree(flags);
-        cudaFree(excl);
-        cudaFree(d_total);
-        cudaFree(tmp);
+        scratch_free(a, s);
+        scratch_free(b, s);
+        scratch_free(flags, s);
+        scratch_free(excl, s);
+        scratch_free(d_total, s);
+        scratch_free(tmp, s);
     }
 };
 
 int reserve(CellSet& c, int64_t need, bool keep, cudaStream_t s)
 {
+    c.s = s;
     if (size_t(need) <= c.cap) return MLODS_OK;
     const size_t cap = std::max<size_t>(size_t(need), c.cap + c.cap / 2);
     uint64_t *a = nullptr, *b = nullptr;
     uint32_t *f = nullptr, *e = nullptr;
-    MLODS_CUDA(cudaMalloc(&a, cap * 8));
-    cudaError_t err = cudaMalloc(&b, cap * 8);
-    if (err == cudaSuccess) err = cudaMalloc(&f, cap * 4);
-    if (err == cudaSuccess) err = cudaMalloc(&e, cap * 4);
-    if (err == cudaSuccess && !c.d_total) err = cudaMalloc(&c.d_total, 256);
+    MLODS_CUDA(pool_alloc(&a, cap * 8, s));
+    cudaError_t err = pool_alloc(&b, cap * 8, s);
+    if (err == cudaSuccess) err = pool_alloc(&f, cap * 4, s);
+    if (err == cudaSuccess) err = pool_alloc(&e, cap * 4, s);
+    if (err == cudaSuccess && !c.d_total) err = pool_alloc(&c.d_total, 256, s);
     if (err == cudaSuccess && keep && c.n > 0) err = cudaMemcpyAsync(a, c.a, size_t(c.n) * 8, cudaMemcpyDeviceToDevice, s);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) {
-        cudaFree(a);
-        cudaFree(b);
-        cudaFree(f);
-        cudaFree(e);
+        scratch_free(a, s);
+        scratch_free(b, s);
+        scratch_free(f, s);
+        scratch_free(e, s);
         return cuda_fail(err, "dc cells: grow", __FILE__, __LINE__);
     }
-    cudaFree(c.a);
-    cudaFree(c.b);
-    cudaFree(c.flags);
-    cudaFree(c.excl);
+    // stream-ordered: the old buffers go after the copy above
+    scratch_free(c.a, s);
+    scratch_free(c.b, s);
+    scratch_free(c.flags, s);
+    scratch_free(c.excl, s);
     c.a = a;
     c.b = b;
     c.flags = f;
@@ -126,10 +142,10 @@ int reserve(CellSet& c, int64_t need, bool keep, cudaStream_t s)
     c.cap = cap;
     const size_t tb = std::max(radix_temp_bytes(int64_t(cap)), scan_temp_bytes(int64_t(cap)));
     if (tb > c.tmp_cap) {
-        cudaFree(c.tmp);
+        scratch_free(c.tmp, s);
         c.tmp = nullptr;
         c.tmp_cap = 0;
-        MLODS_CUDA(cudaMalloc(&c.tmp, tb));
+        MLODS_CUDA(pool_alloc(&c.tmp, tb, s));
         c.tmp_cap = tb;
     }
     return MLODS_OK;
@@ -407,11 +423,11 @@ struct Gen {
     long long* d_begin = nullptr;
     ~Gen()
     {
-        cudaFree(d_proj);
-        cudaFree(d_off);
-        cudaFree(d_scan);
-        cudaFree(d_mm);
-        cudaFree(d_begin);
+        scratch_free(d_proj, s);
+        scratch_free(d_off, s);
+        scratch_free(d_scan, s);
+        scratch_free(d_mm, s);
+        scratch_free(d_begin, s);
     }
 
     // first key of each depth of a sorted set (17 entries)
@@ -421,7 +437,7 @@ struct Gen {
             for (int d = 0; d < 17; ++d) begin[d] = 0;
             return MLODS_OK;
         }
-        if (!d_begin) MLODS_CUDA(cudaMalloc(&d_begin, 17 * sizeof(long long)));
+        if (!d_begin) MLODS_CUDA(pool_alloc(&d_begin, 17 * sizeof(long long), s));
         depth_bounds_kernel<<<1, 32, 0, s>>>(c.a, c.n, d_begin);
         note_launch();
         MLODS_CUDA(cudaGetLastError());
@@ -440,10 +456,10 @@ struct Gen {
         if (cur.n == 0) return MLODS_OK;
         const int64_t n = cur.n;
         if (proj_cap < size_t(n)) {
-            cudaFree(d_proj);
+            scratch_free(d_proj, s);
             d_proj = nullptr;
             proj_cap = 0;
-            MLODS_CUDA(cudaMalloc(&d_proj, size_t(n) * 36));
+            MLODS_CUDA(pool_alloc(&d_proj, size_t(n) * 36, s));
             proj_cap = size_t(n);
         }
         float* c = d_proj;
@@ -471,17 +487,17 @@ struct Gen {
         const int64_t n = sub.n;
         if (n == 0) return MLODS_OK;
         if (off_cap < size_t(n) + 1) {
-            cudaFree(d_off);
+            scratch_free(d_off, s);
             d_off = nullptr;
             off_cap = 0;
-            MLODS_CUDA(cudaMalloc(&d_off, (size_t(n) + 1) * 4));
+            MLODS_CUDA(pool_alloc(&d_off, (size_t(n) + 1) * 4, s));
             off_cap = size_t(n) + 1;
         }
         if (scan_cap < scan_temp_bytes(n)) {
-            cudaFree(d_scan);
+            scratch_free(d_scan, s);
             d_scan = nullptr;
             scan_cap = 0;
-            MLODS_CUDA(cudaMalloc(&d_scan, scan_temp_bytes(n)));
+            MLODS_CUDA(pool_alloc(&d_scan, scan_temp_bytes(n), s));
             scan_cap = scan_temp_bytes(n);
         }
         if (n > (int64_t(1) << 25)) {  // 64 keys each must stay within 32-bit offsets
@@ -508,7 +524,7 @@ struct Gen {
 
     int root_box(const CellSet& c, bool only_depth0, int mn[3], int mx[3], bool* any)
     {
-        if (!d_mm) MLODS_CUDA(cudaMalloc(&d_mm, 8 * sizeof(int)));
+        if (!d_mm) MLODS_CUDA(pool_alloc(&d_mm, 8 * sizeof(int), s));
         const int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
         MLODS_CUDA(cudaMemcpyAsync(d_mm, init, sizeof init, cudaMemcpyHostToDevice, s));
         if (c.n) {
