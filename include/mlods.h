@@ -452,6 +452,13 @@ int mlods_params_file_save(const char* path, const mlods_scene_params* p);
 /* Number of kernels this library has launched in this process (diagnostics). */
 int64_t mlods_kernel_launches(void);
 
+/* Per-call scratch (DC corner fields, grid generation, split global APSS)
+ * comes from a stream-ordered memory pool owned by the library, one per
+ * device, which keeps up to 8 GiB of freed scratch for the next calls.
+ * mlods_release_scratch returns the current device's unused pooled memory to
+ * the system (extension; synchronises the device first). */
+int mlods_release_scratch(void);
+
 #ifdef __cplusplus
 }
 #endif

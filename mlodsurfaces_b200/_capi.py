@@ -156,6 +156,7 @@ SIGNATURES = {
     "mlods_last_stats": (C.c_int, [_P, _I64, _I64, _I32, _I64, C.POINTER(C.c_float)]),
     "mlods_last_iterations": (C.c_int, [_P, _I64]),
     "mlods_kernel_launches": (C.c_int64, []),
+    "mlods_release_scratch": (C.c_int, []),
     "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),
     "mlods_dcgrid_from_points": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, C.POINTER(_P)]),
     "mlods_dcgrid_from_points_device": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, _P, C.POINTER(_P)]),

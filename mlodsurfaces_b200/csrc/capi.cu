@@ -36,17 +36,30 @@ int sm_count_for_current_device()
 // Stream-ordered scratch from a memory pool owned by the library (one per
 // device), which keeps up to 8 GiB of freed scratch for reuse, so per-call
 // buffers of a few GB cost neither a cudaMalloc nor a synchronising cudaFree.
+namespace
+{
+cudaMemPool_t g_pools[64] = {};
+std::mutex g_pools_mu;
+}  // namespace
+
+// The pool of device `dev`, or nullptr if none was made yet.
+cudaMemPool_t scratch_pool(int dev)
+{
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_pools_mu);
+    return g_pools[dev];
+}
+
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s)
 {
-    static cudaMemPool_t pools[64] = {};
-    static std::mutex mu;
+    cudaMemPool_t* pools = g_pools;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 64) return cudaMallocAsync(p, bytes, s);
     cudaMemPool_t pool;
     {
-        std::lock_guard<std::mutex> lock(mu);
+        std::lock_guard<std::mutex> lock(g_pools_mu);
         if (!pools[dev]) {
             cudaMemPoolProps props = {};
             props.allocType = cudaMemAllocationTypePinned;
@@ -68,6 +81,19 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s)
 }
 
 cudaError_t scratch_free(void* p, cudaStream_t s) { return p ? cudaFreeAsync(p, s) : cudaSuccess; }
+
+// Unused memory of the current device's pool back to the system.
+cudaError_t scratch_release()
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool = scratch_pool(dev);
+    if (!pool) return cudaSuccess;
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return e;
+    return cudaMemPoolTrimTo(pool, 0);
+}
 
 namespace
 {
@@ -845,5 +871,11 @@ int mlods_last_iterations(mlods_tree t, int64_t* iterations)
 }
 
 int64_t mlods_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int mlods_release_scratch(void)
+{
+    MLODS_CUDA(scratch_release());
+    return MLODS_OK;
+}
 
 }  // extern "C"

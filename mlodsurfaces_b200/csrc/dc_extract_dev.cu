@@ -337,20 +337,30 @@ __global__ void child_count_check_kernel(const int32_t* __restrict__ kids, int64
     if (cnt != 0 && cnt != 8) atomicExch(bad, 2);
 }
 
+// The stream of the extraction running on this host thread: its buffers come
+// from the library's stream-ordered pool on that stream.
+thread_local cudaStream_t tl_stream = nullptr;
+
+struct StreamScope {
+    explicit StreamScope(cudaStream_t s) { tl_stream = s; }
+    ~StreamScope() { tl_stream = nullptr; }
+};
+
 struct Buf {
     void* p = nullptr;
     size_t cap = 0;
+    cudaStream_t s = tl_stream;
     Buf() = default;
     Buf(const Buf&) = delete;
     Buf& operator=(const Buf&) = delete;
-    ~Buf() { cudaFree(p); }
+    ~Buf() { scratch_free(p, s); }
     int need(size_t bytes)
     {
         if (bytes <= cap) return MLODS_OK;
-        cudaFree(p);
+        scratch_free(p, s);  // stream-ordered: after the work queued on it
         p = nullptr;
         cap = 0;
-        MLODS_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+        MLODS_CUDA(scratch_alloc(&p, std::max<size_t>(bytes, 256), s));
         cap = std::max<size_t>(bytes, 256);
         return MLODS_OK;
     }
@@ -377,6 +387,7 @@ int scan_total(uint32_t* d, int64_t n, Buf& tmp, Buf& total, uint32_t* out_total
 int dc_extract_device(const int4* d_cells, int64_t n_cells, const int64_t* h_depth_begin, int max_depth,
                       const float* d_cf, const float* d_cell_vertex, DeviceMesh& out, bool* used_device, cudaStream_t s)
 {
+    const StreamScope scope(s);
     *used_device = false;
     if (max_depth > 12 || n_cells >= (int64_t(1) << 31)) return MLODS_OK;  // the host version takes it
     Buf kids, bad, begin, tmp, total;

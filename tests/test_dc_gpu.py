@@ -120,6 +120,10 @@ def test_device_buffers_give_the_host_results(dc_setup):
     bad[3, 1] = 1 << 30
     with pytest.raises(MlodsError):
         f.dc_evaluate_device(bad, g.max_depth)
-    # and the host path still works after a refusal
+    # and the host path still works after a refusal, and after the pooled
+    # scratch went back to the system
+    from mlodsurfaces_b200 import _capi as capi
+
+    capi.check(capi.load().mlods_release_scratch())
     again = f.dc_evaluate(g.cells, g.max_depth)
     assert np.array_equal(again[0], want[0], equal_nan=True)
