@@ -856,6 +856,19 @@ def run_batch(args, rank: int = 0, world: int = 1):
     }
 
 
+def latency_by_size(lat, sizes):
+    """p50 / p99 request latency per request-size class (queries)."""
+    lat = np.asarray(lat, float)
+    sizes = np.asarray(sizes)
+    out = {}
+    for name, lo, hi in (("1e3-1e4", 0, 10_000), ("1e4-1e5", 10_000, 100_000), ("1e5-1e6", 100_000, 1 << 62)):
+        sel = (sizes >= lo) & (sizes < hi)
+        if sel.any():
+            out[name] = {"requests": int(sel.sum()), "p50": float(np.percentile(lat[sel], 50)),
+                         "p99": float(np.percentile(lat[sel], 99))}
+    return out
+
+
 def run_serve(args):
     """Serving workload: 8 resident clouds of 0.5-8M points, Poisson request
     arrivals, request sizes log-uniform in [1e3, 1e6] queries, each request
@@ -917,7 +930,7 @@ def run_serve(args):
     iters = args.iters
     # capacity: a closed loop of back-to-back requests
     r0 = np.random.default_rng(5)
-    warm = [request(r0) for _ in range(24)]
+    warm = [request(r0) for _ in range(64)]
     t0 = time.perf_counter()
     tickets = [srv.submit(ci, q, iters, k) for ci, q, k in warm]
     warm_out = [srv.wait(t, timeout_ms=600000)[:2] for t in tickets]
@@ -931,7 +944,7 @@ def run_serve(args):
     while t_next < args.serve_seconds:
         reqs.append((t_next, request(r1)))
         t_next += float(r1.exponential(1.0 / rate))
-    lat, done_q = [], [0]
+    lat, sizes, done_q = [], [], [0]
     lock = threading.Lock()
     pending = []
 
@@ -951,6 +964,7 @@ def run_serve(args):
             t, n = item
             _, _, ms = srv.wait(t, timeout_ms=600000)
             lat.append(ms)
+            sizes.append(n)
             done_q[0] += n
             i += 1
 
@@ -1005,6 +1019,7 @@ def run_serve(args):
                    "max_batch_queries": args.serve_batch,
                    "offered_rate_rps": rate, "closed_loop_capacity_rps": capacity_rps,
                    "seconds": args.serve_seconds},
+        "latency_ms_by_request_size": latency_by_size(lat, sizes),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(np.max(lat)), "per": "request, submit to results in host memory"},
         "e2e": {"value": total_q / elapsed, "unit": "queries/s", "h2d_bytes_per_step": int(12 * total_q / len(reqs)),

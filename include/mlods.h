@@ -346,9 +346,11 @@ int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float* d_q, floa
  * settings must not change while it runs) and answers requests from any
  * host thread: mlods_server_submit queues n host query points for one tree
  * (optionally with their own weight kernel) and returns a ticket at once;
- * worker threads, one per CUDA stream, take everything queued whenever they
+ * worker threads, one per CUDA stream, take what is queued whenever they
  * are free (up to max_batch_queries / max_batch_requests, optionally waiting
- * max_wait_us for more) and project it with the batched launches (grouped
+ * max_wait_us for more; in arrival order, passing over a request that only a
+ * later batch can hold, and cutting one larger than a batch into pieces) and
+ * project it with the batched launches (grouped
  * small requests, large requests on their own); results are written to
  * out_pts / out_nrm (either may be NULL),
  * identical to mlods_project_host on the same tree and kernel.  The query and
@@ -366,7 +368,7 @@ int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float* d_q, floa
 typedef struct mlods_server_config {
     int32_t n_streams;            /* worker threads / CUDA streams (default 2) */
     int32_t max_batch_requests;   /* requests per launch (default 4096) */
-    int64_t max_batch_queries;    /* queries per launch (default 2^21; a larger request runs alone) */
+    int64_t max_batch_queries;    /* queries per batch (default 2^21; a larger request runs in pieces of this size) */
     int64_t max_pending_queries;  /* admission bound on queued queries (default 2^26) */
     int32_t max_wait_us;          /* batching window when less than a batch is queued (default 0) */
     int32_t reserved;

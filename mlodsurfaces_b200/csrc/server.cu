@@ -4,11 +4,11 @@
 // the legacy stream.  Requests (a tree, n host query points, an iteration
 // count, optionally their own weight kernel) are queued by any host thread
 // and answered asynchronously.  Worker threads, one per CUDA stream, take
-// everything queued (up to a batch size) whenever they are free, stage it in
-// pinned memory, and project the whole batch with one persistent launch of
-// the multi-tree kernel (each request is one "cloud" of the launch, with its
-// own tree, kernel and iteration count), so copies of one batch overlap the
-// projection of another.  Admission is bounded: a submit that would queue
+// what is queued (up to a batch size; large requests in pieces, small ones
+// passing over those that do not fit) whenever they are free, stage it in
+// pinned memory, and project the batch with the batched launches (each
+// request or piece is one "cloud", with its own tree, kernel and iteration
+// count), so copies of one batch overlap the projection of another.  Admission is bounded: a submit that would queue
 // more than max_pending queries is refused (MLODS_ERR_CAPACITY) instead of
 // growing host or device memory without limit.  Every wait has a timeout.
 #include <algorithm>
@@ -43,6 +43,16 @@ struct Request {
     Clock::time_point t_submit, t_done;
     int status = -1;  // -1 pending, else an MLODS_* code
     char error[256] = "";
+    int64_t taken = 0;     // queries handed to batches
+    int64_t finished = 0;  // queries whose batch has returned
+    int piece_status = 0;  // first failing piece's status (MLODS_OK = 0 so far)
+};
+
+// A contiguous range of one request's queries: requests larger than a batch
+// run as several pieces, possibly in different batches on different streams.
+struct Piece {
+    Request* r;
+    int64_t off, n;
 };
 
 struct Worker {
@@ -140,10 +150,10 @@ int ensure_capacity(Worker& w, int64_t total, size_t n_req)
 
 // Projects one batch of requests on the worker's stream; host outputs are
 // written before it returns.
-int run_batch(mlods_server_s* S, Worker& w, const std::vector<Request*>& batch)
+int run_batch(mlods_server_s* S, Worker& w, const std::vector<Piece>& batch)
 {
     int64_t total = 0;
-    for (const Request* r : batch) total += r->n;
+    for (const Piece& pc : batch) total += pc.n;
     int rc = ensure_capacity(w, total, batch.size());
     if (rc != MLODS_OK) return rc;
     float* hq = w.h_stage;
@@ -154,9 +164,9 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Request*>& batch)
     float* dn = w.d_buf + 6 * total;
     int64_t off = 0;
     for (size_t i = 0; i < batch.size(); ++i) {
-        const Request* r = batch[i];
+        const Request* r = batch[i].r;
         mlods_tree_s* T = S->trees[size_t(r->tree)];
-        std::memcpy(hq + 3 * off, r->q, size_t(r->n) * 12);
+        std::memcpy(hq + 3 * off, r->q + 3 * batch[i].off, size_t(batch[i].n) * 12);
         CloudArgs& c = w.h_clouds[i];
         fill_cloud_args(T, c, dq + 3 * off, dp + 3 * off, dn + 3 * off, r->iters, -1.f, T->params.blend_rule);
         if (r->own_kernel) c.kc = r->kc;
@@ -164,7 +174,7 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Request*>& batch)
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
         w.h_frames[i] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f, 0u};
         w.h_offsets[i] = off;
-        off += r->n;
+        off += batch[i].n;
     }
     w.h_offsets[batch.size()] = total;
     const size_t nc = batch.size();
@@ -201,18 +211,49 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Request*>& batch)
     MLODS_CUDA(cudaMemcpyAsync(hn, dn, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s));
     MLODS_CUDA(cudaStreamSynchronize(w.s));
     off = 0;
-    for (Request* r : batch) {
-        if (r->out_p) std::memcpy(r->out_p, hp + 3 * off, size_t(r->n) * 12);
-        if (r->out_n) std::memcpy(r->out_n, hn + 3 * off, size_t(r->n) * 12);
-        off += r->n;
+    for (const Piece& pc : batch) {
+        if (pc.r->out_p) std::memcpy(pc.r->out_p + 3 * pc.off, hp + 3 * off, size_t(pc.n) * 12);
+        if (pc.r->out_n) std::memcpy(pc.r->out_n + 3 * pc.off, hn + 3 * off, size_t(pc.n) * 12);
+        off += pc.n;
     }
     return MLODS_OK;
+}
+
+// The next batch, under the server lock: queued requests in arrival order,
+// each taken whole while it fits the batch; one larger than a whole batch is
+// cut into batch-sized pieces (it keeps its place until its last piece is
+// handed out); a request that fits only a later batch is passed over, so
+// small requests do not wait behind large ones.  A request that was passed
+// over heads the queue, so the next batch starts with it.
+void form_batch(mlods_server_s* S, std::vector<Piece>& batch)
+{
+    const int64_t cap = std::max<int64_t>(S->cfg.max_batch_queries, 1);
+    int64_t budget = cap;
+    for (auto it = S->queue.begin(); it != S->queue.end() && budget > 0;) {
+        if (int64_t(batch.size()) >= S->cfg.max_batch_requests) break;
+        Request* r = *it;
+        const int64_t rest = r->n - r->taken;
+        if (rest <= budget) {
+            batch.push_back(Piece{r, r->taken, rest});
+            r->taken += rest;
+            budget -= rest;
+            S->queued -= rest;
+            it = S->queue.erase(it);
+        } else if (budget == cap) {
+            batch.push_back(Piece{r, r->taken, cap});
+            r->taken += cap;
+            budget = 0;
+            S->queued -= cap;
+        } else {
+            ++it;
+        }
+    }
 }
 
 void worker_main(mlods_server_s* S, Worker* w)
 {
     cudaSetDevice(S->device);
-    std::vector<Request*> batch;
+    std::vector<Piece> batch;
     for (;;) {
         batch.clear();
         {
@@ -223,16 +264,7 @@ void worker_main(mlods_server_s* S, Worker* w)
                 S->cv_work.wait_for(lock, std::chrono::microseconds(S->cfg.max_wait_us),
                                     [&] { return S->stopping || S->queued >= S->cfg.max_batch_queries; });
             if (S->stopping) return;
-            int64_t sum = 0;
-            while (!S->queue.empty()) {
-                Request* r = S->queue.front();
-                if (!batch.empty() && sum + r->n > S->cfg.max_batch_queries) break;
-                if (!batch.empty() && int64_t(batch.size()) >= S->cfg.max_batch_requests) break;
-                batch.push_back(r);
-                sum += r->n;
-                S->queue.pop_front();
-            }
-            S->queued -= sum;
+            form_batch(S, batch);
         }
         if (batch.empty()) continue;
         const auto t0 = Clock::now();
@@ -240,12 +272,19 @@ void worker_main(mlods_server_s* S, Worker* w)
         const auto t1 = Clock::now();
         const char* msg = mlods_last_error();
         std::lock_guard<std::mutex> lock(S->mu);
-        for (Request* r : batch) {
-            r->status = rc;
-            r->t_done = t1;
-            if (rc != MLODS_OK) std::snprintf(r->error, sizeof r->error, "%s", msg);
-            ++S->completed;
-            S->queries += r->n;
+        for (const Piece& pc : batch) {
+            Request* r = pc.r;
+            if (rc != MLODS_OK && r->piece_status == MLODS_OK) {
+                r->piece_status = rc;
+                std::snprintf(r->error, sizeof r->error, "%s", msg);
+            }
+            r->finished += pc.n;
+            S->queries += pc.n;
+            if (r->finished == r->n) {  // the request's last piece
+                r->status = r->piece_status;
+                r->t_done = t1;
+                ++S->completed;
+            }
         }
         ++S->batches;
         S->busy_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();

@@ -90,6 +90,28 @@ def test_mixed_requests_equal_projection_alone(projectors):
         srv.close()
 
 
+def test_large_requests_run_in_pieces(projectors):
+    """With a batch of 4000 queries, requests of up to 20000 run as pieces
+    in several batches on both streams while small ones pass them; every
+    result is still the request projected alone."""
+    reqs = make_requests(projectors, 30, seed=13)
+    assert max(len(q) for _, q, _, _ in reqs) > 4000
+    want = expected(projectors, reqs)
+    restore_kernels(projectors)
+    srv = ProjectionServer([f for f, _, _ in projectors], n_streams=2, max_batch_queries=4000)
+    try:
+        tickets = [srv.submit(ti, q, iters, kernel) for ti, q, iters, kernel in reqs]
+        for t, (wp, wn) in zip(tickets, want):
+            p, n, lat = srv.wait(t, timeout_ms=60000)
+            assert np.array_equal(p, wp) and np.array_equal(n, wn)
+        st = srv.stats()
+        assert st["completed"] == len(reqs) and st["queued"] == 0
+        assert st["queries"] == sum(len(q) for _, q, _, _ in reqs)
+        assert st["batches"] > sum(len(q) for _, q, _, _ in reqs) // 4000
+    finally:
+        srv.close()
+
+
 def test_concurrent_submitters(projectors):
     reqs = make_requests(projectors, 24, seed=9)
     want = expected(projectors, reqs)
