@@ -172,11 +172,14 @@ static int ensure_scratch(mlods_tree_s* T, size_t bytes)
 {
     const size_t need = al256(8 * sizeof(int64_t)) + bytes;
     if (T->d_scratch && T->scratch_bytes >= need) return MLODS_OK;
+    // grow by half at least: callers with rising sizes (the grid generator's
+    // levels, a refined mesh) reallocate a few times instead of every call
+    const size_t grown = std::max(need, T->scratch_bytes + T->scratch_bytes / 2);
     if (T->d_scratch) cudaFree(T->d_scratch);
     T->d_scratch = nullptr;
     T->scratch_bytes = 0;
-    MLODS_CUDA(cudaMalloc(&T->d_scratch, need));
-    T->scratch_bytes = need;
+    MLODS_CUDA(cudaMalloc(&T->d_scratch, grown));
+    T->scratch_bytes = grown;
     T->d_stats = static_cast<int64_t*>(T->d_scratch);
     return MLODS_OK;
 }
