@@ -242,6 +242,11 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
         bool failed = false, empty = false, overflow = false;
         float best_d = INFINITY;
         uint32_t best_o = 0xFFFFFFFFu, best_p = 0xFFFFFFFFu;
+        // kNN projection: the previous iteration's k-th distance, grown by the
+        // step, bounds this iteration's (triangle inequality, with a margin for
+        // the float distances), so the walk needs no starting window after the
+        // first iteration
+        float prev_kth = INFINITY, pwx = 0.f, pwy = 0.f, pwz = 0.f;
         for (int it = 0; it < n_iter && !failed; ++it) {
             // the reference keeps the iterate as a float glm::vec3
             const float wx = it == 0 ? q0[0] : float(xd[0] + a.o0);
@@ -256,7 +261,13 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
             float bound;             // squared search radius
             best_d = INFINITY;
             best_o = best_p = 0xFFFFFFFFu;
-            if (MODE != 1) {
+            if (MODE == 0 && it > 0 && prev_kth < INFINITY) {
+                const double ddx = double(wx) - double(pwx), ddy = double(wy) - double(pwy),
+                             ddz = double(wz) - double(pwz);
+                const double step = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+                const double r = (sqrt(double(prev_kth)) + step) * (1.0 + 1e-5) + 1e-30;
+                bound = __double2float_ru(r * r);
+            } else if (MODE != 1) {
                 const uint64_t qc = lattice_code(a, wx, wy, wz);
                 const int64_t pos = warp_upper_bound(a.codes, a.n_pts, qc);
                 w0 = pos - 16 < 0 ? 0 : pos - 16;
@@ -383,7 +394,7 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
                 if (MODE != 1) {
                     if (__any_sync(kFull, cd <= bound && cd < INFINITY)) {
                         warp_merge(best_d, best_o, best_p, cd, co, cp);
-                        bound = __shfl_sync(kFull, best_d, k - 1);
+                        bound = fminf(bound, __shfl_sync(kFull, best_d, k - 1));
                     }
                 }
                 const uint32_t pm = __ballot_sync(kFull, push);
@@ -406,6 +417,10 @@ __global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
             }
             if (MODE == 2) break;
             if (MODE == 0) {
+                prev_kth = __shfl_sync(kFull, best_d, k - 1);
+                pwx = wx;
+                pwy = wy;
+                pwz = wz;
                 if (lane < k && best_p != 0xFFFFFFFFu) {
                     const float4 pl = __ldg(a.spts + best_p);
                     const float4 nn = __ldg(a.snrm + best_p);

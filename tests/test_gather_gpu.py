@@ -190,3 +190,28 @@ def test_global_apss_split_and_fused_forms():
     sel = np.random.default_rng(3).choice(len(q), 64, replace=False)
     o64b, _ = ot.project_global(q[sel], 2, k)
     assert rel_err(full[sel], o64b, diag).max() < TOL_DIAG
+
+
+def test_knn_iterations_in_one_call_equal_one_call_per_iteration():
+    """Inside one call the kNN search of iteration i > 0 starts from the
+    bound that iteration i - 1 leaves (its k-th distance grown by the step);
+    one call per iteration starts every search afresh.  The neighbour sets,
+    and so the projections, are the same bit for bit."""
+    pts, nrm = synth.rbf_blobs(300_000, seed=7)
+    pts = synth.make_tie_free(pts)
+    q = synth.perturbed_queries(pts, 0.01, seed=8)[:20000]
+    k = make_kernel("multi", synth.bbox_diag(pts))
+    t = tree_of(pts, nrm)
+    t.knnMode(True, 32)
+    f = Fastapss(t, k, len(q))
+    f.copyPointsToGPU(len(q), q)
+    one = np.empty((len(q), 3), np.float32)
+    one_n = np.empty((len(q), 3), np.float32)
+    f.project(len(q), one, one_n, 4, k)
+    f.copyPointsToGPU(len(q), q)
+    for _ in range(4):
+        f.project(len(q), None, None, 1, k)
+    step = np.empty((len(q), 3), np.float32)
+    step_n = np.empty((len(q), 3), np.float32)
+    f.project(len(q), step, step_n, 0, k)
+    assert np.array_equal(one, step)
