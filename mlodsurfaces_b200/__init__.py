@@ -7,6 +7,15 @@ mirror of the reference's C++ projection API (``Kernel``, ``APSSOctree``,
 ``APSS``/``Fastapss``) plus seeded synthetic inputs (``synth``).
 """
 from .apss import APSS, APSSOctree, DCGrid, Fastapss, FastapssBatch, GlobalAPSS, Kernel, Mesh, ProjectionServer, unit2bbox  # noqa: F401
-from . import io, synth  # noqa: F401
+from . import io, shard, synth  # noqa: F401
 
-__all__ = ["APSS", "APSSOctree", "DCGrid", "Fastapss", "FastapssBatch", "GlobalAPSS", "Kernel", "Mesh", "ProjectionServer", "io", "synth", "unit2bbox"]
+
+def release_scratch() -> None:
+    """Return the unused memory of the library's per-call scratch pool on the
+    current device (up to 8 GiB of freed scratch is kept for later calls)."""
+    from . import _capi as capi
+
+    capi.check(capi.load().mlods_release_scratch())
+
+__all__ = ["APSS", "APSSOctree", "DCGrid", "Fastapss", "FastapssBatch", "GlobalAPSS", "Kernel", "Mesh", "ProjectionServer",
+           "io", "release_scratch", "shard", "synth", "unit2bbox"]
