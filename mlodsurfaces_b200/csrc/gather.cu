@@ -26,6 +26,10 @@ namespace
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kGCount = 0x7FFFFFFFu;
 constexpr uint32_t kGPoints = 1u << 31;  // entry is a range of sorted point positions
+#ifndef MLODS_GATHER_MIN_BLOCKS
+#define MLODS_GATHER_MIN_BLOCKS 10
+#endif
+constexpr int kGatherMinBlocks = MLODS_GATHER_MIN_BLOCKS;  // resident blocks per SM the register budget aims at
 constexpr int kGatherCap = 256;          // stack entries per warp
 // A range entry holds at most 8 nodes, each pushing at most one entry, so a
 // depth-first walk below any entry adds at most 7 entries per level for the
@@ -219,7 +223,7 @@ __device__ bool fit_cpu(const float* s, double step_max, double x[3], float nrm[
 
 // MODE: 0 = kNN APSS projection, 1 = ball APSS projection, 2 = kNN sets only.
 template <int KTYPE, int MODE>
-__global__ void __launch_bounds__(kGatherThreads) gather_kernel(GatherArgs a)
+__global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kernel(GatherArgs a)
 {
     __shared__ GStack stacks[kGatherThreads / 32];
     const int lane = threadIdx.x & 31;
