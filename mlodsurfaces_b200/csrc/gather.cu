@@ -497,7 +497,15 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kerne
 
 // ---------------------------------------------------------------- global APSS
 
+#ifndef MLODS_GLOBAL_MIN_BLOCKS
+#define MLODS_GLOBAL_MIN_BLOCKS 0
+#endif
 constexpr int kGlobalThreads = 128;
+#if MLODS_GLOBAL_MIN_BLOCKS > 0
+#define MLODS_GLOBAL_BOUNDS __launch_bounds__(kGlobalThreads, MLODS_GLOBAL_MIN_BLOCKS)
+#else
+#define MLODS_GLOBAL_BOUNDS __launch_bounds__(kGlobalThreads)
+#endif
 constexpr int kGlobalTile = 256;  // points per shared-memory tile
 constexpr int kGlobalQpt = 2;     // queries per thread: each point read from shared memory serves two
 
@@ -601,7 +609,7 @@ __device__ __forceinline__ bool global_step(const GlobalArgs& a, const double (&
 // All iterations of kGlobalQpt queries per thread in one launch, every point
 // per iteration: the form for query counts that fill the GPU.
 template <int KTYPE, int NSIG>
-__global__ void __launch_bounds__(kGlobalThreads) global_apss_kernel(GlobalArgs a)
+__global__ void MLODS_GLOBAL_BOUNDS global_apss_kernel(GlobalArgs a)
 {
     constexpr int Q = kGlobalQpt;
     __shared__ float4 s_p[kGlobalTile];
@@ -680,7 +688,7 @@ __global__ void global_split_init_kernel(GlobalArgs a, GlobalSplit g)
 }
 
 template <int KTYPE, int NSIG>
-__global__ void __launch_bounds__(kGlobalThreads) global_split_sums_kernel(GlobalArgs a, GlobalSplit g)
+__global__ void MLODS_GLOBAL_BOUNDS global_split_sums_kernel(GlobalArgs a, GlobalSplit g)
 {
     constexpr int Q = kGlobalQpt;
     __shared__ float4 s_p[kGlobalTile];
