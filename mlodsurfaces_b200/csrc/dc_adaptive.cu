@@ -208,6 +208,28 @@ int upload(CellSet& c, const std::vector<uint64_t>& keys, cudaStream_t s)
     return MLODS_OK;
 }
 
+__global__ void key_cells_kernel(const uint64_t* __restrict__ k, int64_t n, int4* __restrict__ out);
+
+// The sorted set as the caller's int32 (depth, x, y, z) rows and its
+// deepest level (the depth of the last key).
+int cells_to_host(CellSet& c, std::vector<int32_t>& cells_out, int& depth_out, cudaStream_t s)
+{
+    cells_out.resize(size_t(c.n) * 4);
+    depth_out = 0;
+    if (c.n == 0) return MLODS_OK;
+    int4* d = nullptr;
+    MLODS_CUDA(scratch_alloc(reinterpret_cast<void**>(&d), size_t(c.n) * 16, s));
+    key_cells_kernel<<<blocks_for(c.n), kThreads, 0, s>>>(c.a, c.n, d);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cells_out.data(), d, size_t(c.n) * 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    scratch_free(d, s);
+    if (e != cudaSuccess) return cuda_fail(e, "dc cells: download", __FILE__, __LINE__);
+    depth_out = cells_out[cells_out.size() - 4];
+    return MLODS_OK;
+}
+
 int download(const CellSet& c, std::vector<uint64_t>& keys, cudaStream_t s)
 {
     keys.resize(size_t(c.n));
@@ -344,21 +366,26 @@ __global__ void parent_kernel(const uint64_t* __restrict__ k, int64_t n, uint64_
     if (i < n) out[i] = key_parent(k[i]);
 }
 
-// regularize_siblings: the 8 children of every non-root cell's parent; a
-// depth-0 cell contributes the root (the default octree_id), upsample.cpp:48-65
-__global__ void siblings_kernel(const uint64_t* __restrict__ k, int64_t n, uint64_t* __restrict__ out)
+
+// (depth, x, y, z) of every key, for the caller's cell array.
+__global__ void key_cells_kernel(const uint64_t* __restrict__ k, int64_t n, int4* __restrict__ out)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_int4(key_depth(k[i]), key_x(k[i]), key_y(k[i]), key_z(k[i]));
+}
+
+// The 8 children of every cell.
+__global__ void child8_kernel(const uint64_t* __restrict__ k, int64_t n, uint64_t* __restrict__ out)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint64_t key = k[i];
-    if (key_depth(key) <= 0) {
-        for (int c = 0; c < 8; ++c) out[8 * i + c] = make_key(0, 0, 0, 0);
-        return;
-    }
-    const uint64_t p = key_parent(key);
-    const int d = key_depth(key), x = 2 * key_x(p), y = 2 * key_y(p), z = 2 * key_z(p);
+    const int d = key_depth(key) + 1, x = 2 * key_x(key), y = 2 * key_y(key), z = 2 * key_z(key);
     for (int c = 0; c < 8; ++c) out[8 * i + c] = make_key(d, x + (c & 1), y + ((c >> 1) & 1), z + ((c >> 2) & 1));
 }
+
+// The root cell (the default octree_id).
+__global__ void root_key_kernel(uint64_t* __restrict__ out) { *out = make_key(0, 0, 0, 0); }
 
 // First position of each depth in a sorted key set (the depth is the top 4
 // bits of the key): one binary search per depth, thread d, d in [0, 16].
@@ -704,47 +731,93 @@ int uniformize(Gen& G, CellSet& nodes, int max_depth, bool cut, float nd[3], flo
 
 // grade, regularize_up, the optional cut and regularize_siblings
 // (upsample.cpp:40-93, :253-273) on a sorted unique set
+// Adds m keys made by `launch` (which writes them at the given address) to
+// set c and makes it sorted and unique again.
+template <typename Launch>
+int add_sorted(CellSet& c, int64_t m, cudaStream_t s, Launch launch)
+{
+    if (m <= 0) return MLODS_OK;
+    int rc = reserve(c, c.n + m, true, s);
+    if (rc != MLODS_OK) return rc;
+    launch(c.a + c.n);
+    note_launch();
+    MLODS_CUDA(cudaGetLastError());
+    c.n += m;
+    return sort_unique(c, s);
+}
+
+// grade, regularize_up, the optional cut and regularize_siblings on one set
+// per depth: every step makes keys of a single depth (grade and the
+// ancestors one level up, the siblings at their own level), so only that
+// level is sorted again, and the levels concatenated in depth order are the
+// sorted set (the depth is the key's top bits).
 int grade_up_siblings(Gen& G, CellSet& nodes, int cut_depth, CellSet& scratch)
 {
     cudaStream_t s = G.s;
     int64_t begin[17];
     int rc = G.depth_ranges(nodes, begin);
     if (rc != MLODS_OK) return rc;
+    CellSet L[16];
     int deepest = 0;
-    for (int d = 0; d < 16; ++d)
-        if (begin[d + 1] > begin[d]) deepest = d;
-    // grade, deepest level first (the order of the reference's loop)
+    for (int d = 0; d < 16; ++d) {
+        const int64_t n = begin[d + 1] - begin[d];
+        L[d].s = s;
+        if (n == 0) continue;
+        deepest = d;
+        rc = reserve(L[d], n, false, s);
+        if (rc != MLODS_OK) return rc;
+        MLODS_CUDA(cudaMemcpyAsync(L[d].a, nodes.a + begin[d], size_t(n) * 8, cudaMemcpyDeviceToDevice, s));
+        L[d].n = n;
+    }
+    // grade, deepest level first (the order of the reference's loop): the
+    // parents of a cell's 8 corner neighbours join the level above
     for (int d = deepest; d >= 1; --d) {
-        rc = G.grow_level(nodes, d, 8, scratch, [&](const uint64_t* k, int64_t n, uint64_t* out) {
+        const uint64_t* k = L[d].a;
+        const int64_t n = L[d].n;
+        rc = add_sorted(L[d - 1], 8 * n, s, [&](uint64_t* out) {
             grade_kernel<<<blocks_for(n), kThreads, 0, s>>>(k, n, out);
-            note_launch();
         });
         if (rc != MLODS_OK) return rc;
     }
     // regularize_up: every ancestor
     for (int d = deepest; d >= 1; --d) {
-        rc = G.grow_level(nodes, d, 1, scratch, [&](const uint64_t* k, int64_t n, uint64_t* out) {
+        const uint64_t* k = L[d].a;
+        const int64_t n = L[d].n;
+        rc = add_sorted(L[d - 1], n, s, [&](uint64_t* out) {
             parent_kernel<<<blocks_for(n), kThreads, 0, s>>>(k, n, out);
-            note_launch();
         });
         if (rc != MLODS_OK) return rc;
     }
-    if (cut_depth >= 0) {
-        rc = G.depth_ranges(nodes, begin);
+    const int top = cut_depth >= 0 ? std::min(deepest, std::min(cut_depth, 15)) : deepest;
+    // regularize_siblings: a level becomes the children of its cells'
+    // parents (each cell is one of them); depth-0 cells add the root
+    for (int d = 1; d <= top; ++d) {
+        if (L[d].n == 0) continue;
+        const uint64_t* k = L[d].a;
+        const int64_t n = L[d].n;
+        scratch.n = 0;
+        rc = add_sorted(scratch, n, s, [&](uint64_t* out) {
+            parent_kernel<<<blocks_for(n), kThreads, 0, s>>>(k, n, out);
+        });
         if (rc != MLODS_OK) return rc;
-        nodes.n = begin[std::min(cut_depth, 15) + 1];  // sorted by depth: keep the prefix
+        const uint64_t* pk = scratch.a;
+        const int64_t np = scratch.n;
+        L[d].n = 0;
+        rc = add_sorted(L[d], 8 * np, s, [&](uint64_t* out) {
+            child8_kernel<<<blocks_for(np), kThreads, 0, s>>>(pk, np, out);
+        });
+        if (rc != MLODS_OK) return rc;
     }
-    // regularize_siblings
-    rc = reserve(scratch, nodes.n * 8, false, s);
-    if (rc != MLODS_OK) return rc;
-    if (nodes.n) {
-        siblings_kernel<<<blocks_for(nodes.n), kThreads, 0, s>>>(nodes.a, nodes.n, scratch.a);
-        note_launch();
-        MLODS_CUDA(cudaGetLastError());
+    if (L[0].n > 0) {
+        rc = add_sorted(L[0], 1, s, [&](uint64_t* out) { root_key_kernel<<<1, 1, 0, s>>>(out); });
+        if (rc != MLODS_OK) return rc;
     }
-    rc = append(nodes, scratch.a, nodes.n * 8, s);
-    if (rc != MLODS_OK) return rc;
-    return sort_unique(nodes, s);
+    nodes.n = 0;
+    for (int d = 0; d <= top; ++d) {
+        rc = append(nodes, L[d].a, L[d].n, s);
+        if (rc != MLODS_OK) return rc;
+    }
+    return MLODS_OK;
 }
 
 }  // namespace
@@ -783,12 +856,8 @@ int dcgrid_from_points_device(const float* pts, int64_t n, int max_depth, const 
     rc = sort_unique(nodes, s);  // remove_duplicates
     if (rc == MLODS_OK) rc = grade_up_siblings(G, nodes, -1, scratch);  // uniformizeFromPoints
     if (rc != MLODS_OK) return rc;
-    std::vector<uint64_t> keys;
-    rc = download(nodes, keys, s);
+    rc = cells_to_host(nodes, cells_out, depth_out, s);
     if (rc != MLODS_OK) return rc;
-    std::vector<Cell> cells(keys.size());
-    for (size_t i = 0; i < keys.size(); ++i) cells[i] = key_cell(keys[i]);
-    dcg::cells_to_ints(cells, cells_out, depth_out);
     *handled = true;
     return MLODS_OK;
 }
@@ -817,12 +886,8 @@ int dcgrid_adaptive(mlods_tree_s* T, int max_depth, bool cut, cudaStream_t s, st
     float nd[3], no[3];
     rc = uniformize(G, nodes, max_depth, cut, nd, no);
     if (rc != MLODS_OK) return rc;
-    std::vector<uint64_t> keys;
-    rc = download(nodes, keys, s);
+    rc = cells_to_host(nodes, cells_out, depth_out, s);
     if (rc != MLODS_OK) return rc;
-    std::vector<Cell> cells(keys.size());
-    for (size_t i = 0; i < keys.size(); ++i) cells[i] = key_cell(keys[i]);
-    dcg::cells_to_ints(cells, cells_out, depth_out);
     // new2bbox = unit2bbox * sortedOctreeToUnit (scene.cpp:1259-1311), box [-1, 1]^3
     for (int r = 0; r < 3; ++r) {
         for (int c = 0; c < 4; ++c) xform[4 * r + c] = 0.f;
