@@ -630,6 +630,16 @@ class APSS:
     def CPU(self) -> APSSOctree:
         return self.m_apssOctree
 
+    def stop(self) -> None:
+        """APSS::stop (GPUUtils.cu:394-397) ends a CUDA profiler range in the
+        reference; nothing to stop here."""
+
+    def eraseAndRestart(self) -> None:
+        """APSS::eraseAndRestart (GPUUtils.cu:399-404): drops the device data
+        and starts over with an empty octree (build it again before use)."""
+        self.eraseFromGPU()
+        self.m_apssOctree = APSSOctree()
+
 
 class Fastapss(APSS):
     """MLoD projection (Fastapss.h:32-51)."""

@@ -57,3 +57,15 @@ def test_default_params_follow_the_reference():
 def test_error_raises():
     with pytest.raises(capi.MlodsError):
         capi.check(capi.load().mlods_set_params(None, None))
+
+
+def test_apss_lifecycle_methods_without_a_gpu():
+    """APSS::stop is a no-op here; eraseAndRestart leaves an empty octree
+    (GPUUtils.cu:394-404)."""
+    from mlodsurfaces_b200 import APSSOctree, Fastapss
+
+    t = APSSOctree()
+    f = Fastapss(t)
+    f.stop()
+    f.eraseAndRestart()
+    assert isinstance(f.CPU(), APSSOctree) and f.CPU() is not t
