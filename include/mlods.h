@@ -183,6 +183,9 @@ int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out
  * point count).  k <= MLODS_MAX_KNN.  Asynchronous. */
 #define MLODS_MAX_KNN 32
 int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_idx, float* d_d2, void* stream);
+/* The same with host arrays (APSSOctree::getKnn / cpuSphere, CPUUtils.cpp:638-672);
+ * synchronous. */
+int mlods_knn_host(mlods_tree t, int64_t n, const float* q, int32_t k, int32_t* idx, float* d2);
 
 /* ---- dual contouring --------------------------------------------------------
  * Cells are octree nodes (depth, x, y, z) as octree_id (octree.h:18-44) over

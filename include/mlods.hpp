@@ -151,6 +151,8 @@ public:
         m_tree = nullptr;
         check(mlods_tree_build(&i_points[0].x, &normals[0].x, int64_t(i_points.size()), int32_t(maxDepth), nullptr,
                                &m_tree));
+        m_points = i_points;  // the reference keeps the samples on the host too
+        m_normals = normals;
         mlods_tree_info inf{};
         check(mlods_tree_get_info(m_tree, &inf));
         m_bbox.bb = vec3(inf.bbox_min[0], inf.bbox_min[1], inf.bbox_min[2]);
@@ -184,10 +186,50 @@ public:
     }
     bool isAPSS() { return m_knnMode || m_ballMode; }
 
+    // CPUUtils.cpp:665-672: the k nearest samples of x (nearest first).
+    void getKnn(vec3 const& x, unsigned k, std::vector<vec3>& neighbors) const
+    {
+        std::vector<int32_t> idx(k);
+        std::vector<float> d2(k);
+        check(mlods_knn_host(m_tree, 1, &x.x, int32_t(k), idx.data(), d2.data()));
+        neighbors.clear();
+        for (int32_t i : idx)
+            if (i >= 0) neighbors.push_back(m_points[size_t(i)]);
+    }
+
+    // CPUUtils.cpp:638-663: the algebraic sphere u0 + u123.x + u4 |x|^2
+    // fitted to the m_knn nearest samples of qStart, weights kernel.w, float
+    // sums in world coordinates as the reference takes them.
+    void cpuSphere(vec3 const& qStart, float& u0, vec3& u123, float& u4, Kernel const& kernel = Kernel()) const
+    {
+        std::vector<int32_t> idx(m_knn);
+        std::vector<float> d2(m_knn);
+        check(mlods_knn_host(m_tree, 1, &qStart.x, int32_t(m_knn), idx.data(), d2.data()));
+        auto dot = [](vec3 const& a, vec3 const& b) { return a.x * b.x + a.y * b.y + a.z * b.z; };
+        float s_pn = 0.f, s_pp = 0.f, s_w = 0.f;
+        vec3 s_p(0.f, 0.f, 0.f), s_n(0.f, 0.f, 0.f);
+        for (int32_t i : idx) {
+            if (i < 0) continue;
+            const vec3& p = m_points[size_t(i)];
+            const vec3& n = m_normals[size_t(i)];
+            const float wi = kernel.w(p, qStart);
+            s_pn += wi * dot(p, n);
+            s_pp += wi * dot(p, p);
+            s_p = vec3(s_p.x + wi * p.x, s_p.y + wi * p.y, s_p.z + wi * p.z);
+            s_n = vec3(s_n.x + wi * n.x, s_n.y + wi * n.y, s_n.z + wi * n.z);
+            s_w += wi;
+        }
+        const vec3 n_w(s_n.x / s_w, s_n.y / s_w, s_n.z / s_w), p_w(s_p.x / s_w, s_p.y / s_w, s_p.z / s_w);
+        u4 = 0.5f * (s_pn - dot(s_p, n_w)) / (s_pp - dot(s_p, p_w));
+        u123 = vec3((s_n.x - 2 * u4 * s_p.x) / s_w, (s_n.y - 2 * u4 * s_p.y) / s_w, (s_n.z - 2 * u4 * s_p.z) / s_w);
+        u0 = -(dot(s_p, u123) + u4 * s_pp) / s_w;
+    }
+
     mlods_tree handle() const { return m_tree; }
 
 private:
     mlods_tree m_tree = nullptr;
+    std::vector<vec3> m_points, m_normals;
     BBOX m_bbox;
     unsigned m_numberOfNodes = 0, m_depth = 0, m_numberOfLeaves = 0;
     float m_scalingProtectionSphere = 2.f;
@@ -337,6 +379,12 @@ public:
     GlobalAPSS(APSSOctree* apssOctree, const Kernel& kernel, unsigned int nbOfVectors) : GlobalAPSS(apssOctree)
     {
         copyToGPU(kernel, nbOfVectors);
+    }
+
+    // GlobalAPSS.cu:288-291
+    void cpuSphere(vec3 const& qStart, float& u0, vec3& u123, float& u4, Kernel const& kernel = Kernel()) const
+    {
+        m_apssOctree->cpuSphere(qStart, u0, u123, u4, kernel);
     }
 
 protected:

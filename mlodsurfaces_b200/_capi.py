@@ -158,6 +158,7 @@ SIGNATURES = {
     "mlods_kernel_launches": (C.c_int64, []),
     "mlods_release_scratch": (C.c_int, []),
     "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),
+    "mlods_knn_host": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P]),
     "mlods_dcgrid_from_points": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, C.POINTER(_P)]),
     "mlods_dcgrid_from_points_device": (C.c_int, [_P, C.c_int64, C.c_int32, _P, _P, _P, C.POINTER(_P)]),
     "mlods_dcgrid_info": (C.c_int, [_P, _I64, _I32]),

@@ -126,6 +126,7 @@ class APSSOctree:
                                               C.c_void_p(stream or 0), C.byref(h)))
         self._h = h
         self._info = None
+        self._host = (pts, nrm)  # the reference keeps m_points / m_normals on the host too
 
     def build_device(self, d_points, d_normals, maxDepth: int = 12, stream=None) -> None:
         """Build from device tensors (torch CUDA float32, shape (n, 3))."""
@@ -133,6 +134,7 @@ class APSSOctree:
         h = C.c_void_p(0)
         capi.check(self._lib.mlods_tree_build_device(capi.ptr(d_points), capi.ptr(d_normals), int(d_points.shape[0]),
                                                      int(maxDepth), C.c_void_p(stream or 0), C.byref(h)))
+        self._host = None
         self._h = h
         self._info = None
 
@@ -222,6 +224,39 @@ class APSSOctree:
                                        C.c_void_p(torch.cuda.current_stream().cuda_stream)))
         torch.cuda.current_stream().synchronize()
         return idx.cpu().numpy(), d2.cpu().numpy()
+
+    def cpuSphere(self, qStart, kernel: Kernel | None = None):
+        """APSSOctree::cpuSphere (CPUUtils.cpp:638-663): the algebraic sphere
+        u0 + u123.x + u4 |x|^2 fitted to the m_knn nearest points of qStart
+        with weights kernel.w (unweighted by area), summed in float in world
+        coordinates as the reference does.  Returns (u0, u123, u4).  Needs
+        the host arrays given to build()."""
+        host = getattr(self, "_host", None)
+        if host is None:
+            raise ValueError("cpuSphere needs a tree built from host arrays (build, not build_device)")
+        kernel = kernel or Kernel()
+        q = np.asarray(qStart, np.float32).reshape(3)
+        idx, _ = self.knearest(q.reshape(1, 3), int(self.m_knn))
+        f = np.float32
+        s_pn, s_pp, s_w = f(0), f(0), f(0)
+        s_p = np.zeros(3, np.float32)
+        s_n = np.zeros(3, np.float32)
+        for i in idx[0]:
+            if i < 0:
+                continue
+            p = host[0][i]
+            n = host[1][i]
+            wi = f(kernel.w(p, q))
+            s_pn = f(s_pn + f(wi * f(np.dot(p, n))))
+            s_pp = f(s_pp + f(wi * f(np.dot(p, p))))
+            s_p = (s_p + wi * p).astype(np.float32)
+            s_n = (s_n + wi * n).astype(np.float32)
+            s_w = f(s_w + wi)
+        u4 = f(0.5 * (s_pn - f(np.dot(s_p, (s_n / s_w).astype(np.float32))))
+               / (s_pp - f(np.dot(s_p, (s_p / s_w).astype(np.float32)))))
+        u123 = ((s_n - f(2) * u4 * s_p) / s_w).astype(np.float32)
+        u0 = f(-(f(np.dot(s_p, u123)) + u4 * s_pp) / s_w)
+        return float(u0), u123, float(u4)
 
     def getKnn(self, x, k: int):
         """APSSOctree::getKnn (CPUUtils.cpp:665-672): the k nearest points of x."""
@@ -629,6 +664,10 @@ class APSS:
 
     def CPU(self) -> APSSOctree:
         return self.m_apssOctree
+
+    def cpuSphere(self, qStart, kernel: Kernel | None = None):
+        """GlobalAPSS::cpuSphere (GlobalAPSS.cu:288-291): the octree's."""
+        return self.m_apssOctree.cpuSphere(qStart, kernel)
 
     def stop(self) -> None:
         """APSS::stop (GPUUtils.cu:394-397) ends a CUDA profiler range in the

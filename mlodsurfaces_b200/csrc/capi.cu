@@ -702,6 +702,30 @@ int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_i
     return MLODS_OK;
 }
 
+int mlods_knn_host(mlods_tree t, int64_t n, const float* q, int32_t k, int32_t* idx, float* d2)
+{
+    CHECK_TREE(t);
+    if (n <= 0 || n >= (int64_t(1) << 32) || !q || !idx || !d2 || k < 1 || k > MLODS_MAX_KNN) {
+        set_last_error("knn host: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    char* d = nullptr;
+    const size_t qb = size_t(n) * 12, ib = size_t(n) * size_t(k) * 4;
+    MLODS_CUDA(cudaMalloc(&d, qb + 2 * ib));
+    float* d_q = reinterpret_cast<float*>(d);
+    int32_t* d_idx = reinterpret_cast<int32_t*>(d + qb);
+    float* d_d2 = reinterpret_cast<float*>(d + qb + ib);
+    int rc = MLODS_OK;
+    cudaError_t e = cudaMemcpy(d_q, q, qb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) rc = mlods_knn(t, n, d_q, k, d_idx, d_d2, nullptr);
+    if (e == cudaSuccess && rc == MLODS_OK) e = cudaMemcpy(idx, d_idx, ib, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && rc == MLODS_OK) e = cudaMemcpy(d2, d_d2, ib, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (rc != MLODS_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "knn host", __FILE__, __LINE__);
+    return MLODS_OK;
+}
+
 static int dcgrid_points(const float* pts, int64_t n, int32_t max_depth, const float* box_min, const float* box_max,
                          bool device, cudaStream_t s, mlods_dcgrid* out)
 {

@@ -228,6 +228,19 @@ class RefTree:
         ref().ref_tree_export(self._h, *[_ptr(out[k]) for k in keys])
         return out
 
+    def cpu_sphere(self, q, kernel, k=20):
+        """APSSOctree::cpuSphere at each query: (n, 5) of (u0, u123, u4)."""
+        q = _f32(q)
+        out = np.empty((len(q), 5), np.float32)
+        sig = np.ascontiguousarray(np.asarray(kernel.sigmas if len(kernel.sigmas) else [0.0], np.float32))
+        lib = ref()
+        lib.ref_cpu_sphere.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, _P,
+                                       C.c_int, _P]
+        lib.ref_cpu_sphere(self._h, _ptr(q), len(q), int(k), int(kernel.type), float(kernel.sigma),
+                           float(kernel.exponent), float(kernel.constant_shift), _ptr(sig), len(kernel.sigmas),
+                           _ptr(out))
+        return out
+
     def project(self, q, n_iter, kernel, cutoff=2.0, min_depth=0, step_max=-1.0, mode=0, k=20, ball_r=0.1,
                 nthreads=0):
         """Returns (points, normals, seconds) from APSSOctree::projectCPU."""

@@ -157,6 +157,28 @@ double ref_project(void* h, const float* q, float* out_p, float* out_n, int64_t 
     return omp_get_wtime() - t0;
 }
 
+// APSSOctree::cpuSphere (CPUUtils.cpp:638-663) at nq queries with the k
+// nearest points: out = (u0, u123.x, u123.y, u123.z, u4) per query.
+void ref_cpu_sphere(void* h, const float* q, int64_t nq, int k, int ktype, float sigma, float exponent, float shift,
+                    const float* sigmas, int nsig, float* out)
+{
+    auto* rt = static_cast<RefTree*>(h);
+    APSSOctree& t = rt->tree;
+    t.knnMode(true, unsigned(k));
+    const Kernel kern = make_kernel(ktype, sigma, exponent, shift, sigmas, nsig);
+    for (int64_t i = 0; i < nq; ++i) {
+        float u0 = 0.f, u4 = 0.f;
+        glm::vec3 u123(0.f);
+        t.cpuSphere(glm::vec3(q[3 * i], q[3 * i + 1], q[3 * i + 2]), u0, u123, u4, kern);
+        out[5 * i] = u0;
+        out[5 * i + 1] = u123.x;
+        out[5 * i + 2] = u123.y;
+        out[5 * i + 3] = u123.z;
+        out[5 * i + 4] = u4;
+    }
+    t.knnMode(false, unsigned(k));
+}
+
 // Builds a kd-tree over the points with kdTree::build defaults (depth 12,
 // 1 point per leaf) and returns k nearest neighbours, sorted by distance.
 void ref_kdtree_knn(const float* pts, int64_t n, const float* q, int64_t nq, int k, int32_t* out_idx,

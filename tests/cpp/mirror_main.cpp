@@ -51,6 +51,22 @@ int main(int argc, char** argv)
     std::vector<vec3> cpu(q.size()), cpun(q.size());
     for (size_t i = 0; i < q.size(); ++i) apss.projectCPU(q[i], cpu[i], cpun[i], 10, k);
     write_vec3(argv[5], cpu);
+    if (argc > 7) {  // APSSOctree::cpuSphere at the queries: u0, u123, u4 per query
+        std::vector<float> u;
+        for (const vec3& x : q) {
+            float u0 = 0.f, u4 = 0.f;
+            vec3 u123(0.f, 0.f, 0.f);
+            tree->cpuSphere(x, u0, u123, u4, k);
+            u.insert(u.end(), {u0, u123.x, u123.y, u123.z, u4});
+        }
+        FILE* f = std::fopen(argv[7], "wb");
+        if (!f) return 2;
+        std::fwrite(u.data(), sizeof(float), u.size(), f);
+        std::fclose(f);
+        std::vector<vec3> nb;
+        tree->getKnn(q[0], 8, nb);
+        if (nb.size() != 8) return 3;
+    }
     std::printf("nodes %u depth %u\n", tree->nbOfNodes(), tree->computeDepth());
     delete tree;
     return 0;

@@ -39,7 +39,8 @@ def test_mirror_projects_like_the_reference_protocol(tmp_path):
         arr.astype(np.float32).tofile(tmp_path / f"{name}.bin")
     sigma_rel = 0.04  # in units of the box radius, as the -s CLI option
     res = subprocess.run([str(exe), str(tmp_path / "p.bin"), str(tmp_path / "n.bin"), str(tmp_path / "q.bin"),
-                          str(tmp_path / "gpu.bin"), str(tmp_path / "cpu.bin"), str(sigma_rel)],
+                          str(tmp_path / "gpu.bin"), str(tmp_path / "cpu.bin"), str(sigma_rel),
+                          str(tmp_path / "sphere.bin")],
                          capture_output=True, text=True, timeout=300)
     assert res.returncode == 0, res.stderr
     gpu = np.fromfile(tmp_path / "gpu.bin", np.float32).reshape(-1, 3)
@@ -56,3 +57,7 @@ def test_mirror_projects_like_the_reference_protocol(tmp_path):
     c64, _ = ot.project_mlod(q, 10, k, rule=1, cutoff=3.0)
     assert rel_err(gpu, g64, diag).max() < TOL_DIAG
     assert rel_err(cpu, c64, diag).max() < TOL_DIAG
+    # APSSOctree::cpuSphere against the reference's own (CPUUtils.cpp:638-663)
+    u = np.fromfile(tmp_path / "sphere.bin", np.float32).reshape(-1, 5)
+    ref_u = oracle.RefTree(pts, nrm, 12).cpu_sphere(q, k, 20)
+    assert np.allclose(u, ref_u, rtol=2e-3, atol=2e-3 * np.abs(ref_u).max(axis=0))

@@ -215,3 +215,15 @@ def test_knn_iterations_in_one_call_equal_one_call_per_iteration():
     step_n = np.empty((len(q), 3), np.float32)
     f.project(len(q), step, step_n, 0, k)
     assert np.array_equal(one, step)
+
+
+def test_cpu_sphere_matches_the_reference():
+    """APSSOctree.cpuSphere (CPUUtils.cpp:638-663): the sphere fitted to the
+    20 nearest samples, against the reference's own on its kd-tree."""
+    pts, nrm = synth.torus(20000, seed=93)
+    q = synth.perturbed_queries(pts, 0.01, seed=94)[:50]
+    k = make_kernel("gauss", synth.bbox_diag(pts))
+    t = tree_of(pts, nrm)
+    got = np.array([[u0, *u123, u4] for u0, u123, u4 in (t.cpuSphere(x, k) for x in q)], np.float32)
+    ref_u = oracle.RefTree(pts, nrm, 12).cpu_sphere(q, k, 20)
+    assert np.allclose(got, ref_u, rtol=2e-3, atol=2e-3 * np.abs(ref_u).max(axis=0))
