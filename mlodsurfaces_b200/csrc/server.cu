@@ -46,6 +46,7 @@ struct Request {
     int64_t taken = 0;     // queries handed to batches
     int64_t finished = 0;  // queries whose batch has returned
     int piece_status = 0;  // first failing piece's status (MLODS_OK = 0 so far)
+    bool cancelled = false;  // no further pieces will be handed out
 };
 
 // A contiguous range of one request's queries: requests larger than a batch
@@ -280,7 +281,8 @@ void worker_main(mlods_server_s* S, Worker* w)
             }
             r->finished += pc.n;
             S->queries += pc.n;
-            if (r->finished == r->n) {  // the request's last piece
+            // the request's last piece, or the last one in flight of a cancelled request
+            if (r->finished == r->n || (r->cancelled && r->finished == r->taken)) {
                 r->status = r->piece_status;
                 r->t_done = t1;
                 ++S->completed;
@@ -319,10 +321,18 @@ void stop_server(mlods_server_s* S)
     {
         std::lock_guard<std::mutex> lock(S->mu);
         S->stopping = true;
-        // queued requests are cancelled; batches in flight finish
+        // queued requests are cancelled; batches in flight finish, and a
+        // request with pieces in flight is answered when its last one returns
         for (Request* r : S->queue) {
-            r->status = MLODS_ERR_STATE;
-            std::snprintf(r->error, sizeof r->error, "server stopped before the request ran");
+            r->cancelled = true;
+            if (r->piece_status == MLODS_OK) {
+                r->piece_status = MLODS_ERR_STATE;
+                std::snprintf(r->error, sizeof r->error, "server stopped before the request ran");
+            }
+            if (r->finished == r->taken) {
+                r->status = r->piece_status;
+                r->t_done = Clock::now();
+            }
         }
         S->queue.clear();
         S->queued = 0;

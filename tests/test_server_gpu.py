@@ -172,3 +172,10 @@ def test_close_with_queued_work_returns(projectors):
         srv.submit(0, q, 10)
     srv.close()  # cancels what is queued, finishes the running batch, joins
     srv.close()
+    # requests cut into pieces: closing while some of a request's pieces are
+    # in flight and the rest are queued waits for those pieces, then returns
+    srv = ProjectionServer([f], n_streams=2, max_batch_queries=3000)
+    big = np.concatenate([q] * 3)
+    for _ in range(6):
+        srv.submit(0, big, 10)
+    srv.close()
