@@ -338,7 +338,7 @@ def run_ours(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
     launches0 = lib.mlods_kernel_launches()
-    step_ms, kern_ms, visits, rounds, max_stack = [], [], [], [], 0
+    step_ms, kern_ms, visits, rounds, searches, max_stack = [], [], [], [], [], 0
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -352,6 +352,7 @@ def run_ours(args, rank, world, local_rank):
         kern_ms.append(st["kernel_ms"])
         visits.append(st["node_visits"])
         rounds.append(st["rounds"])
+        searches.append(st["iterations"])
         max_stack = max(max_stack, st["max_stack"])
         if st["overflows"]:
             raise RuntimeError(f"{st['overflows']} queries overflowed the traversal stack")
@@ -485,6 +486,8 @@ def run_ours(args, rank, world, local_rank):
         "kernel_ms": kms,
         "converge_exact": conv,
         "converge_tol": conv_tol,
+        "neighbour_searches_per_query_iteration": (statistics.mean(searches) / len(q) / args.iters
+                                                   if spec.get("knn") else None),
         "traversal": None if spec.get("knn") or spec.get("global") else {
             "visits_per_query_iteration": mean_visits / len(q) / args.iters,
             "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),

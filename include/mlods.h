@@ -290,7 +290,10 @@ int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_
                      float* kernel_ms);
 /* Iterations the last MLoD projection on this tree ran, summed over its
  * queries: n x n_iterations, fewer under a convergence mode (each query
- * counts the iterations it evaluated).  Extension; synchronises. */
+ * counts the iterations it evaluated).  After a kNN projection: the
+ * iterations that searched the octree for their neighbours; the others kept
+ * the previous iteration's k points, which the step provably left the k
+ * nearest, and only ranked them again.  Extension; synchronises. */
 int mlods_last_iterations(mlods_tree t, int64_t* iterations);
 
 /* ---- batched projection over many resident trees (extension) ---------------

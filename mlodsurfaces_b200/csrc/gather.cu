@@ -30,6 +30,10 @@ constexpr uint32_t kGPoints = 1u << 31;  // entry is a range of sorted point pos
 #define MLODS_GATHER_MIN_BLOCKS 10
 #endif
 constexpr int kGatherMinBlocks = MLODS_GATHER_MIN_BLOCKS;  // resident blocks per SM the register budget aims at
+#ifndef MLODS_KNN_MIN_BLOCKS
+#define MLODS_KNN_MIN_BLOCKS MLODS_GATHER_MIN_BLOCKS
+#endif
+constexpr int kKnnMinBlocks = MLODS_KNN_MIN_BLOCKS;  // the same for the kNN projection
 constexpr int kGatherCap = 256;          // stack entries per warp
 // A range entry holds at most 8 nodes, each pushing at most one entry, so a
 // depth-first walk below any entry adds at most 7 entries per level for the
@@ -44,6 +48,18 @@ static_assert(kBatchPopLimit > 0, "gather stack too small for a depth-first walk
 struct GStack {
     uint32_t first[kGatherCap];
     uint32_t cnt[kGatherCap];
+};
+
+// Per-warp state of a kNN projection query between iterations (uniform over
+// the warp, so it is kept in shared memory rather than in every lane's
+// registers): the previous iterate p, its k-th squared distance, and bounds
+// from the last octree search, carried to p by the triangle inequality:
+// every point outside the kept k is at least out_lo away from p, the
+// (k+1)-th nearest at most out_hi.
+struct KnnCarry {
+    double out_lo, out_hi;
+    float kth, px, py, pz;
+    uint32_t searches;  // octree searches of this warp
 };
 
 __device__ __forceinline__ float kd_dist2(const float4 p, float qx, float qy, float qz)
@@ -82,14 +98,20 @@ __device__ __forceinline__ void warp_sort(float& d, uint32_t& o, uint32_t& p, bo
 }
 
 // Ascending best list (d, o, p) merged with candidate batch (cd, co, cp).
-__device__ __forceinline__ void warp_merge(float& d, uint32_t& o, uint32_t& p, float cd, uint32_t co, uint32_t cp)
+// `lost` receives this lane's entry that left the union (the 32 largest of
+// list and batch, one per lane): their minimum is the union's 33rd distance.
+__device__ __forceinline__ void warp_merge(float& d, uint32_t& o, uint32_t& p, float cd, uint32_t co, uint32_t cp,
+                                           float& lost)
 {
     const int lane = threadIdx.x & 31;
     warp_sort(cd, co, cp, true);
     if (key_less(cd, co, d, o)) {
+        lost = d;
         d = cd;
         o = co;
         p = cp;
+    } else {
+        lost = cd;
     }
 #pragma unroll
     for (int j = 16; j > 0; j >>= 1) {
@@ -110,6 +132,13 @@ __device__ __forceinline__ float warp_sum_f(float v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_min_f(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
     return v;
 }
 
@@ -223,11 +252,14 @@ __device__ bool fit_cpu(const float* s, double step_max, double x[3], float nrm[
 
 // MODE: 0 = kNN APSS projection, 1 = ball APSS projection, 2 = kNN sets only.
 template <int KTYPE, int MODE>
-__global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kernel(GatherArgs a)
+__global__ void __launch_bounds__(kGatherThreads, MODE == 0 ? kKnnMinBlocks : kGatherMinBlocks) gather_kernel(GatherArgs a)
 {
     __shared__ GStack stacks[kGatherThreads / 32];
+    __shared__ KnnCarry carries[kGatherThreads / 32];
     const int lane = threadIdx.x & 31;
     GStack& st = stacks[threadIdx.x >> 5];
+    KnnCarry& carry = carries[threadIdx.x >> 5];
+    if (MODE == 0 && lane == 0) carry.searches = 0;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const int k = a.k;
     const double r2ball = double(a.ball_r) * double(a.ball_r);
@@ -246,11 +278,6 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kerne
         bool failed = false, empty = false, overflow = false;
         float best_d = INFINITY;
         uint32_t best_o = 0xFFFFFFFFu, best_p = 0xFFFFFFFFu;
-        // kNN projection: the previous iteration's k-th distance, grown by the
-        // step, bounds this iteration's (triangle inequality, with a margin for
-        // the float distances), so the walk needs no starting window after the
-        // first iteration
-        float prev_kth = INFINITY, pwx = 0.f, pwy = 0.f, pwz = 0.f;
         for (int it = 0; it < n_iter && !failed; ++it) {
             // the reference keeps the iterate as a float glm::vec3
             const float wx = it == 0 ? q0[0] : float(xd[0] + a.o0);
@@ -262,36 +289,80 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kerne
             for (int c = 0; c < 9; ++c) acc[c] = 0.f;
             int found = 0;
             int64_t w0 = 0, w1 = 0;  // Morton window already in the best list
-            float bound;             // squared search radius
-            best_d = INFINITY;
-            best_o = best_p = 0xFFFFFFFFu;
-            if (MODE == 0 && it > 0 && prev_kth < INFINITY) {
-                const double ddx = double(wx) - double(pwx), ddy = double(wy) - double(pwy),
-                             ddz = double(wz) - double(pwz);
-                const double step = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
-                const double r = (sqrt(double(prev_kth)) + step) * (1.0 + 1e-5) + 1e-30;
-                bound = __double2float_ru(r * r);
-            } else if (MODE != 1) {
-                const uint64_t qc = lattice_code(a, wx, wy, wz);
-                const int64_t pos = warp_upper_bound(a.codes, a.n_pts, qc);
-                w0 = pos - 16 < 0 ? 0 : pos - 16;
-                w1 = w0 + 32 > a.n_pts ? a.n_pts : w0 + 32;
-                w0 = w1 - 32 < 0 ? 0 : w1 - 32;
-                const int64_t j = w0 + lane;
-                if (j < w1) {
-                    const float4 p = __ldg(a.wspts + j);
-                    best_d = kd_dist2(p, wx, wy, wz);
-                    best_o = __float_as_uint(p.w);
-                    best_p = uint32_t(j);
+            // squared search radius: for the kNN projection an upper bound on
+            // the (k+1)-th distance, so that the search also bounds the points
+            // it leaves out; for the kNN sets the k-th
+            float bound = INFINITY;
+            bool search = true;
+            double step = 0.0;
+            double out_hi = INFINITY;
+            if (MODE == 0 && it > 0) {
+                const double ddx = double(wx) - double(carry.px), ddy = double(wy) - double(carry.py),
+                             ddz = double(wz) - double(carry.pz);
+                step = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+                out_hi = carry.out_hi;
+                // The kept points are now at most sqrt(kth) + step away, the
+                // others at least out_lo - step (margins of 1e-5 cover the
+                // float distances): if those bounds are apart, a search would
+                // return the same k points, so they are only ranked again.
+                const double r_in = sqrt(double(carry.kth)) * (1.0 + 1e-5);
+                const double out_lo = carry.out_lo;
+                const bool kept = __shfl_sync(kFull, best_p, k - 1) != 0xFFFFFFFFu;
+                __syncwarp();  // every lane has read the carry before lane 0 updates it
+                if (kept && (r_in + step) * (1.0 + 1e-5) < (out_lo - step) * (1.0 - 1e-5)) {
+                    search = false;
+                    if (lane < k) {
+                        best_d = kd_dist2(__ldg(a.wspts + best_p), wx, wy, wz);
+                    } else {
+                        best_d = INFINITY;
+                        best_o = best_p = 0xFFFFFFFFu;
+                    }
+                    // after a short step they are mostly still in order
+                    const float dn = __shfl_down_sync(kFull, best_d, 1);
+                    const uint32_t on = __shfl_down_sync(kFull, best_o, 1);
+                    if (__any_sync(kFull, lane < k - 1 && key_less(dn, on, best_d, best_o)))
+                        warp_sort(best_d, best_o, best_p, false);
+                    if (lane == 0) {
+                        carry.out_lo = out_lo - step;
+                        carry.out_hi = out_hi + step;
+                    }
                 }
-                warp_sort(best_d, best_o, best_p, false);
-                bound = __shfl_sync(kFull, best_d, k - 1);
-            } else {
-                bound = float(r2ball) * (1.f + 1e-6f);
+            }
+            if (search) {
+                best_d = INFINITY;
+                best_o = best_p = 0xFFFFFFFFu;
+                if (MODE == 0 && it > 0 && out_hi < INFINITY) {
+                    const double r = (out_hi + step) * (1.0 + 1e-5) + 1e-30;
+                    bound = __double2float_ru(r * r);
+                } else if (MODE != 1) {
+                    const uint64_t qc = lattice_code(a, wx, wy, wz);
+                    const int64_t pos = warp_upper_bound(a.codes, a.n_pts, qc);
+                    w0 = pos - 16 < 0 ? 0 : pos - 16;
+                    w1 = w0 + 32 > a.n_pts ? a.n_pts : w0 + 32;
+                    w0 = w1 - 32 < 0 ? 0 : w1 - 32;
+                    const int64_t j = w0 + lane;
+                    if (j < w1) {
+                        const float4 p = __ldg(a.wspts + j);
+                        best_d = kd_dist2(p, wx, wy, wz);
+                        best_o = __float_as_uint(p.w);
+                        best_p = uint32_t(j);
+                    }
+                    warp_sort(best_d, best_o, best_p, false);
+                    if (MODE == 0 && k == 32) {
+                        // a 33rd point beside the window bounds the 33rd distance
+                        const int64_t xp = w1 < a.n_pts ? w1 : w0 - 1;
+                        const float xd2 = xp >= 0 ? kd_dist2(__ldg(a.wspts + xp), wx, wy, wz) : INFINITY;
+                        bound = fmaxf(__shfl_sync(kFull, best_d, 31), xd2);
+                    } else {
+                        bound = __shfl_sync(kFull, best_d, MODE == 0 ? k : k - 1);
+                    }
+                } else {
+                    bound = float(r2ball) * (1.f + 1e-6f);
+                }
             }
             // ---- octree walk
-            int top = 1;
-            if (lane == 0) {
+            int top = search ? 1 : 0;
+            if (lane == 0 && search) {
                 st.first[0] = 0;
                 st.cnt[0] = 1u;
             }
@@ -397,8 +468,13 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kerne
                 }
                 if (MODE != 1) {
                     if (__any_sync(kFull, cd <= bound && cd < INFINITY)) {
-                        warp_merge(best_d, best_o, best_p, cd, co, cp);
-                        bound = fminf(bound, __shfl_sync(kFull, best_d, k - 1));
+                        float lost = INFINITY;
+                        warp_merge(best_d, best_o, best_p, cd, co, cp, lost);
+                        // the (k+1)-th (kNN projection) or k-th distance so far
+                        if (MODE == 0 && k == 32)
+                            bound = fminf(bound, warp_min_f(lost));
+                        else
+                            bound = fminf(bound, __shfl_sync(kFull, best_d, MODE == 0 ? k : k - 1));
                     }
                 }
                 const uint32_t pm = __ballot_sync(kFull, push);
@@ -421,10 +497,24 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kerne
             }
             if (MODE == 2) break;
             if (MODE == 0) {
-                prev_kth = __shfl_sync(kFull, best_d, k - 1);
-                pwx = wx;
-                pwy = wy;
-                pwz = wz;
+                const float kth = __shfl_sync(kFull, best_d, k - 1);
+                if (lane == 0) {
+                    carry.kth = kth;
+                    carry.px = wx;
+                    carry.py = wy;
+                    carry.pz = wz;
+                    if (search) {
+                        // every point left out is at least sqrt(bound) away
+                        // (it was pruned, rejected or ranked beyond the k-th
+                        // against a bound no smaller than the final one), and
+                        // the (k+1)-th nearest at most: bound never fell below it
+                        const double lb = sqrt(double(bound));
+                        carry.out_lo = lb * (1.0 - 1e-5);
+                        carry.out_hi = lb * (1.0 + 1e-5);
+                        ++carry.searches;
+                    }
+                }
+                __syncwarp();
                 if (lane < k && best_p != 0xFFFFFFFFu) {
                     const float4 pl = __ldg(a.spts + best_p);
                     const float4 nn = __ldg(a.snrm + best_p);
@@ -493,6 +583,8 @@ __global__ void __launch_bounds__(kGatherThreads, kGatherMinBlocks) gather_kerne
     }
     if (lane == 0 && a.stats && overflows)
         atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[2]), (unsigned long long)overflows);
+    if (MODE == 0 && lane == 0 && a.stats && carry.searches)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.stats[5]), (unsigned long long)carry.searches);
 }
 
 // ---------------------------------------------------------------- global APSS

@@ -192,29 +192,37 @@ def test_global_apss_split_and_fused_forms():
     assert rel_err(full[sel], o64b, diag).max() < TOL_DIAG
 
 
-def test_knn_iterations_in_one_call_equal_one_call_per_iteration():
-    """Inside one call the kNN search of iteration i > 0 starts from the
-    bound that iteration i - 1 leaves (its k-th distance grown by the step);
-    one call per iteration starts every search afresh.  The neighbour sets,
-    and so the projections, are the same bit for bit."""
+@pytest.mark.parametrize("k", [32, 20])
+def test_knn_iterations_in_one_call_equal_one_call_per_iteration(k):
+    """Inside one call the kNN iteration i > 0 either keeps the k points of
+    iteration i - 1, when the step provably leaves them the k nearest, or
+    searches from the bound that iteration i - 1 leaves (its (k+1)-th distance
+    grown by the step); one call per iteration searches every time from the
+    points around the query's Morton position.  The neighbour sets, and so
+    the projections, are the same bit for bit, and most later iterations keep
+    their neighbours."""
     pts, nrm = synth.rbf_blobs(300_000, seed=7)
     pts = synth.make_tie_free(pts)
     q = synth.perturbed_queries(pts, 0.01, seed=8)[:20000]
-    k = make_kernel("multi", synth.bbox_diag(pts))
+    kern = make_kernel("multi", synth.bbox_diag(pts))
     t = tree_of(pts, nrm)
-    t.knnMode(True, 32)
-    f = Fastapss(t, k, len(q))
+    t.knnMode(True, k)
+    f = Fastapss(t, kern, len(q))
+    iters = 8
     f.copyPointsToGPU(len(q), q)
     one = np.empty((len(q), 3), np.float32)
     one_n = np.empty((len(q), 3), np.float32)
-    f.project(len(q), one, one_n, 4, k)
+    f.project(len(q), one, one_n, iters, kern)
+    searches = f.last_stats()["iterations"]
+    assert len(q) <= searches < len(q) * iters // 2
     f.copyPointsToGPU(len(q), q)
-    for _ in range(4):
-        f.project(len(q), None, None, 1, k)
     step = np.empty((len(q), 3), np.float32)
     step_n = np.empty((len(q), 3), np.float32)
-    f.project(len(q), step, step_n, 0, k)
-    assert np.array_equal(one, step)
+    for i in range(iters):
+        last = i == iters - 1
+        f.project(len(q), step if last else None, step_n if last else None, 1, kern)
+        assert f.last_stats()["iterations"] == len(q)
+    assert np.array_equal(one, step) and np.array_equal(one_n, step_n)
 
 
 def test_cpu_sphere_matches_the_reference():
