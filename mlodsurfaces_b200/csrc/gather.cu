@@ -31,9 +31,9 @@ constexpr uint32_t kGPoints = 1u << 31;  // entry is a range of sorted point pos
 #endif
 constexpr int kGatherMinBlocks = MLODS_GATHER_MIN_BLOCKS;  // resident blocks per SM the register budget aims at
 #ifndef MLODS_KNN_MIN_BLOCKS
-#define MLODS_KNN_MIN_BLOCKS MLODS_GATHER_MIN_BLOCKS
+#define MLODS_KNN_MIN_BLOCKS 9
 #endif
-constexpr int kKnnMinBlocks = MLODS_KNN_MIN_BLOCKS;  // the same for the kNN projection
+constexpr int kKnnMinBlocks = MLODS_KNN_MIN_BLOCKS;  // the same for the kNN projection (56 registers)
 constexpr int kGatherCap = 256;          // stack entries per warp
 // A range entry holds at most 8 nodes, each pushing at most one entry, so a
 // depth-first walk below any entry adds at most 7 entries per level for the
@@ -52,13 +52,13 @@ struct GStack {
 
 // Per-warp state of a kNN projection query between iterations (uniform over
 // the warp, so it is kept in shared memory rather than in every lane's
-// registers): the previous iterate p, its k-th squared distance, and bounds
-// from the last octree search, carried to p by the triangle inequality:
+// registers): the previous iterate p and bounds from the last octree
+// search, carried to p by the triangle inequality:
 // every point outside the kept k is at least out_lo away from p, the
 // (k+1)-th nearest at most out_hi.
 struct KnnCarry {
     double out_lo, out_hi;
-    float kth, px, py, pz;
+    float px, py, pz;
     uint32_t searches;  // octree searches of this warp
 };
 
@@ -132,6 +132,13 @@ __device__ __forceinline__ float warp_sum_f(float v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_max_f(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
     return v;
 }
 
@@ -294,46 +301,62 @@ __global__ void __launch_bounds__(kGatherThreads, MODE == 0 ? kKnnMinBlocks : kG
             // it leaves out; for the kNN sets the k-th
             float bound = INFINITY;
             bool search = true;
-            double step = 0.0;
-            double out_hi = INFINITY;
+            float warm = INFINITY;  // kNN projection, iteration > 0: the search's starting bound
             if (MODE == 0 && it > 0) {
                 const double ddx = double(wx) - double(carry.px), ddy = double(wy) - double(carry.py),
                              ddz = double(wz) - double(carry.pz);
-                step = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
-                out_hi = carry.out_hi;
-                // The kept points are now at most sqrt(kth) + step away, the
-                // others at least out_lo - step (margins of 1e-5 cover the
-                // float distances): if those bounds are apart, a search would
-                // return the same k points, so they are only ranked again.
-                const double r_in = sqrt(double(carry.kth)) * (1.0 + 1e-5);
-                const double out_lo = carry.out_lo;
-                const bool kept = __shfl_sync(kFull, best_p, k - 1) != 0xFFFFFFFFu;
+                const double step = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+                const double out_lo = carry.out_lo, out_hi = carry.out_hi;
                 __syncwarp();  // every lane has read the carry before lane 0 updates it
-                if (kept && (r_in + step) * (1.0 + 1e-5) < (out_lo - step) * (1.0 - 1e-5)) {
-                    search = false;
+                // the previous (k+1)-th nearest point is at most out_hi + step away
+                const double r = (out_hi + step) * (1.0 + 1e-5) + 1e-30;
+                warm = __double2float_ru(r * r);
+                if (__shfl_sync(kFull, best_p, k - 1) != 0xFFFFFFFFu) {
+                    // the kept points' distances from the new iterate
                     if (lane < k) {
                         best_d = kd_dist2(__ldg(a.wspts + best_p), wx, wy, wz);
                     } else {
                         best_d = INFINITY;
                         best_o = best_p = 0xFFFFFFFFu;
                     }
-                    // after a short step they are mostly still in order
-                    const float dn = __shfl_down_sync(kFull, best_d, 1);
-                    const uint32_t on = __shfl_down_sync(kFull, best_o, 1);
-                    if (__any_sync(kFull, lane < k - 1 && key_less(dn, on, best_d, best_o)))
-                        warp_sort(best_d, best_o, best_p, false);
-                    if (lane == 0) {
-                        carry.out_lo = out_lo - step;
-                        carry.out_hi = out_hi + step;
+                    const float dmax = warp_max_f(lane < k ? best_d : 0.f);
+                    // Every other point is at least out_lo - step away: if all
+                    // kept points are nearer (margins of 1e-5 cover the float
+                    // distances), a search would return the same k points, so
+                    // they are only ranked again.
+                    if (sqrt(double(dmax)) * (1.0 + 1e-5) < (out_lo - step) * (1.0 - 1e-5)) {
+                        search = false;
+                        // after a short step they are mostly still in order
+                        const float dn = __shfl_down_sync(kFull, best_d, 1);
+                        const uint32_t on = __shfl_down_sync(kFull, best_o, 1);
+                        if (__any_sync(kFull, lane < k - 1 && key_less(dn, on, best_d, best_o)))
+                            warp_sort(best_d, best_o, best_p, false);
+                        if (lane == 0) {
+                            carry.out_lo = out_lo - step;
+                            carry.out_hi = out_hi + step;
+                        }
+                    } else if (a.n_pts > k) {
+                        // the kept k and one other point bound the (k+1)-th
+                        // distance: the first sorted position after the
+                        // nearest kept point's that none of them holds
+                        uint32_t c = __shfl_sync(kFull, best_p, 0), xp = 0xFFFFFFFFu;
+                        for (int t = 0; t <= k; ++t) {
+                            c = c + 1u == uint32_t(a.n_pts) ? 0u : c + 1u;
+                            if (!__any_sync(kFull, lane < k && best_p == c)) {
+                                xp = c;
+                                break;
+                            }
+                        }
+                        if (xp != 0xFFFFFFFFu)
+                            warm = fminf(warm, fmaxf(dmax, kd_dist2(__ldg(a.wspts + xp), wx, wy, wz)));
                     }
                 }
             }
             if (search) {
                 best_d = INFINITY;
                 best_o = best_p = 0xFFFFFFFFu;
-                if (MODE == 0 && it > 0 && out_hi < INFINITY) {
-                    const double r = (out_hi + step) * (1.0 + 1e-5) + 1e-30;
-                    bound = __double2float_ru(r * r);
+                if (MODE == 0 && it > 0 && warm < INFINITY) {
+                    bound = warm;
                 } else if (MODE != 1) {
                     const uint64_t qc = lattice_code(a, wx, wy, wz);
                     const int64_t pos = warp_upper_bound(a.codes, a.n_pts, qc);
@@ -497,9 +520,7 @@ __global__ void __launch_bounds__(kGatherThreads, MODE == 0 ? kKnnMinBlocks : kG
             }
             if (MODE == 2) break;
             if (MODE == 0) {
-                const float kth = __shfl_sync(kFull, best_d, k - 1);
                 if (lane == 0) {
-                    carry.kth = kth;
                     carry.px = wx;
                     carry.py = wy;
                     carry.pz = wz;

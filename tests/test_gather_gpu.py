@@ -196,11 +196,12 @@ def test_global_apss_split_and_fused_forms():
 def test_knn_iterations_in_one_call_equal_one_call_per_iteration(k):
     """Inside one call the kNN iteration i > 0 either keeps the k points of
     iteration i - 1, when the step provably leaves them the k nearest, or
-    searches from the bound that iteration i - 1 leaves (its (k+1)-th distance
-    grown by the step); one call per iteration searches every time from the
-    points around the query's Morton position.  The neighbour sets, and so
-    the projections, are the same bit for bit, and most later iterations keep
-    their neighbours."""
+    searches from a bound on the (k+1)-th distance taken from iteration i - 1
+    (its k points and one other at their new distances, or the (k+1)-th
+    distance grown by the step); one call per iteration searches every time
+    from the points around the query's Morton position.  The neighbour sets,
+    and so the projections, are the same bit for bit, and most later
+    iterations keep their neighbours."""
     pts, nrm = synth.rbf_blobs(300_000, seed=7)
     pts = synth.make_tie_free(pts)
     q = synth.perturbed_queries(pts, 0.01, seed=8)[:20000]
