@@ -639,19 +639,25 @@ __device__ __forceinline__ float global_weight(const KernelConsts& kc, float d2)
     return w;
 }
 
-// Sums over the points [p_begin, p_end) for kGlobalQpt queries per thread
-// (local-frame float positions lx, ly, lz): every point contributes
+// Sums over the points [p_begin, p_end) for the kGlobalQpt = 2 queries of a
+// thread (local-frame float positions lx, ly, lz): every point contributes
 // w(p_i, q) a_i {1, n_i, p_i - q, (p_i - q).n_i, |p_i - q|^2}
 // (APSSOctree::APSSStats, CPUUtils.cpp:515-528).  Points stream through
-// shared memory in tiles; per-tile float partial sums are added to `tot` in
-// double.  Every thread of the block calls it (it synchronises the block).
+// shared memory in tiles, each value stored twice ({v, v}), so that one
+// packed f32x2 instruction (sm_100) does the arithmetic of both queries:
+// the same roundings, in the same order, as two scalar instructions.  Per-
+// tile float partial sums are added to `tot` in double.  Every thread of the
+// block calls it (it synchronises the block).
 template <int KTYPE, int NSIG>
 __device__ __forceinline__ void global_pair_sums(const GlobalArgs& a, int64_t p_begin, int64_t p_end,
                                                  const float (&lx)[kGlobalQpt], const float (&ly)[kGlobalQpt],
                                                  const float (&lz)[kGlobalQpt], double (&tot)[kGlobalQpt][9],
-                                                 float4* s_p, float4* s_n)
+                                                 float4* s_pd, float4* s_nd)
 {
-    constexpr int Q = kGlobalQpt;
+    static_assert(kGlobalQpt == 2, "the packed pair sums serve two queries per thread");
+    // p - q as p + (-q): the same rounding as the subtraction
+    const float2 mqx = make_float2(-lx[0], -lx[1]), mqy = make_float2(-ly[0], -ly[1]),
+                 mqz = make_float2(-lz[0], -lz[1]);
     for (int64_t base = p_begin; base < p_end; base += kGlobalTile) {
         __syncthreads();
         for (int j = threadIdx.x; j < kGlobalTile; j += kGlobalThreads) {
@@ -660,43 +666,60 @@ __device__ __forceinline__ void global_pair_sums(const GlobalArgs& a, int64_t p_
                 const float4 p = __ldg(a.spts + g);
                 const float4 nn = __ldg(a.snrm + g);
                 const float ar = __ldg(a.area + __float_as_uint(p.w));
-                s_p[j] = make_float4(p.x, p.y, p.z, ar);
-                s_n[j] = nn;
+                s_pd[2 * j] = make_float4(p.x, p.x, p.y, p.y);
+                s_pd[2 * j + 1] = make_float4(p.z, p.z, ar, ar);
+                s_nd[2 * j] = make_float4(nn.x, nn.x, nn.y, nn.y);
+                s_nd[2 * j + 1] = make_float4(nn.z, nn.z, 0.f, 0.f);
             } else {  // zero area: no contribution
-                s_p[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-                s_n[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                s_pd[2 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                s_pd[2 * j + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                s_nd[2 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                s_nd[2 * j + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
         }
         __syncthreads();
-        float acc[Q][9];
+        float2 acc[9];
 #pragma unroll
-        for (int u = 0; u < Q; ++u)
-#pragma unroll
-            for (int c = 0; c < 9; ++c) acc[u][c] = 0.f;
+        for (int c = 0; c < 9; ++c) acc[c] = make_float2(0.f, 0.f);
 #pragma unroll 2
         for (int j = 0; j < kGlobalTile; ++j) {
-            const float4 p = s_p[j];
-            const float4 nn = s_n[j];
+            const float4 pa = s_pd[2 * j], pb = s_pd[2 * j + 1];
+            const float4 na = s_nd[2 * j], nb = s_nd[2 * j + 1];
+            const float2 nx = make_float2(na.x, na.y), ny = make_float2(na.z, na.w), nz = make_float2(nb.x, nb.y);
+            const float2 dx = __fadd2_rn(make_float2(pa.x, pa.y), mqx);
+            const float2 dy = __fadd2_rn(make_float2(pa.z, pa.w), mqy);
+            const float2 dz = __fadd2_rn(make_float2(pb.x, pb.y), mqz);
+            const float2 dd = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            float2 w;
+            if (KTYPE == MLODS_GAUSSIAN_MULTIPLE && NSIG > 0) {
+                w = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int u = 0; u < Q; ++u) {
-                const float dx = p.x - lx[u], dy = p.y - ly[u], dz = p.z - lz[u];
-                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const float w = global_weight<KTYPE, NSIG>(a.kc, dd) * p.w;
-                acc[u][0] += w;
-                acc[u][1] = fmaf(w, nn.x, acc[u][1]);
-                acc[u][2] = fmaf(w, nn.y, acc[u][2]);
-                acc[u][3] = fmaf(w, nn.z, acc[u][3]);
-                acc[u][4] = fmaf(w, dx, acc[u][4]);
-                acc[u][5] = fmaf(w, dy, acc[u][5]);
-                acc[u][6] = fmaf(w, dz, acc[u][6]);
-                acc[u][7] = fmaf(w, fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z)), acc[u][7]);
-                acc[u][8] = fmaf(w, dd, acc[u][8]);
+                for (int i = 0; i < NSIG; ++i) {
+                    const float2 t = __fmul2_rn(dd, make_float2(a.kc.ms_scale[i], a.kc.ms_scale[i]));
+                    const float2 e = make_float2(exp2f(t.x), exp2f(t.y));
+                    w = __ffma2_rn(e, make_float2(a.kc.ms_w[i], a.kc.ms_w[i]), w);
+                }
+                if (w.x == 0.f) w.x = a.kc.shift;  // Kernel.cpp:70-74
+                if (w.y == 0.f) w.y = a.kc.shift;
+            } else {
+                w = make_float2(global_weight<KTYPE, NSIG>(a.kc, dd.x), global_weight<KTYPE, NSIG>(a.kc, dd.y));
             }
+            w = __fmul2_rn(w, make_float2(pb.z, pb.w));
+            acc[0] = __fadd2_rn(acc[0], w);
+            acc[1] = __ffma2_rn(w, nx, acc[1]);
+            acc[2] = __ffma2_rn(w, ny, acc[2]);
+            acc[3] = __ffma2_rn(w, nz, acc[3]);
+            acc[4] = __ffma2_rn(w, dx, acc[4]);
+            acc[5] = __ffma2_rn(w, dy, acc[5]);
+            acc[6] = __ffma2_rn(w, dz, acc[6]);
+            acc[7] = __ffma2_rn(w, __ffma2_rn(dx, nx, __ffma2_rn(dy, ny, __fmul2_rn(dz, nz))), acc[7]);
+            acc[8] = __ffma2_rn(w, dd, acc[8]);
         }
 #pragma unroll
-        for (int u = 0; u < Q; ++u)
-#pragma unroll
-            for (int c = 0; c < 9; ++c) tot[u][c] += double(acc[u][c]);
+        for (int c = 0; c < 9; ++c) {
+            tot[0][c] += double(acc[c].x);
+            tot[1][c] += double(acc[c].y);
+        }
     }
 }
 
@@ -725,8 +748,8 @@ template <int KTYPE, int NSIG>
 __global__ void MLODS_GLOBAL_BOUNDS global_apss_kernel(GlobalArgs a)
 {
     constexpr int Q = kGlobalQpt;
-    __shared__ float4 s_p[kGlobalTile];
-    __shared__ float4 s_n[kGlobalTile];
+    __shared__ float4 s_pd[2 * kGlobalTile];
+    __shared__ float4 s_nd[2 * kGlobalTile];
     const int64_t q_first = int64_t(blockIdx.x) * kGlobalThreads * Q + threadIdx.x;
     double xd[Q][3];
     float nrm[Q][3];
@@ -754,7 +777,7 @@ __global__ void MLODS_GLOBAL_BOUNDS global_apss_kernel(GlobalArgs a)
 #pragma unroll
             for (int c = 0; c < 9; ++c) tot[u][c] = 0.0;
         }
-        global_pair_sums<KTYPE, NSIG>(a, 0, a.n_pts, lx, ly, lz, tot, s_p, s_n);
+        global_pair_sums<KTYPE, NSIG>(a, 0, a.n_pts, lx, ly, lz, tot, s_pd, s_nd);
 #pragma unroll
         for (int u = 0; u < Q; ++u) {
             if (!valid[u] || failed[u]) continue;
@@ -804,8 +827,8 @@ template <int KTYPE, int NSIG>
 __global__ void MLODS_GLOBAL_BOUNDS global_split_sums_kernel(GlobalArgs a, GlobalSplit g)
 {
     constexpr int Q = kGlobalQpt;
-    __shared__ float4 s_p[kGlobalTile];
-    __shared__ float4 s_n[kGlobalTile];
+    __shared__ float4 s_pd[2 * kGlobalTile];
+    __shared__ float4 s_nd[2 * kGlobalTile];
     const int64_t q_first = int64_t(blockIdx.x) * kGlobalThreads * Q + threadIdx.x;
     const int64_t p_begin = int64_t(blockIdx.y) * g.chunk_pts;
     const int64_t p_end = p_begin + g.chunk_pts < a.n_pts ? p_begin + g.chunk_pts : a.n_pts;
@@ -821,7 +844,7 @@ __global__ void MLODS_GLOBAL_BOUNDS global_split_sums_kernel(GlobalArgs a, Globa
 #pragma unroll
         for (int c = 0; c < 9; ++c) tot[u][c] = 0.0;
     }
-    global_pair_sums<KTYPE, NSIG>(a, p_begin, p_end, lx, ly, lz, tot, s_p, s_n);
+    global_pair_sums<KTYPE, NSIG>(a, p_begin, p_end, lx, ly, lz, tot, s_pd, s_nd);
 #pragma unroll
     for (int u = 0; u < Q; ++u) {
         const int64_t qi = q_first + int64_t(u) * kGlobalThreads;
