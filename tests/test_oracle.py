@@ -129,3 +129,48 @@ def test_synth_tie_free_and_deterministic():
     assert p.mean() > 100.0  # translated far from the origin
     p, n = synth.torus_knot(5000, seed=4)
     assert p.shape == (5000, 3)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference shim not built in this checkout")
+@pytest.mark.parametrize("kind", ["gauss", "multi", "singular"])
+@pytest.mark.parametrize("cutoff,min_depth", [(1.4, 0), (2.0, 3), (3.0, 0)])
+def test_oracle_mlod_matches_live_reference_across_kernels(kind, cutoff, min_depth):
+    """The CPU-rule MLoD restatement against APSSOctree::projectCPU for every
+    kernel family, at the cutoffs of the reference's parameter files and
+    with a minimum traversal depth."""
+    pts, nrm = synth.rbf_blobs(4000, seed=17, translate=0.0)
+    pts = synth.make_tie_free(pts)
+    rt = oracle.RefTree(pts, nrm, 12)
+    ot = oracle.OracleTree(pts, nrm, 12)
+    diag = synth.bbox_diag(pts)
+    q = synth.perturbed_queries(pts, 0.01, seed=18)[:150]
+    k = make_kernel(kind, diag)
+    rp, _, _ = rt.project(q, 4, k, cutoff=cutoff, min_depth=min_depth)
+    op, _ = ot.project_mlod(q, 4, k, rule=1, cutoff=cutoff, min_depth=min_depth)
+    # the reference sums the moments in float32; the rational kernel's
+    # weights span many orders of magnitude, so its sums round more
+    # (measured up to 4.3e-6 diag against the FP64 restatement)
+    assert rel_err(op, rp, diag).max() < (1e-5 if kind == "singular" else 2e-6)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference shim not built in this checkout")
+@pytest.mark.parametrize("mode", ["knn", "ball", "global"])
+def test_oracle_apss_modes_match_live_reference(mode):
+    """kNN (k = 32), ball and global APSS restatements against the
+    reference's APSSOctree::projectCPU in those modes."""
+    pts, nrm = synth.torus(3000, seed=23)
+    pts = synth.make_tie_free(pts)
+    rt = oracle.RefTree(pts, nrm, 12)
+    ot = oracle.OracleTree(pts, nrm, 12)
+    diag = synth.bbox_diag(pts)
+    q = synth.perturbed_queries(pts, 0.01, seed=24)[:120]
+    k = make_kernel("gauss", diag)
+    if mode == "global":
+        rp, _, _ = rt.project(q, 3, k, mode=1)
+        op, _ = ot.project_global(q, 3, k)
+    else:
+        m = 2 if mode == "knn" else 3
+        r = 0.05 * diag
+        rp, _, _ = rt.project(q, 3, k, mode=m, k=32, ball_r=r)
+        op, _ = oracle.project_apss(pts, nrm, q, 3, k, mode=m - 2, k=32, ball_r=r, step_max=ot.radius)
+    assert rel_err(op, rp, diag).max() < 2e-6
