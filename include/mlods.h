@@ -293,7 +293,8 @@ int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_
  * counts the iterations it evaluated).  After a kNN projection: the
  * iterations that searched the octree for their neighbours; the others kept
  * the previous iteration's k points, which the step provably left the k
- * nearest, and only ranked them again.  Extension; synchronises. */
+ * nearest, and only ranked them again.  0 after a global or ball
+ * projection.  Extension; synchronises. */
 int mlods_last_iterations(mlods_tree t, int64_t* iterations);
 
 /* ---- batched projection over many resident trees (extension) ---------------
