@@ -32,7 +32,8 @@ extern "C" {
 #define MLODS_GAUSSIAN 0
 #define MLODS_SINGULAR 1          /* the reference's "rational" kernel */
 #define MLODS_GAUSSIAN_MULTIPLE 2
-#define MLODS_MAX_SIGMAS 16
+/* sigmas held in mlods_kernel itself; longer lists go through sigmas_ext */
+#define MLODS_INLINE_SIGMAS 16
 
 /* ---- projection modes (APSS subclasses and APSSOctree modes) ----------- */
 #define MLODS_MODE_MLOD 0    /* Fastapss::project (Fastapss.cu:439-455) */
@@ -46,14 +47,22 @@ extern "C" {
 
 /* Kernel value type; mirrors class Kernel (Kernel.h:24-60).  sigma and sigmas
  * are absolute lengths (already multiplied by the box radius, as
- * scene::setNewKernel does, scene.cpp:1025-1033). */
+ * scene::setNewKernel does, scene.cpp:1025-1033).  Like the reference's
+ * Kernel::sigmas (a std::vector, Kernel.cpp:110-128, copied to a device array
+ * of its size by GPUUtils.cu:262-272) the list has no fixed length: up to
+ * MLODS_INLINE_SIGMAS sigmas sit in sigmas[]; a longer list is read from
+ * sigmas_ext (n_sigmas host floats; sigmas[] is then ignored).  The library
+ * copies the list when the kernel is set or a request is submitted, so
+ * sigmas_ext need only live for that call.  The reference's own parameter
+ * files use up to 30 terms (data/rhino-holes.params). */
 typedef struct mlods_kernel {
     int32_t type;            /* MLODS_GAUSSIAN / _SINGULAR / _GAUSSIAN_MULTIPLE */
     float sigma;             /* Kernel::sigma */
     float exponent;          /* Kernel::exponent */
     float constant_shift;    /* Kernel::constant_shift */
-    int32_t n_sigmas;        /* Kernel::sigmas.size(), <= MLODS_MAX_SIGMAS */
-    float sigmas[MLODS_MAX_SIGMAS];
+    int32_t n_sigmas;        /* Kernel::sigmas.size() */
+    float sigmas[MLODS_INLINE_SIGMAS];
+    const float* sigmas_ext; /* n_sigmas sigmas when n_sigmas > MLODS_INLINE_SIGMAS, else unused (NULL) */
 } mlods_kernel;
 
 /* Projection options; mirror APSS::setScalingProtectionSphere / setMinDepth

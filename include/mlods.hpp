@@ -104,9 +104,11 @@ public:
         k.sigma = sigma;
         k.exponent = exponent;
         k.constant_shift = constant_shift;
-        if (sigmas.size() > MLODS_MAX_SIGMAS) throw Error(MLODS_ERR_CAPACITY, "mlods: too many sigmas");
         k.n_sigmas = int32_t(sigmas.size());
-        for (size_t i = 0; i < sigmas.size(); ++i) k.sigmas[i] = sigmas[i];
+        if (sigmas.size() > MLODS_INLINE_SIGMAS)
+            k.sigmas_ext = sigmas.data();  // read while this Kernel is alive and unchanged
+        else
+            for (size_t i = 0; i < sigmas.size(); ++i) k.sigmas[i] = sigmas[i];
         return k;
     }
 };
@@ -272,8 +274,11 @@ public:
     virtual void eraseFromGPU() { erasePointsFromGPU(); }
 
     // APSSOctree::projectCPU semantics (CPU blend rule, CPUUtils.cpp:621-636),
-    // evaluated on the device for one query.  Re-entrant; slow per call --
-    // batch callers should use project().
+    // evaluated on the device for one query.  Re-entrant: every call has its
+    // own device buffers, work counter and statistics, and re-applying
+    // unchanged options writes nothing, so host threads may call it at once
+    // on one tree, as the reference's OpenMP loops do (scene.cpp:982-986).
+    // Slow per call -- batch callers should use project().
     virtual void projectCPU(vec3 const& qStart, vec3& outputPoint, vec3& outputNormal, unsigned int n_iterations,
                             Kernel const& kernel = Kernel(), float stepMaxSize = -1.f) const
     {

@@ -24,7 +24,7 @@ MLODS_ERR_TIMEOUT = 5
 GAUSSIAN = 0
 SINGULAR = 1
 GAUSSIAN_MULTIPLE = 2
-MAX_SIGMAS = 16
+INLINE_SIGMAS = 16
 MAX_KNN = 32
 
 MODE_MLOD = 0
@@ -50,7 +50,8 @@ class mlods_kernel(C.Structure):
         ("exponent", C.c_float),
         ("constant_shift", C.c_float),
         ("n_sigmas", C.c_int32),
-        ("sigmas", C.c_float * MAX_SIGMAS),
+        ("sigmas", C.c_float * INLINE_SIGMAS),
+        ("sigmas_ext", C.POINTER(C.c_float)),
     ]
 
 

@@ -81,16 +81,22 @@ class Kernel:
         return 1.0
 
     def to_c(self) -> capi.mlods_kernel:
-        if len(self.sigmas) > capi.MAX_SIGMAS:
-            raise ValueError(f"at most {capi.MAX_SIGMAS} sigmas are supported")
+        """The C kernel value.  Sigma lists longer than the inline array
+        (the reference's files go up to 30 terms) travel through
+        ``sigmas_ext``; the array is kept alive on the returned structure."""
         k = capi.mlods_kernel()
         k.type = int(self.type)
         k.sigma = float(self.sigma)
         k.exponent = float(self.exponent)
         k.constant_shift = float(self.constant_shift)
         k.n_sigmas = len(self.sigmas)
-        for i, s in enumerate(self.sigmas):
-            k.sigmas[i] = float(s)
+        if len(self.sigmas) > capi.INLINE_SIGMAS:
+            ext = (C.c_float * len(self.sigmas))(*[float(s) for s in self.sigmas])
+            k._sigmas_keepalive = ext
+            k.sigmas_ext = C.cast(ext, C.POINTER(C.c_float))
+        else:
+            for i, s in enumerate(self.sigmas):
+                k.sigmas[i] = float(s)
         return k
 
 
@@ -576,6 +582,22 @@ class APSS:
                 raise ValueError("output arrays must be C-contiguous float32 with at least n rows")
         capi.check(self._lib.mlods_project(self.m_apssOctree.handle, self._q, int(nbOfVectors), int(n_iterations),
                                            float(stepMaxSize), capi.ptr(op), capi.ptr(on), C.c_void_p(0)))
+
+    def projectCPU(self, qStart, n_iterations: int, kernel: Kernel | None = None, stepMaxSize: float = -1.0):
+        """APSSOctree::projectCPU semantics (CPU blend rule, CPUUtils.cpp:621-636)
+        for one query or an (n, 3) array, evaluated on the device without
+        touching the query buffer: (points, normals).  Re-entrant: host threads
+        may call it at once on one tree."""
+        self._sync_params()
+        q = np.ascontiguousarray(np.asarray(qStart, np.float32).reshape(-1, 3))
+        op = np.empty_like(q)
+        on = np.empty_like(q)
+        capi.check(self._lib.mlods_project_host(self.m_apssOctree.handle, len(q), capi.ptr(q), capi.ptr(op),
+                                                capi.ptr(on), int(n_iterations), float(stepMaxSize),
+                                                capi.BLEND_CPU, C.c_void_p(0)))
+        if np.ndim(qStart) == 1:
+            return op[0], on[0]
+        return op, on
 
     def project_device(self, d_q, d_out_p, d_out_n, n_iterations: int, stepMaxSize: float = -1.0,
                        stream=None) -> None:

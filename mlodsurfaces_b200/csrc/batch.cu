@@ -242,9 +242,20 @@ int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* ou
             set_last_error("batch_create: tree %d is null", i);
             return MLODS_ERR_INVALID;
         }
+        if (trees[i]->device != trees[0]->device) {
+            delete b;
+            set_last_error("batch_create: tree %d is on device %d, tree 0 on device %d", i, trees[i]->device,
+                           trees[0]->device);
+            return MLODS_ERR_INVALID;
+        }
         b->trees.push_back(trees[i]);
     }
-    cudaGetDevice(&b->device);
+    b->device = trees[0]->device;
+    DeviceGuard guard(b->device);
+    if (guard.err != cudaSuccess) {
+        delete b;
+        return cuda_fail(guard.err, "batch_create: select device", __FILE__, __LINE__);
+    }
     cudaError_t e = cudaMalloc(&b->d_clouds, size_t(n_trees) * sizeof(CloudArgs));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_offsets, size_t(n_trees + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_frames, size_t(n_trees) * sizeof(BatchFrame));
@@ -264,6 +275,7 @@ int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* ou
 int mlods_batch_free(mlods_batch b)
 {
     if (!b) return MLODS_OK;
+    DeviceGuard guard(b->device);
     drop_graph(b);
     cudaFree(b->d_clouds);
     cudaFree(b->d_offsets);
@@ -286,6 +298,7 @@ int mlods_batch_project(mlods_batch b, const int64_t* offsets, const float* d_q,
         set_last_error("batch_project: bad arguments");
         return MLODS_ERR_INVALID;
     }
+    MLODS_ON_DEVICE(b->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int64_t total = 0;
     int rc = batch_prepare(b, offsets, d_q, d_out_pts, d_out_nrm, n_iterations, s, &total);
@@ -300,6 +313,7 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
         set_last_error("batch_tune: bad arguments");
         return MLODS_ERR_INVALID;
     }
+    MLODS_ON_DEVICE(b->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int64_t total = 0;
     int rc = batch_prepare(b, offsets, d_q, d_out_pts, d_out_nrm, n_iterations, s, &total);
@@ -347,6 +361,7 @@ int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int6
         set_last_error("batch_stats: no batch has run yet");
         return MLODS_ERR_STATE;
     }
+    MLODS_ON_DEVICE(b->device);
     int64_t h[6] = {0, 0, 0, 0, 0, 0};
     float ms = 0.f;
     MLODS_CUDA(cudaEventSynchronize(b->ev1));

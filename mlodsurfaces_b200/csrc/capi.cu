@@ -130,9 +130,13 @@ int validate_kernel(const mlods_kernel* k)
         set_last_error("unknown kernel type %d", k->type);
         return MLODS_ERR_INVALID;
     }
-    if (k->n_sigmas < 0 || k->n_sigmas > MLODS_MAX_SIGMAS) {
-        set_last_error("n_sigmas=%d out of range [0, %d]", k->n_sigmas, MLODS_MAX_SIGMAS);
-        return MLODS_ERR_CAPACITY;
+    if (k->n_sigmas < 0) {
+        set_last_error("n_sigmas=%d is negative", k->n_sigmas);
+        return MLODS_ERR_INVALID;
+    }
+    if (k->n_sigmas > MLODS_INLINE_SIGMAS && !k->sigmas_ext) {
+        set_last_error("n_sigmas=%d needs sigmas_ext (more than %d sigmas)", k->n_sigmas, MLODS_INLINE_SIGMAS);
+        return MLODS_ERR_INVALID;
     }
     if (k->type == MLODS_GAUSSIAN_MULTIPLE && k->n_sigmas == 0) {
         set_last_error("multi-Gaussian kernel needs at least one sigma");
@@ -145,7 +149,54 @@ int validate_kernel(const mlods_kernel* k)
     return MLODS_OK;
 }
 
-KernelConsts make_kernel_consts(const mlods_kernel& k)
+namespace
+{
+// Device tables of long multi-Gaussian sigma lists, one per distinct list and
+// device, kept until the process exits: trees, batches and server requests
+// may share them and a captured graph may still read them, so they are never
+// freed while the library is loaded.  At most kMaxSigmaTables per device.
+constexpr size_t kMaxSigmaTables = 4096;
+struct SigmaTable {
+    int device;
+    std::vector<float2> terms;
+    float2* d;
+};
+std::vector<SigmaTable> g_sigma_tables;
+std::mutex g_sigma_mu;
+
+int intern_sigma_table(const std::vector<float2>& terms, const float2** out)
+{
+    int dev = 0;
+    MLODS_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_sigma_mu);
+    size_t on_dev = 0;
+    for (const SigmaTable& t : g_sigma_tables) {
+        if (t.device != dev) continue;
+        ++on_dev;
+        if (t.terms.size() == terms.size() &&
+            std::memcmp(t.terms.data(), terms.data(), terms.size() * sizeof(float2)) == 0) {
+            *out = t.d;
+            return MLODS_OK;
+        }
+    }
+    if (on_dev >= kMaxSigmaTables) {
+        set_last_error("more than %zu distinct long sigma lists on device %d", kMaxSigmaTables, dev);
+        return MLODS_ERR_CAPACITY;
+    }
+    float2* d = nullptr;
+    MLODS_CUDA(cudaMalloc(&d, terms.size() * sizeof(float2)));
+    const cudaError_t e = cudaMemcpy(d, terms.data(), terms.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_fail(e, "sigma table upload", __FILE__, __LINE__);
+    }
+    g_sigma_tables.push_back(SigmaTable{dev, terms, d});
+    *out = d;
+    return MLODS_OK;
+}
+}  // namespace
+
+int make_kernel_consts(const mlods_kernel& k, KernelConsts* out)
 {
     KernelConsts c;
     std::memset(&c, 0, sizeof c);
@@ -158,12 +209,23 @@ KernelConsts make_kernel_consts(const mlods_kernel& k)
     c.g_scale = float(-log2e / (2.0 * sg * sg));
     const double v = std::max(double(k.constant_shift), 1e-4);
     c.num = float(std::pow(v, double(k.exponent)));
-    for (int i = 0; i < k.n_sigmas && i < MLODS_MAX_SIGMAS; ++i) {
-        const double s = k.sigmas[i];
-        c.ms_scale[i] = float(-log2e / (2.0 * s * s));
-        c.ms_w[i] = float(1.0 / (s * s * s));
+    const float* sig = k.n_sigmas > MLODS_INLINE_SIGMAS ? k.sigmas_ext : k.sigmas;
+    std::vector<float2> terms(static_cast<size_t>(std::max(k.n_sigmas, 0)));
+    for (int i = 0; i < k.n_sigmas; ++i) {
+        const double s = sig[i];
+        terms[size_t(i)] = make_float2(float(-log2e / (2.0 * s * s)), float(1.0 / (s * s * s)));
     }
-    return c;
+    if (k.n_sigmas <= MLODS_INLINE_SIGMAS) {
+        for (int i = 0; i < k.n_sigmas; ++i) {
+            c.ms_scale[i] = terms[size_t(i)].x;
+            c.ms_w[i] = terms[size_t(i)].y;
+        }
+    } else if (k.type == MLODS_GAUSSIAN_MULTIPLE) {
+        const int rc = intern_sigma_table(terms, &c.ms_ext);
+        if (rc != MLODS_OK) return rc;
+    }
+    *out = c;
+    return MLODS_OK;
 }
 
 // Ensures the tree's projection scratch holds `bytes` bytes (plus the stats
@@ -253,13 +315,20 @@ static int ensure_events(mlods_tree_s* T)
 // Global, kNN and ball APSS projections (GlobalAPSS::project, GlobalAPSS.cu:203-235;
 // APSSOctree::projectAPSSCPU, CPUUtils.cpp:690-737).
 static int project_apss_impl(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
-                             float step_max, cudaStream_t s)
+                             float step_max, cudaStream_t s, const CallScratch* cs)
 {
-    int rc = ensure_scratch(T, 0);
-    if (rc != MLODS_OK) return rc;
-    rc = ensure_events(T);
-    if (rc != MLODS_OK) return rc;
-    MLODS_CUDA(cudaMemsetAsync(T->d_stats, 0, 8 * sizeof(int64_t), s));
+    int64_t* stats = nullptr;
+    if (cs) {
+        stats = cs->stats;
+    } else {
+        int rc = ensure_scratch(T, 0);
+        if (rc != MLODS_OK) return rc;
+        rc = ensure_events(T);
+        if (rc != MLODS_OK) return rc;
+        stats = T->d_stats;
+    }
+    cudaEvent_t ev0 = cs ? nullptr : T->ev_start, ev1 = cs ? nullptr : T->ev_stop;
+    MLODS_CUDA(cudaMemsetAsync(stats, 0, 8 * sizeof(int64_t), s));
     const float sm = step_max < 0.f ? T->root_radius : step_max;
     const int mode = T->params.mode;
     if (mode == MLODS_MODE_GLOBAL) {
@@ -278,14 +347,18 @@ static int project_apss_impl(mlods_tree_s* T, int64_t n, const float* d_q, float
         g.o1 = T->origin[1];
         g.o2 = T->origin[2];
         g.kc = T->kc;
-        MLODS_CUDA(cudaEventRecord(T->ev_start, s));
+        if (ev0) MLODS_CUDA(cudaEventRecord(ev0, s));
         MLODS_CUDA(launch_global_apss(g, T->kc.type, s));
-        MLODS_CUDA(cudaEventRecord(T->ev_stop, s));
-        T->timed = true;
+        if (ev1) {
+            MLODS_CUDA(cudaEventRecord(ev1, s));
+            T->timed = true;
+        }
         return MLODS_OK;
     }
     GatherArgs g;
     fill_gather_args(T, g);
+    g.counter = reinterpret_cast<unsigned int*>(stats + 3);
+    g.stats = stats;
     g.q_in = d_q;
     g.nq = n;
     g.out_p = d_out_p;
@@ -306,16 +379,25 @@ static int project_apss_impl(mlods_tree_s* T, int64_t n, const float* d_q, float
         }
         g.ball_r = T->kernel.sigmas[0] * 3;
     }
-    MLODS_CUDA(cudaEventRecord(T->ev_start, s));
+    if (ev0) MLODS_CUDA(cudaEventRecord(ev0, s));
     MLODS_CUDA(launch_gather(g, mode == MLODS_MODE_KNN ? kGatherKnnApss : kGatherBallApss, T->kc.type,
                              sm_count_for_current_device(), s));
-    MLODS_CUDA(cudaEventRecord(T->ev_stop, s));
-    T->timed = true;
+    if (ev1) {
+        MLODS_CUDA(cudaEventRecord(ev1, s));
+        T->timed = true;
+    }
     return MLODS_OK;
 }
 
+size_t project_call_bytes(const mlods_tree_s* T, int64_t n)
+{
+    if (T->params.mode != MLODS_MODE_MLOD) return 0;
+    const bool reorder = T->params.reorder != 0 && n > 1;
+    return reorder ? al256(size_t(n) * 4) + query_order_temp_bytes(n) : 0;
+}
+
 int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
-                    float step_max, cudaStream_t s, int rule_override)
+                    float step_max, cudaStream_t s, int rule_override, const CallScratch* cs)
 {
     if (!T->kernel_set) {
         set_last_error("project: no kernel set (call mlods_set_kernel first)");
@@ -330,13 +412,25 @@ int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p
         return MLODS_ERR_INVALID;
     }
     if (T->params.mode != MLODS_MODE_MLOD)
-        return project_apss_impl(T, n, d_q, d_out_p, d_out_n, iters, step_max, s);
+        return project_apss_impl(T, n, d_q, d_out_p, d_out_n, iters, step_max, s, cs);
     const bool reorder = T->params.reorder != 0 && n > 1;
-    const size_t order_bytes = reorder ? al256(size_t(n) * 4) + query_order_temp_bytes(n) : 0;
-    int rc = ensure_scratch(T, order_bytes);
-    if (rc != MLODS_OK) return rc;
-    char* base = static_cast<char*>(T->d_scratch) + al256(8 * sizeof(int64_t));
-    MLODS_CUDA(cudaMemsetAsync(T->d_stats, 0, 8 * sizeof(int64_t), s));
+    const size_t order_bytes = project_call_bytes(T, n);
+    char* base = nullptr;
+    int64_t* stats = nullptr;
+    if (cs) {
+        if (cs->bytes < order_bytes) {
+            set_last_error("project: call scratch of %zu bytes, %zu needed", cs->bytes, order_bytes);
+            return MLODS_ERR_INVALID;
+        }
+        base = cs->base;
+        stats = cs->stats;
+    } else {
+        const int rc = ensure_scratch(T, order_bytes);
+        if (rc != MLODS_OK) return rc;
+        base = static_cast<char*>(T->d_scratch) + al256(8 * sizeof(int64_t));
+        stats = T->d_stats;
+    }
+    MLODS_CUDA(cudaMemsetAsync(stats, 0, 8 * sizeof(int64_t), s));
     uint32_t* d_order = nullptr;
     if (reorder) {
         d_order = reinterpret_cast<uint32_t*>(base);
@@ -349,9 +443,13 @@ int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p
     fill_cloud_args(T, a.cloud, d_q, d_out_p, d_out_n, iters, step_max, rule);
     a.order = d_order;
     a.nq = n;
-    a.counter = reinterpret_cast<unsigned int*>(T->d_stats + 3);
-    a.stats = T->d_stats;
-    rc = ensure_events(T);
+    a.counter = reinterpret_cast<unsigned int*>(stats + 3);
+    a.stats = stats;
+    if (cs) {
+        MLODS_CUDA(launch_mlod_project(a, T->kc.type, rule, sm_count_for_current_device(), s));
+        return MLODS_OK;
+    }
+    const int rc = ensure_events(T);
     if (rc != MLODS_OK) return rc;
     MLODS_CUDA(cudaEventRecord(T->ev_start, s));
     MLODS_CUDA(launch_mlod_project(a, T->kc.type, rule, sm_count_for_current_device(), s));
@@ -364,13 +462,15 @@ int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p
 
 using namespace mlods;
 
-#define CHECK_TREE(t)                                  \
-    do {                                               \
-        if (!(t)) {                                    \
-            set_last_error("null tree handle");        \
-            return MLODS_ERR_INVALID;                  \
-        }                                              \
-    } while (0)
+// Opens an entry point on a tree: rejects a null handle and makes the tree's
+// device current until the function returns (a process may hold trees on
+// several GPUs).
+#define CHECK_TREE(t)                            \
+    if (!(t)) {                                  \
+        set_last_error("null tree handle");      \
+        return MLODS_ERR_INVALID;                \
+    }                                            \
+    MLODS_ON_DEVICE((t)->device)
 
 extern "C" {
 
@@ -447,6 +547,7 @@ int mlods_tree_build(const float* pts, const float* nrm, int64_t n, int32_t max_
 int mlods_tree_free(mlods_tree t)
 {
     if (!t) return MLODS_OK;
+    MLODS_ON_DEVICE(t->device);
     free_tree_device(t);
     cudaFree(t->d_scratch);
     if (t->ev_start) cudaEventDestroy(t->ev_start);
@@ -489,10 +590,20 @@ int mlods_tree_export(mlods_tree t, int32_t* depth, int32_t* parent, int32_t* fi
 int mlods_set_kernel(mlods_tree t, const mlods_kernel* k)
 {
     CHECK_TREE(t);
-    const int rc = validate_kernel(k);
+    int rc = validate_kernel(k);
+    if (rc != MLODS_OK) return rc;
+    KernelConsts kc;
+    rc = make_kernel_consts(*k, &kc);
     if (rc != MLODS_OK) return rc;
     t->kernel = *k;
-    t->kc = make_kernel_consts(*k);
+    t->kernel.sigmas_ext = nullptr;  // the caller's array need not outlive this call
+    if (k->n_sigmas > MLODS_INLINE_SIGMAS) {
+        t->sigmas_long.assign(k->sigmas_ext, k->sigmas_ext + k->n_sigmas);
+        t->kernel.sigmas[0] = k->sigmas_ext[0];
+    } else {
+        t->sigmas_long.clear();
+    }
+    t->kc = kc;
     t->kernel_set = true;
     return MLODS_OK;
 }
@@ -517,7 +628,10 @@ int mlods_set_params(mlods_tree t, const mlods_params* p)
         set_last_error("unknown convergence mode %d", p->converge);
         return MLODS_ERR_INVALID;
     }
-    t->params = *p;
+    // unchanged options are not written again, so that callers which re-apply
+    // the same options before every call (the C++ mirror's projectCPU, run
+    // from many host threads at once) only read them
+    if (std::memcmp(&t->params, p, sizeof *p) != 0) t->params = *p;
     return MLODS_OK;
 }
 
@@ -644,16 +758,31 @@ int mlods_project_host(mlods_tree t, int64_t n, const float* q, float* out_pts, 
         return MLODS_ERR_INVALID;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    float* d = nullptr;
-    MLODS_CUDA(cudaMalloc(&d, size_t(n) * 9 * sizeof(float)));
+    // Everything this call writes on the device -- queries, results, work
+    // counter, statistics, query order -- is its own (stream-ordered memory
+    // from the library's pool), so calls from several host threads on one
+    // tree may overlap, as the reference's projectCPU calls do inside its
+    // OpenMP loops (scene.cpp:982-986).
+    const size_t io_bytes = al256(size_t(n) * 9 * sizeof(float));
+    const size_t stats_bytes = al256(8 * sizeof(int64_t));
+    const size_t call_bytes = project_call_bytes(t, n);
+    void* mem = nullptr;
+    MLODS_CUDA(scratch_alloc(&mem, io_bytes + stats_bytes + call_bytes, s));
+    float* d = static_cast<float*>(mem);
+    CallScratch cs;
+    cs.stats = reinterpret_cast<int64_t*>(static_cast<char*>(mem) + io_bytes);
+    cs.base = static_cast<char*>(mem) + io_bytes + stats_bytes;
+    cs.bytes = call_bytes;
     cudaError_t e = cudaMemcpyAsync(d, q, size_t(n) * 12, cudaMemcpyHostToDevice, s);
     int rc = MLODS_OK;
-    if (e == cudaSuccess) rc = project_buffers(t, n, d, d + 3 * n, d + 6 * n, n_iterations, step_max, s, blend_rule);
+    if (e == cudaSuccess)
+        rc = project_buffers(t, n, d, d + 3 * n, d + 6 * n, n_iterations, step_max, s, blend_rule, &cs);
     if (e == cudaSuccess && rc == MLODS_OK) e = cudaMemcpyAsync(out_pts, d + 3 * n, size_t(n) * 12, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && rc == MLODS_OK && out_nrm)
         e = cudaMemcpyAsync(out_nrm, d + 6 * n, size_t(n) * 12, cudaMemcpyDeviceToHost, s);
+    const cudaError_t ef = scratch_free(mem, s);
+    if (e == cudaSuccess) e = ef;
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d);
     if (rc != MLODS_OK) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "project_host", __FILE__, __LINE__);
     return MLODS_OK;

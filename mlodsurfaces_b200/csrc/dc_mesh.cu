@@ -589,6 +589,7 @@ int mlods_mesh_project(mlods_tree t, mlods_mesh m, int32_t n_iterations, void* s
         set_last_error("mesh project: bad arguments");
         return MLODS_ERR_INVALID;
     }
+    MLODS_ON_DEVICE(t->device);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (m->dev) {
         const int rc = dmesh_project(t, *m->dev, n_iterations, s);
@@ -606,6 +607,7 @@ int mlods_dc_mesh(mlods_tree t, mlods_dcgrid g, int32_t use_normals, int32_t ref
         set_last_error("dc mesh: bad arguments");
         return MLODS_ERR_INVALID;
     }
+    MLODS_ON_DEVICE(t->device);
     *out = nullptr;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int64_t n = int64_t(g->cells.size() / 4);

@@ -94,11 +94,19 @@ struct KernelConsts {
     float exponent;
     float g_scale;     // gaussian: -log2(e) / (2 sigma^2)
     float num;         // singular: max(shift, 1e-4)^exponent
-    float ms_scale[MLODS_MAX_SIGMAS];  // multi: -log2(e) / (2 sigma_i^2)
-    float ms_w[MLODS_MAX_SIGMAS];      // multi: 1 / sigma_i^3
+    float ms_scale[MLODS_INLINE_SIGMAS];  // multi: -log2(e) / (2 sigma_i^2)
+    float ms_w[MLODS_INLINE_SIGMAS];      // multi: 1 / sigma_i^3
+    // multi-Gaussian kernels with more than MLODS_INLINE_SIGMAS terms: all
+    // nsig pairs {ms_scale_i, ms_w_i} in device memory (a table the library
+    // keeps for the life of the process, shared by every kernel with the
+    // same sigmas); nullptr otherwise
+    const float2* ms_ext;
 };
 
-KernelConsts make_kernel_consts(const mlods_kernel& k);
+// Fills the constants of a validated kernel.  A multi-Gaussian kernel with
+// more than MLODS_INLINE_SIGMAS terms gets its device table on the current
+// device (allocated on first use of that sigma list).
+int make_kernel_consts(const mlods_kernel& k, KernelConsts* out);
 // Checks a kernel as mlods_set_kernel does; sets the error message.
 int validate_kernel(const mlods_kernel* k);
 
@@ -111,7 +119,14 @@ __device__ __forceinline__ float kernel_weight(const KernelConsts& kc, float d2)
         return exp2f(d2 * kc.g_scale) + kc.shift;
     } else if (KTYPE == MLODS_GAUSSIAN_MULTIPLE) {
         float s = 0.f;
-        for (int i = 0; i < kc.nsig; ++i) s = fmaf(exp2f(d2 * kc.ms_scale[i]), kc.ms_w[i], s);
+        if (kc.nsig <= MLODS_INLINE_SIGMAS) {
+            for (int i = 0; i < kc.nsig; ++i) s = fmaf(exp2f(d2 * kc.ms_scale[i]), kc.ms_w[i], s);
+        } else {
+            for (int i = 0; i < kc.nsig; ++i) {
+                const float2 t = __ldg(kc.ms_ext + i);
+                s = fmaf(exp2f(d2 * t.x), t.y, s);
+            }
+        }
         return s;
     } else {
         return kc.num * exp2f(-kc.exponent * __log2f(d2 + kc.shift));
@@ -128,6 +143,29 @@ int sm_count_for_current_device();
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 cudaError_t scratch_free(void* p, cudaStream_t s);
 
+// Makes `dev` the calling thread's current device for the life of the guard
+// and restores the previous one afterwards (a tree, batch or server holds
+// memory of the device it was made on; dev < 0 leaves the device alone).
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int dev)
+    {
+        if (dev < 0) return;
+        int cur = 0;
+        err = cudaGetDevice(&cur);
+        if (err != cudaSuccess || cur == dev) return;
+        err = cudaSetDevice(dev);
+        if (err == cudaSuccess) prev = cur;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 // Error-reporting helpers (host).
 void set_last_error(const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
@@ -137,5 +175,12 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
         cudaError_t _e = (call);                                                      \
         if (_e != cudaSuccess) return ::mlods::cuda_fail(_e, #call, __FILE__, __LINE__); \
     } while (0)
+
+// Opens an entry point that works on memory of device `dev`: makes it current
+// until the function returns, or fails with MLODS_ERR_CUDA.
+#define MLODS_ON_DEVICE(dev)                                                              \
+    ::mlods::DeviceGuard _mlods_device_guard(dev);                                        \
+    if (_mlods_device_guard.err != cudaSuccess)                                           \
+        return ::mlods::cuda_fail(_mlods_device_guard.err, "select device", __FILE__, __LINE__)
 
 }  // namespace mlods

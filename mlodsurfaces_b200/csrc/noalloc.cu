@@ -12,10 +12,13 @@
 // allocates nothing; the price is an upper bound on the queries per call.
 //
 // Setup happens once per device on the first call (cudaGetSymbolAddress of
-// the array, with that device current); make that first call outside any
-// stream capture.  Every call reuses the same array: calls that overlap in
-// time on one device (two streams, two host threads) race on it and must be
-// serialised by the caller.
+// the array, with the tree's device current); make that first call outside
+// any stream capture.  The address belongs to the device's context: if the
+// context is destroyed and recreated (cudaDeviceReset), the next call sees a
+// new context identifier and repeats the setup, which allocates nothing.
+// Every call reuses the same array: calls that overlap in time on one device
+// (two streams, two host threads) race on it and must be serialised by the
+// caller.
 #include <algorithm>
 #include <mutex>
 
@@ -36,9 +39,43 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
+struct ScratchSetup {
+    void* ptr = nullptr;           // device address of the array in that context
+    unsigned long long ctx = 0;    // identifier of the context it was taken in (0: unknown)
+};
+ScratchSetup g_scratch[kMaxDevices];
 
 inline size_t al256(size_t v) { return (v + 255) / 256 * 256; }
+
+// Identifier of the calling thread's current context (the driver's
+// cuCtxGetCurrent + cuCtxGetId, reached through the runtime so that the
+// library does not link the driver library), or 0 when there is none or the
+// driver cannot tell.
+unsigned long long current_context_id()
+{
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        (void)cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    void* ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx) return 0;
+    unsigned long long id = 0;
+    return get_id(ctx, &id) == 0 ? id : 0;
+}
 
 // Device address of this device's copy of the scratch array.
 int scratch_for_current_device(char** out)
@@ -50,7 +87,8 @@ int scratch_for_current_device(char** out)
         return MLODS_ERR_CAPACITY;
     }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    ScratchSetup& su = g_scratch[dev];
+    if (!su.ptr || current_context_id() != su.ctx) {
         const size_t need = kStatsBytes + al256(size_t(kNoAllocMaxQueries) * 4) +
                             query_order_temp_bytes(kNoAllocMaxQueries);
         if (need > kNoAllocScratchBytes) {
@@ -60,10 +98,14 @@ int scratch_for_current_device(char** out)
         }
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-        g_scratch_ptr[dev] = p;
+        if (e != cudaSuccess || !p) {
+            su.ptr = nullptr;
+            return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+        }
+        su.ptr = p;
+        su.ctx = current_context_id();  // the context now exists
     }
-    *out = static_cast<char*>(g_scratch_ptr[dev]);
+    *out = static_cast<char*>(su.ptr);
     return MLODS_OK;
 }
 
@@ -79,6 +121,7 @@ extern "C" int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float
         set_last_error("null tree handle");
         return MLODS_ERR_INVALID;
     }
+    MLODS_ON_DEVICE(t->device);
     if (!d_q || !d_out_pts || !d_out_nrm) {
         set_last_error("project_device_noalloc: null buffer");
         return MLODS_ERR_INVALID;

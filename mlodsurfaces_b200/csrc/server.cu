@@ -332,6 +332,7 @@ void stop_server(mlods_server_s* S)
             if (r->finished == r->taken) {
                 r->status = r->piece_status;
                 r->t_done = Clock::now();
+                ++S->completed;
             }
         }
         S->queue.clear();
@@ -388,7 +389,13 @@ int mlods_server_create(const mlods_tree* trees, int32_t n_trees, const mlods_se
             set_last_error("server create: tree %d is not in MLoD mode", i);
             return MLODS_ERR_INVALID;
         }
+        if (trees[i]->device != trees[0]->device) {
+            set_last_error("server create: tree %d is on device %d, tree 0 on device %d", i, trees[i]->device,
+                           trees[0]->device);
+            return MLODS_ERR_INVALID;
+        }
     }
+    MLODS_ON_DEVICE(trees[0]->device);
     auto* S = new (std::nothrow) mlods_server_s();
     if (!S) {
         set_last_error("server create: host allocation failed");
@@ -396,7 +403,7 @@ int mlods_server_create(const mlods_tree* trees, int32_t n_trees, const mlods_se
     }
     S->trees.assign(trees, trees + n_trees);
     S->cfg = c;
-    cudaGetDevice(&S->device);
+    S->device = trees[0]->device;
     for (int i = 0; i < c.n_streams; ++i) {
         auto* w = new (std::nothrow) Worker();
         cudaError_t e = w ? cudaStreamCreateWithFlags(&w->s, cudaStreamNonBlocking) : cudaErrorMemoryAllocation;
@@ -443,7 +450,16 @@ int mlods_server_submit(mlods_server s, int32_t tree, int64_t n, const float* q,
             return rc;
         }
         r->own_kernel = true;
-        r->kc = make_kernel_consts(*kernel);
+        int krc = MLODS_OK;
+        {
+            DeviceGuard guard(s->device);
+            krc = guard.err != cudaSuccess ? cuda_fail(guard.err, "server submit: select device", __FILE__, __LINE__)
+                                           : make_kernel_consts(*kernel, &r->kc);
+        }
+        if (krc != MLODS_OK) {
+            delete r;
+            return krc;
+        }
     }
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stopping) {

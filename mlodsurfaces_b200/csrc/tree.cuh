@@ -34,7 +34,8 @@ struct mlods_tree_s {
     int64_t bounds_stride = 0;
 
     // configuration
-    mlods_kernel kernel{};
+    mlods_kernel kernel{};                 // sigmas_ext is always null here
+    std::vector<float> sigmas_long;        // the sigmas when there are more than MLODS_INLINE_SIGMAS
     mlods::KernelConsts kc{};
     mlods_params params{};
     bool kernel_set = false;
@@ -79,10 +80,25 @@ namespace mlods
 // Builds the tree from device arrays (xyz float triples).
 int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t n, int max_depth, cudaStream_t s);
 void free_tree_device(mlods_tree_s* T);
+// Scratch of one projection call that must not share the tree's: a
+// zero-initialised-by-the-callee statistics block of 8 int64 (visits, max
+// stack, overflows, work counter, ...) and `bytes` bytes of device memory at
+// `base` (at least project_call_bytes).
+struct CallScratch {
+    int64_t* stats;
+    char* base;
+    size_t bytes;
+};
+// Device scratch bytes (beyond the statistics block) one projection call of n
+// queries needs with the tree's current options.
+size_t project_call_bytes(const mlods_tree_s* T, int64_t n);
 // Projects n device queries through the tree with its current kernel and
 // options (the mode selects MLoD, global, kNN or ball APSS).  Asynchronous.
+// Without `cs` the call uses the tree's own scratch, statistics and timing
+// events (calls on one tree must then be ordered); with `cs` it touches none of
+// them, so calls from several host threads may overlap.
 int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p, float* d_out_n, int iters,
-                    float step_max, cudaStream_t s, int rule_override = -1);
+                    float step_max, cudaStream_t s, int rule_override = -1, const CallScratch* cs = nullptr);
 struct CloudArgs;
 // Fills the per-tree part of a projection launch.
 void fill_cloud_args(const mlods_tree_s* T, CloudArgs& c, const float* d_q, float* d_out_p, float* d_out_n,

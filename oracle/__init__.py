@@ -22,21 +22,28 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libmlods_oracle.so"
 REF_SO = HERE / "_ref" / "libmlods_ref.so"
-REF_ROOT = Path(os.environ.get("MLODS_REF_ROOT", "/root/reference"))
+# The reference project's root (sources/, lib/, data/), from $MLODS_REF_ROOT;
+# the compiled checkers under _ref/ are used without it.
+REF_ROOT = Path(os.environ["MLODS_REF_ROOT"]) if os.environ.get("MLODS_REF_ROOT") else None
+REFDC_SO = HERE / "_ref" / "libmlods_refdc.so"
+REF_DATA = HERE / "_ref" / "data"
 
 _P = C.c_void_p
 _orc = None
 _ref = None
 
 
-def build(with_ref: bool = True) -> None:
-    """Compile the oracle (and the reference shim when the sources exist)."""
+def build(with_ref: bool = True, ref_root=None) -> None:
+    """Compile the oracle, and the reference checkers when the reference
+    project is at ``ref_root`` (default $MLODS_REF_ROOT)."""
+    root = Path(ref_root) if ref_root else REF_ROOT
     targets = ["oracle"]
-    if with_ref and (REF_ROOT / "sources" / "apss").is_dir():
-        targets.append("ref")
+    if with_ref and root is not None and (root / "sources" / "apss").is_dir():
+        targets += ["ref", "refdc", "refdata"]
         if shutil.which("nvcc"):  # the reference's own GPU path, for the GPU-side pins
             targets.append("refgpu")
-    subprocess.run(["make", "-s", "-C", str(HERE), f"REF_ROOT={REF_ROOT}"] + targets, check=True)
+    args = [f"REF_ROOT={root}"] if root is not None else []
+    subprocess.run(["make", "-s", "-C", str(HERE)] + args + targets, check=True)
 
 
 def ref_available() -> bool:
@@ -354,3 +361,169 @@ class RefGpuGlobal:
         if ms < 0:
             raise ValueError("query count out of the reference's launch range")
         return op, on, ms
+
+
+# ---------------------------------------------------------------- reference DC
+# The reference's own dual-contouring and point-set code (oracle/_ref/
+# libmlods_refdc.so, built from scene/upsample.cpp, dual-contouring/octree.h,
+# dual_contouring.h and apss/Pn.cpp).  Every projection it asks for is made by
+# a Python callable project(pts (n,3) float32, iters, step_max, cpu_rule) ->
+# (points, normals), so a test can hand it the projections of the library
+# under test and compare everything else bit for bit.
+REFDC_PROJECT_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,
+                               C.c_float, C.c_int32)
+_refdc = None
+
+
+def refdc_available() -> bool:
+    return REFDC_SO.exists()
+
+
+def refdc() -> C.CDLL:
+    global _refdc
+    if _refdc is None:
+        if not REFDC_SO.exists():
+            raise FileNotFoundError(f"{REFDC_SO} not built (needs the reference sources)")
+        lib = C.CDLL(os.fspath(REFDC_SO))
+        lib.refdc_grid_adaptive.restype = _P
+        lib.refdc_grid_adaptive.argtypes = [REFDC_PROJECT_FN, _P, C.c_int32, C.c_int32]
+        lib.refdc_grid_points.restype = _P
+        lib.refdc_grid_points.argtypes = [_P, C.c_int64, C.c_int32]
+        lib.refdc_grid_size.restype = C.c_int64
+        lib.refdc_grid_size.argtypes = [_P]
+        lib.refdc_grid_max_depth.restype = C.c_int32
+        lib.refdc_grid_max_depth.argtypes = [_P]
+        lib.refdc_grid_projected.restype = C.c_int64
+        lib.refdc_grid_projected.argtypes = [_P]
+        lib.refdc_grid_cells.argtypes = [_P, _P]
+        lib.refdc_grid_xform.argtypes = [_P, _P]
+        lib.refdc_grid_free.argtypes = [_P]
+        lib.refdc_mesh.restype = _P
+        lib.refdc_mesh.argtypes = [_P, REFDC_PROJECT_FN, _P, C.c_int32]
+        lib.refdc_mesh_sizes.argtypes = [_P] + [C.POINTER(C.c_int64)] * 5
+        lib.refdc_mesh_get.argtypes = [_P] * 8
+        lib.refdc_mesh_free.argtypes = [_P]
+        lib.refpn_load.restype = _P
+        lib.refpn_load.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_int64)]
+        lib.refpn_get.argtypes = [_P, _P, _P, C.POINTER(C.c_int64), _P, _P]
+        lib.refpn_free.argtypes = [_P]
+        lib.refpn_order.argtypes = [_P, C.c_int64, C.c_int32, _P]
+        _refdc = lib
+    return _refdc
+
+
+def _refdc_callback(project):
+    def cb(_ctx, n, pts, nrm, iters, step_max, cpu_rule):
+        try:
+            p = np.ctypeslib.as_array(pts, shape=(int(n), 3))
+            nn = np.ctypeslib.as_array(nrm, shape=(int(n), 3))
+            op, on = project(p.copy(), int(iters), float(step_max), int(cpu_rule))
+            p[:] = op
+            nn[:] = on
+        except BaseException as e:  # an exception cannot cross the C frames
+            _refdc_callback.error = e
+    return REFDC_PROJECT_FN(cb)
+
+
+def _refdc_raise():
+    err = getattr(_refdc_callback, "error", None)
+    _refdc_callback.error = None
+    if err is not None:
+        raise err
+
+
+class RefDCGrid:
+    """A DC grid made by the reference's OctreeGenerator and uniformize*."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def adaptive(cls, project, max_depth: int, cut: bool = False) -> "RefDCGrid":
+        """OctreeGenerator::generate + uniformize (scene.cpp:155-167, :1297)."""
+        cb = _refdc_callback(project)
+        h = refdc().refdc_grid_adaptive(cb, None, int(max_depth), int(bool(cut)))
+        _refdc_raise()
+        return cls(h)
+
+    @classmethod
+    def from_points(cls, pts, max_depth: int) -> "RefDCGrid":
+        """generateFromPoints + uniformizeFromPoints over [-1, 1]^3."""
+        pts = _f32(pts)
+        return cls(refdc().refdc_grid_points(_ptr(pts), len(pts), int(max_depth)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            refdc().refdc_grid_free(self._h)
+            self._h = None
+
+    def cells(self) -> np.ndarray:
+        out = np.empty((int(refdc().refdc_grid_size(self._h)), 4), np.int32)
+        refdc().refdc_grid_cells(self._h, _ptr(out))
+        return out
+
+    @property
+    def max_depth(self) -> int:
+        return int(refdc().refdc_grid_max_depth(self._h))
+
+    @property
+    def projected(self) -> int:
+        return int(refdc().refdc_grid_projected(self._h))
+
+    def xform(self) -> np.ndarray:
+        out = np.empty(12, np.float32)
+        refdc().refdc_grid_xform(self._h, _ptr(out))
+        return out
+
+    def mesh(self, project, refine_rounds: int = 2) -> dict:
+        """scene::computeDualContouring after the grid: corner field (one
+        projection per corner slot), extraction, transform, projection and
+        refine_rounds x (smooth, subdivide, project)."""
+        cb = _refdc_callback(project)
+        lib = refdc()
+        h = lib.refdc_mesh(self._h, cb, None, int(refine_rounds))
+        _refdc_raise()
+        try:
+            sz = [C.c_int64() for _ in range(5)]
+            lib.refdc_mesh_sizes(h, *[C.byref(s) for s in sz])
+            nc, nev, nei, nv, ni = (int(s.value) for s in sz)
+            out = {"corner_keys": np.empty((nc, 3), np.int32), "corner_vals": np.empty(nc, np.float32),
+                   "ext_vertices": np.empty((nev, 3), np.float32), "ext_indices": np.empty(nei, np.uint32),
+                   "vertices": np.empty((nv, 3), np.float32), "normals": np.empty((nv, 3), np.float32),
+                   "indices": np.empty(ni, np.uint32)}
+            lib.refdc_mesh_get(h, *[_ptr(out[k]) for k in ("corner_keys", "corner_vals", "ext_vertices",
+                                                             "ext_indices", "vertices", "normals", "indices")])
+        finally:
+            lib.refdc_mesh_free(h)
+        return out
+
+
+def refpn_load(path, normalize: bool = True) -> dict:
+    """Pn::load (Pn.cpp:102-164) with Pn::normalize (Pn.cpp:262-290)."""
+    lib = refdc()
+    n = C.c_int64()
+    h = lib.refpn_load(os.fsencode(str(path)), int(bool(normalize)), C.byref(n))
+    try:
+        pts = np.empty((int(n.value), 3), np.float32)
+        nrm = np.empty((int(n.value), 3), np.float32)
+        nn = C.c_int64()
+        off = np.empty(3, np.float32)
+        norme = np.empty(1, np.float32)
+        lib.refpn_get(h, _ptr(pts), _ptr(nrm), C.byref(nn), _ptr(off), _ptr(norme))
+    finally:
+        lib.refpn_free(h)
+    return {"pts": pts, "nrm": nrm[: int(nn.value)], "offset": off, "norme": float(norme[0])}
+
+
+def refpn_order(pts, grid: int = 64) -> np.ndarray:
+    """The positions after Pn::order(grid) (Pn.cpp:388-445)."""
+    pts = _f32(pts)
+    out = np.empty_like(pts)
+    refdc().refpn_order(_ptr(pts), len(pts), int(grid), _ptr(out))
+    return out
+
+
+def ref_data(name: str):
+    """Path of a copy of one of the reference's shipped files (data/), or None."""
+    p = REF_DATA / name
+    return p if p.exists() else None

@@ -49,7 +49,6 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define ORC_MAX_SIGMAS 64
 #define ORC_PI_REF 3.14159265 /* the reference's literal, Fastapss.cu:93 */
 
 enum { ORC_GAUSSIAN = 0, ORC_SINGULAR = 1, ORC_GAUSSIAN_MULTIPLE = 2 }; /* Kernel.h:37 */
@@ -59,7 +58,7 @@ typedef struct {
     int type;
     double sigma, exponent, shift;
     int nsig;
-    double sigmas[ORC_MAX_SIGMAS];
+    const double* sigmas; /* the caller's array, any length (Kernel::sigmas is a std::vector) */
 } orc_kernel;
 
 /* ---------------------------------------------------------------- tree */
@@ -368,8 +367,8 @@ static void kernel_from_args(orc_kernel* k, int type, double sigma, double expon
     k->sigma = sigma;
     k->exponent = exponent;
     k->shift = shift;
-    k->nsig = nsig < ORC_MAX_SIGMAS ? nsig : ORC_MAX_SIGMAS;
-    for (int i = 0; i < k->nsig; ++i) k->sigmas[i] = sigmas[i];
+    k->nsig = nsig;
+    k->sigmas = sigmas;
 }
 
 /* Kernel::w (Kernel.cpp:64-83) and KernelGPU::w (GPUUtils.cu:243-257), in double. */

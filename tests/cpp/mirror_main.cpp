@@ -5,6 +5,7 @@
 // writes the projections for the test to compare.
 #include <cstdio>
 #include <cstdlib>
+#include <thread>
 #include <vector>
 
 #include "mlods.hpp"
@@ -51,6 +52,24 @@ int main(int argc, char** argv)
     std::vector<vec3> cpu(q.size()), cpun(q.size());
     for (size_t i = 0; i < q.size(); ++i) apss.projectCPU(q[i], cpu[i], cpun[i], 10, k);
     write_vec3(argv[5], cpu);
+    // the same calls from 16 host threads at once, interleaved over the
+    // queries as an OpenMP static schedule with chunk 1 would deal them
+    // (scene.cpp:982-986): results must equal the serial ones bit for bit
+    std::vector<vec3> par(q.size()), parn(q.size());
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < 16; ++t)
+            pool.emplace_back([&, t] {
+                for (size_t i = size_t(t); i < q.size(); i += 16) apss.projectCPU(q[i], par[i], parn[i], 10, k);
+            });
+        for (std::thread& th : pool) th.join();
+    }
+    for (size_t i = 0; i < q.size(); ++i)
+        if (par[i].x != cpu[i].x || par[i].y != cpu[i].y || par[i].z != cpu[i].z || parn[i].x != cpun[i].x ||
+            parn[i].y != cpun[i].y || parn[i].z != cpun[i].z) {
+            std::fprintf(stderr, "threaded projectCPU differs from the serial result at query %zu\n", i);
+            return 4;
+        }
     if (argc > 7) {  // APSSOctree::cpuSphere at the queries: u0, u123, u4 per query
         std::vector<float> u;
         for (const vec3& x : q) {

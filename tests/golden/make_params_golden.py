@@ -3,9 +3,12 @@
 their fields decoded in the order of scene::loadParameters
 (sources/scene/scene.cpp:1183-1250).
 
-    python tests/golden/make_params_golden.py [reference_root]
+    python tests/golden/make_params_golden.py <reference_root>
+
+(reference_root: the reference project's root, or $MLODS_REF_ROOT)
 """
 import json
+import os
 import struct
 import sys
 from pathlib import Path
@@ -30,7 +33,10 @@ def decode(raw: bytes) -> dict:
 
 
 def main():
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MLODS_REF_ROOT")
+    if not arg:
+        sys.exit("usage: make_params_golden.py <reference_root> (or set MLODS_REF_ROOT)")
+    root = Path(arg)
     files = sorted((root / "data").glob("*.params"))
     data = {f.stem: {"hex": f.read_bytes().hex(), "fields": decode(f.read_bytes())} for f in files}
     out = Path(__file__).with_name("params_reference.json")

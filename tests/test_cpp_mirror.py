@@ -1,7 +1,8 @@
 """The C++ mirror of the reference classes (include/mlods.hpp) compiles
 against the C ABI and, driven like scene::projectPoints (ten one-iteration
 project calls on the in-place buffer) and scene::projectPointsOnCPU
-(projectCPU per query), agrees with the FP64 oracle."""
+(projectCPU per query, serially and from 16 host threads at once on one tree,
+bit-identical), agrees with the FP64 oracle."""
 import subprocess
 from pathlib import Path
 
@@ -20,7 +21,7 @@ ROOT = Path(__file__).resolve().parents[1]
 def compile_mirror(tmp: Path) -> Path:
     exe = tmp / "mirror_main"
     cmd = ["g++", "-std=c++17", "-O2", f"-I{ROOT / 'include'}", str(ROOT / "tests" / "cpp" / "mirror_main.cpp"),
-           "-o", str(exe), f"-L{LIB_PATH.parent}", "-lmlods", f"-Wl,-rpath,{LIB_PATH.parent}"]
+           "-o", str(exe), f"-L{LIB_PATH.parent}", "-lmlods", f"-Wl,-rpath,{LIB_PATH.parent}", "-pthread"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     return exe
 
