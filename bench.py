@@ -45,7 +45,7 @@ def parse_args():
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
-    ap.add_argument("--check-queries", type=int, default=2048, help="queries checked against the FP64 oracle")
+    ap.add_argument("--check-queries", type=int, default=65536, help="queries checked against the FP64 oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["precision", "knn", "global", "torus", "dc", "batch", "serve"],
                     default="precision",
@@ -116,23 +116,21 @@ def n_points_for(args):
     return args.n_points
 
 
-def config_dict(args, tree_mb=None):
+def config_dict(args):
+    """The workload, the same on both arms (what each arm evaluates with it
+    is the line's "semantics")."""
     spec = SPECS[args.workload]
     n = n_points_for(args)
-    d = {
+    return {
         "workload": spec["desc"],
         "n_points": n,
         "n_queries_per_gpu": n,
         "iterations": args.iters,
         "kernel": spec["kernel_desc"],
         "cutoff": spec["cutoff"],
-        "blend_rule": spec["rule_desc"],
         "parallelism": f"replicated tree, queries sharded, {args.gpus} GPU(s)",
         "l2": "L2 flushed (256 MB write) before every timed step",
     }
-    if tree_mb is not None:
-        d["tree_mb"] = round(tree_mb, 1)
-    return d
 
 
 class ClockSampler:
@@ -191,9 +189,19 @@ class ClockSampler:
 
 # DRAM bytes (read + write) of one projection launch of the default workload
 # (2M points, 2M queries, 10 iterations), from a single-pass ncu capture of
-# dram__bytes_read.sum + dram__bytes_write.sum: see
-# profiles/mlod_project_kernel_precision_2M_launches.md.
+# dram__bytes_read.sum + dram__bytes_write.sum of mlod_project_kernel on that
+# workload (python bench.py --steps 2 --warmup 1 under ncu --metrics ...).
 PROFILED_TRAFFIC = {("precision", 2_000_000, 10): 515.25e6 + 168.89e6}
+# Counters of the same kernel from a `--set full` capture of the workload
+# scaled to 200k points (one launch, -k mlod_project -s 3 -c 1): the limits
+# the algorithmic-bytes figure does not show.
+PROFILED_COUNTERS = {
+    "precision": {"capture": "ncu --set full, precision workload at 200k points, one launch",
+                  "issue_slots_active_pct": 84.4, "warp_instructions_per_node_visit": 10.6,
+                  "threads_active_per_instruction": 27.75, "l2_throughput_pct": 19.2, "l1_throughput_pct": 69.2,
+                  "fp32_fma_pipe_pct": 28.0, "alu_pipe_pct": 49.4, "xu_pipe_pct": 32.4, "fp64_pipe_pct": 4.3,
+                  "l2_hit_rate_pct": 99.9},
+}
 
 
 def max_over_ranks(values, world: int, device):
@@ -235,7 +243,7 @@ def synth_radius(pts) -> float:
     return float(np.linalg.norm(p.max(0).astype(np.float64) - p.min(0).astype(np.float64)) / 2)
 
 
-def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out, tol_out=None):
+def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out, tol_out=None, local_out=None, origin=None):
     """CPU baseline leg: the reference's own CPU path (oracle/_ref) timed on a
     bounded query sample with every host thread, and the GPU outputs checked
     against the FP64 oracle on a sample of queries."""
@@ -284,7 +292,14 @@ def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out, tol_out=Non
     out["err_vs_fp64"] = {"max": float(err.max()), "p99": float(np.percentile(err, 99)),
                           "max_beyond_f32_output_rounding": float(excess.max()),
                           "p99_beyond_f32_output_rounding": float(np.percentile(excess, 99)),
-                          "queries_checked": int(len(sel))}
+                          "queries_checked": int(len(sel)), "unit": "fraction of the bounding-box diagonal",
+                          "frame": "world coordinates (float32 output)"}
+    if local_out is not None:
+        el = np.linalg.norm(local_out[sel].astype(np.float64) - (x64 - origin), axis=1) / diag
+        out["err_vs_fp64"]["local_frame"] = {
+            "max": float(el.max()), "p99": float(np.percentile(el, 99)),
+            "note": "results written relative to the tree's origin (local_output): the error of the "
+                    "projection itself, without the rounding of a float32 coordinate far from the world origin"}
     if tol_out is not None:  # the converged outputs against the full-iteration FP64 result
         xt = tol_out[sel].astype(np.float64)
         errt = np.linalg.norm(xt - x64, axis=1) / diag
@@ -434,6 +449,16 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms_max = max_over_ranks([statistics.mean(e2e_ms)], world, dev)[0]
     e2e_value = job_throughput(world, len(q), 1, e2e_ms_max)
     out_host = d_p.cpu().numpy()
+    out_local = None
+    if not spec.get("knn") and not spec.get("global"):
+        # the same projection written relative to the tree's origin: the
+        # double iterate before the world-frame float rounding
+        f.local_output = True
+        step()
+        torch.cuda.synchronize(dev)
+        out_local = d_p.cpu().numpy()
+        f.local_output = False
+        f._sync_params()
 
     # ---- roofline of the projection kernel (algorithmic bytes per launch)
     mean_visits = statistics.mean(visits)
@@ -448,9 +473,17 @@ def run_ours(args, rank, world, local_rank):
     kms = statistics.mean(kern_ms)
     achieved = bytes_per_launch / (kms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
+    traffic = PROFILED_TRAFFIC.get((args.workload, n_points_for(args), args.iters))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": PROFILED_TRAFFIC.get((args.workload, n_points_for(args), args.iters)),
-                "note": f"{roof_note}; peak {peak_kind}"}
+                "traffic": traffic, "note": f"{roof_note}; peak {peak_kind}"}
+    if not spec.get("knn"):
+        # what actually limits the walk: the node records are reread from
+        # L1/L2, not from DRAM, and the instruction issue is the bound
+        roofline["served_from"] = "L1/L2: the algorithmic node bytes are rereads of records already on chip"
+        roofline["measured"] = dict(PROFILED_COUNTERS.get(args.workload, {}))
+        if traffic:
+            roofline["measured"]["dram_gbs"] = traffic / (kms / 1e3) / 1e9
+            roofline["measured"]["dram_frac_of_peak"] = traffic / (kms / 1e3) / 1e9 / peak
     if spec.get("global"):  # every pair evaluates len(sigmas) exponentials on the special-function units
         nsig = len(kernel.sigmas)
         ex2 = float(len(q)) * len(pts) * args.iters * nsig / (kms / 1e3) / 1e9
@@ -475,7 +508,9 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f32 (f64 sphere solve)",
         "data": spec["data"],
-        "config": config_dict(args, tree_mb),
+        "config": config_dict(args),
+        "semantics": spec["rule_desc"],
+        "tree_mb": round(tree_mb, 1),
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                        "per": f"request of {len(q)} queries x {args.iters} iterations"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h_q.numel() * 4),
@@ -495,7 +530,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result.update(cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, out_host, tol_out))
+        result.update(cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, out_host, tol_out, out_local,
+                                             np.array(inf.origin[:], np.float64)))
         if conv_tol is not None and "err_vs_fp64_converge_tol" in result:
             conv_tol["err_vs_fp64"] = result.pop("err_vs_fp64_converge_tol")
     return result
@@ -1079,6 +1115,7 @@ def run_reference(args, rank):
         "dtype": "f32",
         "data": spec["data"],
         "config": config_dict(args),
+        "semantics": f"the reference's CPU path (APSSOctree::{cpu_path_name(wl)}, its CPU blend rule)",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -81,9 +81,28 @@ typedef struct mlods_params {
     float ball_radius;   /* radius for MLODS_MODE_BALL; < 0 uses 3 * sigmas[0] (default 0.1) */
     int32_t blend_rule;  /* MLODS_BLEND_GPU (default) or MLODS_BLEND_CPU */
     int32_t reorder;     /* 1: process queries in Morton order (results are identical) */
-    float prune_tol;     /* reserved (0) */
+    float prune_tol;     /* extension, default 0 (off: the reference's walk).  > 0: kernel-weight
+                            pruning of the MLoD walk -- a node the walk would open is taken as an
+                            aggregate instead when a bound on what its whole subtree can weigh,
+                            f * w(distance to the node's bounding sphere) * its area (the kernel
+                            decreases with distance), is below prune_tol times the weight of one
+                            average sample at the query, w(0) * mean area.  Fewer node visits;
+                            results move by at most what the dropped subtrees could weigh.
+                            Applies to projections of one tree (queries_per_warp 1 or 2, which
+                            it requires); the grouped launches of a batch walk without it. */
     int32_t converge;    /* MLODS_CONVERGE_* (default MLODS_CONVERGE_OFF) */
     float converge_tol;  /* step length for MLODS_CONVERGE_TOL (absolute units) */
+    int32_t local_output; /* extension, default 0.  1: MLoD results are written relative to the
+                             tree's origin (mlods_tree_info.origin) instead of in world
+                             coordinates, so a cloud far from the world origin keeps full
+                             float precision in its output.  Ignored when the output buffer
+                             is the input buffer (the in-place query-buffer protocol). */
+    int32_t queries_per_warp; /* extension: the MLoD walk schedule.  1 (default): one query per warp.
+                                 2 or 4: that many queries that are neighbours in processing order
+                                 share one walk of the tree (node loads and traversal bookkeeping
+                                 paid once); each query's arithmetic is unchanged, only the order
+                                 of its float sums differs, so results agree with 1 to float
+                                 rounding.  mlods_tune_schedule picks it by timing. */
 } mlods_params;
 
 typedef struct mlods_tree_s* mlods_tree;
@@ -305,6 +324,14 @@ int mlods_last_stats(mlods_tree t, int64_t* node_visits, int64_t* rounds, int32_
  * nearest, and only ranked them again.  0 after a global or ball
  * projection.  Extension; synchronises. */
 int mlods_last_iterations(mlods_tree t, int64_t* iterations);
+/* Counters of the last MLoD projection on this tree.  lane_visits: node
+ * evaluations, where a node that the queries of one warp's shared walk
+ * (queries_per_warp = 2 or 4) all need is evaluated, and counted, once (equals
+ * node_visits of mlods_last_stats with one query per warp).  pruned: nodes
+ * that kernel-weight pruning (mlods_params.prune_tol) took as aggregates
+ * instead of opening, per query.  Either pointer may be NULL.  Extension;
+ * synchronises. */
+int mlods_last_walk_counts(mlods_tree t, int64_t* lane_visits, int64_t* pruned);
 
 /* ---- batched projection over many resident trees (extension) ---------------
  * No counterpart in the reference, which projects one tree per launch

@@ -67,6 +67,8 @@ class mlods_params(C.Structure):
         ("prune_tol", C.c_float),
         ("converge", C.c_int32),
         ("converge_tol", C.c_float),
+        ("local_output", C.c_int32),
+        ("queries_per_warp", C.c_int32),
     ]
 
 
@@ -156,6 +158,7 @@ SIGNATURES = {
     "mlods_project_host": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, C.c_int32, _P]),
     "mlods_last_stats": (C.c_int, [_P, _I64, _I64, _I32, _I64, C.POINTER(C.c_float)]),
     "mlods_last_iterations": (C.c_int, [_P, _I64]),
+    "mlods_last_walk_counts": (C.c_int, [_P, _I64, _I64]),
     "mlods_kernel_launches": (C.c_int64, []),
     "mlods_release_scratch": (C.c_int, []),
     "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),

@@ -499,6 +499,8 @@ class APSS:
         self.prune_tol = 0.0
         self.converge = capi.CONVERGE_OFF
         self.converge_tol = 0.0
+        self.local_output = False  # extension: results relative to the tree's origin (non in-place calls)
+        self.queries_per_warp = 1  # extension: the walk schedule (1 or 2 queries per warp)
         self._n_uploaded = 0
         q = C.c_void_p(0)
         capi.check(self._lib.mlods_queries_create(C.byref(q)))
@@ -528,6 +530,8 @@ class APSS:
         p.prune_tol = float(self.prune_tol)
         p.converge = int(self.converge)
         p.converge_tol = float(self.converge_tol)
+        p.local_output = 1 if self.local_output else 0
+        p.queries_per_warp = int(self.queries_per_warp)
         return p
 
     def _mode(self) -> int:
@@ -666,8 +670,11 @@ class APSS:
                                               C.byref(o), C.byref(ms)))
         it = C.c_int64(0)
         capi.check(self._lib.mlods_last_iterations(self.m_apssOctree.handle, C.byref(it)))
+        lv = C.c_int64(0)
+        pr = C.c_int64(0)
+        capi.check(self._lib.mlods_last_walk_counts(self.m_apssOctree.handle, C.byref(lv), C.byref(pr)))
         return {"node_visits": v.value, "rounds": r.value, "max_stack": m.value, "overflows": o.value,
-                "kernel_ms": ms.value, "iterations": it.value}
+                "kernel_ms": ms.value, "iterations": it.value, "lane_visits": lv.value, "pruned": pr.value}
 
     # -- options, GPUUtils.h:40-43
     def setScalingProtectionSphere(self, val: float) -> None:

@@ -228,6 +228,29 @@ int make_kernel_consts(const mlods_kernel& k, KernelConsts* out)
     return MLODS_OK;
 }
 
+// Kernel weight at squared distance d2 on the host, from the same constants
+// the device uses (Kernel::w, Kernel.cpp:64-83).
+static double kernel_weight_host(const KernelConsts& kc, double d2)
+{
+    const double ln2 = 0.6931471805599453;
+    if (kc.type == MLODS_GAUSSIAN) return std::exp(d2 * kc.g_scale * ln2) + kc.shift;
+    if (kc.type == MLODS_GAUSSIAN_MULTIPLE) {
+        double s = 0.0;
+        if (kc.nsig <= MLODS_INLINE_SIGMAS) {
+            for (int i = 0; i < kc.nsig; ++i) s += std::exp(d2 * kc.ms_scale[i] * ln2) * kc.ms_w[i];
+            return s;
+        }
+        std::vector<float2> t(static_cast<size_t>(kc.nsig));
+        if (cudaMemcpy(t.data(), kc.ms_ext, t.size() * sizeof(float2), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return 0.0;  // no pruning rather than a wrong threshold
+        }
+        for (const float2& v : t) s += std::exp(d2 * v.x * ln2) * v.y;
+        return s;
+    }
+    return double(kc.num) * std::exp(-double(kc.exponent) * std::log(d2 + kc.shift));
+}
+
 // Ensures the tree's projection scratch holds `bytes` bytes (plus the stats
 // block at its start).
 static int ensure_scratch(mlods_tree_s* T, size_t bytes)
@@ -264,6 +287,15 @@ void fill_cloud_args(const mlods_tree_s* T, CloudArgs& c, const float* d_q, floa
     c.q_in = d_q;
     c.out_p = d_out_p;
     c.out_n = d_out_n;
+    // in place, the buffer must stay in world coordinates for the next call
+    c.local_out = (T->params.local_output != 0 && d_out_p != d_q) ? 1 : 0;
+    c.qpw = T->params.queries_per_warp;
+    // kernel-weight pruning: a subtree is dropped below prune_tol times the
+    // weight of one average sample sitting at the query (w(0) x mean area)
+    c.prune_thr = 0.f;
+    if (T->params.prune_tol > 0.f && T->n_pts > 0)
+        c.prune_thr = float(double(T->params.prune_tol) * kernel_weight_host(T->kc, 0.0) *
+                            (double(T->root_mass) / double(T->n_pts)));
 }
 
 // Pruning margin of the neighbour searches: points may sit up to half a
@@ -445,6 +477,7 @@ int project_buffers(mlods_tree_s* T, int64_t n, const float* d_q, float* d_out_p
     a.nq = n;
     a.counter = reinterpret_cast<unsigned int*>(stats + 3);
     a.stats = stats;
+    a.queries_per_warp = T->params.queries_per_warp;
     if (cs) {
         MLODS_CUDA(launch_mlod_project(a, T->kc.type, rule, sm_count_for_current_device(), s));
         return MLODS_OK;
@@ -491,6 +524,8 @@ void mlods_default_params(mlods_params* p)
     p->prune_tol = 0.f;
     p->converge = MLODS_CONVERGE_OFF;
     p->converge_tol = 0.f;
+    p->local_output = 0;
+    p->queries_per_warp = 1;
 }
 
 int mlods_tree_build_device(const float* d_pts, const float* d_nrm, int64_t n, int32_t max_depth, void* stream,
@@ -624,8 +659,20 @@ int mlods_set_params(mlods_tree t, const mlods_params* p)
         set_last_error("min_depth must be >= 0");
         return MLODS_ERR_INVALID;
     }
+    if (!(p->prune_tol >= 0.f)) {
+        set_last_error("prune_tol must be >= 0");
+        return MLODS_ERR_INVALID;
+    }
+    if (p->prune_tol > 0.f && p->queries_per_warp == 4) {
+        set_last_error("prune_tol > 0 needs queries_per_warp 1 or 2");
+        return MLODS_ERR_INVALID;
+    }
     if (p->converge < MLODS_CONVERGE_OFF || p->converge > MLODS_CONVERGE_TOL) {
         set_last_error("unknown convergence mode %d", p->converge);
+        return MLODS_ERR_INVALID;
+    }
+    if (p->queries_per_warp != 1 && p->queries_per_warp != 2 && p->queries_per_warp != 4) {
+        set_last_error("queries_per_warp=%d: the walk takes 1, 2 or 4 queries per warp", p->queries_per_warp);
         return MLODS_ERR_INVALID;
     }
     // unchanged options are not written again, so that callers which re-apply
@@ -1023,6 +1070,16 @@ int mlods_last_iterations(mlods_tree t, int64_t* iterations)
     int64_t h[6] = {0, 0, 0, 0, 0, 0};
     if (t->d_stats) MLODS_CUDA(cudaMemcpy(h, t->d_stats, sizeof h, cudaMemcpyDeviceToHost));
     *iterations = h[5];
+    return MLODS_OK;
+}
+
+int mlods_last_walk_counts(mlods_tree t, int64_t* lane_visits, int64_t* pruned)
+{
+    CHECK_TREE(t);
+    int64_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (t->d_stats) MLODS_CUDA(cudaMemcpy(h, t->d_stats, sizeof h, cudaMemcpyDeviceToHost));
+    if (lane_visits) *lane_visits = h[6];
+    if (pruned) *pruned = h[7];
     return MLODS_OK;
 }
 

@@ -183,6 +183,47 @@ __global__ void vertex_kernel(const int4* __restrict__ cells, int64_t n_cells, i
     const int edges[12][2] = {{0, 1}, {0, 2}, {1, 3}, {2, 3}, {4, 5}, {4, 6}, {5, 7}, {6, 7},
                               {0, 4}, {1, 5}, {2, 6}, {3, 7}};
     const int4 c = cells[ci];
+    if (!corner_n) {
+        // The reference's zero normal field (scene.cpp:1355-1358): its QEF
+        // has A = 0, so the vertex is the mass point of the crossings
+        // (QEF::center, dual_contouring.h:98-111), computed here in float in
+        // the reference's order with every operation rounded once, so that
+        // the vertex is the reference's bit for bit: x = -fu / (fv - fu),
+        // p = x v + (1 - x) u (intersection, :116-121), sum += p, sum / count.
+        const float wf = 1.0f / float(int64_t(1) << max_depth);
+        float sum[3] = {0.f, 0.f, 0.f};
+        int cnt = 0;
+        for (int e = 0; e < 12; ++e) {
+            const int ka = edges[e][0], kb = edges[e][1];
+            const float fa = corner_f[8 * ci + ka], fb = corner_f[8 * ci + kb];
+            if ((fa < 0.f) == (fb < 0.f)) continue;
+            int64_t la[3], lb[3];
+            corner_lattice(c, ka, max_depth, la);
+            corner_lattice(c, kb, max_depth, lb);
+            const float x = -__fdiv_rn(fa, __fsub_rn(fb, fa));
+            const float omx = __fsub_rn(1.f, x);
+            for (int r = 0; r < 3; ++r) {
+                const float u = __fmul_rn(float(la[r]), wf), v = __fmul_rn(float(lb[r]), wf);
+                sum[r] = __fadd_rn(sum[r], __fadd_rn(__fmul_rn(x, v), __fmul_rn(omx, u)));
+            }
+            ++cnt;
+        }
+        // no crossing (a minimal edge through a larger cell, :163-169) or a
+        // NaN mass point: the cell centre (unit_octree::center, octree.h:808-812)
+        const float width = 1.0f / float(int64_t(1) << c.x);
+        const int pos[3] = {c.y, c.z, c.w};
+        float out[3];
+        bool bad = cnt == 0;
+        for (int r = 0; r < 3; ++r) {
+            out[r] = cnt ? __fdiv_rn(sum[r], float(cnt)) : 0.f;
+            bad = bad || isnan(out[r]);
+        }
+        if (bad)
+            for (int r = 0; r < 3; ++r) out[r] = __fmul_rn(__fadd_rn(float(pos[r]), 0.5f), width);
+        for (int r = 0; r < 3; ++r) vertex[3 * ci + r] = out[r];
+        n_cross[ci] = cnt;
+        return;
+    }
     const double w = 1.0 / double(int64_t(1) << max_depth);
     const double width = 1.0 / double(int64_t(1) << c.x);
     const double lo[3] = {c.y * width, c.z * width, c.w * width};

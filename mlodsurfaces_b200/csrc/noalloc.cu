@@ -170,6 +170,7 @@ extern "C" int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float
     a.nq = n;
     a.counter = reinterpret_cast<unsigned int*>(stats + 3);
     a.stats = stats;
+    a.queries_per_warp = t->params.queries_per_warp;
     MLODS_CUDA(launch_mlod_project(a, t->kc.type, rule, sm_count_for_current_device(), s));
     return MLODS_OK;
 }

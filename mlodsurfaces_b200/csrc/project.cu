@@ -40,19 +40,22 @@ namespace mlods
 namespace
 {
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr uint32_t kEntCount = 0x00FFFFFFu;
+constexpr uint32_t kEntCount = 0x00FFFFFFu;   // bits 0-23: nodes in the range
+constexpr int kEntLiveShift = 24;             // bits 24-27: the warp's queries the range is live for
 constexpr uint32_t kEntNoBlend = 1u << 31;
 constexpr uint32_t kEntLastOnly = 1u << 30;  // CPU rule multi-point leaf: only the last point is weighted
 constexpr float kPiRef = 3.14159265f;         // the reference's literal (Fastapss.cu:93)
 
-// Per-warp stack of sibling ranges.  e = {first, count|flags, f, A},
-// pg = {dP, g}; cnt repeats the count word so the pop scan reads 4 bytes.
-template <int CAP>
+// Per-warp stack of sibling ranges: h = {first, count | live mask | flags},
+// v[x] = {f, A, dP, g} of query x of the warp; cnt repeats the count word so
+// that the pop scan reads 4 bytes.
+template <int CAP, int QPW>
 struct WarpStack {
-    uint4 e[CAP];
-    float2 pg[CAP];
+    uint2 h[CAP];
+    float4 v[CAP][QPW];
     uint32_t cnt[CAP];
 };
+static_assert(sizeof(uint2) * 2 == sizeof(float4), "the stack arrays stay 16-byte aligned for even CAP");
 
 __device__ __forceinline__ int warp_incl_scan_i(int v)
 {
@@ -141,17 +144,35 @@ __device__ __forceinline__ float weight_n(const KernelConsts& kc, float d2)
 }
 
 struct WalkStats {
-    uint32_t visits = 0, rounds = 0, iterations = 0;
+    uint32_t pruned = 0;        // near nodes taken as aggregates by kernel-weight pruning (lane sum)
+    uint32_t visits = 0;        // query-node visits (nodes each query's own walk touches)
+    uint32_t lane_visits = 0;   // node evaluations of the warp (a node shared by the queries counts once)
+    uint32_t rounds = 0, iterations = 0;
     int max_top = 0;
     bool overflow = false;
 };
 
-// Projects query qi of one tree: n_iter iterations (fewer with a convergence
-// mode), result written to out_p/out_n (world frame).  KTYPE / RULE < 0 take
-// the kernel type / blend rule from c at run time.
-template <int KTYPE, int NSIG, int RULE, int CAP>
-__device__ __forceinline__ void project_query(const CloudArgs& c, uint32_t qi, WarpStack<CAP>& st, WalkStats& ws)
+// Projects the nq (<= QPW) queries qi[0..nq) of one tree together: n_iter
+// iterations each (fewer with a convergence mode), results written to
+// out_p / out_n (world frame, or local with c.local_out).  KTYPE / RULE < 0
+// take the kernel type / blend rule from c at run time.
+//
+// The queries of a warp are neighbours in Morton order, so their walks touch
+// nearly the same nodes: the warp walks the union once.  Every stack range
+// carries the set of queries it is live for (the queries for which the parent
+// was near); a lane evaluates its node for each live query -- distance,
+// blend weight, kernel weight -- and the node is opened for the queries that
+// find it near, or ends the walk as an aggregate for those that find it far.
+// Node loads, the pop / push bookkeeping and the leaf logic are paid once for
+// all the warp's queries.  Each query's arithmetic is exactly that of its own
+// walk (QPW = 1 is the one-query-per-warp walk); only the lane on which a
+// node's contribution is accumulated, and so the order of the float sums,
+// depends on the partner query.
+template <int KTYPE, int NSIG, int RULE, int CAP, int QPW, bool PRUNE = false>
+__device__ __forceinline__ void project_queries(const CloudArgs& c, const uint32_t (&qi)[QPW], int nq,
+                                                WarpStack<CAP, QPW>& st, WalkStats& ws)
 {
+    static_assert(QPW >= 1 && QPW <= 4, "one to four queries per warp");
     const bool gpu_rule = RULE < 0 ? c.rule == MLODS_BLEND_GPU : RULE == MLODS_BLEND_GPU;
     const int lane = threadIdx.x & 31;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -163,21 +184,40 @@ __device__ __forceinline__ void project_query(const CloudArgs& c, uint32_t qi, W
     const float cutoff = c.cutoff;
     const int min_depth = c.min_depth;
 
-    // the iterate, in the tree's local frame, in double
-    double qd[3] = {double(c.q_in[3 * int64_t(qi)]) - c.o0, double(c.q_in[3 * int64_t(qi) + 1]) - c.o1,
-                    double(c.q_in[3 * int64_t(qi) + 2]) - c.o2};
-    float nrm[3] = {0.f, 0.f, 0.f};
-    bool failed = false;
-    for (int it = 0; it < c.n_iter && !failed; ++it) {
-        const float qx = float(qd[0]), qy = float(qd[1]), qz = float(qd[2]);
-        float acc[9];
+    // lane x < nq holds the iterate of query x in the tree's local frame, in
+    // double; the other lanes shadow query 0 (their results are not written)
+    uint32_t my_q = qi[0];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) acc[k] = 0.f;
+    for (int x = 1; x < QPW; ++x)
+        if (lane == x && x < nq) my_q = qi[x];
+    double qd[3] = {double(c.q_in[3 * int64_t(my_q)]) - c.o0, double(c.q_in[3 * int64_t(my_q) + 1]) - c.o1,
+                    double(c.q_in[3 * int64_t(my_q) + 2]) - c.o2};
+    float nrm[3] = {0.f, 0.f, 0.f};
+    uint32_t live = (1u << nq) - 1u;  // queries still iterating (warp-uniform)
+    uint32_t failed = 0;
+    for (int it = 0; it < c.n_iter && live; ++it) {
+        float qx[QPW], qy[QPW], qz[QPW];
+        {
+            const float mx = float(qd[0]), my = float(qd[1]), mz = float(qd[2]);
+#pragma unroll
+            for (int x = 0; x < QPW; ++x) {  // lane x holds query x's iterate
+                qx[x] = __shfl_sync(kFull, mx, x);
+                qy[x] = __shfl_sync(kFull, my, x);
+                qz[x] = __shfl_sync(kFull, mz, x);
+            }
+        }
+        float acc[QPW][9];
+#pragma unroll
+        for (int x = 0; x < QPW; ++x)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc[x][k] = 0.f;
         int top = 1;
         if (lane == 0) {
-            st.e[0] = make_uint4(0u, 1u | kEntNoBlend, __float_as_uint(1.f), 0u);
-            st.pg[0] = make_float2(0.f, 0.f);
-            st.cnt[0] = 1u | kEntNoBlend;
+            const uint32_t w0 = 1u | kEntNoBlend | (live << kEntLiveShift);
+            st.h[0] = make_uint2(0u, w0);
+#pragma unroll
+            for (int x = 0; x < QPW; ++x) st.v[0][x] = make_float4(1.f, 0.f, 0.f, 0.f);
+            st.cnt[0] = w0;
         }
         __syncwarp();
         while (top > 0) {
@@ -197,18 +237,20 @@ __device__ __forceinline__ void project_query(const CloudArgs& c, uint32_t qi, W
             const int e = __popc(hb) - 1;
             const int r_start = 31 - __clz(hb);
             const int slot = top - 1 - e;
-            const uint4 E = st.e[slot];
-            const float2 PG = st.pg[slot];
+            const uint2 E = st.h[slot];
+            float4 V[QPW];
+#pragma unroll
+            for (int x = 0; x < QPW; ++x) V[x] = st.v[slot][x];
             const uint32_t r_first = E.x, r_cnt = E.y;
-            const float r_f = __uint_as_float(E.z), r_A = __uint_as_float(E.w);
-            const float r_dP = PG.x, r_g = PG.y;
+            const uint32_t r_live = (r_cnt >> kEntLiveShift) & ((1u << QPW) - 1u);
             const int r_len = partial ? 32 : int(r_cnt & kEntCount);
             const int old_top = top;
             if (!partial) top -= npop;
-            ws.visits += uint32_t(total);
+            ws.lane_visits += uint32_t(total);
+            ws.visits += QPW == 1 ? uint32_t(total) : __reduce_add_sync(kFull, active ? uint32_t(__popc(r_live)) : 0u);
             ++ws.rounds;
 
-            // ---- evaluate one node per lane
+            // ---- evaluate one node per lane, for each of its live queries
             const uint32_t node = r_first + uint32_t(lane - r_start);
             float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f), p4 = g4;
             float4 x4 = make_float4(0.f, 0.f, __uint_as_float(kLeafBit | 1u), 0.f);
@@ -218,94 +260,118 @@ __device__ __forceinline__ void project_query(const CloudArgs& c, uint32_t qi, W
                 x4 = __ldg(naux + node);
             }
             const float cr = cutoff * g4.w;
-            const float cx = g4.x - qx, cy = g4.y - qy, cz = g4.z - qz;
-            const float dist = sqrtf(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
-            float beta = 1.f, kcon = 0.f;
-            if (active && !(r_cnt & kEntNoBlend)) {
-                const float dC = fmaxf(dist - cr, 0.f);
-                const float t = __fdividef(r_dP, r_dP + dC);
-                beta = 0.5f - 0.5f * __cosf(kPiRef * t);
-                kcon = (1.f - beta) * r_g * (gpu_rule ? p4.w : 1.f);
-            }
-            // segmented sum over the range (blend ranges hold <= 8 lanes)
-            {
-                const int seg_end = r_start + r_len;
+            const bool blend = active && !(r_cnt & kEntNoBlend);
+            const int seg_end = r_start + r_len;
+            float dist[QPW], f[QPW], A[QPW];
+#pragma unroll
+            for (int x = 0; x < QPW; ++x) {
+                const float cx = g4.x - qx[x], cy = g4.y - qy[x], cz = g4.z - qz[x];
+                dist[x] = sqrtf(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
+                float beta = 1.f, kcon = 0.f;
+                if (blend && ((r_live >> x) & 1u)) {
+                    const float dC = fmaxf(dist[x] - cr, 0.f);
+                    const float t = __fdividef(V[x].z, V[x].z + dC);
+                    beta = 0.5f - 0.5f * __cosf(kPiRef * t);
+                    kcon = (1.f - beta) * V[x].w * (gpu_rule ? p4.w : 1.f);
+                }
+                // segmented sum over the range (blend ranges hold <= 8 lanes)
 #pragma unroll
                 for (int o = 1; o < 8; o <<= 1) {
                     const float nv = __shfl_down_sync(kFull, kcon, o);
                     if (lane + o < seg_end) kcon += nv;
                 }
+                const float K = __shfl_sync(kFull, kcon, r_start);
+                f[x] = V[x].x * beta;
+                A[x] = V[x].y + K;
             }
-            const float K = __shfl_sync(kFull, kcon, r_start);
-            float f = r_f * beta;
-            const float A = r_A + K;
             if (!gpu_rule && (r_cnt & kEntLastOnly) && (partial || node != r_first + uint32_t(r_len) - 1u))
-                f = 0.f;
+#pragma unroll
+                for (int x = 0; x < QPW; ++x) f[x] = 0.f;
 
-            const float px = p4.x - qx, py = p4.y - qy, pz = p4.z - qz;
-            const float d2 = fmaf(px, px, fmaf(py, py, pz * pz));
-            const float w = weight_n<KTYPE, NSIG>(c.kc, d2);
             const uint32_t info = __float_as_uint(x4.z);
             const uint32_t nfirst = __float_as_uint(x4.y);
             const bool leaf = (info & kLeafBit) != 0;
             const bool multi = (info & kMultiBit) != 0;
             const uint32_t cnt = node_count(info);
-            bool terminal = false, push = false;
-            uint32_t p_cnt = 0;
-            float p_dP = 0.f, p_g = 0.f;
-            if (active) {
-                if (leaf) {
-                    if (!multi) {
-                        terminal = true;
-                    } else {
-                        push = true;
-                        p_cnt = cnt | kEntNoBlend | (gpu_rule ? 0u : kEntLastOnly);
-                    }
-                } else if (node_depth(info) < min_depth) {
-                    push = true;
-                    p_cnt = cnt | kEntNoBlend;
-                } else if (dist > cr) {
-                    terminal = true;
-                } else {
-                    push = true;
-                    p_cnt = cnt;
-                    p_dP = cr - dist;
-                    p_g = f * w / (gpu_rule ? p4.w : float(cnt));
+            // opened for every live query whatever its distance: the points of
+            // a multi-point leaf, the children of a node above min_depth
+            const bool opens_all = leaf ? multi : node_depth(info) < min_depth;
+            uint32_t term = 0, near = 0;
+            if (active && !opens_all) {
+#pragma unroll
+                for (int x = 0; x < QPW; ++x) {
+                    if (!((r_live >> x) & 1u)) continue;
+                    if (leaf || dist[x] > cr) term |= 1u << x;
+                    else near |= 1u << x;
                 }
             }
-            if (terminal) {
-                const float4 n4 = __ldg(nnc + node);
-                const float coef = fmaf(f, w, A);
-                const float cm = coef * p4.w;
-                acc[0] += cm;
-                acc[1] = fmaf(coef, n4.x, acc[1]);
-                acc[2] = fmaf(coef, n4.y, acc[2]);
-                acc[3] = fmaf(coef, n4.z, acc[3]);
-                acc[4] = fmaf(cm, px, acc[4]);
-                acc[5] = fmaf(cm, py, acc[5]);
-                acc[6] = fmaf(cm, pz, acc[6]);
-                acc[7] = fmaf(coef, fmaf(px, n4.x, fmaf(py, n4.y, fmaf(pz, n4.z, n4.w))), acc[7]);
-                acc[8] = fmaf(coef, fmaf(d2, p4.w, x4.x), acc[8]);
+            if (PRUNE && near) {
+                // kernel-weight pruning (extension, off by default): a near
+                // node whose whole subtree can weigh no more than the
+                // threshold -- the kernel decreases with distance, so w at
+                // the distance to the node's bounding sphere bounds every
+                // point in it -- is taken as an aggregate instead of opened
+#pragma unroll
+                for (int x = 0; x < QPW; ++x) {
+                    if (!((near >> x) & 1u)) continue;
+                    const float dmin = fmaxf(dist[x] - g4.w, 0.f);
+                    const float wub = weight_n<KTYPE, NSIG>(c.kc, dmin * dmin);
+                    if (f[x] * wub * p4.w < c.prune_thr) {
+                        near &= ~(1u << x);
+                        term |= 1u << x;
+                        ++ws.pruned;
+                    }
+                }
+            }
+            const uint32_t child_live = active ? (opens_all ? r_live : near) : 0u;
+            const bool push = child_live != 0;
+            const uint32_t p_cnt = cnt | (child_live << kEntLiveShift) |
+                                   (opens_all ? (kEntNoBlend | (leaf && !gpu_rule ? kEntLastOnly : 0u)) : 0u);
+
+            float4 n4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (term) n4 = __ldg(nnc + node);
+            float pv_dP[QPW], pv_g[QPW];
+#pragma unroll
+            for (int x = 0; x < QPW; ++x) {
+                const float px = p4.x - qx[x], py = p4.y - qy[x], pz = p4.z - qz[x];
+                const float d2 = fmaf(px, px, fmaf(py, py, pz * pz));
+                const float w = weight_n<KTYPE, NSIG>(c.kc, d2);
+                pv_dP[x] = cr - dist[x];
+                pv_g[x] = f[x] * w / (gpu_rule ? p4.w : float(cnt));
+                if ((term >> x) & 1u) {
+                    const float coef = fmaf(f[x], w, A[x]);
+                    const float cm = coef * p4.w;
+                    acc[x][0] += cm;
+                    acc[x][1] = fmaf(coef, n4.x, acc[x][1]);
+                    acc[x][2] = fmaf(coef, n4.y, acc[x][2]);
+                    acc[x][3] = fmaf(coef, n4.z, acc[x][3]);
+                    acc[x][4] = fmaf(cm, px, acc[x][4]);
+                    acc[x][5] = fmaf(cm, py, acc[x][5]);
+                    acc[x][6] = fmaf(cm, pz, acc[x][6]);
+                    acc[x][7] = fmaf(coef, fmaf(px, n4.x, fmaf(py, n4.y, fmaf(pz, n4.z, n4.w))), acc[x][7]);
+                    acc[x][8] = fmaf(coef, fmaf(d2, p4.w, x4.x), acc[x][8]);
+                }
             }
             // ---- push child ranges (every lane has read its entry: the
             // shuffles above depend on those reads)
             __syncwarp();
             if (partial && lane == 0) {
-                uint4 rest = st.e[old_top - 1];
+                uint2 rest = st.h[old_top - 1];
                 rest.x += 32u;
                 rest.y -= 32u;
-                st.e[old_top - 1] = rest;
+                st.h[old_top - 1] = rest;
                 st.cnt[old_top - 1] = rest.y;
             }
             const uint32_t pm = __ballot_sync(kFull, push);
             const int npush = __popc(pm);
             if (top + npush > CAP) {
-                ws.overflow = true;  // the query is reported as failed
+                ws.overflow = true;  // the warp's live queries are reported as failed
             } else {
                 if (push) {
                     const int pos = top + __popc(pm & lt_mask);
-                    st.e[pos] = make_uint4(nfirst, p_cnt, __float_as_uint(f), __float_as_uint(A));
-                    st.pg[pos] = make_float2(p_dP, p_g);
+                    st.h[pos] = make_uint2(nfirst, p_cnt);
+#pragma unroll
+                    for (int x = 0; x < QPW; ++x) st.v[pos][x] = make_float4(f[x], A[x], pv_dP[x], pv_g[x]);
                     st.cnt[pos] = p_cnt;
                 }
                 top += npush;
@@ -313,75 +379,133 @@ __device__ __forceinline__ void project_query(const CloudArgs& c, uint32_t qi, W
             if (top > ws.max_top) ws.max_top = top;
             __syncwarp();
         }
-        ++ws.iterations;
-        float s[9];
+        ws.iterations += uint32_t(__popc(live));
+        // warp sums; lane x then fits query x (the other lanes repeat query 0)
+        float sv[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) s[k] = warp_sum_f(acc[k]);
-        double x[3];
-        if (ws.overflow || !fit_sphere(s, double(c.step_max), gpu_rule, x, nrm)) {
-            failed = true;
-            break;
+        for (int k = 0; k < 9; ++k) {
+            sv[k] = warp_sum_f(acc[0][k]);
+#pragma unroll
+            for (int x = 1; x < QPW; ++x) {
+                const float t = warp_sum_f(acc[x][k]);
+                if (lane == x) sv[k] = t;
+            }
         }
-        // the projection of the float query just evaluated
-        qd[0] = double(qx) + x[0];
-        qd[1] = double(qy) + x[1];
-        qd[2] = double(qz) + x[2];
-        if (c.conv_mode == MLODS_CONVERGE_EXACT) {
-            // the next iteration would evaluate the same float query: every
-            // remaining iteration returns this result again
-            if (float(qd[0]) == qx && float(qd[1]) == qy && float(qd[2]) == qz) break;
-        } else if (c.conv_mode == MLODS_CONVERGE_TOL) {
-            if (x[0] * x[0] + x[1] * x[1] + x[2] * x[2] < double(c.conv_tol) * double(c.conv_tol)) break;
+        const bool mine = lane < QPW && ((live >> lane) & 1u);
+        double xr[3] = {0.0, 0.0, 0.0};
+        const bool ok = !ws.overflow && fit_sphere(sv, double(c.step_max), gpu_rule, xr, nrm);
+        bool stop = false;
+        if (mine && !ok) {
+            failed |= 1u << lane;
+            stop = true;
+        } else if (mine) {
+            // the projection of the float query just evaluated
+            const float fx = float(qd[0]), fy = float(qd[1]), fz = float(qd[2]);
+            qd[0] = double(fx) + xr[0];
+            qd[1] = double(fy) + xr[1];
+            qd[2] = double(fz) + xr[2];
+            if (c.conv_mode == MLODS_CONVERGE_EXACT) {
+                // the next iteration would evaluate the same float query:
+                // every remaining iteration returns this result again
+                stop = float(qd[0]) == fx && float(qd[1]) == fy && float(qd[2]) == fz;
+            } else if (c.conv_mode == MLODS_CONVERGE_TOL) {
+                stop = xr[0] * xr[0] + xr[1] * xr[1] + xr[2] * xr[2] < double(c.conv_tol) * double(c.conv_tol);
+            }
         }
+        live &= ~__ballot_sync(kFull, mine && stop);
     }
-    if (lane == 0) {
-        float* op = c.out_p + 3 * int64_t(qi);
-        float* on = c.out_n + 3 * int64_t(qi);
+    failed = __reduce_or_sync(kFull, failed);
+    if (lane < nq) {
+        float* op = c.out_p + 3 * int64_t(my_q);
+        float* on = c.out_n + 3 * int64_t(my_q);
         // on failure (Fastapss.cu:385-391) the point stays where the failing
         // iteration started and the normal is zero
-        op[0] = float(qd[0] + c.o0);
-        op[1] = float(qd[1] + c.o1);
-        op[2] = float(qd[2] + c.o2);
-        on[0] = failed ? 0.f : nrm[0];
-        on[1] = failed ? 0.f : nrm[1];
-        on[2] = failed ? 0.f : nrm[2];
+        const bool bad = (failed >> lane) & 1u;
+        if (c.local_out) {
+            op[0] = float(qd[0]);
+            op[1] = float(qd[1]);
+            op[2] = float(qd[2]);
+        } else {
+            op[0] = float(qd[0] + c.o0);
+            op[1] = float(qd[1] + c.o1);
+            op[2] = float(qd[2] + c.o2);
+        }
+        on[0] = bad ? 0.f : nrm[0];
+        on[1] = bad ? 0.f : nrm[1];
+        on[2] = bad ? 0.f : nrm[2];
     }
 }
 
-__device__ __forceinline__ void flush_stats(int64_t* stats, int64_t visits, int64_t rounds, int max_top,
-                                            int64_t overflows, int64_t iterations)
-{
-    if ((threadIdx.x & 31) != 0 || !stats) return;
-    atomicAdd(reinterpret_cast<unsigned long long*>(&stats[0]), (unsigned long long)visits);
-    atomicAdd(reinterpret_cast<unsigned long long*>(&stats[4]), (unsigned long long)rounds);
-    atomicAdd(reinterpret_cast<unsigned long long*>(&stats[5]), (unsigned long long)iterations);
-    atomicMax(reinterpret_cast<unsigned long long*>(&stats[1]), (unsigned long long)max_top);
-    if (overflows) atomicAdd(reinterpret_cast<unsigned long long*>(&stats[2]), (unsigned long long)overflows);
-}
-
-template <int KTYPE, int NSIG, int RULE, int CAP>
-__global__ void __launch_bounds__(kProjectThreads, kProjectMinBlocks) mlod_project_kernel(ProjectArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31;
-    WarpStack<CAP>& st = reinterpret_cast<WarpStack<CAP>*>(smem_raw)[threadIdx.x >> 5];
-    int64_t visits = 0, rounds = 0, overflows = 0, iterations = 0;
-    int max_top = 0;
-    for (;;) {
-        unsigned int qs = 0;
-        if (lane == 0) qs = atomicAdd(a.counter, 1u);
-        qs = __shfl_sync(kFull, qs, 0);
-        if (int64_t(qs) >= a.nq) break;
-        const uint32_t qi = a.order ? a.order[qs] : qs;
-        WalkStats ws;
-        project_query<KTYPE, NSIG, RULE, CAP>(a.cloud, qi, st, ws);
+// Per-warp totals of the walks, kept in 64 bits across queries.
+struct WarpTotals {
+    WalkStats sum;  // max_top only
+    int64_t overflows = 0;
+    int64_t visits = 0, lane_visits = 0, rounds = 0, iterations = 0, pruned = 0;
+    __device__ void add(const WalkStats& ws, int nq)
+    {
+        pruned += ws.pruned;
         visits += ws.visits;
+        lane_visits += ws.lane_visits;
         rounds += ws.rounds;
         iterations += ws.iterations;
-        max_top = max(max_top, ws.max_top);
-        overflows += ws.overflow ? 1 : 0;
+        if (ws.max_top > sum.max_top) sum.max_top = ws.max_top;
+        overflows += ws.overflow ? nq : 0;
     }
-    flush_stats(a.stats, visits, rounds, max_top, overflows, iterations);
+    __device__ void flush(int64_t* stats)
+    {
+        if ((threadIdx.x & 31) != 0 || !stats) return;
+        atomicAdd(reinterpret_cast<unsigned long long*>(&stats[0]), (unsigned long long)visits);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&stats[4]), (unsigned long long)rounds);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&stats[5]), (unsigned long long)iterations);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&stats[6]), (unsigned long long)lane_visits);
+        atomicMax(reinterpret_cast<unsigned long long*>(&stats[1]), (unsigned long long)sum.max_top);
+        if (overflows) atomicAdd(reinterpret_cast<unsigned long long*>(&stats[2]), (unsigned long long)overflows);
+    }
+    // per-lane counts, summed over the warp first
+    __device__ void flush_pruned(int64_t* stats)
+    {
+        unsigned long long p = (unsigned long long)pruned;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(kFull, p, o);
+        if ((threadIdx.x & 31) == 0 && stats && p) atomicAdd(reinterpret_cast<unsigned long long*>(&stats[7]), p);
+    }
+};
+
+// Blocks per SM the single-tree kernel is compiled for and its stack
+// capacity: one query per warp fits 48 registers at 10 blocks; two and four
+// need more registers (64, 96) and wider stack entries.
+template <int QPW>
+struct WalkShape {
+    static constexpr int kMinBlocks = QPW == 1 ? kProjectMinBlocks : (QPW == 2 ? kProjectPairMinBlocks : 5);
+    static constexpr int kCap = QPW == 1 ? kProjectStackCap : kProjectPairStackCap;
+};
+
+template <int KTYPE, int NSIG, int RULE, int QPW, bool PRUNE>
+__global__ void __launch_bounds__(kProjectThreads, WalkShape<QPW>::kMinBlocks) mlod_project_kernel(ProjectArgs a)
+{
+    constexpr int CAP = WalkShape<QPW>::kCap;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    WarpStack<CAP, QPW>& st = reinterpret_cast<WarpStack<CAP, QPW>*>(smem_raw)[threadIdx.x >> 5];
+    WarpTotals tot;
+    for (;;) {
+        unsigned int qs = 0;
+        if (lane == 0) qs = atomicAdd(a.counter, unsigned(QPW));
+        qs = __shfl_sync(kFull, qs, 0);
+        if (int64_t(qs) >= a.nq) break;
+        const int nq = int(min(int64_t(QPW), a.nq - int64_t(qs)));
+        uint32_t qi[QPW];
+#pragma unroll
+        for (int x = 0; x < QPW; ++x) {
+            const uint32_t s = qs + uint32_t(x < nq ? x : 0);
+            qi[x] = a.order ? __ldg(a.order + s) : s;
+        }
+        WalkStats ws;
+        project_queries<KTYPE, NSIG, RULE, CAP, QPW, PRUNE>(a.cloud, qi, nq, st, ws);
+        tot.add(ws, nq);
+    }
+    tot.flush(a.stats);
+    tot.flush_pruned(a.stats);
 }
 
 // Many trees, one launch per kernel specialisation.  The warps of a launch
@@ -396,12 +520,12 @@ __global__ void __launch_bounds__(kProjectThreads, kBatchMinBlocks)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpStack<CAP>& st = reinterpret_cast<WarpStack<CAP>*>(smem_raw)[warp];
-    CloudArgs* cache = reinterpret_cast<CloudArgs*>(smem_raw + (kProjectThreads / 32) * sizeof(WarpStack<CAP>)) + warp;
+    WarpStack<CAP, 1>& st = reinterpret_cast<WarpStack<CAP, 1>*>(smem_raw)[warp];
+    CloudArgs* cache =
+        reinterpret_cast<CloudArgs*>(smem_raw + (kProjectThreads / 32) * sizeof(WarpStack<CAP, 1>)) + warp;
     int cached = -1;
     int64_t c_lo = 0, c_hi = 0, c_base = 0;  // slot range and first global index of the cached cloud
-    int64_t visits = 0, rounds = 0, overflows = 0, iterations = 0;
-    int max_top = 0;
+    WarpTotals tot;
     for (;;) {
         unsigned int qs = 0;
         if (lane == 0) qs = atomicAdd(counter, 1u);
@@ -428,17 +552,14 @@ __global__ void __launch_bounds__(kProjectThreads, kBatchMinBlocks)
                 __syncwarp();
             }
         }
-        const uint32_t qi = uint32_t(g - c_base);
+        const uint32_t qi[1] = {uint32_t(g - c_base)};
         WalkStats ws;
-        project_query<KTYPE, NSIG, RULE, CAP>(*cache, qi, st, ws);
-        visits += ws.visits;
-        rounds += ws.rounds;
-        iterations += ws.iterations;
-        max_top = max(max_top, ws.max_top);
-        overflows += ws.overflow ? 1 : 0;
+        project_queries<KTYPE, NSIG, RULE, CAP, 1>(*cache, qi, 1, st, ws);
+        tot.add(ws, 1);
         __syncwarp();  // every lane is done with the cached arguments
     }
-    flush_stats(b.stats, visits, rounds, max_top, overflows, iterations);
+    tot.flush(b.stats);
+    tot.flush_pruned(b.stats);
 }
 
 template <typename Kern>
@@ -453,33 +574,37 @@ int64_t persistent_grid(Kern kern, size_t smem, int64_t work_warps, int sm_count
     return grid < 1 ? 1 : grid;
 }
 
-template <int KTYPE, int NSIG, int RULE>
+template <int KTYPE, int NSIG, int RULE, int QPW>
 cudaError_t launch_typed(const ProjectArgs& a, int sm_count, cudaStream_t s)
 {
-    constexpr int CAP = kProjectStackCap;
-    auto kern = mlod_project_kernel<KTYPE, NSIG, RULE, CAP>;
-    const size_t smem = size_t(kProjectThreads / 32) * sizeof(WarpStack<CAP>);
+    constexpr int CAP = WalkShape<QPW>::kCap;
+    // kernel-weight pruning is a variant of its own (four queries per warp
+    // has none), so the default walk carries none of its code
+    constexpr bool kCanPrune = QPW <= 2;
+    auto kern = (kCanPrune && a.cloud.prune_thr > 0.f) ? mlod_project_kernel<KTYPE, NSIG, RULE, QPW, kCanPrune>
+                                                       : mlod_project_kernel<KTYPE, NSIG, RULE, QPW, false>;
+    const size_t smem = size_t(kProjectThreads / 32) * sizeof(WarpStack<CAP, QPW>);
     cudaError_t e = cudaSuccess;
-    const int64_t grid = persistent_grid(kern, smem, a.nq, sm_count, &e);
+    const int64_t grid = persistent_grid(kern, smem, (a.nq + QPW - 1) / QPW, sm_count, &e);
     if (e != cudaSuccess) return e;
     kern<<<unsigned(grid), kProjectThreads, smem, s>>>(a);
     note_launch();
     return cudaGetLastError();
 }
 
-template <int RULE>
+template <int RULE, int QPW>
 cudaError_t launch_rule(const ProjectArgs& a, int ktype, int sm_count, cudaStream_t s)
 {
-    if (ktype == MLODS_GAUSSIAN) return launch_typed<MLODS_GAUSSIAN, 0, RULE>(a, sm_count, s);
-    if (ktype == MLODS_SINGULAR) return launch_typed<MLODS_SINGULAR, 0, RULE>(a, sm_count, s);
+    if (ktype == MLODS_GAUSSIAN) return launch_typed<MLODS_GAUSSIAN, 0, RULE, QPW>(a, sm_count, s);
+    if (ktype == MLODS_SINGULAR) return launch_typed<MLODS_SINGULAR, 0, RULE, QPW>(a, sm_count, s);
     switch (a.cloud.kc.nsig) {
-    case 2: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 2, RULE>(a, sm_count, s);
-    case 3: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 3, RULE>(a, sm_count, s);
-    case 4: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 4, RULE>(a, sm_count, s);
-    case 5: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 5, RULE>(a, sm_count, s);
-    case 6: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 6, RULE>(a, sm_count, s);
-    case 8: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 8, RULE>(a, sm_count, s);
-    default: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 0, RULE>(a, sm_count, s);
+    case 2: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 2, RULE, QPW>(a, sm_count, s);
+    case 3: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 3, RULE, QPW>(a, sm_count, s);
+    case 4: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 4, RULE, QPW>(a, sm_count, s);
+    case 5: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 5, RULE, QPW>(a, sm_count, s);
+    case 6: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 6, RULE, QPW>(a, sm_count, s);
+    case 8: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 8, RULE, QPW>(a, sm_count, s);
+    default: return launch_typed<MLODS_GAUSSIAN_MULTIPLE, 0, RULE, QPW>(a, sm_count, s);
     }
 }
 
@@ -551,7 +676,7 @@ cudaError_t launch_batch_typed(const BatchArgs& b, const BatchGroup& g, unsigned
 {
     constexpr int CAP = kProjectStackCap;
     auto kern = mlod_batch_kernel<KTYPE, NSIG, RULE, CAP>;
-    const size_t smem = size_t(kProjectThreads / 32) * (sizeof(WarpStack<CAP>) + sizeof(CloudArgs));
+    const size_t smem = size_t(kProjectThreads / 32) * (sizeof(WarpStack<CAP, 1>) + sizeof(CloudArgs));
     cudaError_t e = cudaSuccess;
     int64_t grid = persistent_grid(kern, smem, g.slot_end - g.slot_begin, sm_count, &e);
     if (e != cudaSuccess) return e;
@@ -601,8 +726,14 @@ cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_i
 
 cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int sm_count, cudaStream_t s)
 {
-    if (rule == MLODS_BLEND_GPU) return launch_rule<MLODS_BLEND_GPU>(a, ktype, sm_count, s);
-    return launch_rule<MLODS_BLEND_CPU>(a, ktype, sm_count, s);
+    if (rule == MLODS_BLEND_GPU) {
+        if (a.queries_per_warp == 4) return launch_rule<MLODS_BLEND_GPU, 4>(a, ktype, sm_count, s);
+        if (a.queries_per_warp == 2) return launch_rule<MLODS_BLEND_GPU, 2>(a, ktype, sm_count, s);
+        return launch_rule<MLODS_BLEND_GPU, 1>(a, ktype, sm_count, s);
+    }
+    if (a.queries_per_warp == 4) return launch_rule<MLODS_BLEND_CPU, 4>(a, ktype, sm_count, s);
+    if (a.queries_per_warp == 2) return launch_rule<MLODS_BLEND_CPU, 2>(a, ktype, sm_count, s);
+    return launch_rule<MLODS_BLEND_CPU, 1>(a, ktype, sm_count, s);
 }
 
 int64_t batch_solo_min_queries(int sm_count)
@@ -650,6 +781,7 @@ void plan_batch_groups(const CloudArgs* clouds, const int64_t* q_offsets, int n_
             g.slot_begin = g.slot_end = slot;
             if (own) {
                 g.solo = i;
+                g.queries_per_warp = clouds[i].qpw;
                 g.solo_args = clouds[i];
                 const int64_t o = q_offsets[i];
                 g.solo_args.q_in = clouds[i].q_in - 3 * o;
@@ -681,6 +813,7 @@ cudaError_t launch_mlod_batch(const BatchArgs& b, const std::vector<BatchGroup>&
             a.nq = g.slot_end - g.slot_begin;
             a.counter = counter;
             a.stats = b.stats;
+            a.queries_per_warp = g.queries_per_warp;
             const cudaError_t e = launch_mlod_project(a, g.ktype, g.rule, sm_count, s);
             if (e != cudaSuccess) return e;
             continue;

@@ -20,10 +20,19 @@ namespace mlods
 #ifndef MLODS_PROJECT_STACK_CAP
 #define MLODS_PROJECT_STACK_CAP 160
 #endif
-constexpr int kProjectThreads = 128;                          // 4 warps per block, one query per warp at a time
+#ifndef MLODS_PROJECT_PAIR_MIN_BLOCKS
+#define MLODS_PROJECT_PAIR_MIN_BLOCKS 8
+#endif
+#ifndef MLODS_PROJECT_PAIR_STACK_CAP
+#define MLODS_PROJECT_PAIR_STACK_CAP 128
+#endif
+constexpr int kProjectThreads = 128;                          // 4 warps per block, one walk per warp at a time
 constexpr int kProjectMinBlocks = MLODS_PROJECT_MIN_BLOCKS;  // 10 -> 40 warps per SM, <= 48 registers
 constexpr int kProjectStackCap = MLODS_PROJECT_STACK_CAP;    // sibling ranges per warp (28 bytes each)
 constexpr int kBatchMinBlocks = MLODS_BATCH_MIN_BLOCKS;      // the batch kernel keeps more registers (64)
+// the paired walk (two queries per warp): more registers and a wider stack entry
+constexpr int kProjectPairMinBlocks = MLODS_PROJECT_PAIR_MIN_BLOCKS;
+constexpr int kProjectPairStackCap = MLODS_PROJECT_PAIR_STACK_CAP;
 
 // One tree and its projection settings, plus the query buffers it serves.
 struct CloudArgs {
@@ -38,8 +47,11 @@ struct CloudArgs {
     int conv_mode;          // MLODS_CONVERGE_*
     float conv_tol;
     const float* q_in;      // world xyz
-    float* out_p;           // world xyz (may alias q_in)
+    float* out_p;           // world xyz (may alias q_in), or relative to the origin with local_out
     float* out_n;
+    int local_out;          // 1: out_p holds the result relative to (o0, o1, o2)
+    int qpw;                // the tree's walk schedule (queries per warp) for launches of its own
+    float prune_thr;        // > 0: kernel-weight pruning threshold (prune_tol * w(0) * mean sample area)
 };
 
 struct ProjectArgs {
@@ -47,7 +59,9 @@ struct ProjectArgs {
     const uint32_t* order;  // processing order (Morton), or nullptr
     int64_t nq;
     unsigned int* counter;  // work counter, zero before launch
-    int64_t* stats;         // [0] visits, [1] max stack, [2] overflows, [3] counter, [4] rounds, [5] iterations
+    int64_t* stats;         // [0] query-node visits, [1] max stack, [2] overflows, [3] counter, [4] rounds,
+                            // [5] query-iterations, [6] lane visits (a node shared by a warp's queries once)
+    int queries_per_warp = 1;  // 1, or 2: consecutive queries of `order` share one walk
 };
 
 // Many trees in one launch: clouds[c] serves the global query range
@@ -81,6 +95,7 @@ struct BatchGroup {
     int64_t slot_begin, slot_end;
     int solo = -1;
     CloudArgs solo_args;
+    int queries_per_warp = 1;  // the solo cloud's walk schedule
 };
 
 // Per-cloud frame used to key queries: the group-ordered rank of the cloud

@@ -20,6 +20,7 @@ struct mlods_tree_s {
     float BB[3] = {0, 0, 0};
     double origin[3] = {0, 0, 0};
     float root_radius = 0.f;  // BBOX::radius of the root box, float as the reference
+    float root_mass = 0.f;    // sum of the sample areas (the root's m0)
 
     // device data
     mlods::NodeArrays nodes{};             // n_nodes + n_extra records (one allocation at nodes.geom)

@@ -1,8 +1,9 @@
 // tree_build.cu -- device octree build with the reference's exact topology.
 //
 // The reference builds its octree on the host by recursive midpoint splits
-// (CPUUtils.cpp:271-329): split = (bb + BB) / 2 in double, child boxes stored
-// as float, 1 point per leaf, depth <= maxDepth.  Each axis splits
+// (CPUUtils.cpp:271-329): split = (bb + BB) / 2.0 with the sum of the float
+// bounds rounded to float first (so every split is a float value), child
+// boxes stored as float, 1 point per leaf, depth <= maxDepth.  Each axis splits
 // independently, so the split values form one binary table per axis that
 // depends only on the root box.  A point's cell at every depth is therefore a
 // binary descent through three tables, its path a Morton code (x lowest bit,
@@ -592,7 +593,11 @@ int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t 
             const int64_t so = (int64_t(1) << d) - 1;
             const int64_t w = int64_t(1) << d;
             for (int64_t k = 0; k < w; ++k) {
-                const double sp = (double(B[bo + k]) + double(B[bo + k + 1])) / 2.0;
+                // `(bb[0] + BB[0]) / 2.0` with float bounds (CPUUtils.cpp:286-288):
+                // the sum rounds to float before the division in double, so
+                // the split is itself a float value
+                const float bsum = B[bo + k] + B[bo + k + 1];
+                const double sp = double(bsum) / 2.0;
                 S[so + k] = sp;
                 B[bn + 2 * k] = B[bo + k];
                 B[bn + 2 * k + 1] = float(sp);
@@ -793,6 +798,11 @@ int build_tree(mlods_tree_s* T, const float* d_pts, const float* d_nrm, int64_t 
     note_launch();
     NODE_CHECK(cudaGetLastError(), "sorted points");
     NODE_CHECK(cudaStreamSynchronize(s), "sync build");
+    {
+        float4 root_pm;  // {pbar, m0} of the root: the total sample area
+        NODE_CHECK(cudaMemcpy(&root_pm, T->nodes.pm, sizeof root_pm, cudaMemcpyDeviceToHost), "root mass");
+        T->root_mass = root_pm.w;
+    }
     cudaFree(nodebuf);
     cudaFree(bump.base);
 #undef NODE_CHECK

@@ -200,12 +200,13 @@ def perturbed_queries(points: np.ndarray, rel_sigma: float = 0.01, seed: int = 3
 
 def split_tables(lo: float, hi: float, depth: int):
     """Per-axis split values (float64) and child bounds (float32) of the
-    reference recursion (CPUUtils.cpp:286-292, :321-323) for one axis."""
+    reference recursion (CPUUtils.cpp:286-292, :321-323) for one axis: the
+    float bounds are added in float, then halved in double."""
     bounds = [np.array([lo, hi], dtype=F32)]
     splits = []
     for _ in range(depth):
         b = bounds[-1]
-        s = (b[:-1].astype(np.float64) + b[1:].astype(np.float64)) / 2.0
+        s = (b[:-1] + b[1:]).astype(F32).astype(np.float64) / 2.0
         splits.append(s)
         nb = np.empty(2 * len(b) - 1, dtype=F32)
         nb[0::2] = b

@@ -8,7 +8,7 @@
  * (mlodsurfaces_b200, libmlods.so) never links, loads or calls it.
  *
  * What it restates, function by function (paths inside the reference project):
- *   - octree build: recursive midpoint split in double of float bounds, child
+ *   - octree build: recursive midpoint split (float sum of the float bounds, halved in double), child
  *     boxes stored as float, 1 point per leaf, depth <= max_depth, child slot
  *     c = xi + 2 yi + 4 zi                     sources/apss/CPUUtils.cpp:271-329
  *   - tight root box                            sources/apss/CPUUtils.cpp:571-579
@@ -127,7 +127,9 @@ static void build_rec(bnode_vec* nv, int32_t id, const float* pts, int32_t* idx,
     memcpy(bb, nv->v[id].bb, sizeof bb);
     memcpy(BB, nv->v[id].BB, sizeof BB);
     double split[3];
-    for (int a = 0; a < 3; ++a) split[a] = ((double)bb[a] + (double)BB[a]) / 2.0;
+    /* the reference's `(bb[0] + BB[0]) / 2.0` (CPUUtils.cpp:286-288): the two
+     * float bounds are added in float, then halved in double */
+    for (int a = 0; a < 3; ++a) split[a] = (double)(float)(bb[a] + BB[a]) / 2.0;
     int32_t cnt[8] = {0};
     unsigned char* slot = (unsigned char*)malloc((size_t)(e - s));
     for (int32_t i = s; i < e; ++i) {

@@ -230,3 +230,38 @@ def test_tiny_clouds(name, rule):
     assert np.array_equal(op[failed], q[failed])
     scale = max(float(np.ptp(pts, axis=0).max()), 1.0)
     assert np.abs(op[~failed] - x64[~failed]).max(initial=0.0) < TOL_DIAG * scale
+
+
+@pytest.mark.parametrize("kind", ["gauss", "multi", "singular"])
+@pytest.mark.parametrize("rule", [BLEND_GPU, BLEND_CPU])
+@pytest.mark.parametrize("qpw", [2, 4])
+def test_paired_walk_matches_fp64_and_single_walk(torus20k, kind, rule, qpw):
+    """Two or four queries per warp: each query's arithmetic is its own
+    walk's, only the order of the float sums changes -- FP64 within 1e-5
+    diag, and the one-query walk within float rounding of the moments; the
+    same query-node visits."""
+    pts, nrm, q, ot = torus20k
+    diag = synth.bbox_diag(pts)
+    k = make_kernel(kind, diag)
+    t = APSSOctree()
+    t.build(pts, nrm)
+    outs = {}
+    for w in (1, qpw):
+        f = Fastapss(t)
+        f.copyToGPU(k, len(q))
+        f.setScalingProtectionSphere(3.0)
+        f.blend_rule = rule
+        f.queries_per_warp = w
+        f.copyPointsToGPU(len(q), q)
+        op = np.empty((len(q), 3), np.float32)
+        on = np.empty((len(q), 3), np.float32)
+        f.project(len(q), op, on, 10, k)
+        outs[w] = (op, on, f.last_stats())
+    rp, rn = ot.project_mlod(q, 10, k, rule=rule, cutoff=3.0)
+    op2, on2, st2 = outs[qpw]
+    assert rel_err(op2, rp, diag).max() < TOL_DIAG
+    assert rel_err(op2, outs[1][0], diag).max() < 1e-6
+    ok = np.linalg.norm(rn, axis=1) > 0.5
+    assert ((on2[ok] * rn[ok]).sum(1) > 1 - 1e-4).all()
+    assert st2["overflows"] == 0
+    assert st2["node_visits"] == outs[1][2]["node_visits"]  # query-node visits: the reference's walk
