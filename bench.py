@@ -54,11 +54,15 @@ def parse_args():
                          "CPU-path semantics; dc: 5M-point torus knot, adaptive depth-9 dual contouring; "
                          "batch: 64 resident clouds (about 40M points) in one graph launch")
     ap.add_argument("--clouds", type=int, default=64)
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="batch: also time the reference's own GPU kernel on every cloud (slow: host tree builds)")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: request arrivals per second (0 = 70%% of "
                                                                "the measured capacity)")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
     ap.add_argument("--serve-batch", type=int, default=1 << 18, help="serve: largest batch in queries")
     ap.add_argument("--dc-depth", type=int, default=9)
+    ap.add_argument("--schedule", choices=["auto", "1", "2", "4"], default="auto",
+                    help="MLoD walk schedule (queries per warp); auto: the library's autotuner picks it")
     return ap.parse_args()
 
 
@@ -192,6 +196,7 @@ class ClockSampler:
 # dram__bytes_read.sum + dram__bytes_write.sum of mlod_project_kernel on that
 # workload (python bench.py --steps 2 --warmup 1 under ncu --metrics ...).
 PROFILED_TRAFFIC = {("precision", 2_000_000, 10): 515.25e6 + 168.89e6}
+PRUNE_TOL = 1e-6  # the tolerance of the reported kernel-weight pruning run
 # Counters of the same kernel from a `--set full` capture of the workload
 # scaled to 200k points (one launch, -k mlod_project -s 3 -c 1): the limits
 # the algorithmic-bytes figure does not show.
@@ -243,7 +248,8 @@ def synth_radius(pts) -> float:
     return float(np.linalg.norm(p.max(0).astype(np.float64) - p.min(0).astype(np.float64)) / 2)
 
 
-def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out, tol_out=None, local_out=None, origin=None):
+def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out, tol_out=None, local_out=None, origin=None,
+                           prune_out=None):
     """CPU baseline leg: the reference's own CPU path (oracle/_ref) timed on a
     bounded query sample with every host thread, and the GPU outputs checked
     against the FP64 oracle on a sample of queries."""
@@ -300,6 +306,13 @@ def cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, gpu_out, tol_out=Non
             "max": float(el.max()), "p99": float(np.percentile(el, 99)),
             "note": "results written relative to the tree's origin (local_output): the error of the "
                     "projection itself, without the rounding of a float32 coordinate far from the world origin"}
+    if prune_out is not None:  # the pruned walk against the unpruned FP64 result
+        xp = prune_out[sel].astype(np.float64)
+        errp = np.linalg.norm(xp - x64, axis=1) / diag
+        excp = np.linalg.norm(np.maximum(np.abs(xp - x64) - half_ulp, 0.0), axis=1) / diag
+        out["err_vs_fp64_pruned"] = {"max": float(errp.max()), "p99": float(np.percentile(errp, 99)),
+                                     "max_beyond_f32_output_rounding": float(excp.max()),
+                                     "queries_checked": int(len(sel))}
     if tol_out is not None:  # the converged outputs against the full-iteration FP64 result
         xt = tol_out[sel].astype(np.float64)
         errt = np.linalg.norm(xt - x64, axis=1) / diag
@@ -343,6 +356,17 @@ def run_ours(args, rank, world, local_rank):
     def step():
         f.project_device(d_q, d_p, d_n, args.iters, stream=sptr)
 
+    # the walk schedule (queries per warp) picked by the library's autotuner
+    # on this workload, before the warm-up and outside the timed region
+    schedule = None
+    if not spec.get("knn") and not spec.get("global"):
+        if args.schedule == "auto":
+            schedule = f.tune_schedule(d_q, args.iters, stream=sptr)
+            schedule["note"] = "mlods_tune_schedule: device ms of one projection launch per candidate"
+        else:
+            f.queries_per_warp = int(args.schedule)
+            schedule = {"queries_per_warp": int(args.schedule), "note": "set by --schedule"}
+
     for _ in range(max(args.warmup, 0)):
         step()
     torch.cuda.synchronize(dev)
@@ -353,7 +377,7 @@ def run_ours(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
     launches0 = lib.mlods_kernel_launches()
-    step_ms, kern_ms, visits, rounds, searches, max_stack = [], [], [], [], [], 0
+    step_ms, kern_ms, visits, lane_visits, rounds, searches, max_stack = [], [], [], [], [], [], 0
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -366,6 +390,7 @@ def run_ours(args, rank, world, local_rank):
         st = f.last_stats()
         kern_ms.append(st["kernel_ms"])
         visits.append(st["node_visits"])
+        lane_visits.append(st.get("lane_visits", st["node_visits"]))
         rounds.append(st["rounds"])
         searches.append(st["iterations"])
         max_stack = max(max_stack, st["max_stack"])
@@ -424,6 +449,42 @@ def run_ours(args, rank, world, local_rank):
         f.converge_tol = 0.0
         f._sync_params()
         step()  # back to the full-iteration outputs
+        torch.cuda.synchronize(dev)
+
+    # ---- kernel-weight pruning (an option, off in every figure above): the
+    # same steps with prune_tol = 1e-6, visits, time and (below) FP64 error
+    pruning, prune_out = None, None
+    if world == 1 and not spec.get("knn") and not spec.get("global"):
+        qpw = f.queries_per_warp
+        f.prune_tol = PRUNE_TOL
+        f.queries_per_warp = min(qpw, 2)
+        step()
+        torch.cuda.synchronize(dev)
+        pms, pv, pp = [], [], []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            pms.append(e0.elapsed_time(e1))
+            st = f.last_stats()
+            pv.append(st["node_visits"])
+            pp.append(st["pruned"])
+        prune_out = d_p.cpu().numpy()
+        pruning = {"prune_tol": PRUNE_TOL, "queries_per_warp": f.queries_per_warp,
+                   "ms_per_step": statistics.mean(pms), "ms_per_step_off": total_ms_max / args.steps,
+                   "visits_per_query_iteration": statistics.mean(pv) / len(q) / args.iters,
+                   "visits_per_query_iteration_off": statistics.mean(visits) / len(q) / args.iters,
+                   "pruned_per_query_iteration": statistics.mean(pp) / len(q) / args.iters,
+                   "note": "a near node is taken as an aggregate when f * w(distance to its bounding sphere) * "
+                           "area < prune_tol * w(0) * mean sample area"}
+        f.prune_tol = 0.0
+        f.queries_per_warp = qpw
+        f._sync_params()
+        step()  # back to the reference walk's outputs
         torch.cuda.synchronize(dev)
 
     # ---- end to end through the public C ABI with host buffers (Fastapss protocol)
@@ -519,21 +580,28 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "roofline": roofline,
         "kernel_ms": kms,
+        "schedule": schedule,
         "converge_exact": conv,
         "converge_tol": conv_tol,
+        "pruning": pruning,
         "neighbour_searches_per_query_iteration": (statistics.mean(searches) / len(q) / args.iters
                                                    if spec.get("knn") else None),
         "traversal": None if spec.get("knn") or spec.get("global") else {
             "visits_per_query_iteration": mean_visits / len(q) / args.iters,
-            "lane_utilisation": mean_visits / (32.0 * statistics.mean(rounds)),
-            "max_stack_ranges": max_stack},
+            "node_evaluations_per_query_iteration": statistics.mean(lane_visits) / len(q) / args.iters,
+            "lane_utilisation": statistics.mean(lane_visits) / (32.0 * statistics.mean(rounds)),
+            "max_stack_ranges": max_stack,
+            "note": "visits: nodes each query's walk touches (the reference's traversal); node evaluations: "
+                    "what the warps computed, a node shared by the queries of one warp's walk counted once"},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result.update(cpu_baseline_and_check(args, pts, nrm, q, diag, kernel, out_host, tol_out, out_local,
-                                             np.array(inf.origin[:], np.float64)))
+                                             np.array(inf.origin[:], np.float64), prune_out))
         if conv_tol is not None and "err_vs_fp64_converge_tol" in result:
             conv_tol["err_vs_fp64"] = result.pop("err_vs_fp64_converge_tol")
+        if pruning is not None and "err_vs_fp64_pruned" in result:
+            pruning["err_vs_fp64"] = result.pop("err_vs_fp64_pruned")
     return result
 
 
@@ -765,6 +833,54 @@ def batch_placement(specs, world: int, iters: int) -> list[int]:
     return shard.assign_clouds(work, nbytes, world, capacity=150 * 10**9)
 
 
+def batch_fp64_sample(clouds, out, counts, iters, per_cloud: int = 16):
+    """Error of the batch outputs against the FP64 restatement on a few
+    queries of every cloud (fraction of each cloud's bounding-box diagonal,
+    beyond float32 output rounding)."""
+    import oracle
+
+    rng = np.random.default_rng(11)
+    worst, worst_ex, n = 0.0, 0.0, 0
+    off = 0
+    for (pts, nrm, q, diag, k, depth), c in zip(clouds, counts):
+        sel = rng.choice(c, min(per_cloud, c), replace=False)
+        x64, _ = oracle.OracleTree(pts, nrm, depth).project_mlod(q[sel], iters, k, rule=0, cutoff=2.0)
+        x = out[off + sel].astype(np.float64)
+        half = np.abs(np.spacing(x64.astype(np.float32)).astype(np.float64)) / 2
+        worst = max(worst, float((np.linalg.norm(x - x64, axis=1) / diag).max()))
+        worst_ex = max(worst_ex, float((np.linalg.norm(np.maximum(np.abs(x - x64) - half, 0), axis=1) / diag).max()))
+        n += len(sel)
+        off += c
+    return {"max": worst, "max_beyond_f32_output_rounding": worst_ex, "queries_checked": n,
+            "clouds_checked": len(clouds), "unit": "fraction of each cloud's bounding-box diagonal"}
+
+
+def batch_reference_gpu(clouds, qs, iters, ours_qps, sample: int = 65536):
+    """The reference's own GPU kernel (Fastapss.cu built for sm_100a,
+    oracle/_ref) on every cloud, called as the application calls it: one
+    call of one iteration per timer tick, `iters` calls, on up to `sample`
+    queries of each cloud; its trees are built on the host by the reference."""
+    import oracle
+
+    if not oracle.refgpu_available():
+        return {"unavailable": "reference GPU kernel not built"}
+    tot_q, tot_ms, build_s = 0, 0.0, 0.0
+    for (pts, nrm, q, diag, k, depth), qq in zip(clouds, qs):
+        t0 = time.time()
+        rg = oracle.RefGpu(pts, nrm, k, cutoff=2.0, max_depth=depth)
+        build_s += time.time() - t0
+        sel = qq[:sample]
+        _, _, ms = rg.project(sel, calls=iters, iters_per_call=1)
+        tot_q += len(sel)
+        tot_ms += ms
+        del rg
+    ref_qps = tot_q / (tot_ms / 1e3)
+    return {"value": ref_qps, "unit": "queries/s", "queries_timed": tot_q, "host_tree_builds_s": build_s,
+            "ours_over_reference": ours_qps / ref_qps,
+            "note": f"Fastapss::project per cloud, {iters} calls of 1 iteration (the application's timer "
+                    f"pattern), first {sample} queries of each cloud, device time"}
+
+
 def run_batch(args, rank: int = 0, world: int = 1):
     """Batched workload: every cloud's tree resident, all queries projected
     by one graph launch per step (launch shape tuned), against the same work
@@ -802,7 +918,11 @@ def run_batch(args, rank: int = 0, world: int = 1):
     d_n = torch.empty_like(d_q)
     b = FastapssBatch(projectors)
     iters = args.iters
-    b.tune(counts, d_q, d_p, d_n, iters)
+    # the autotuner ranks the launch shapes on one-iteration runs (cheap; the
+    # ranking carries over to the full iteration count)
+    t_tune = time.time()
+    b.tune(counts, d_q, d_p, d_n, 1)
+    tune_s = time.time() - t_tune
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device="cuda")
     for _ in range(max(args.warmup, 0)):
         b.project_device(counts, d_q, d_p, d_n, iters, use_graph=True)
@@ -831,7 +951,13 @@ def run_batch(args, rank: int = 0, world: int = 1):
         torch.distributed.barrier()
     clk = clocks.stop()
     # the same work as one launch per cloud (the reference's one-object-per-call
-    # form), warmed up and timed like the batch, and its outputs compared
+    # form) with the batch's walk schedule and query order, warmed up and
+    # timed like the batch, and its outputs compared
+    st = b.last_stats()
+    for f in projectors:
+        if st["queries_per_warp"]:
+            f.queries_per_warp = st["queries_per_warp"]
+        f.reorder = bool(st["reorder"])
     batch_p, batch_n = d_p.clone(), d_n.clone()
     off = 0
     views = []
@@ -863,7 +989,8 @@ def run_batch(args, rank: int = 0, world: int = 1):
     kms = statistics.mean(kern_ms)
     achieved = (total * 36 + 64 * statistics.mean(visits)) / (kms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    st = b.last_stats()
+    err = batch_fp64_sample(clouds, batch_p.cpu().numpy(), counts, iters) if rank == 0 else None
+    ref_gpu = batch_reference_gpu(clouds, qs, iters, value) if (rank == 0 and args.ref_gpu) else None
     return {
         "metric": "queries projected/s, 64 resident clouds in one graph launch",
         "value": value,
@@ -882,9 +1009,15 @@ def run_batch(args, rank: int = 0, world: int = 1):
                    "parallelism": (f"whole clouds per GPU, {world} GPUs (rank 0: {len(clouds)} clouds, "
                                    f"{n_points} points)") if world > 1 else "1 GPU",
                    "kernels": "Gaussian / multi-Gaussian / rational drawn per cloud", "tree_depths": "7..10",
-                   "launch": f"CUDA graph, query order {'Morton' if st['reorder'] else 'input'}, grid "
-                             f"{st['grid_pct']}% of the persistent size",
+                   "launch": "one persistent queue-kernel launch per step (after the Morton ordering), "
+                             "captured in a CUDA graph",
                    "l2": "L2 flushed (256 MB write) before every timed step"},
+        "schedule": {"queries_per_warp": st["queries_per_warp"], "chunk": st["chunk"],
+                     "query_order": "Morton" if st["reorder"] else "input", "grid_pct": st["grid_pct"],
+                     "tuner_seconds": tune_s,
+                     "note": "picked by mlods_batch_tune from 6 candidate launch shapes timed on 1-iteration runs"},
+        "err_vs_fp64": err,
+        "reference_gpu": ref_gpu,
         "one_launch_per_cloud_ms": per_cloud_ms,
         "outputs_equal_one_launch_per_cloud": same,
         "gpu_launches": int(launches),

@@ -201,6 +201,18 @@ int mlods_project_host(mlods_tree t, int64_t n, const float* q, float* out_pts, 
 int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out_pts, float* d_out_nrm,
                          int32_t n_iterations, float step_max, void* stream);
 
+/* ---- walk schedule autotuner (extension) -----------------------------------
+ * Times the MLoD projection of the n device queries d_q (n_iterations steps,
+ * the tree's kernel and options, outputs to scratch) with each walk schedule
+ * -- 1, 2 and 4 queries per warp (4 is skipped under pruning) -- after one
+ * untimed run of each, and keeps the fastest in the tree's options
+ * (mlods_params.queries_per_warp), which every later single-tree projection
+ * uses.  *chosen receives it; ms (may be NULL) the three device times in
+ * milliseconds (-1 for a skipped one).  The results of the schedules agree to
+ * float rounding.  Synchronises. */
+int mlods_tune_schedule(mlods_tree t, int64_t n, const float* d_q, int32_t n_iterations, void* stream,
+                        int32_t* chosen, float* ms);
+
 /* ---- neighbour gathers -----------------------------------------------------
  * k nearest neighbours of n device query points (world xyz), as the
  * reference kd-tree's knearest (kdTreeNN.h:416-461, :590-600) which
@@ -336,21 +348,29 @@ int mlods_last_walk_counts(mlods_tree t, int64_t* lane_visits, int64_t* pruned);
 /* ---- batched projection over many resident trees (extension) ---------------
  * No counterpart in the reference, which projects one tree per launch
  * (Fastapss::project, Fastapss.cu:439-455).  A batch holds a fixed list of
- * trees; mlods_batch_project projects, in a few persistent kernel launches on
- * one stream (one per kernel specialisation shared by the smaller trees, one
- * per tree with at least 8 queries per resident warp), the
- * device query buffer d_q (float xyz, concatenated per tree: tree i owns
- * queries [offsets[i], offsets[i+1]), offsets is a HOST array of n_trees + 1
- * entries starting at 0) onto their trees, writing d_out_pts/d_out_nrm in the
- * same layout.  Every tree must be in MLODS_MODE_MLOD with a kernel set; each
- * tree's own cutoff, min_depth, blend rule and convergence mode apply, and the
- * step clamp is each tree's root box radius.  Results equal per-tree
- * mlods_project_device calls bit for bit.  With use_graph != 0 the work is
+ * trees; mlods_batch_project projects, in ONE persistent kernel launch on one
+ * stream (after the Morton ordering of the queries), the device query buffer
+ * d_q (float xyz, concatenated per tree: tree i owns queries
+ * [offsets[i], offsets[i+1]), offsets is a HOST array of n_trees + 1 entries
+ * starting at 0) onto their trees, writing d_out_pts/d_out_nrm in the same
+ * layout.  The launch's warps pull chunks of a tree's queries from a device
+ * work queue, the trees with the most work first, and walk each chunk with
+ * the tree's own specialisation of the walk (kernel family and terms, blend
+ * rule, queries per warp), so trees of any size and kernel share the launch.
+ * Every tree must be in MLODS_MODE_MLOD with a kernel set; each tree's own
+ * cutoff, min_depth, blend rule and convergence mode apply (pruning does not),
+ * and the step clamp is each tree's root box radius.  Every tree is walked
+ * with its own queries_per_warp (4 runs as 2) unless mlods_batch_tune picked
+ * one schedule for all; results equal per-tree mlods_project_device calls
+ * with the same schedule bit for bit.  With use_graph != 0 the work is
  * captured once in a CUDA graph and replayed while buffers, offsets, tree
  * settings and n_iterations stay the same (the stream must not be capturing).
- * mlods_batch_tune times a few launch shapes on the given buffers (it runs the
- * projection four times) and keeps the fastest for later calls.  The trees
- * must outlive the batch and must not be rebuilt while it exists. */
+ * mlods_batch_tune (the batch's autotuner) times, on the given buffers, walk
+ * schedules (one or two queries per warp for every tree), chunk sizes (16 to
+ * 256 queries), Morton or input order and the share of the resident grid --
+ * each candidate run once untimed and once timed -- and keeps the fastest
+ * for later calls.  The trees must outlive the batch and must not be rebuilt
+ * while it exists. */
 typedef struct mlods_batch_s* mlods_batch;
 int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* out);
 int mlods_batch_free(mlods_batch b);
@@ -358,9 +378,14 @@ int mlods_batch_project(mlods_batch b, const int64_t* offsets, const float* d_q,
                         int32_t n_iterations, int32_t use_graph, void* stream);
 int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, float* d_out_pts, float* d_out_nrm,
                      int32_t n_iterations, void* stream);
-/* Statistics of the last batch launch (synchronises); any pointer may be NULL. */
+/* Statistics of the last batch launch (synchronises): query-node visits,
+ * rounds, overflows, device time (ordering and kernel), the launch shape in
+ * use (reorder, grid_pct, queries_per_warp -- 0: each tree's own -- and
+ * chunk) and node evaluations (lane_visits, see mlods_last_walk_counts).  Any
+ * pointer may be NULL. */
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
-                      int32_t* reorder, int32_t* grid_pct);
+                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int32_t* chunk,
+                      int64_t* lane_visits);
 
 /* ---- projection without device allocation (extension) ----------------------
  * No counterpart in the reference.  Same computation and results as

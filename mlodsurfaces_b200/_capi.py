@@ -159,6 +159,8 @@ SIGNATURES = {
     "mlods_last_stats": (C.c_int, [_P, _I64, _I64, _I32, _I64, C.POINTER(C.c_float)]),
     "mlods_last_iterations": (C.c_int, [_P, _I64]),
     "mlods_last_walk_counts": (C.c_int, [_P, _I64, _I64]),
+    "mlods_tune_schedule": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_float)]),
     "mlods_kernel_launches": (C.c_int64, []),
     "mlods_release_scratch": (C.c_int, []),
     "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),
@@ -174,7 +176,7 @@ SIGNATURES = {
     "mlods_batch_free": (C.c_int, [_P]),
     "mlods_batch_project": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, _P]),
     "mlods_batch_tune": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
-    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32]),
+    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32, _I32, _I32, _I64]),
     "mlods_project_device_noalloc": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
     "mlods_dcgrid_adaptive": (C.c_int, [_P, C.c_int32, C.c_int32, _P, C.POINTER(_P)]),
     "mlods_dcgrid_xform": (C.c_int, [_P, _P, _I64]),

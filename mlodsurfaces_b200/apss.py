@@ -611,6 +611,18 @@ class APSS:
                                                   capi.ptr(d_out_p), capi.ptr(d_out_n), int(n_iterations),
                                                   float(stepMaxSize), C.c_void_p(stream or 0)))
 
+    def tune_schedule(self, d_q, n_iterations: int, stream=None) -> dict:
+        """mlods_tune_schedule: times the walk schedules on the device queries
+        d_q (torch CUDA float32 (n, 3)) and keeps the fastest as this
+        object's queries_per_warp.  Returns {"queries_per_warp": q, "ms": {1: .., 2: .., 4: ..}}."""
+        self._sync_params()
+        chosen = C.c_int32(0)
+        ms = (C.c_float * 3)()
+        capi.check(self._lib.mlods_tune_schedule(self.m_apssOctree.handle, int(d_q.shape[0]), capi.ptr(d_q),
+                                                 int(n_iterations), C.c_void_p(stream or 0), C.byref(chosen), ms))
+        self.queries_per_warp = int(chosen.value)
+        return {"queries_per_warp": int(chosen.value), "ms": {w: float(m) for w, m in zip((1, 2, 4), ms)}}
+
     def dc_evaluate(self, cells, max_depth: int, xform=None, use_normals: bool = False):
         """Corner field and per-cell vertex of a DC grid (scene.cpp:1346-1394,
         dual_contouring.h:124-176): (corner_f (n, 8), vertex (n, 3) in the unit
@@ -783,10 +795,14 @@ class FastapssBatch:
         ms = C.c_float(0)
         ro = C.c_int32(0)
         gp = C.c_int32(0)
+        qw = C.c_int32(0)
+        ch = C.c_int32(0)
+        lv = C.c_int64(0)
         capi.check(self._lib.mlods_batch_stats(self._b, C.byref(v), C.byref(r), C.byref(o), C.byref(ms),
-                                               C.byref(ro), C.byref(gp)))
+                                               C.byref(ro), C.byref(gp), C.byref(qw), C.byref(ch), C.byref(lv)))
         return {"node_visits": v.value, "rounds": r.value, "overflows": o.value, "kernel_ms": ms.value,
-                "reorder": ro.value, "grid_pct": gp.value}
+                "reorder": ro.value, "grid_pct": gp.value, "queries_per_warp": qw.value, "chunk": ch.value,
+                "lane_visits": lv.value}
 
 
 class ProjectionServer:

@@ -1,15 +1,17 @@
-// batch.cu -- many resident trees projected by a few persistent launches.
+// batch.cu -- many resident trees projected by ONE persistent launch.
 //
 // No counterpart in the reference (one tree, one launch per call).  The batch
-// keeps per-tree launch arguments on the device, orders all queries by
-// (tree, Morton code) with one radix sort, and runs, per kernel
-// specialisation, mlod_batch_kernel over the smaller trees, whose warps pull
-// queries from a shared counter across trees so that trees of very different
-// sizes load-balance inside one launch; each large tree runs the single-tree
-// kernel over its own slot range.  With use_graph the
-// memset/order/kernel sequence is captured once in a CUDA graph and replayed
-// while the buffers and sizes stay the same.  A small autotuner picks the
-// query order (Morton or input order) and the grid size by timing.
+// keeps per-tree launch arguments on the device, orders each tree's queries
+// in Morton order (one radix sort over all of them, the tree index as the key
+// prefix, so every tree keeps its own query range), cuts each tree's range
+// into chunks, and runs the queue kernel (project.cu): its warps pull chunks
+// from a device counter -- the trees with the most work first -- and walk
+// each with the tree's own specialisation of the walk, so trees of very
+// different sizes and kernels load-balance inside a single launch.  With
+// use_graph the memset / order / kernel sequence is captured once in a CUDA
+// graph and replayed while the buffers and sizes stay the same.  The
+// autotuner (mlods_batch_tune) times walk schedules (queries per warp),
+// chunk sizes, query orders and grid sizes and keeps the fastest.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -25,17 +27,21 @@ struct mlods_batch_s {
     mlods::CloudArgs* d_clouds = nullptr;
     int64_t* d_offsets = nullptr;
     mlods::BatchFrame* d_frames = nullptr;
-    int64_t* d_rank_slot = nullptr;
-    int32_t* d_rank_cloud = nullptr;
-    int64_t* d_stats = nullptr;  // stats block (8 int64) then one work counter per group
-    std::vector<mlods::BatchGroup> groups;
+    int64_t* d_stats = nullptr;  // statistics block (8 int64) then the chunk counter
+    mlods::QueueChunk* d_chunks = nullptr;
+    size_t chunk_cap = 0;
+    int64_t n_chunks = 0;
     void* d_order_buf = nullptr;
     size_t order_bytes = 0;
-    std::vector<mlods::CloudArgs> h_clouds;  // last uploaded
+    // what the device holds (re-uploaded when it changes)
+    std::vector<mlods::CloudArgs> h_clouds;
     std::vector<int64_t> h_offsets;
-    // tuned launch shape
-    int reorder = 1;
-    int grid_pct = 100;
+    int h_chunk = -1;
+    // launch shape (the tuner's pick)
+    int reorder = 1;     // Morton order inside each tree
+    int grid_pct = 100;  // share of the resident blocks launched
+    int chunk = 64;      // slots per chunk (a multiple of 4)
+    int qpw = 0;         // queries per warp for every tree; 0: each tree's own setting
     // graph cache
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -59,7 +65,7 @@ namespace mlods
 namespace
 {
 inline size_t up256(size_t v) { return (v + 255) / 256 * 256; }
-constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + kMaxBatchGroups * sizeof(unsigned int);
+constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + 256;  // statistics, then the chunk counter
 
 void drop_graph(mlods_batch_s* b)
 {
@@ -76,23 +82,22 @@ int enqueue(mlods_batch_s* b, const float* d_q, int64_t total, bool timed, cudaS
 {
     const int n = int(b->trees.size());
     MLODS_CUDA(cudaMemsetAsync(b->d_stats, 0, kStatsBytes, s));
-    // the order groups the clouds by kernel specialisation (always needed),
-    // with Morton order inside each cloud when reorder is on
-    uint32_t* order = static_cast<uint32_t*>(b->d_order_buf);
-    void* tmp = static_cast<char*>(b->d_order_buf) + up256(size_t(total) * 4);
-    MLODS_CUDA(compute_batch_order(d_q, total, b->d_offsets, n, b->d_frames, b->reorder != 0, order, tmp, s));
-    BatchArgs a;
+    uint32_t* order = nullptr;
+    if (b->reorder) {
+        order = static_cast<uint32_t*>(b->d_order_buf);
+        void* tmp = static_cast<char*>(b->d_order_buf) + up256(size_t(total) * 4);
+        MLODS_CUDA(compute_batch_order(d_q, total, b->d_offsets, n, b->d_frames, true, order, tmp, s));
+    }
+    QueueArgs a;
     a.clouds = b->d_clouds;
     a.q_offsets = b->d_offsets;
-    a.n_clouds = n;
-    a.total = total;
+    a.chunks = b->d_chunks;
+    a.n_chunks = b->n_chunks;
     a.order = order;
-    a.rank_slot = b->d_rank_slot;
-    a.rank_cloud = b->d_rank_cloud;
-    a.counters = reinterpret_cast<unsigned int*>(b->d_stats + 8);
+    a.counter = reinterpret_cast<unsigned int*>(b->d_stats + 8);
     a.stats = b->d_stats;
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev0, s));
-    MLODS_CUDA(launch_mlod_batch(a, b->groups, sm_count_for_current_device(), b->grid_pct, s));
+    MLODS_CUDA(launch_mlod_queue(a, sm_count_for_current_device(), b->grid_pct, s));
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev1, s));
     if (timed) b->ran = true;
     return MLODS_OK;
@@ -130,39 +135,48 @@ int batch_prepare(mlods_batch_s* b, const int64_t* offsets, const float* d_q, fl
             set_last_error("batch: tree %d is not in MLoD mode", i);
             return MLODS_ERR_INVALID;
         }
+        // each cloud's arguments address its own slice of the buffers
         fill_cloud_args(T, clouds[size_t(i)], d_q + 3 * offsets[i], d_p + 3 * offsets[i], d_n + 3 * offsets[i], iters,
                         -1.f, T->params.blend_rule);
+        CloudArgs& c = clouds[size_t(i)];
+        if (b->qpw) c.qpw = b->qpw;
+        if (c.qpw == 4) c.qpw = 2;  // the queue kernel walks one or two queries per warp
+        c.prune_thr = 0.f;          // the queue kernel walks without pruning
         float ext = 0.f;
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
-        frames[size_t(i)] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f, 0u};
-    }
-    std::vector<BatchGroup> groups;
-    std::vector<int64_t> rank_slot(static_cast<size_t>(n) + 1);
-    std::vector<int32_t> rank_cloud(static_cast<size_t>(n));
-    plan_batch_groups(clouds.data(), offsets, n, frames.data(), rank_slot.data(), rank_cloud.data(), groups,
-                      batch_solo_min_queries(sm_count_for_current_device()));
-    if (int(groups.size()) > kMaxBatchGroups) {
-        set_last_error("batch: %zu kernel specialisations exceed the %d supported", groups.size(), kMaxBatchGroups);
-        return MLODS_ERR_CAPACITY;
+        frames[size_t(i)] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f,
+                                       uint32_t(i)};
     }
     const bool same = b->h_clouds.size() == clouds.size() && b->h_offsets.size() == size_t(n + 1) &&
+                      b->h_chunk == b->chunk &&
                       std::memcmp(b->h_clouds.data(), clouds.data(), clouds.size() * sizeof(CloudArgs)) == 0 &&
                       std::memcmp(b->h_offsets.data(), offsets, size_t(n + 1) * sizeof(int64_t)) == 0;
     if (!same) {
         drop_graph(b);
+        std::vector<QueueChunk> chunks;
+        if (build_queue_chunks(clouds.data(), offsets, n, b->chunk, chunks) != MLODS_OK) {
+            set_last_error("batch: chunk size %d is not a multiple of 4", b->chunk);
+            return MLODS_ERR_INVALID;
+        }
+        if (b->chunk_cap < chunks.size()) {
+            cudaFree(b->d_chunks);
+            b->d_chunks = nullptr;
+            b->chunk_cap = 0;
+            MLODS_CUDA(cudaMalloc(&b->d_chunks, chunks.size() * sizeof(QueueChunk)));
+            b->chunk_cap = chunks.size();
+        }
+        MLODS_CUDA(cudaMemcpyAsync(b->d_chunks, chunks.data(), chunks.size() * sizeof(QueueChunk),
+                                   cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaMemcpyAsync(b->d_clouds, clouds.data(), clouds.size() * sizeof(CloudArgs),
                                    cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaMemcpyAsync(b->d_offsets, offsets, size_t(n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaMemcpyAsync(b->d_frames, frames.data(), frames.size() * sizeof(BatchFrame),
                                    cudaMemcpyHostToDevice, s));
-        MLODS_CUDA(cudaMemcpyAsync(b->d_rank_slot, rank_slot.data(), rank_slot.size() * sizeof(int64_t),
-                                   cudaMemcpyHostToDevice, s));
-        MLODS_CUDA(cudaMemcpyAsync(b->d_rank_cloud, rank_cloud.data(), rank_cloud.size() * sizeof(int32_t),
-                                   cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+        b->n_chunks = int64_t(chunks.size());
         b->h_clouds = clouds;
         b->h_offsets.assign(offsets, offsets + n + 1);
-        b->groups = groups;
+        b->h_chunk = b->chunk;
     }
     const size_t need = up256(size_t(total) * 4) + query_order_temp_bytes(total);
     if (b->order_bytes < need) {
@@ -259,8 +273,6 @@ int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* ou
     cudaError_t e = cudaMalloc(&b->d_clouds, size_t(n_trees) * sizeof(CloudArgs));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_offsets, size_t(n_trees + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_frames, size_t(n_trees) * sizeof(BatchFrame));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_rank_slot, size_t(n_trees + 1) * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_rank_cloud, size_t(n_trees) * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_stats, kStatsBytes);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
@@ -280,9 +292,8 @@ int mlods_batch_free(mlods_batch b)
     cudaFree(b->d_clouds);
     cudaFree(b->d_offsets);
     cudaFree(b->d_frames);
-    cudaFree(b->d_rank_slot);
-    cudaFree(b->d_rank_cloud);
     cudaFree(b->d_stats);
+    cudaFree(b->d_chunks);
     cudaFree(b->d_order_buf);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -309,49 +320,65 @@ int mlods_batch_project(mlods_batch b, const int64_t* offsets, const float* d_q,
 int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, float* d_out_pts, float* d_out_nrm,
                      int32_t n_iterations, void* stream)
 {
-    if (!b || !offsets || !d_q || !d_out_pts || !d_out_nrm) {
+    if (!b || !offsets || !d_q || !d_out_pts || !d_out_nrm || n_iterations < 0) {
         set_last_error("batch_tune: bad arguments");
         return MLODS_ERR_INVALID;
     }
     MLODS_ON_DEVICE(b->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int64_t total = 0;
-    int rc = batch_prepare(b, offsets, d_q, d_out_pts, d_out_nrm, n_iterations, s, &total);
-    if (rc != MLODS_OK) return rc;
+    // walk schedule, chunk size, query order and grid size
     struct Cand {
-        int reorder, pct;
+        int qpw, chunk, reorder, pct;
     };
-    const Cand cands[] = {{1, 100}, {0, 100}, {1, 85}, {1, 70}};
+    const Cand cands[] = {{1, 64, 1, 100}, {2, 64, 1, 100}, {2, 256, 1, 100}, {2, 16, 1, 100},
+                          {2, 64, 0, 100}, {2, 64, 1, 85}};
     float best = INFINITY;
-    Cand pick = cands[0];
+    Cand pick = cands[1];
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    MLODS_CUDA(cudaEventCreate(&t0));
+    cudaError_t ce = cudaEventCreate(&t1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(t0);
+        return cuda_fail(ce, "batch_tune: events", __FILE__, __LINE__);
+    }
+    int rc = MLODS_OK;
     for (const Cand& c : cands) {
+        b->qpw = c.qpw;
+        b->chunk = c.chunk;
         b->reorder = c.reorder;
         b->grid_pct = c.pct;
-        cudaEvent_t t0, t1;
-        MLODS_CUDA(cudaEventCreate(&t0));
-        MLODS_CUDA(cudaEventCreate(&t1));
-        MLODS_CUDA(cudaEventRecord(t0, s));
+        int64_t total = 0;
+        rc = batch_prepare(b, offsets, d_q, d_out_pts, d_out_nrm, n_iterations, s, &total);
+        if (rc != MLODS_OK) break;
+        // one run to load the kernels and settle the caches, one timed
         rc = batch_run(b, d_q, d_out_pts, d_out_nrm, total, n_iterations, 0, s);
-        MLODS_CUDA(cudaEventRecord(t1, s));
-        MLODS_CUDA(cudaEventSynchronize(t1));
+        if (rc != MLODS_OK) break;
+        ce = cudaEventRecord(t0, s);
+        if (ce == cudaSuccess) rc = batch_run(b, d_q, d_out_pts, d_out_nrm, total, n_iterations, 0, s);
+        if (ce == cudaSuccess && rc == MLODS_OK) ce = cudaEventRecord(t1, s);
+        if (ce == cudaSuccess && rc == MLODS_OK) ce = cudaEventSynchronize(t1);
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, t0, t1);
-        cudaEventDestroy(t0);
-        cudaEventDestroy(t1);
-        if (rc != MLODS_OK) return rc;
+        if (ce == cudaSuccess && rc == MLODS_OK) ce = cudaEventElapsedTime(&ms, t0, t1);
+        if (ce != cudaSuccess) rc = cuda_fail(ce, "batch_tune: timing", __FILE__, __LINE__);
+        if (rc != MLODS_OK) break;
         if (ms < best) {
             best = ms;
             pick = c;
         }
     }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    b->qpw = pick.qpw;
+    b->chunk = pick.chunk;
     b->reorder = pick.reorder;
     b->grid_pct = pick.pct;
     drop_graph(b);
-    return MLODS_OK;
+    return rc;
 }
 
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
-                      int32_t* reorder, int32_t* grid_pct)
+                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int32_t* chunk,
+                      int64_t* lane_visits)
 {
     if (!b) {
         set_last_error("null batch");
@@ -362,7 +389,7 @@ int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int6
         return MLODS_ERR_STATE;
     }
     MLODS_ON_DEVICE(b->device);
-    int64_t h[6] = {0, 0, 0, 0, 0, 0};
+    int64_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     float ms = 0.f;
     MLODS_CUDA(cudaEventSynchronize(b->ev1));
     MLODS_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
@@ -373,6 +400,9 @@ int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int6
     if (kernel_ms) *kernel_ms = ms;
     if (reorder) *reorder = b->reorder;
     if (grid_pct) *grid_pct = b->grid_pct;
+    if (queries_per_warp) *queries_per_warp = b->qpw;
+    if (chunk) *chunk = b->chunk;
+    if (lane_visits) *lane_visits = h[6];
     return MLODS_OK;
 }
 

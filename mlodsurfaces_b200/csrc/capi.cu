@@ -846,6 +846,57 @@ int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out
     return project_buffers(t, n, d_q, d_out_pts, d_out_nrm, n_iterations, step_max, static_cast<cudaStream_t>(stream));
 }
 
+int mlods_tune_schedule(mlods_tree t, int64_t n, const float* d_q, int32_t n_iterations, void* stream,
+                        int32_t* chosen, float* ms)
+{
+    CHECK_TREE(t);
+    if (!d_q || n <= 0 || n_iterations < 0) {
+        set_last_error("tune schedule: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    if (!t->kernel_set) {
+        set_last_error("tune schedule: no kernel set (call mlods_set_kernel first)");
+        return MLODS_ERR_STATE;
+    }
+    if (t->params.mode != MLODS_MODE_MLOD) {
+        set_last_error("tune schedule: only the MLoD walk has schedules");
+        return MLODS_ERR_INVALID;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int cands[3] = {1, 2, 4};
+    float* out = nullptr;
+    MLODS_CUDA(scratch_alloc(reinterpret_cast<void**>(&out), size_t(n) * 6 * sizeof(float), s));
+    const int saved = t->params.queries_per_warp;
+    int best = saved;
+    float best_ms = INFINITY;
+    int rc = MLODS_OK;
+    for (int i = 0; i < 3 && rc == MLODS_OK; ++i) {
+        float this_ms = -1.f;
+        if (!(cands[i] == 4 && t->params.prune_tol > 0.f)) {
+            t->params.queries_per_warp = cands[i];
+            // one run to load the kernel and settle the caches, one timed
+            for (int rep = 0; rep < 2 && rc == MLODS_OK; ++rep)
+                rc = project_buffers(t, n, d_q, out, out + 3 * n, n_iterations, -1.f, s);
+            if (rc == MLODS_OK) {
+                cudaError_t e = cudaEventSynchronize(t->ev_stop);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&this_ms, t->ev_start, t->ev_stop);
+                if (e != cudaSuccess) rc = cuda_fail(e, "tune schedule: timing", __FILE__, __LINE__);
+            }
+            if (rc == MLODS_OK && this_ms < best_ms) {
+                best_ms = this_ms;
+                best = cands[i];
+            }
+        }
+        if (ms) ms[i] = this_ms;
+    }
+    t->params.queries_per_warp = rc == MLODS_OK ? best : saved;
+    const cudaError_t ef = scratch_free(out, s);
+    if (rc != MLODS_OK) return rc;
+    if (ef != cudaSuccess) return cuda_fail(ef, "tune schedule: free", __FILE__, __LINE__);
+    if (chosen) *chosen = best;
+    return MLODS_OK;
+}
+
 int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_idx, float* d_d2, void* stream)
 {
     CHECK_TREE(t);

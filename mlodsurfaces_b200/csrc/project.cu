@@ -508,58 +508,119 @@ __global__ void __launch_bounds__(kProjectThreads, WalkShape<QPW>::kMinBlocks) m
     tot.flush_pruned(a.stats);
 }
 
-// Many trees, one launch per kernel specialisation.  The warps of a launch
-// take slots of their group's range; the query at slot s is order[s] in the
-// concatenated buffers and belongs to the cloud whose offset range holds it.
-// A warp copies its cloud's arguments to shared memory when the cloud
-// changes (consecutive slots mostly share one), so the walk reads them as
-// cheaply as the single-tree kernel reads its parameters.
-template <int KTYPE, int NSIG, int RULE, int CAP>
-__global__ void __launch_bounds__(kProjectThreads, kBatchMinBlocks)
-    mlod_batch_kernel(BatchArgs b, int64_t slot_begin, int64_t slot_end, unsigned int* counter)
+// ---- many trees in one persistent launch ---------------------------------
+// Each warp's shared-memory region holds the stack of the widest walk the
+// queue kernel runs (two queries per warp) and a copy of the current cloud's
+// launch arguments.
+constexpr int kQueueCap1 = kProjectStackCap;
+constexpr int kQueueCap2 = kProjectPairStackCap;
+constexpr size_t kQueueStackBytes = sizeof(WarpStack<kQueueCap1, 1>) > sizeof(WarpStack<kQueueCap2, 2>)
+                                        ? sizeof(WarpStack<kQueueCap1, 1>)
+                                        : sizeof(WarpStack<kQueueCap2, 2>);
+constexpr size_t kQueueWarpBytes = (kQueueStackBytes + sizeof(CloudArgs) + 15) / 16 * 16;
+
+// Walks the queries at slots [s0, s1) of the batch order, QPW at a time, with
+// one specialisation of the walk; `base` is the cloud's first global query
+// index (its arguments address its own queries).  Kept out of line: the
+// queue kernel calls one of these per chunk, so each keeps its own registers
+// and its specialised inner loop.
+template <int KTYPE, int NSIG, int RULE, int QPW>
+__device__ __noinline__ void walk_chunk(const CloudArgs& c, const uint32_t* __restrict__ order, int64_t base,
+                                        int64_t s0, int64_t s1, unsigned char* stack_raw, WarpTotals& tot)
+{
+    constexpr int CAP = QPW == 1 ? kQueueCap1 : kQueueCap2;
+    WarpStack<CAP, QPW>& st = *reinterpret_cast<WarpStack<CAP, QPW>*>(stack_raw);
+    for (int64_t s = s0; s < s1; s += QPW) {
+        const int nq = int(min(int64_t(QPW), s1 - s));
+        uint32_t qi[QPW];
+#pragma unroll
+        for (int x = 0; x < QPW; ++x) {
+            const int64_t slot = s + (x < nq ? x : 0);
+            qi[x] = uint32_t((order ? int64_t(__ldg(order + slot)) : slot) - base);
+        }
+        WalkStats ws;
+        project_queries<KTYPE, NSIG, RULE, CAP, QPW>(c, qi, nq, st, ws);
+        tot.add(ws, nq);
+    }
+}
+
+// The specialisation of the walk a cloud runs with: kernel family and number
+// of multi-Gaussian terms (2-6 and 8 have their own code, other counts share
+// one), blend rule, queries per warp.
+inline int walk_spec_id(const CloudArgs& c)
+{
+    int k = 8;  // multi-Gaussian, terms counted at run time
+    if (c.kc.type == MLODS_GAUSSIAN) k = 0;
+    else if (c.kc.type == MLODS_SINGULAR) k = 1;
+    else if (c.kc.nsig >= 2 && c.kc.nsig <= 6) k = c.kc.nsig;
+    else if (c.kc.nsig == 8) k = 7;
+    const int rule = c.rule == MLODS_BLEND_GPU ? 0 : 1;
+    const int q = c.qpw == 2 ? 1 : 0;
+    return (q * 2 + rule) * 9 + k;
+}
+
+template <int RULE, int QPW>
+__device__ __forceinline__ void walk_chunk_k(int k, const CloudArgs& c, const uint32_t* order, int64_t base,
+                                             int64_t s0, int64_t s1, unsigned char* st, WarpTotals& tot)
+{
+    switch (k) {
+    case 0: walk_chunk<MLODS_GAUSSIAN, 0, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 1: walk_chunk<MLODS_SINGULAR, 0, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 2: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 2, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 3: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 3, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 4: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 4, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 5: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 5, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 6: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 6, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 7: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 8, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    default: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 0, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    }
+}
+
+// Every cloud of a batch in ONE persistent launch: the warps pull chunks (a
+// cloud and a run of its slots in the batch order) from a device work queue
+// and walk each with the cloud's own specialisation; a warp copies a cloud's
+// launch arguments to shared memory when it moves to another cloud.  Chunks
+// start at multiples of 4 slots from their cloud's first slot, so the queries
+// that share a walk are those a launch of the cloud alone would pair: the
+// results equal per-tree launches bit for bit.
+__global__ void __launch_bounds__(kProjectThreads, kProjectPairMinBlocks) mlod_queue_kernel(QueueArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpStack<CAP, 1>& st = reinterpret_cast<WarpStack<CAP, 1>*>(smem_raw)[warp];
-    CloudArgs* cache =
-        reinterpret_cast<CloudArgs*>(smem_raw + (kProjectThreads / 32) * sizeof(WarpStack<CAP, 1>)) + warp;
+    unsigned char* region = smem_raw + size_t(warp) * kQueueWarpBytes;
+    CloudArgs* cache = reinterpret_cast<CloudArgs*>(region + kQueueStackBytes);
     int cached = -1;
-    int64_t c_lo = 0, c_hi = 0, c_base = 0;  // slot range and first global index of the cached cloud
+    int64_t base = 0;
     WarpTotals tot;
     for (;;) {
-        unsigned int qs = 0;
-        if (lane == 0) qs = atomicAdd(counter, 1u);
-        qs = __shfl_sync(kFull, qs, 0);
-        const int64_t slot = slot_begin + int64_t(qs);
-        if (slot >= slot_end) break;
-        const int64_t g = int64_t(__ldg(b.order + slot));
-        if (slot < c_lo || slot >= c_hi) {
-            // the cloud owning this slot: binary search over the rank table
-            int lo = 0, hi = b.n_clouds;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (slot >= __ldg(b.rank_slot + mid)) lo = mid; else hi = mid;
-            }
-            const int cl = __ldg(b.rank_cloud + lo);
-            c_lo = __ldg(b.rank_slot + lo);
-            c_hi = __ldg(b.rank_slot + lo + 1);
-            c_base = __ldg(b.q_offsets + cl);
-            if (cl != cached) {
-                const uint32_t* src = reinterpret_cast<const uint32_t*>(b.clouds + cl);
-                uint32_t* dst = reinterpret_cast<uint32_t*>(cache);
-                for (int w = lane; w < int(sizeof(CloudArgs) / 4); w += 32) dst[w] = __ldg(src + w);
-                cached = cl;
-                __syncwarp();
-            }
+        unsigned int ci = 0;
+        if (lane == 0) ci = atomicAdd(a.counter, 1u);
+        ci = __shfl_sync(kFull, ci, 0);
+        if (int64_t(ci) >= a.n_chunks) break;
+        const QueueChunk ch = a.chunks[ci];
+        if (ch.cloud != cached) {
+            __syncwarp();  // every lane is done with the previous arguments
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(a.clouds + ch.cloud);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(cache);
+            for (int w = lane; w < int(sizeof(CloudArgs) / 4); w += 32) dst[w] = __ldg(src + w);
+            cached = ch.cloud;
+            base = __ldg(a.q_offsets + ch.cloud);
+            __syncwarp();
         }
-        const uint32_t qi[1] = {uint32_t(g - c_base)};
-        WalkStats ws;
-        project_queries<KTYPE, NSIG, RULE, CAP, 1>(*cache, qi, 1, st, ws);
-        tot.add(ws, 1);
-        __syncwarp();  // every lane is done with the cached arguments
+        const int spec = ch.spec;
+        const int k = spec % 9, rule = (spec / 9) & 1, q2 = spec / 18;
+        if (q2) {
+            if (rule == 0) walk_chunk_k<MLODS_BLEND_GPU, 2>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end,
+                                                            region, tot);
+            else walk_chunk_k<MLODS_BLEND_CPU, 2>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end, region, tot);
+        } else {
+            if (rule == 0) walk_chunk_k<MLODS_BLEND_GPU, 1>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end,
+                                                            region, tot);
+            else walk_chunk_k<MLODS_BLEND_CPU, 1>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end, region, tot);
+        }
     }
-    tot.flush(b.stats);
-    tot.flush_pruned(b.stats);
+    tot.flush(a.stats);
+    tot.flush_pruned(a.stats);
 }
 
 template <typename Kern>
@@ -670,50 +731,6 @@ __global__ void reorganize_kernel(float* __restrict__ q, const uint32_t* __restr
 
 inline size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 
-template <int KTYPE, int NSIG, int RULE>
-cudaError_t launch_batch_typed(const BatchArgs& b, const BatchGroup& g, unsigned int* counter, int sm_count,
-                               int grid_scale_pct, cudaStream_t s)
-{
-    constexpr int CAP = kProjectStackCap;
-    auto kern = mlod_batch_kernel<KTYPE, NSIG, RULE, CAP>;
-    const size_t smem = size_t(kProjectThreads / 32) * (sizeof(WarpStack<CAP, 1>) + sizeof(CloudArgs));
-    cudaError_t e = cudaSuccess;
-    int64_t grid = persistent_grid(kern, smem, g.slot_end - g.slot_begin, sm_count, &e);
-    if (e != cudaSuccess) return e;
-    if (grid_scale_pct > 0 && grid_scale_pct < 100) grid = std::max<int64_t>(1, grid * grid_scale_pct / 100);
-    kern<<<unsigned(grid), kProjectThreads, smem, s>>>(b, g.slot_begin, g.slot_end, counter);
-    note_launch();
-    return cudaGetLastError();
-}
-
-template <int RULE>
-cudaError_t launch_batch_rule(const BatchArgs& b, const BatchGroup& g, unsigned int* counter, int sm_count,
-                              int pct, cudaStream_t s)
-{
-    if (g.ktype == MLODS_GAUSSIAN) return launch_batch_typed<MLODS_GAUSSIAN, 0, RULE>(b, g, counter, sm_count, pct, s);
-    if (g.ktype == MLODS_SINGULAR) return launch_batch_typed<MLODS_SINGULAR, 0, RULE>(b, g, counter, sm_count, pct, s);
-    switch (g.nsig) {
-    case 2: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 2, RULE>(b, g, counter, sm_count, pct, s);
-    case 3: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 3, RULE>(b, g, counter, sm_count, pct, s);
-    case 4: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 4, RULE>(b, g, counter, sm_count, pct, s);
-    case 5: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 5, RULE>(b, g, counter, sm_count, pct, s);
-    case 6: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 6, RULE>(b, g, counter, sm_count, pct, s);
-    case 8: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 8, RULE>(b, g, counter, sm_count, pct, s);
-    default: return launch_batch_typed<MLODS_GAUSSIAN_MULTIPLE, 0, RULE>(b, g, counter, sm_count, pct, s);
-    }
-}
-
-// the specialisation a cloud's kernel runs with: multi-Gaussian kernels with
-// 2-6 or 8 terms have their own instantiation, other counts share one
-inline int spec_nsig(const KernelConsts& kc)
-{
-    if (kc.type != MLODS_GAUSSIAN_MULTIPLE) return 0;
-    switch (kc.nsig) {
-    case 2: case 3: case 4: case 5: case 6: case 8: return kc.nsig;
-    default: return 0;
-    }
-}
-
 }  // namespace
 
 cudaError_t launch_reorganize(float* d_q, const uint32_t* d_invalid, int64_t n_invalid, uint32_t end_valid,
@@ -736,94 +753,36 @@ cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int s
     return launch_rule<MLODS_BLEND_CPU, 1>(a, ktype, sm_count, s);
 }
 
-int64_t batch_solo_min_queries(int sm_count)
+int build_queue_chunks(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, int chunk,
+                       std::vector<QueueChunk>& out)
 {
-    return 8 * int64_t(kProjectMinBlocks) * (kProjectThreads / 32) * sm_count;
-}
-
-void plan_batch_groups(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, BatchFrame* frames,
-                       int64_t* rank_slot, int32_t* rank_cloud, std::vector<BatchGroup>& groups, int64_t solo_min)
-{
-    auto key = [&](int i) {
-        const CloudArgs& c = clouds[i];
-        return (c.rule == MLODS_BLEND_GPU ? 0 : 1) * 1024 + c.kc.type * 32 + spec_nsig(c.kc);
-    };
-    auto count = [&](int i) { return q_offsets[i + 1] - q_offsets[i]; };
-    // the largest clouds (at least solo_min queries) run on their own
-    std::vector<char> solo(static_cast<size_t>(n_clouds), 0);
-    if (solo_min > 0) {
-        std::vector<int> by_size;
-        for (int i = 0; i < n_clouds; ++i)
-            if (count(i) >= solo_min) by_size.push_back(i);
-        std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) { return count(a) > count(b); });
-        for (size_t k = 0; k < by_size.size() && k < size_t(kMaxSoloClouds); ++k) solo[size_t(by_size[k])] = 1;
-    }
+    if (chunk < 4 || chunk % 4 != 0) return MLODS_ERR_INVALID;
+    // the clouds with the most work first (query count x iterations): the
+    // last chunks handed out are small ones, so the launch ends evenly
     std::vector<int> idx(static_cast<size_t>(n_clouds));
     for (int i = 0; i < n_clouds; ++i) idx[size_t(i)] = i;
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
-        if (key(a) != key(b)) return key(a) < key(b);
-        return solo[size_t(a)] > solo[size_t(b)];
-    });
-    groups.clear();
-    int64_t slot = 0;
-    for (int r = 0; r < n_clouds; ++r) {
-        const int i = idx[size_t(r)];
-        frames[i].rank = uint32_t(r);
-        rank_slot[r] = slot;
-        rank_cloud[r] = i;
-        const int64_t n = count(i);
-        const bool own = solo[size_t(i)] != 0;
-        if (own || groups.empty() || groups.back().solo >= 0 || key(idx[size_t(r - 1)]) != key(i)) {
-            BatchGroup g;
-            g.ktype = clouds[i].kc.type;
-            g.nsig = spec_nsig(clouds[i].kc);
-            g.rule = clouds[i].rule;
-            g.slot_begin = g.slot_end = slot;
-            if (own) {
-                g.solo = i;
-                g.queries_per_warp = clouds[i].qpw;
-                g.solo_args = clouds[i];
-                const int64_t o = q_offsets[i];
-                g.solo_args.q_in = clouds[i].q_in - 3 * o;
-                g.solo_args.out_p = clouds[i].out_p - 3 * o;
-                g.solo_args.out_n = clouds[i].out_n - 3 * o;
-            }
-            groups.push_back(g);
-        }
-        slot += n;
-        groups.back().slot_end = slot;
+    auto work = [&](int i) { return (q_offsets[i + 1] - q_offsets[i]) * int64_t(std::max(clouds[i].n_iter, 1)); };
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return work(a) > work(b); });
+    out.clear();
+    for (int i : idx) {
+        const int spec = walk_spec_id(clouds[i]);
+        for (int64_t s = q_offsets[i]; s < q_offsets[i + 1]; s += chunk)
+            out.push_back(QueueChunk{i, spec, s, std::min(s + chunk, q_offsets[i + 1])});
     }
-    rank_slot[n_clouds] = slot;
-    groups.erase(std::remove_if(groups.begin(), groups.end(),
-                                [](const BatchGroup& g) { return g.slot_end == g.slot_begin; }),
-                 groups.end());
+    return MLODS_OK;
 }
 
-cudaError_t launch_mlod_batch(const BatchArgs& b, const std::vector<BatchGroup>& groups, int sm_count,
-                              int grid_scale_pct, cudaStream_t s)
+cudaError_t launch_mlod_queue(const QueueArgs& a, int sm_count, int grid_pct, cudaStream_t s)
 {
-    if (int(groups.size()) > kMaxBatchGroups) return cudaErrorInvalidValue;
-    for (size_t k = 0; k < groups.size(); ++k) {
-        const BatchGroup& g = groups[k];
-        unsigned int* counter = b.counters + k;
-        if (g.solo >= 0) {
-            ProjectArgs a;
-            a.cloud = g.solo_args;
-            a.order = b.order + g.slot_begin;
-            a.nq = g.slot_end - g.slot_begin;
-            a.counter = counter;
-            a.stats = b.stats;
-            a.queries_per_warp = g.queries_per_warp;
-            const cudaError_t e = launch_mlod_project(a, g.ktype, g.rule, sm_count, s);
-            if (e != cudaSuccess) return e;
-            continue;
-        }
-        const cudaError_t e = g.rule == MLODS_BLEND_GPU
-                                  ? launch_batch_rule<MLODS_BLEND_GPU>(b, g, counter, sm_count, grid_scale_pct, s)
-                                  : launch_batch_rule<MLODS_BLEND_CPU>(b, g, counter, sm_count, grid_scale_pct, s);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+    const size_t smem = size_t(kProjectThreads / 32) * kQueueWarpBytes;
+    cudaError_t e = cudaSuccess;
+    // one warp per chunk at most
+    int64_t grid = persistent_grid(mlod_queue_kernel, smem, a.n_chunks, sm_count, &e);
+    if (e != cudaSuccess) return e;
+    if (grid_pct > 0 && grid_pct < 100) grid = std::max<int64_t>(1, grid * grid_pct / 100);
+    mlod_queue_kernel<<<unsigned(grid), kProjectThreads, smem, s>>>(a);
+    note_launch();
+    return cudaGetLastError();
 }
 
 size_t query_order_temp_bytes(int64_t n)

@@ -64,14 +64,13 @@ struct Worker {
     mlods::CloudArgs* h_clouds = nullptr;  // pinned
     int64_t* h_offsets = nullptr;
     mlods::BatchFrame* h_frames = nullptr;
-    int64_t* h_rank_slot = nullptr;
-    int32_t* h_rank_cloud = nullptr;
     mlods::CloudArgs* d_clouds = nullptr;
     int64_t* d_offsets = nullptr;
     mlods::BatchFrame* d_frames = nullptr;
-    int64_t* d_rank_slot = nullptr;
-    int32_t* d_rank_cloud = nullptr;
     size_t cloud_cap = 0;
+    mlods::QueueChunk* h_chunks = nullptr;  // pinned
+    mlods::QueueChunk* d_chunks = nullptr;
+    size_t chunk_cap = 0;
     int64_t* d_stats = nullptr;
     void* d_order = nullptr;  // query order and its sort buffers
     std::thread thread;
@@ -101,7 +100,8 @@ namespace mlods
 namespace
 {
 inline size_t al256(size_t v) { return (v + 255) / 256 * 256; }
-constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + kMaxBatchGroups * sizeof(unsigned int);
+constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + 256;  // statistics, then the chunk counter
+constexpr int kServeChunk = 64;  // queries per work-queue chunk
 
 int grow_pinned(void** p, size_t bytes)
 {
@@ -139,10 +139,6 @@ int ensure_capacity(Worker& w, int64_t total, size_t n_req)
         if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_clouds), cap * sizeof(CloudArgs));
         if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_offsets), (cap + 1) * sizeof(int64_t));
         if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_frames), cap * sizeof(BatchFrame));
-        if (rc == MLODS_OK) rc = grow_pinned(reinterpret_cast<void**>(&w.h_rank_slot), (cap + 1) * sizeof(int64_t));
-        if (rc == MLODS_OK) rc = grow_pinned(reinterpret_cast<void**>(&w.h_rank_cloud), cap * sizeof(int32_t));
-        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_rank_slot), (cap + 1) * sizeof(int64_t));
-        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_rank_cloud), cap * sizeof(int32_t));
         if (rc != MLODS_OK) return rc;
         w.cloud_cap = cap;
     }
@@ -173,41 +169,45 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Piece>& batch)
         if (r->own_kernel) c.kc = r->kc;
         float ext = 0.f;
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
-        w.h_frames[i] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f, 0u};
+        c.prune_thr = 0.f;  // the queue kernel walks without pruning
+        if (c.qpw == 4) c.qpw = 2;
+        w.h_frames[i] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f,
+                                   uint32_t(i)};
         w.h_offsets[i] = off;
         off += batch[i].n;
     }
     w.h_offsets[batch.size()] = total;
     const size_t nc = batch.size();
-    std::vector<BatchGroup> groups;
-    plan_batch_groups(w.h_clouds, w.h_offsets, int(nc), w.h_frames, w.h_rank_slot, w.h_rank_cloud, groups,
-                      batch_solo_min_queries(sm_count_for_current_device()));
-    if (int(groups.size()) > kMaxBatchGroups) {
-        set_last_error("server: %zu launches exceed the %d supported", groups.size(), kMaxBatchGroups);
-        return MLODS_ERR_CAPACITY;
+    std::vector<QueueChunk> chunks;
+    rc = build_queue_chunks(w.h_clouds, w.h_offsets, int(nc), kServeChunk, chunks);
+    if (rc != MLODS_OK) return rc;
+    if (w.chunk_cap < chunks.size()) {
+        const size_t cap = std::max(chunks.size(), w.chunk_cap + w.chunk_cap / 2);
+        rc = grow_pinned(reinterpret_cast<void**>(&w.h_chunks), cap * sizeof(QueueChunk));
+        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_chunks), cap * sizeof(QueueChunk));
+        if (rc != MLODS_OK) return rc;
+        w.chunk_cap = cap;
     }
+    std::memcpy(w.h_chunks, chunks.data(), chunks.size() * sizeof(QueueChunk));
     MLODS_CUDA(cudaMemcpyAsync(dq, hq, size_t(total) * 12, cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_clouds, w.h_clouds, nc * sizeof(CloudArgs), cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_offsets, w.h_offsets, (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemcpyAsync(w.d_frames, w.h_frames, nc * sizeof(BatchFrame), cudaMemcpyHostToDevice, w.s));
-    MLODS_CUDA(cudaMemcpyAsync(w.d_rank_slot, w.h_rank_slot, (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+    MLODS_CUDA(cudaMemcpyAsync(w.d_chunks, w.h_chunks, chunks.size() * sizeof(QueueChunk), cudaMemcpyHostToDevice,
                                w.s));
-    MLODS_CUDA(cudaMemcpyAsync(w.d_rank_cloud, w.h_rank_cloud, nc * sizeof(int32_t), cudaMemcpyHostToDevice, w.s));
     MLODS_CUDA(cudaMemsetAsync(w.d_stats, 0, kStatsBytes, w.s));
     uint32_t* order = static_cast<uint32_t*>(w.d_order);
     char* tmp = static_cast<char*>(w.d_order) + al256(size_t(total) * 4);
     MLODS_CUDA(compute_batch_order(dq, total, w.d_offsets, int(nc), w.d_frames, true, order, tmp, w.s));
-    BatchArgs a;
+    QueueArgs a;
     a.clouds = w.d_clouds;
     a.q_offsets = w.d_offsets;
-    a.n_clouds = int(nc);
-    a.total = total;
+    a.chunks = w.d_chunks;
+    a.n_chunks = int64_t(chunks.size());
     a.order = order;
-    a.rank_slot = w.d_rank_slot;
-    a.rank_cloud = w.d_rank_cloud;
-    a.counters = reinterpret_cast<unsigned int*>(w.d_stats + 8);
+    a.counter = reinterpret_cast<unsigned int*>(w.d_stats + 8);
     a.stats = w.d_stats;
-    MLODS_CUDA(launch_mlod_batch(a, groups, sm_count_for_current_device(), 100, w.s));
+    MLODS_CUDA(launch_mlod_queue(a, sm_count_for_current_device(), 100, w.s));
     MLODS_CUDA(cudaMemcpyAsync(hp, dp, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s));
     MLODS_CUDA(cudaMemcpyAsync(hn, dn, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s));
     MLODS_CUDA(cudaStreamSynchronize(w.s));
@@ -302,10 +302,8 @@ void destroy_worker(Worker* w)
     cudaFreeHost(w->h_clouds);
     cudaFreeHost(w->h_offsets);
     cudaFreeHost(w->h_frames);
-    cudaFreeHost(w->h_rank_slot);
-    cudaFreeHost(w->h_rank_cloud);
-    cudaFree(w->d_rank_slot);
-    cudaFree(w->d_rank_cloud);
+    cudaFreeHost(w->h_chunks);
+    cudaFree(w->d_chunks);
     cudaFree(w->d_buf);
     cudaFree(w->d_clouds);
     cudaFree(w->d_offsets);

@@ -98,16 +98,55 @@ def test_graph_replay_and_tuning(setup):
         assert torch.equal(d_p, ref_p) and torch.equal(d_n, ref_n)
     b.tune(counts, d_q, d_p, d_n, 4)
     st = b.last_stats()
-    assert st["grid_pct"] in (70, 85, 100) and st["reorder"] in (0, 1)
+    assert st["grid_pct"] in (85, 100) and st["reorder"] in (0, 1)
+    assert st["queries_per_warp"] in (1, 2) and st["chunk"] % 4 == 0
     d_p.fill_(float("nan"))
     b.project_device(counts, d_q, d_p, d_n, 4, use_graph=True)
     torch.cuda.synchronize()
-    assert torch.equal(d_p, ref_p) and torch.equal(d_n, ref_n)
+    # the tuner's schedule applies to every tree: per-tree launches with the
+    # same schedule (and the tuned query order) give the same bits
+    saved = [f.queries_per_warp for f in projectors]
+    saved_order = [f.reorder for f in projectors]
+    try:
+        for f in projectors:
+            f.queries_per_warp = st["queries_per_warp"]
+            f.reorder = bool(st["reorder"])
+        tuned_p, tuned_n = _per_tree(projectors, queries, 4)
+    finally:
+        for f, w, r in zip(projectors, saved, saved_order):
+            f.queries_per_warp = w
+            f.reorder = r
+    assert torch.equal(d_p, tuned_p) and torch.equal(d_n, tuned_n)
     # a change of iteration count re-captures
-    ref2_p, _ = _per_tree(projectors, queries, 2)
+    try:
+        for f in projectors:
+            f.queries_per_warp = st["queries_per_warp"]
+            f.reorder = bool(st["reorder"])
+        ref2_p, _ = _per_tree(projectors, queries, 2)
+    finally:
+        for f, w, r in zip(projectors, saved, saved_order):
+            f.queries_per_warp = w
+            f.reorder = r
     b.project_device(counts, d_q, d_p, d_n, 2, use_graph=True)
     torch.cuda.synchronize()
     assert torch.equal(d_p, ref2_p)
+
+
+def test_batch_with_paired_walks_equals_per_tree(setup):
+    """Trees set to two queries per warp: the single launch pairs the same
+    queries as each tree's own launch (chunks start at multiples of 4)."""
+    projectors, queries = setup
+    saved = [f.queries_per_warp for f in projectors]
+    try:
+        for f in projectors:
+            f.queries_per_warp = 2
+        ref_p, ref_n = _per_tree(projectors, queries, 5)
+        b = FastapssBatch(projectors)
+        p, n, _ = _batched(b, queries, 5)
+    finally:
+        for f, w in zip(projectors, saved):
+            f.queries_per_warp = w
+    assert torch.equal(p, ref_p) and torch.equal(n, ref_n)
 
 
 def test_batch_rejects_bad_input(setup):

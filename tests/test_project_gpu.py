@@ -265,3 +265,65 @@ def test_paired_walk_matches_fp64_and_single_walk(torus20k, kind, rule, qpw):
     assert ((on2[ok] * rn[ok]).sum(1) > 1 - 1e-4).all()
     assert st2["overflows"] == 0
     assert st2["node_visits"] == outs[1][2]["node_visits"]  # query-node visits: the reference's walk
+
+
+def test_schedule_tuner_picks_a_timed_schedule(torus20k):
+    """mlods_tune_schedule times the 1, 2 and 4 queries-per-warp walks on the
+    caller's queries and keeps the fastest; projections with it stay within
+    1e-5 diag of FP64."""
+    torch = pytest.importorskip("torch")
+    pts, nrm, q, ot = torus20k
+    diag = synth.bbox_diag(pts)
+    k = make_kernel("multi", diag)
+    t = APSSOctree()
+    t.build(pts, nrm)
+    f = Fastapss(t, k)
+    f.setScalingProtectionSphere(3.0)
+    d_q = torch.from_numpy(q).cuda()
+    res = f.tune_schedule(d_q, 10)
+    assert res["queries_per_warp"] in (1, 2, 4)
+    assert all(m > 0 for m in res["ms"].values())
+    assert res["ms"][res["queries_per_warp"]] == min(res["ms"].values())
+    assert f.queries_per_warp == res["queries_per_warp"]
+    d_p = torch.empty_like(d_q)
+    d_n = torch.empty_like(d_q)
+    f.project_device(d_q, d_p, d_n, 10)
+    torch.cuda.synchronize()
+    rp, _ = ot.project_mlod(q, 10, k, rule=0, cutoff=3.0)
+    assert rel_err(d_p.cpu().numpy(), rp, diag).max() < TOL_DIAG
+
+
+def test_kernel_weight_pruning_is_bounded_and_off_by_default(torus20k):
+    """prune_tol = 0 is the reference's walk (bit-identical to no option);
+    a small tolerance drops subtrees that can weigh almost nothing: fewer or
+    equal visits, results within 1e-5 diag of FP64."""
+    torch = pytest.importorskip("torch")
+    pts, nrm, q, ot = torus20k
+    diag = synth.bbox_diag(pts)
+    k = make_kernel("gauss", diag)
+    t = APSSOctree()
+    t.build(pts, nrm)
+    d_q = torch.from_numpy(q).cuda()
+    out = {}
+    for tol in (0.0, 1e-6, 1e-3):
+        f = Fastapss(t, k)
+        f.setScalingProtectionSphere(3.0)
+        f.prune_tol = tol
+        d_p = torch.empty_like(d_q)
+        d_n = torch.empty_like(d_q)
+        f.project_device(d_q, d_p, d_n, 10)
+        torch.cuda.synchronize()
+        out[tol] = (d_p.cpu().numpy(), f.last_stats())
+    base = Fastapss(t, k)
+    base.setScalingProtectionSphere(3.0)
+    d_p = torch.empty_like(d_q)
+    d_n = torch.empty_like(d_q)
+    base.project_device(d_q, d_p, d_n, 10)
+    torch.cuda.synchronize()
+    assert np.array_equal(out[0.0][0], d_p.cpu().numpy()) and out[0.0][1]["pruned"] == 0
+    rp, _ = ot.project_mlod(q, 10, k, rule=0, cutoff=3.0)
+    for tol in (1e-6, 1e-3):
+        p, st = out[tol]
+        assert st["node_visits"] <= out[0.0][1]["node_visits"]
+        assert rel_err(p, rp, diag).max() < TOL_DIAG
+    assert out[1e-3][1]["pruned"] > 0
