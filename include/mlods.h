@@ -353,8 +353,8 @@ int mlods_last_walk_counts(mlods_tree t, int64_t* lane_visits, int64_t* pruned);
  * d_q (float xyz, concatenated per tree: tree i owns queries
  * [offsets[i], offsets[i+1]), offsets is a HOST array of n_trees + 1 entries
  * starting at 0) onto their trees, writing d_out_pts/d_out_nrm in the same
- * layout.  The launch's warps pull chunks of a tree's queries from a device
- * work queue, the trees with the most work first, and walk each chunk with
+ * layout.  The launch's warps take a tree's queries one or two at a time from
+ * a device counter, the trees with the most work first, and walk them with
  * the tree's own specialisation of the walk (kernel family and terms, blend
  * rule, queries per warp), so trees of any size and kernel share the launch.
  * Every tree must be in MLODS_MODE_MLOD with a kernel set; each tree's own
@@ -366,8 +366,8 @@ int mlods_last_walk_counts(mlods_tree t, int64_t* lane_visits, int64_t* pruned);
  * captured once in a CUDA graph and replayed while buffers, offsets, tree
  * settings and n_iterations stay the same (the stream must not be capturing).
  * mlods_batch_tune (the batch's autotuner) times, on the given buffers, walk
- * schedules (one or two queries per warp for every tree), chunk sizes (16 to
- * 256 queries), Morton or input order and the share of the resident grid --
+ * schedules (one or two queries per warp for every tree), Morton or input
+ * order and the share of the resident grid --
  * each candidate run once untimed and once timed -- and keeps the fastest
  * for later calls.  The trees must outlive the batch and must not be rebuilt
  * while it exists. */
@@ -380,12 +380,10 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
                      int32_t n_iterations, void* stream);
 /* Statistics of the last batch launch (synchronises): query-node visits,
  * rounds, overflows, device time (ordering and kernel), the launch shape in
- * use (reorder, grid_pct, queries_per_warp -- 0: each tree's own -- and
- * chunk) and node evaluations (lane_visits, see mlods_last_walk_counts).  Any
- * pointer may be NULL. */
+ * use (reorder, grid_pct, queries_per_warp) and node evaluations
+ * (lane_visits, see mlods_last_walk_counts).  Any pointer may be NULL. */
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
-                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int32_t* chunk,
-                      int64_t* lane_visits);
+                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int64_t* lane_visits);
 
 /* ---- projection without device allocation (extension) ----------------------
  * No counterpart in the reference.  Same computation and results as
@@ -418,17 +416,22 @@ int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float* d_q, floa
  * are free (up to max_batch_queries / max_batch_requests, optionally waiting
  * max_wait_us for more; in arrival order, passing over a request that only a
  * later batch can hold, and cutting one larger than a batch into pieces) and
- * project it with the batched launches (grouped
- * small requests, large requests on their own); results are written to
- * out_pts / out_nrm (either may be NULL),
- * identical to mlods_project_host on the same tree and kernel.  The query and
- * output arrays must stay valid until the ticket is waited for.
- * Admission: a submit that would leave more than max_pending_queries queued
- * returns MLODS_ERR_CAPACITY.  The bounds are the server's memory footprint:
- * a batch in flight holds 36 bytes of device buffers and 36 bytes of pinned
- * staging per query (plus its sort scratch), so device memory stays within
- * n_streams x max_batch_queries x 36 bytes beside the resident trees, and
- * queued work within max_pending_queries.  mlods_server_wait blocks at most timeout_ms
+ * project it with one launch of the queue kernel (every request or piece
+ * walked with its own tree, kernel and iteration count); results are written
+ * to out_pts / out_nrm (either may be NULL), identical to mlods_project_host
+ * on the same tree and kernel (with two queries per warp a request cut into
+ * pieces pairs its queries within each piece: equal to float rounding).  The
+ * query and output arrays must stay valid until the ticket is waited for.
+ * Memory admission, by device footprint: a batch in flight holds, in the
+ * library's stream-ordered pool, 36 bytes of query / result buffers and
+ * about 24 bytes of ordering scratch per query plus its per-request
+ * arguments (mlods_server_batch_bytes gives the exact figure), and returns
+ * them when it finishes; a worker forms its next batch only from what fits
+ * max_device_bytes minus the batches already in flight, so requests are
+ * taken up as batches finish and their memory frees up.  A submit whose
+ * footprint (its device bytes when run, plus 36 bytes of pinned staging per
+ * query) would take the queued work beyond max_pending_bytes returns
+ * MLODS_ERR_CAPACITY.  mlods_server_wait blocks at most timeout_ms
  * (MLODS_ERR_TIMEOUT after that; wait again later), returns the request's
  * status and its latency from submit to results on the host, and retires the
  * ticket.  mlods_server_free cancels queued requests, lets running batches
@@ -436,8 +439,11 @@ int mlods_project_device_noalloc(mlods_tree t, int64_t n, const float* d_q, floa
 typedef struct mlods_server_config {
     int32_t n_streams;            /* worker threads / CUDA streams (default 2) */
     int32_t max_batch_requests;   /* requests per launch (default 4096) */
-    int64_t max_batch_queries;    /* queries per batch (default 2^21; a larger request runs in pieces of this size) */
-    int64_t max_pending_queries;  /* admission bound on queued queries (default 2^26) */
+    int64_t max_batch_queries;    /* queries per batch at most (default 2^18; larger requests run in pieces) */
+    int64_t max_device_bytes;     /* device memory the batches in flight may hold together; 0 (default):
+                                     half the device memory free when the server is created */
+    int64_t max_pending_bytes;    /* admission bound on the footprint of queued requests; 0 (default):
+                                     eight times max_device_bytes */
     int32_t max_wait_us;          /* batching window when less than a batch is queued (default 0) */
     int32_t reserved;
 } mlods_server_config;
@@ -449,6 +455,14 @@ int mlods_server_submit(mlods_server s, int32_t tree, int64_t n, const float* q,
 int mlods_server_wait(mlods_server s, uint64_t ticket, int32_t timeout_ms, double* latency_ms);
 int mlods_server_stats(mlods_server s, int64_t* completed, int64_t* batches, int64_t* queries, int64_t* queued,
                        double* busy_ms);
+/* Device bytes the batches in flight hold now and at most so far, the
+ * footprint of the queued requests, and the two budgets in force (after the
+ * defaults are resolved).  Any pointer may be NULL. */
+int mlods_server_memory(mlods_server s, int64_t* in_flight_bytes, int64_t* peak_in_flight_bytes,
+                        int64_t* pending_bytes, int64_t* max_device_bytes, int64_t* max_pending_bytes);
+/* Device bytes one batch of n_queries queries from n_requests requests (or
+ * pieces) holds while in flight. */
+int64_t mlods_server_batch_bytes(int64_t n_queries, int64_t n_requests);
 int mlods_server_free(mlods_server s);
 
 /* ---- point-set and parameter files (Pn.cpp:102-290, scene.cpp:1183-1250) --

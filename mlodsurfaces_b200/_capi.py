@@ -103,7 +103,8 @@ class mlods_server_config(C.Structure):
         ("n_streams", C.c_int32),
         ("max_batch_requests", C.c_int32),
         ("max_batch_queries", C.c_int64),
-        ("max_pending_queries", C.c_int64),
+        ("max_device_bytes", C.c_int64),
+        ("max_pending_bytes", C.c_int64),
         ("max_wait_us", C.c_int32),
         ("reserved", C.c_int32),
     ]
@@ -176,7 +177,7 @@ SIGNATURES = {
     "mlods_batch_free": (C.c_int, [_P]),
     "mlods_batch_project": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, _P]),
     "mlods_batch_tune": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
-    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32, _I32, _I32, _I64]),
+    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32, _I32, _I64]),
     "mlods_project_device_noalloc": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
     "mlods_dcgrid_adaptive": (C.c_int, [_P, C.c_int32, C.c_int32, _P, C.POINTER(_P)]),
     "mlods_dcgrid_xform": (C.c_int, [_P, _P, _I64]),
@@ -198,6 +199,8 @@ SIGNATURES = {
     "mlods_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int32, C.POINTER(C.c_double)]),
     "mlods_server_stats": (C.c_int, [_P, _I64, _I64, _I64, _I64, C.POINTER(C.c_double)]),
     "mlods_server_free": (C.c_int, [_P]),
+    "mlods_server_memory": (C.c_int, [_P, _I64, _I64, _I64, _I64, _I64]),
+    "mlods_server_batch_bytes": (C.c_int64, [C.c_int64, C.c_int64]),
     "mlods_cloud_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_P)]),
     "mlods_cloud_info": (C.c_int, [_P, _I64, _I32, _P, C.POINTER(C.c_float)]),
     "mlods_cloud_get": (C.c_int, [_P, _P, _P]),

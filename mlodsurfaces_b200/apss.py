@@ -796,13 +796,11 @@ class FastapssBatch:
         ro = C.c_int32(0)
         gp = C.c_int32(0)
         qw = C.c_int32(0)
-        ch = C.c_int32(0)
         lv = C.c_int64(0)
         capi.check(self._lib.mlods_batch_stats(self._b, C.byref(v), C.byref(r), C.byref(o), C.byref(ms),
-                                               C.byref(ro), C.byref(gp), C.byref(qw), C.byref(ch), C.byref(lv)))
+                                               C.byref(ro), C.byref(gp), C.byref(qw), C.byref(lv)))
         return {"node_visits": v.value, "rounds": r.value, "overflows": o.value, "kernel_ms": ms.value,
-                "reorder": ro.value, "grid_pct": gp.value, "queries_per_warp": qw.value, "chunk": ch.value,
-                "lane_visits": lv.value}
+                "reorder": ro.value, "grid_pct": gp.value, "queries_per_warp": qw.value, "lane_visits": lv.value}
 
 
 class ProjectionServer:
@@ -815,8 +813,9 @@ class ProjectionServer:
     batches, one multi-tree launch per batch, on ``n_streams`` worker streams.
     """
 
-    def __init__(self, projectors, n_streams: int = 2, max_batch_queries: int = 1 << 21,
-                 max_batch_requests: int = 4096, max_pending_queries: int = 1 << 26, max_wait_us: int = 0):
+    def __init__(self, projectors, n_streams: int = 2, max_batch_queries: int = 1 << 18,
+                 max_batch_requests: int = 4096, max_device_bytes: int = 0, max_pending_bytes: int = 0,
+                 max_wait_us: int = 0):
         self._lib = capi.load()
         self._projectors = list(projectors)
         for p in self._projectors:
@@ -828,7 +827,8 @@ class ProjectionServer:
         cfg.n_streams = int(n_streams)
         cfg.max_batch_queries = int(max_batch_queries)
         cfg.max_batch_requests = int(max_batch_requests)
-        cfg.max_pending_queries = int(max_pending_queries)
+        cfg.max_device_bytes = int(max_device_bytes)
+        cfg.max_pending_bytes = int(max_pending_bytes)
         cfg.max_wait_us = int(max_wait_us)
         handles = (C.c_void_p * len(self._projectors))(*[p.m_apssOctree.handle.value for p in self._projectors])
         s = C.c_void_p(0)
@@ -863,6 +863,19 @@ class ProjectionServer:
                                                 C.byref(busy)))
         return {"completed": c.value, "batches": b.value, "queries": q.value, "queued": qd.value,
                 "busy_ms": busy.value}
+
+    def memory(self):
+        """Device bytes in flight (now, peak), footprint of the queued work and
+        the two budgets (mlods_server_memory)."""
+        v = [C.c_int64(0) for _ in range(5)]
+        capi.check(self._lib.mlods_server_memory(self._s, *[C.byref(x) for x in v]))
+        return dict(zip(("in_flight_bytes", "peak_in_flight_bytes", "pending_bytes", "max_device_bytes",
+                         "max_pending_bytes"), (x.value for x in v)))
+
+    @staticmethod
+    def batch_bytes(n_queries: int, n_requests: int = 1) -> int:
+        """Device bytes a batch of n_queries from n_requests holds in flight."""
+        return int(capi.load().mlods_server_batch_bytes(int(n_queries), int(n_requests)))
 
     def close(self) -> None:
         if getattr(self, "_s", None):

@@ -4,14 +4,15 @@
 // keeps per-tree launch arguments on the device, orders each tree's queries
 // in Morton order (one radix sort over all of them, the tree index as the key
 // prefix, so every tree keeps its own query range), cuts each tree's range
-// into chunks, and runs the queue kernel (project.cu): its warps pull chunks
-// from a device counter -- the trees with the most work first -- and walk
-// each with the tree's own specialisation of the walk, so trees of very
-// different sizes and kernels load-balance inside a single launch.  With
+// and runs the queue kernel (project.cu): its warps take a tree's queries
+// two (or one) at a time from a device counter -- the trees with the most
+// work first -- and walk them with the tree's own specialisation of the
+// walk, so trees of very different sizes and kernels load-balance inside a
+// single launch.  With
 // use_graph the memset / order / kernel sequence is captured once in a CUDA
 // graph and replayed while the buffers and sizes stay the same.  The
 // autotuner (mlods_batch_tune) times walk schedules (queries per warp),
-// chunk sizes, query orders and grid sizes and keeps the fastest.
+// query orders and grid sizes and keeps the fastest.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -24,24 +25,20 @@ struct mlods_batch_s {
     std::vector<mlods_tree_s*> trees;
     int device = 0;
     // device state
-    mlods::CloudArgs* d_clouds = nullptr;
     int64_t* d_offsets = nullptr;
     mlods::BatchFrame* d_frames = nullptr;
-    int64_t* d_stats = nullptr;  // statistics block (8 int64) then the chunk counter
-    mlods::QueueChunk* d_chunks = nullptr;
-    size_t chunk_cap = 0;
-    int64_t n_chunks = 0;
+    int64_t* d_stats = nullptr;  // statistics block (8 int64) then one 64-bit slot counter per launch group
+    size_t stats_bytes = 0;
     void* d_order_buf = nullptr;
     size_t order_bytes = 0;
-    // what the device holds (re-uploaded when it changes)
+    // what the launches use (re-uploaded when it changes)
     std::vector<mlods::CloudArgs> h_clouds;
     std::vector<int64_t> h_offsets;
-    int h_chunk = -1;
     // launch shape (the tuner's pick)
     int reorder = 1;     // Morton order inside each tree
     int grid_pct = 100;  // share of the resident blocks launched
-    int chunk = 64;      // slots per chunk (a multiple of 4)
-    int qpw = 0;         // queries per warp for every tree; 0: each tree's own setting
+    int qpw = 0;         // queries per warp for every tree; 0: the trees' own setting (the largest, at most 2)
+    int run_qpw = 1;     // the schedule the launches use
     // graph cache
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -65,7 +62,6 @@ namespace mlods
 namespace
 {
 inline size_t up256(size_t v) { return (v + 255) / 256 * 256; }
-constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + 256;  // statistics, then the chunk counter
 
 void drop_graph(mlods_batch_s* b)
 {
@@ -81,7 +77,7 @@ void drop_graph(mlods_batch_s* b)
 int enqueue(mlods_batch_s* b, const float* d_q, int64_t total, bool timed, cudaStream_t s)
 {
     const int n = int(b->trees.size());
-    MLODS_CUDA(cudaMemsetAsync(b->d_stats, 0, kStatsBytes, s));
+    MLODS_CUDA(cudaMemsetAsync(b->d_stats, 0, b->stats_bytes, s));
     uint32_t* order = nullptr;
     if (b->reorder) {
         order = static_cast<uint32_t*>(b->d_order_buf);
@@ -89,15 +85,14 @@ int enqueue(mlods_batch_s* b, const float* d_q, int64_t total, bool timed, cudaS
         MLODS_CUDA(compute_batch_order(d_q, total, b->d_offsets, n, b->d_frames, true, order, tmp, s));
     }
     QueueArgs a;
-    a.clouds = b->d_clouds;
-    a.q_offsets = b->d_offsets;
-    a.chunks = b->d_chunks;
-    a.n_chunks = b->n_chunks;
+    a.clouds = b->h_clouds.data();
+    a.q_offsets = b->h_offsets.data();
+    a.n_clouds = n;
     a.order = order;
-    a.counter = reinterpret_cast<unsigned int*>(b->d_stats + 8);
+    a.counters = reinterpret_cast<unsigned long long*>(b->d_stats + 8);
     a.stats = b->d_stats;
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev0, s));
-    MLODS_CUDA(launch_mlod_queue(a, sm_count_for_current_device(), b->grid_pct, s));
+    MLODS_CUDA(launch_mlod_queue(a, b->run_qpw, sm_count_for_current_device(), b->grid_pct, s));
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev1, s));
     if (timed) b->ran = true;
     return MLODS_OK;
@@ -139,44 +134,32 @@ int batch_prepare(mlods_batch_s* b, const int64_t* offsets, const float* d_q, fl
         fill_cloud_args(T, clouds[size_t(i)], d_q + 3 * offsets[i], d_p + 3 * offsets[i], d_n + 3 * offsets[i], iters,
                         -1.f, T->params.blend_rule);
         CloudArgs& c = clouds[size_t(i)];
-        if (b->qpw) c.qpw = b->qpw;
-        if (c.qpw == 4) c.qpw = 2;  // the queue kernel walks one or two queries per warp
-        c.prune_thr = 0.f;          // the queue kernel walks without pruning
+        c.prune_thr = 0.f;  // the queue kernel walks without pruning
         float ext = 0.f;
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
         frames[size_t(i)] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f,
                                        uint32_t(i)};
     }
+    // one schedule for the whole launch: the tuner's, else the largest the
+    // trees ask for (the queue kernel walks one or two queries per warp)
+    int q = b->qpw;
+    if (!q)
+        for (const CloudArgs& c : clouds) q = std::max(q, c.qpw);
+    q = q >= 2 ? 2 : 1;
+    if (q != b->run_qpw) drop_graph(b);
+    b->run_qpw = q;
+    for (CloudArgs& c : clouds) c.qpw = q;
     const bool same = b->h_clouds.size() == clouds.size() && b->h_offsets.size() == size_t(n + 1) &&
-                      b->h_chunk == b->chunk &&
                       std::memcmp(b->h_clouds.data(), clouds.data(), clouds.size() * sizeof(CloudArgs)) == 0 &&
                       std::memcmp(b->h_offsets.data(), offsets, size_t(n + 1) * sizeof(int64_t)) == 0;
     if (!same) {
         drop_graph(b);
-        std::vector<QueueChunk> chunks;
-        if (build_queue_chunks(clouds.data(), offsets, n, b->chunk, chunks) != MLODS_OK) {
-            set_last_error("batch: chunk size %d is not a multiple of 4", b->chunk);
-            return MLODS_ERR_INVALID;
-        }
-        if (b->chunk_cap < chunks.size()) {
-            cudaFree(b->d_chunks);
-            b->d_chunks = nullptr;
-            b->chunk_cap = 0;
-            MLODS_CUDA(cudaMalloc(&b->d_chunks, chunks.size() * sizeof(QueueChunk)));
-            b->chunk_cap = chunks.size();
-        }
-        MLODS_CUDA(cudaMemcpyAsync(b->d_chunks, chunks.data(), chunks.size() * sizeof(QueueChunk),
-                                   cudaMemcpyHostToDevice, s));
-        MLODS_CUDA(cudaMemcpyAsync(b->d_clouds, clouds.data(), clouds.size() * sizeof(CloudArgs),
-                                   cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaMemcpyAsync(b->d_offsets, offsets, size_t(n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaMemcpyAsync(b->d_frames, frames.data(), frames.size() * sizeof(BatchFrame),
                                    cudaMemcpyHostToDevice, s));
         MLODS_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
-        b->n_chunks = int64_t(chunks.size());
         b->h_clouds = clouds;
         b->h_offsets.assign(offsets, offsets + n + 1);
-        b->h_chunk = b->chunk;
     }
     const size_t need = up256(size_t(total) * 4) + query_order_temp_bytes(total);
     if (b->order_bytes < need) {
@@ -270,10 +253,12 @@ int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* ou
         delete b;
         return cuda_fail(guard.err, "batch_create: select device", __FILE__, __LINE__);
     }
-    cudaError_t e = cudaMalloc(&b->d_clouds, size_t(n_trees) * sizeof(CloudArgs));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_offsets, size_t(n_trees + 1) * sizeof(int64_t));
+    // statistics, then a 64-bit slot counter for each launch group of kQueueMaxClouds trees
+    const size_t n_groups = size_t(queue_groups(n_trees));
+    b->stats_bytes = (8 * sizeof(int64_t) + n_groups * sizeof(uint64_t) + 255) / 256 * 256;
+    cudaError_t e = cudaMalloc(&b->d_offsets, size_t(n_trees + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_frames, size_t(n_trees) * sizeof(BatchFrame));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_stats, kStatsBytes);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_stats, b->stats_bytes);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
     if (e != cudaSuccess) {
@@ -289,11 +274,9 @@ int mlods_batch_free(mlods_batch b)
     if (!b) return MLODS_OK;
     DeviceGuard guard(b->device);
     drop_graph(b);
-    cudaFree(b->d_clouds);
     cudaFree(b->d_offsets);
     cudaFree(b->d_frames);
     cudaFree(b->d_stats);
-    cudaFree(b->d_chunks);
     cudaFree(b->d_order_buf);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -326,12 +309,11 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
     }
     MLODS_ON_DEVICE(b->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // walk schedule, chunk size, query order and grid size
+    // walk schedule, query order and grid size
     struct Cand {
-        int qpw, chunk, reorder, pct;
+        int qpw, reorder, pct;
     };
-    const Cand cands[] = {{1, 64, 1, 100}, {2, 64, 1, 100}, {2, 256, 1, 100}, {2, 16, 1, 100},
-                          {2, 64, 0, 100}, {2, 64, 1, 85}};
+    const Cand cands[] = {{1, 1, 100}, {2, 1, 100}, {2, 0, 100}, {2, 1, 85}};
     float best = INFINITY;
     Cand pick = cands[1];
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -344,7 +326,6 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
     int rc = MLODS_OK;
     for (const Cand& c : cands) {
         b->qpw = c.qpw;
-        b->chunk = c.chunk;
         b->reorder = c.reorder;
         b->grid_pct = c.pct;
         int64_t total = 0;
@@ -369,7 +350,6 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     b->qpw = pick.qpw;
-    b->chunk = pick.chunk;
     b->reorder = pick.reorder;
     b->grid_pct = pick.pct;
     drop_graph(b);
@@ -377,8 +357,7 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
 }
 
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
-                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int32_t* chunk,
-                      int64_t* lane_visits)
+                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int64_t* lane_visits)
 {
     if (!b) {
         set_last_error("null batch");
@@ -400,8 +379,7 @@ int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int6
     if (kernel_ms) *kernel_ms = ms;
     if (reorder) *reorder = b->reorder;
     if (grid_pct) *grid_pct = b->grid_pct;
-    if (queries_per_warp) *queries_per_warp = b->qpw;
-    if (chunk) *chunk = b->chunk;
+    if (queries_per_warp) *queries_per_warp = b->run_qpw;
     if (lane_visits) *lane_visits = h[6];
     return MLODS_OK;
 }

@@ -30,6 +30,7 @@
 // from one persistent launch.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "primitives.cuh"
 #include "project.cuh"
@@ -509,44 +510,31 @@ __global__ void __launch_bounds__(kProjectThreads, WalkShape<QPW>::kMinBlocks) m
 }
 
 // ---- many trees in one persistent launch ---------------------------------
-// Each warp's shared-memory region holds the stack of the widest walk the
-// queue kernel runs (two queries per warp) and a copy of the current cloud's
-// launch arguments.
-constexpr int kQueueCap1 = kProjectStackCap;
-constexpr int kQueueCap2 = kProjectPairStackCap;
-constexpr size_t kQueueStackBytes = sizeof(WarpStack<kQueueCap1, 1>) > sizeof(WarpStack<kQueueCap2, 2>)
-                                        ? sizeof(WarpStack<kQueueCap1, 1>)
-                                        : sizeof(WarpStack<kQueueCap2, 2>);
-constexpr size_t kQueueWarpBytes = (kQueueStackBytes + sizeof(CloudArgs) + 15) / 16 * 16;
-
-// Walks the queries at slots [s0, s1) of the batch order, QPW at a time, with
-// one specialisation of the walk; `base` is the cloud's first global query
-// index (its arguments address its own queries).  Kept out of line: the
-// queue kernel calls one of these per chunk, so each keeps its own registers
-// and its specialised inner loop.
-template <int KTYPE, int NSIG, int RULE, int QPW>
-__device__ __noinline__ void walk_chunk(const CloudArgs& c, const uint32_t* __restrict__ order, int64_t base,
-                                        int64_t s0, int64_t s1, unsigned char* stack_raw, WarpTotals& tot)
-{
-    constexpr int CAP = QPW == 1 ? kQueueCap1 : kQueueCap2;
-    WarpStack<CAP, QPW>& st = *reinterpret_cast<WarpStack<CAP, QPW>*>(stack_raw);
-    for (int64_t s = s0; s < s1; s += QPW) {
-        const int nq = int(min(int64_t(QPW), s1 - s));
-        uint32_t qi[QPW];
-#pragma unroll
-        for (int x = 0; x < QPW; ++x) {
-            const int64_t slot = s + (x < nq ? x : 0);
-            qi[x] = uint32_t((order ? int64_t(__ldg(order + slot)) : slot) - base);
-        }
-        WalkStats ws;
-        project_queries<KTYPE, NSIG, RULE, CAP, QPW>(c, qi, nq, st, ws);
-        tot.add(ws, nq);
-    }
-}
+// The launch arguments of up to kQueueMaxClouds clouds travel BY VALUE in the
+// queue kernel's parameters (__grid_constant__: read in place from the
+// parameter bank), as the single-tree kernel's one cloud does: the walk
+// reads them from read-only memory that no store can alias.  The clouds are
+// laid out along a virtual slot line, the clouds with the most work first,
+// each padded to a multiple of 4 slots, so that the queries a warp takes
+// together are those a launch of the cloud alone would pair.
+struct QueueLaunch {
+    const uint32_t* order;
+    unsigned long long* counter;
+    int64_t* stats;
+    int n;                          // clouds in this launch
+    int64_t v_total;                // length of the virtual slot line
+    int64_t vbase[kQueueMaxClouds + 1];  // virtual start of the j-th cloud in processing order
+    int64_t base[kQueueMaxClouds];  // first slot (and global query index) of each cloud
+    int64_t len[kQueueMaxClouds];   // its query count
+    int32_t cloud_at[kQueueMaxClouds];  // the cloud at the j-th place of the line
+    int32_t spec[kQueueMaxClouds];  // its walk specialisation
+    CloudArgs clouds[kQueueMaxClouds];
+};
+static_assert(sizeof(QueueLaunch) <= 32000, "queue launch parameters must fit the 32 KB kernel parameter space");
 
 // The specialisation of the walk a cloud runs with: kernel family and number
 // of multi-Gaussian terms (2-6 and 8 have their own code, other counts share
-// one), blend rule, queries per warp.
+// one) and blend rule.
 inline int walk_spec_id(const CloudArgs& c)
 {
     int k = 8;  // multi-Gaussian, terms counted at run time
@@ -554,73 +542,71 @@ inline int walk_spec_id(const CloudArgs& c)
     else if (c.kc.type == MLODS_SINGULAR) k = 1;
     else if (c.kc.nsig >= 2 && c.kc.nsig <= 6) k = c.kc.nsig;
     else if (c.kc.nsig == 8) k = 7;
-    const int rule = c.rule == MLODS_BLEND_GPU ? 0 : 1;
-    const int q = c.qpw == 2 ? 1 : 0;
-    return (q * 2 + rule) * 9 + k;
+    return (c.rule == MLODS_BLEND_GPU ? 0 : 1) * 9 + k;
 }
 
-template <int RULE, int QPW>
-__device__ __forceinline__ void walk_chunk_k(int k, const CloudArgs& c, const uint32_t* order, int64_t base,
-                                             int64_t s0, int64_t s1, unsigned char* st, WarpTotals& tot)
+template <int RULE, int CAP, int QPW>
+__device__ __forceinline__ void walk_k(int k, const CloudArgs& c, const uint32_t (&qi)[QPW], int nq,
+                                       WarpStack<CAP, QPW>& st, WalkStats& ws)
 {
     switch (k) {
-    case 0: walk_chunk<MLODS_GAUSSIAN, 0, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    case 1: walk_chunk<MLODS_SINGULAR, 0, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    case 2: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 2, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    case 3: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 3, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    case 4: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 4, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    case 5: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 5, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    case 6: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 6, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    case 7: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 8, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
-    default: walk_chunk<MLODS_GAUSSIAN_MULTIPLE, 0, RULE, QPW>(c, order, base, s0, s1, st, tot); break;
+    case 0: project_queries<MLODS_GAUSSIAN, 0, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 1: project_queries<MLODS_SINGULAR, 0, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 2: project_queries<MLODS_GAUSSIAN_MULTIPLE, 2, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 3: project_queries<MLODS_GAUSSIAN_MULTIPLE, 3, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 4: project_queries<MLODS_GAUSSIAN_MULTIPLE, 4, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 5: project_queries<MLODS_GAUSSIAN_MULTIPLE, 5, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 6: project_queries<MLODS_GAUSSIAN_MULTIPLE, 6, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 7: project_queries<MLODS_GAUSSIAN_MULTIPLE, 8, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    default: project_queries<MLODS_GAUSSIAN_MULTIPLE, 0, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
     }
 }
 
-// Every cloud of a batch in ONE persistent launch: the warps pull chunks (a
-// cloud and a run of its slots in the batch order) from a device work queue
-// and walk each with the cloud's own specialisation; a warp copies a cloud's
-// launch arguments to shared memory when it moves to another cloud.  Chunks
-// start at multiples of 4 slots from their cloud's first slot, so the queries
-// that share a walk are those a launch of the cloud alone would pair: the
-// results equal per-tree launches bit for bit.
-__global__ void __launch_bounds__(kProjectThreads, kProjectPairMinBlocks) mlod_queue_kernel(QueueArgs a)
+// Every cloud of a group in ONE persistent launch: each warp takes QPW
+// consecutive virtual slots from the counter (consecutive warps take
+// consecutive queries, as in the single-tree kernel, so the warps working at
+// any moment share node records in L1 and L2), finds their cloud by binary
+// search over the line and walks them with the cloud's own specialisation;
+// the kernel is compiled with the schedule's registers and blocks per SM.
+template <int QPW>
+__global__ void __launch_bounds__(kProjectThreads, WalkShape<QPW>::kMinBlocks)
+    mlod_queue_kernel(const __grid_constant__ QueueLaunch p)
 {
+    constexpr int CAP = WalkShape<QPW>::kCap;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned char* region = smem_raw + size_t(warp) * kQueueWarpBytes;
-    CloudArgs* cache = reinterpret_cast<CloudArgs*>(region + kQueueStackBytes);
-    int cached = -1;
-    int64_t base = 0;
+    const int lane = threadIdx.x & 31;
+    WarpStack<CAP, QPW>& st = reinterpret_cast<WarpStack<CAP, QPW>*>(smem_raw)[threadIdx.x >> 5];
     WarpTotals tot;
     for (;;) {
-        unsigned int ci = 0;
-        if (lane == 0) ci = atomicAdd(a.counter, 1u);
-        ci = __shfl_sync(kFull, ci, 0);
-        if (int64_t(ci) >= a.n_chunks) break;
-        const QueueChunk ch = a.chunks[ci];
-        if (ch.cloud != cached) {
-            __syncwarp();  // every lane is done with the previous arguments
-            const uint32_t* src = reinterpret_cast<const uint32_t*>(a.clouds + ch.cloud);
-            uint32_t* dst = reinterpret_cast<uint32_t*>(cache);
-            for (int w = lane; w < int(sizeof(CloudArgs) / 4); w += 32) dst[w] = __ldg(src + w);
-            cached = ch.cloud;
-            base = __ldg(a.q_offsets + ch.cloud);
-            __syncwarp();
+        unsigned long long v = 0;
+        if (lane == 0) v = atomicAdd(p.counter, (unsigned long long)QPW);
+        v = __shfl_sync(kFull, v, 0);
+        if (int64_t(v) >= p.v_total) break;
+        int lo = 0, hi = p.n;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (int64_t(v) >= p.vbase[mid]) lo = mid; else hi = mid;
         }
-        const int spec = ch.spec;
-        const int k = spec % 9, rule = (spec / 9) & 1, q2 = spec / 18;
-        if (q2) {
-            if (rule == 0) walk_chunk_k<MLODS_BLEND_GPU, 2>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end,
-                                                            region, tot);
-            else walk_chunk_k<MLODS_BLEND_CPU, 2>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end, region, tot);
-        } else {
-            if (rule == 0) walk_chunk_k<MLODS_BLEND_GPU, 1>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end,
-                                                            region, tot);
-            else walk_chunk_k<MLODS_BLEND_CPU, 1>(k, *cache, a.order, base, ch.slot_begin, ch.slot_end, region, tot);
+        const int ci = p.cloud_at[lo];
+        const int64_t off = int64_t(v) - p.vbase[lo];
+        const int nq = int(min(int64_t(QPW), p.len[ci] - off));
+        if (nq <= 0) continue;  // the padding at the end of a cloud
+        const int64_t b = p.base[ci];
+        uint32_t qi[QPW];
+#pragma unroll
+        for (int x = 0; x < QPW; ++x) {
+            const int64_t slot = b + off + (x < nq ? x : 0);
+            qi[x] = uint32_t((p.order ? int64_t(__ldg(p.order + slot)) : slot) - b);
         }
+        const CloudArgs& c = p.clouds[ci];
+        const int sp = p.spec[ci];
+        WalkStats ws;
+        if (sp < 9) walk_k<MLODS_BLEND_GPU, CAP, QPW>(sp, c, qi, nq, st, ws);
+        else walk_k<MLODS_BLEND_CPU, CAP, QPW>(sp - 9, c, qi, nq, st, ws);
+        tot.add(ws, nq);
     }
-    tot.flush(a.stats);
-    tot.flush_pruned(a.stats);
+    tot.flush(p.stats);
+    tot.flush_pruned(p.stats);
 }
 
 template <typename Kern>
@@ -753,36 +739,59 @@ cudaError_t launch_mlod_project(const ProjectArgs& a, int ktype, int rule, int s
     return launch_rule<MLODS_BLEND_CPU, 1>(a, ktype, sm_count, s);
 }
 
-int build_queue_chunks(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, int chunk,
-                       std::vector<QueueChunk>& out)
+namespace
 {
-    if (chunk < 4 || chunk % 4 != 0) return MLODS_ERR_INVALID;
-    // the clouds with the most work first (query count x iterations): the
-    // last chunks handed out are small ones, so the launch ends evenly
-    std::vector<int> idx(static_cast<size_t>(n_clouds));
-    for (int i = 0; i < n_clouds; ++i) idx[size_t(i)] = i;
-    auto work = [&](int i) { return (q_offsets[i + 1] - q_offsets[i]) * int64_t(std::max(clouds[i].n_iter, 1)); };
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return work(a) > work(b); });
-    out.clear();
-    for (int i : idx) {
-        const int spec = walk_spec_id(clouds[i]);
-        for (int64_t s = q_offsets[i]; s < q_offsets[i + 1]; s += chunk)
-            out.push_back(QueueChunk{i, spec, s, std::min(s + chunk, q_offsets[i + 1])});
+template <int QPW>
+cudaError_t launch_queue_typed(const QueueArgs& a, int sm_count, int grid_pct, cudaStream_t s)
+{
+    constexpr int CAP = WalkShape<QPW>::kCap;
+    const size_t smem = size_t(kProjectThreads / 32) * sizeof(WarpStack<CAP, QPW>);
+    const int n_groups = queue_groups(a.n_clouds);
+    for (int g = 0; g < n_groups; ++g) {
+        const int c0 = g * kQueueMaxClouds, nc = std::min(kQueueMaxClouds, a.n_clouds - c0);
+        QueueLaunch p;
+        std::memset(&p, 0, sizeof p);
+        p.order = a.order;
+        p.counter = a.counters + g;
+        p.stats = a.stats;
+        p.n = nc;
+        std::vector<int> idx(static_cast<size_t>(nc));
+        for (int i = 0; i < nc; ++i) {
+            idx[size_t(i)] = i;
+            p.clouds[i] = a.clouds[c0 + i];
+            p.base[i] = a.q_offsets[c0 + i];
+            p.len[i] = a.q_offsets[c0 + i + 1] - a.q_offsets[c0 + i];
+            p.spec[i] = walk_spec_id(p.clouds[i]);
+        }
+        // the clouds with the most work first, so that the launch ends on small ones
+        auto work = [&](int i) { return p.len[i] * int64_t(std::max(p.clouds[i].n_iter, 1)); };
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return work(x) > work(y); });
+        int64_t v = 0;
+        for (int j = 0; j < nc; ++j) {
+            p.cloud_at[j] = idx[size_t(j)];
+            p.vbase[j] = v;
+            v += (p.len[idx[size_t(j)]] + 3) / 4 * 4;
+        }
+        p.vbase[nc] = v;
+        p.v_total = v;
+        if (v == 0) continue;
+        cudaError_t e = cudaSuccess;
+        int64_t grid = persistent_grid(mlod_queue_kernel<QPW>, smem, (v + QPW - 1) / QPW, sm_count, &e);
+        if (e != cudaSuccess) return e;
+        if (grid_pct > 0 && grid_pct < 100) grid = std::max<int64_t>(1, grid * grid_pct / 100);
+        mlod_queue_kernel<QPW><<<unsigned(grid), kProjectThreads, smem, s>>>(p);
+        note_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
     }
-    return MLODS_OK;
+    return cudaSuccess;
 }
+}  // namespace
 
-cudaError_t launch_mlod_queue(const QueueArgs& a, int sm_count, int grid_pct, cudaStream_t s)
+cudaError_t launch_mlod_queue(const QueueArgs& a, int queries_per_warp, int sm_count, int grid_pct, cudaStream_t s)
 {
-    const size_t smem = size_t(kProjectThreads / 32) * kQueueWarpBytes;
-    cudaError_t e = cudaSuccess;
-    // one warp per chunk at most
-    int64_t grid = persistent_grid(mlod_queue_kernel, smem, a.n_chunks, sm_count, &e);
-    if (e != cudaSuccess) return e;
-    if (grid_pct > 0 && grid_pct < 100) grid = std::max<int64_t>(1, grid * grid_pct / 100);
-    mlod_queue_kernel<<<unsigned(grid), kProjectThreads, smem, s>>>(a);
-    note_launch();
-    return cudaGetLastError();
+    if (queries_per_warp == 2) return launch_queue_typed<2>(a, sm_count, grid_pct, s);
+    return launch_queue_typed<1>(a, sm_count, grid_pct, s);
 }
 
 size_t query_order_temp_bytes(int64_t n)

@@ -18,7 +18,7 @@ namespace mlods
 #define MLODS_PROJECT_STACK_CAP 160
 #endif
 #ifndef MLODS_PROJECT_PAIR_MIN_BLOCKS
-#define MLODS_PROJECT_PAIR_MIN_BLOCKS 8
+#define MLODS_PROJECT_PAIR_MIN_BLOCKS 7
 #endif
 #ifndef MLODS_PROJECT_PAIR_STACK_CAP
 #define MLODS_PROJECT_PAIR_STACK_CAP 128
@@ -60,34 +60,33 @@ struct ProjectArgs {
     int queries_per_warp = 1;  // 1, or 2: consecutive queries of `order` share one walk
 };
 
-// Many trees in ONE persistent launch.  A chunk is a run of consecutive
-// slots of the batch order that all belong to one cloud; the warps of the
-// queue kernel pull chunks from a device counter.  order[slot] is the global
-// index of the query at that slot (nullptr: slot = query index); the queries
-// of cloud c occupy the global range [q_offsets[c], q_offsets[c + 1]), and the
-// slots of its chunks lie in that same range.
-struct QueueChunk {
-    int32_t cloud;
-    int32_t spec;          // walk specialisation (kernel family, terms, blend rule, queries per warp)
-    int64_t slot_begin, slot_end;
-};
-
+// Many trees in ONE persistent launch.  The queries of cloud c occupy the
+// global range [q_offsets[c], q_offsets[c + 1]) of the concatenated buffers,
+// and the same range of slots of the batch order: order[slot] is the global
+// index of the query processed at that slot (nullptr: slot = query index).
+// The warps of the queue kernel take queries_per_warp consecutive slots of
+// one cloud at a time from a device counter, as the single-tree kernel does
+// over one cloud.
 struct QueueArgs {
-    const CloudArgs* clouds;   // each cloud's q_in / out_p / out_n address its own range
-    const int64_t* q_offsets;  // n_clouds + 1 entries
-    const QueueChunk* chunks;
-    int64_t n_chunks;
-    const uint32_t* order;
-    unsigned int* counter;     // chunk counter, zero before launch
-    int64_t* stats;            // as ProjectArgs::stats
+    const CloudArgs* clouds;   // host array: each cloud's q_in / out_p / out_n address its own range
+    const int64_t* q_offsets;  // host array, n_clouds + 1 entries
+    int n_clouds;
+    const uint32_t* order;     // device
+    unsigned long long* counters;  // device: one 64-bit slot counter per launch group, zero before launch
+    int64_t* stats;            // device, as ProjectArgs::stats
 };
 
-// The chunks of a batch: each cloud's slot range cut into runs of `chunk`
-// slots (a multiple of 4, so the queries that share a walk are those a launch
-// of the cloud alone would pair), the clouds with the most work first.
-int build_queue_chunks(const CloudArgs* clouds, const int64_t* q_offsets, int n_clouds, int chunk,
-                       std::vector<QueueChunk>& out);
-cudaError_t launch_mlod_queue(const QueueArgs& a, int sm_count, int grid_pct, cudaStream_t s);
+// Clouds per launch of the queue kernel: their launch arguments travel by
+// value in the kernel's parameters (within the 32 KB parameter limit); a
+// batch of more clouds runs as consecutive launches of up to this many.
+constexpr int kQueueMaxClouds = 80;
+inline int queue_groups(int n_clouds) { return (n_clouds + kQueueMaxClouds - 1) / kQueueMaxClouds; }
+
+// The queue kernel over every group of clouds (usually one launch); every
+// cloud is walked queries_per_warp (1 or 2) queries at a time, the pairs
+// aligned to the cloud's first slot, so that results equal per-tree
+// launches with the same schedule bit for bit.
+cudaError_t launch_mlod_queue(const QueueArgs& a, int queries_per_warp, int sm_count, int grid_pct, cudaStream_t s);
 
 // Per-cloud frame used to key queries: the cloud's rank in the batch order
 // (clouds of a batch keep their own rank: their slots are their query range)

@@ -4,13 +4,20 @@
 // the legacy stream.  Requests (a tree, n host query points, an iteration
 // count, optionally their own weight kernel) are queued by any host thread
 // and answered asynchronously.  Worker threads, one per CUDA stream, take
-// what is queued (up to a batch size; large requests in pieces, small ones
-// passing over those that do not fit) whenever they are free, stage it in
-// pinned memory, and project the batch with the batched launches (each
-// request or piece is one "cloud", with its own tree, kernel and iteration
-// count), so copies of one batch overlap the projection of another.  Admission is bounded: a submit that would queue
-// more than max_pending queries is refused (MLODS_ERR_CAPACITY) instead of
-// growing host or device memory without limit.  Every wait has a timeout.
+// what is queued whenever they are free (up to a batch size; large requests
+// in pieces, small ones passing over those that do not fit), stage it in
+// pinned memory, and project the batch with one launch of the queue kernel
+// (each request or piece is one "cloud", with its own tree, kernel and
+// iteration count), so copies of one batch overlap the projection of another.
+//
+// Admission follows the device memory: a batch's device buffers (queries,
+// results, ordering scratch, launch arguments) come from the library's
+// stream-ordered pool, sized for that batch, and go back when it finishes; a
+// worker forms a batch only from what fits the device budget minus the
+// batches in flight, so queued requests are taken up as batches finish and
+// memory frees up.  A submit whose footprint would take the queued work
+// beyond its own bound is refused (MLODS_ERR_CAPACITY) instead of growing
+// host or device memory without limit.  Every wait has a timeout.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -56,23 +63,17 @@ struct Piece {
     int64_t off, n;
 };
 
+// Host-side staging of one worker (pinned, grown on demand); the device
+// buffers of a batch come from the stream-ordered pool per batch.
 struct Worker {
     cudaStream_t s = nullptr;
-    float* h_stage = nullptr;  // pinned: 9 floats per query (q, p, n)
+    float* h_stage = nullptr;  // 9 floats per query (q, p, n)
     size_t h_cap = 0;
-    float* d_buf = nullptr;  // 9 floats per query
-    mlods::CloudArgs* h_clouds = nullptr;  // pinned
+    mlods::CloudArgs* h_clouds = nullptr;
     int64_t* h_offsets = nullptr;
     mlods::BatchFrame* h_frames = nullptr;
-    mlods::CloudArgs* d_clouds = nullptr;
-    int64_t* d_offsets = nullptr;
-    mlods::BatchFrame* d_frames = nullptr;
     size_t cloud_cap = 0;
-    mlods::QueueChunk* h_chunks = nullptr;  // pinned
-    mlods::QueueChunk* d_chunks = nullptr;
-    size_t chunk_cap = 0;
     int64_t* d_stats = nullptr;
-    void* d_order = nullptr;  // query order and its sort buffers
     std::thread thread;
 };
 
@@ -80,13 +81,16 @@ struct Worker {
 
 struct mlods_server_s {
     std::vector<mlods_tree_s*> trees;
-    mlods_server_config cfg{};
+    mlods_server_config cfg{};  // budgets resolved at creation
     int device = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Request*> queue;
     std::unordered_map<uint64_t, Request*> live;
-    int64_t queued = 0;
+    int64_t queued = 0;          // queries waiting for a batch
+    int64_t pending_bytes = 0;   // footprint of the queued queries
+    int64_t in_flight = 0;       // device bytes held by the batches in flight
+    int64_t peak_in_flight = 0;
     uint64_t next_ticket = 1;
     bool stopping = false;
     std::vector<Worker*> workers;
@@ -100,8 +104,53 @@ namespace mlods
 namespace
 {
 inline size_t al256(size_t v) { return (v + 255) / 256 * 256; }
-constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + 256;  // statistics, then the chunk counter
-constexpr int kServeChunk = 64;  // queries per work-queue chunk
+// statistics, then a 64-bit slot counter for each launch group of
+// kQueueMaxClouds pieces (max_batch_requests is at most kMaxServeGroups groups)
+constexpr int kMaxServeGroups = 64;
+constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + kMaxServeGroups * sizeof(uint64_t);
+
+// Device layout of one batch of n queries from r requests or pieces.
+struct BatchLayout {
+    size_t qpn, order, temp, offsets, frames, total;
+};
+
+BatchLayout batch_layout(int64_t n, int64_t r)
+{
+    BatchLayout L;
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        const size_t here = at;
+        at += al256(bytes);
+        return here;
+    };
+    // (the launch arguments travel in the kernel's parameters)
+    L.qpn = take(size_t(n) * 36);
+    L.order = take(size_t(n) * 4);
+    L.temp = take(query_order_temp_bytes(n));
+    L.offsets = take(size_t(r + 1) * sizeof(int64_t));
+    L.frames = take(size_t(r) * sizeof(BatchFrame));
+    L.total = at;
+    return L;
+}
+
+int64_t batch_bytes(int64_t n, int64_t r) { return n > 0 ? int64_t(batch_layout(n, r).total) : 0; }
+
+// Footprint of a queued request's n remaining queries: its device bytes when
+// it runs alone, plus its pinned staging.
+int64_t request_bytes(int64_t n) { return n > 0 ? batch_bytes(n, 1) + n * 36 : 0; }
+
+// The most queries a batch of r requests can hold within `bytes` of device
+// memory (0 if not even one).
+int64_t queries_within(int64_t bytes, int64_t r)
+{
+    if (batch_bytes(1, r) > bytes) return 0;
+    int64_t lo = 1, hi = std::max<int64_t>(1, bytes / 36);
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo + 1) / 2;
+        if (batch_bytes(mid, r) <= bytes) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
 
 int grow_pinned(void** p, size_t bytes)
 {
@@ -111,23 +160,10 @@ int grow_pinned(void** p, size_t bytes)
     return MLODS_OK;
 }
 
-int grow_device(void** p, size_t bytes)
-{
-    cudaFree(*p);
-    *p = nullptr;
-    MLODS_CUDA(cudaMalloc(p, bytes));
-    return MLODS_OK;
-}
-
 int ensure_capacity(Worker& w, int64_t total, size_t n_req)
 {
     if (w.h_cap < size_t(total)) {
-        int rc = grow_pinned(reinterpret_cast<void**>(&w.h_stage), size_t(total) * 36);
-        if (rc != MLODS_OK) return rc;
-        rc = grow_device(reinterpret_cast<void**>(&w.d_buf), size_t(total) * 36);
-        if (rc != MLODS_OK) return rc;
-        const size_t ob = al256(size_t(total) * 4) + query_order_temp_bytes(total);
-        rc = grow_device(&w.d_order, ob);
+        const int rc = grow_pinned(reinterpret_cast<void**>(&w.h_stage), size_t(total) * 36);
         if (rc != MLODS_OK) return rc;
         w.h_cap = size_t(total);
     }
@@ -136,81 +172,78 @@ int ensure_capacity(Worker& w, int64_t total, size_t n_req)
         int rc = grow_pinned(reinterpret_cast<void**>(&w.h_clouds), cap * sizeof(CloudArgs));
         if (rc == MLODS_OK) rc = grow_pinned(reinterpret_cast<void**>(&w.h_offsets), (cap + 1) * sizeof(int64_t));
         if (rc == MLODS_OK) rc = grow_pinned(reinterpret_cast<void**>(&w.h_frames), cap * sizeof(BatchFrame));
-        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_clouds), cap * sizeof(CloudArgs));
-        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_offsets), (cap + 1) * sizeof(int64_t));
-        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_frames), cap * sizeof(BatchFrame));
         if (rc != MLODS_OK) return rc;
         w.cloud_cap = cap;
     }
     return MLODS_OK;
 }
 
-// Projects one batch of requests on the worker's stream; host outputs are
-// written before it returns.
+// Projects one batch of requests on the worker's stream with device buffers
+// from the stream-ordered pool (returned before this returns); host outputs
+// are written before it returns.
 int run_batch(mlods_server_s* S, Worker& w, const std::vector<Piece>& batch)
 {
     int64_t total = 0;
     for (const Piece& pc : batch) total += pc.n;
-    int rc = ensure_capacity(w, total, batch.size());
+    const size_t nc = batch.size();
+    const BatchLayout L = batch_layout(total, int64_t(nc));
+    int rc = ensure_capacity(w, total, nc);
     if (rc != MLODS_OK) return rc;
+    char* mem = nullptr;
+    MLODS_CUDA(scratch_alloc(reinterpret_cast<void**>(&mem), L.total, w.s));
+    float* dq = reinterpret_cast<float*>(mem + L.qpn);
+    float* dp = dq + 3 * total;
+    float* dn = dq + 6 * total;
+    uint32_t* order = reinterpret_cast<uint32_t*>(mem + L.order);
+    int64_t* d_offsets = reinterpret_cast<int64_t*>(mem + L.offsets);
+    BatchFrame* d_frames = reinterpret_cast<BatchFrame*>(mem + L.frames);
     float* hq = w.h_stage;
     float* hp = w.h_stage + 3 * total;
     float* hn = w.h_stage + 6 * total;
-    float* dq = w.d_buf;
-    float* dp = w.d_buf + 3 * total;
-    float* dn = w.d_buf + 6 * total;
     int64_t off = 0;
-    for (size_t i = 0; i < batch.size(); ++i) {
+    int qpw = 1;  // one schedule per launch: the largest the batch's trees ask for
+    for (size_t i = 0; i < nc; ++i) {
         const Request* r = batch[i].r;
         mlods_tree_s* T = S->trees[size_t(r->tree)];
         std::memcpy(hq + 3 * off, r->q + 3 * batch[i].off, size_t(batch[i].n) * 12);
         CloudArgs& c = w.h_clouds[i];
         fill_cloud_args(T, c, dq + 3 * off, dp + 3 * off, dn + 3 * off, r->iters, -1.f, T->params.blend_rule);
         if (r->own_kernel) c.kc = r->kc;
+        c.prune_thr = 0.f;  // the queue kernel walks without pruning
+        qpw = std::max(qpw, std::min(c.qpw, 2));
         float ext = 0.f;
         for (int a = 0; a < 3; ++a) ext = std::max(ext, T->BB[a] - T->bb[a]);
-        c.prune_thr = 0.f;  // the queue kernel walks without pruning
-        if (c.qpw == 4) c.qpw = 2;
         w.h_frames[i] = BatchFrame{T->origin[0], T->origin[1], T->origin[2], ext > 0.f ? 1.f / ext : 1.f,
                                    uint32_t(i)};
         w.h_offsets[i] = off;
         off += batch[i].n;
     }
-    w.h_offsets[batch.size()] = total;
-    const size_t nc = batch.size();
-    std::vector<QueueChunk> chunks;
-    rc = build_queue_chunks(w.h_clouds, w.h_offsets, int(nc), kServeChunk, chunks);
-    if (rc != MLODS_OK) return rc;
-    if (w.chunk_cap < chunks.size()) {
-        const size_t cap = std::max(chunks.size(), w.chunk_cap + w.chunk_cap / 2);
-        rc = grow_pinned(reinterpret_cast<void**>(&w.h_chunks), cap * sizeof(QueueChunk));
-        if (rc == MLODS_OK) rc = grow_device(reinterpret_cast<void**>(&w.d_chunks), cap * sizeof(QueueChunk));
-        if (rc != MLODS_OK) return rc;
-        w.chunk_cap = cap;
+    w.h_offsets[nc] = total;
+    cudaError_t e = cudaMemcpyAsync(dq, hq, size_t(total) * 12, cudaMemcpyHostToDevice, w.s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_offsets, w.h_offsets, (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, w.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_frames, w.h_frames, nc * sizeof(BatchFrame), cudaMemcpyHostToDevice, w.s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.d_stats, 0, kStatsBytes, w.s);
+    if (e == cudaSuccess)
+        e = compute_batch_order(dq, total, d_offsets, int(nc), d_frames, true, order, mem + L.temp, w.s);
+    if (e == cudaSuccess) {
+        QueueArgs a;
+        a.clouds = w.h_clouds;
+        a.q_offsets = w.h_offsets;
+        a.n_clouds = int(nc);
+        a.order = order;
+        a.counters = reinterpret_cast<unsigned long long*>(w.d_stats + 8);
+        a.stats = w.d_stats;
+        e = launch_mlod_queue(a, qpw, sm_count_for_current_device(), 100, w.s);
     }
-    std::memcpy(w.h_chunks, chunks.data(), chunks.size() * sizeof(QueueChunk));
-    MLODS_CUDA(cudaMemcpyAsync(dq, hq, size_t(total) * 12, cudaMemcpyHostToDevice, w.s));
-    MLODS_CUDA(cudaMemcpyAsync(w.d_clouds, w.h_clouds, nc * sizeof(CloudArgs), cudaMemcpyHostToDevice, w.s));
-    MLODS_CUDA(cudaMemcpyAsync(w.d_offsets, w.h_offsets, (nc + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, w.s));
-    MLODS_CUDA(cudaMemcpyAsync(w.d_frames, w.h_frames, nc * sizeof(BatchFrame), cudaMemcpyHostToDevice, w.s));
-    MLODS_CUDA(cudaMemcpyAsync(w.d_chunks, w.h_chunks, chunks.size() * sizeof(QueueChunk), cudaMemcpyHostToDevice,
-                               w.s));
-    MLODS_CUDA(cudaMemsetAsync(w.d_stats, 0, kStatsBytes, w.s));
-    uint32_t* order = static_cast<uint32_t*>(w.d_order);
-    char* tmp = static_cast<char*>(w.d_order) + al256(size_t(total) * 4);
-    MLODS_CUDA(compute_batch_order(dq, total, w.d_offsets, int(nc), w.d_frames, true, order, tmp, w.s));
-    QueueArgs a;
-    a.clouds = w.d_clouds;
-    a.q_offsets = w.d_offsets;
-    a.chunks = w.d_chunks;
-    a.n_chunks = int64_t(chunks.size());
-    a.order = order;
-    a.counter = reinterpret_cast<unsigned int*>(w.d_stats + 8);
-    a.stats = w.d_stats;
-    MLODS_CUDA(launch_mlod_queue(a, sm_count_for_current_device(), 100, w.s));
-    MLODS_CUDA(cudaMemcpyAsync(hp, dp, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s));
-    MLODS_CUDA(cudaMemcpyAsync(hn, dn, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s));
-    MLODS_CUDA(cudaStreamSynchronize(w.s));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hp, dp, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hn, dn, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s);
+    const cudaError_t ef = scratch_free(mem, w.s);  // stream-ordered: after the copies
+    if (e == cudaSuccess) e = ef;
+    const cudaError_t es = cudaStreamSynchronize(w.s);
+    if (e == cudaSuccess) e = es;
+    if (rc != MLODS_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "server batch", __FILE__, __LINE__);
     off = 0;
     for (const Piece& pc : batch) {
         if (pc.r->out_p) std::memcpy(pc.r->out_p + 3 * pc.off, hp + 3 * off, size_t(pc.n) * 12);
@@ -221,34 +254,44 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Piece>& batch)
 }
 
 // The next batch, under the server lock: queued requests in arrival order,
-// each taken whole while it fits the batch; one larger than a whole batch is
-// cut into batch-sized pieces (it keeps its place until its last piece is
-// handed out); a request that fits only a later batch is passed over, so
-// small requests do not wait behind large ones.  A request that was passed
-// over heads the queue, so the next batch starts with it.
-void form_batch(mlods_server_s* S, std::vector<Piece>& batch)
+// each taken whole while it fits the batch -- at most max_batch_queries and
+// max_batch_requests, and no more device memory than the budget leaves beside
+// the batches in flight; one larger than what a batch can hold is cut into
+// pieces (it keeps its place until its last piece is handed out); a request
+// that fits only a later batch is passed over, so small requests do not wait
+// behind large ones.  A request that was passed over heads the queue, so the
+// next batch starts with it.  Returns the batch's device bytes (0: nothing
+// fits until memory frees up).
+int64_t form_batch(mlods_server_s* S, std::vector<Piece>& batch)
 {
-    const int64_t cap = std::max<int64_t>(S->cfg.max_batch_queries, 1);
-    int64_t budget = cap;
-    for (auto it = S->queue.begin(); it != S->queue.end() && budget > 0;) {
+    const int64_t avail = S->cfg.max_device_bytes - S->in_flight;
+    int64_t total = 0;
+    for (auto it = S->queue.begin(); it != S->queue.end();) {
         if (int64_t(batch.size()) >= S->cfg.max_batch_requests) break;
+        const int64_t nr = int64_t(batch.size()) + 1;
+        const int64_t cap = std::min(S->cfg.max_batch_queries, queries_within(avail, nr));
+        const int64_t room = cap - total;
+        if (room <= 0) break;
         Request* r = *it;
         const int64_t rest = r->n - r->taken;
-        if (rest <= budget) {
-            batch.push_back(Piece{r, r->taken, rest});
-            r->taken += rest;
-            budget -= rest;
-            S->queued -= rest;
-            it = S->queue.erase(it);
-        } else if (budget == cap) {
-            batch.push_back(Piece{r, r->taken, cap});
-            r->taken += cap;
-            budget = 0;
-            S->queued -= cap;
+        int64_t take = 0;
+        if (rest <= room) {
+            take = rest;
+        } else if (batch.empty()) {
+            take = room;  // a piece as large as the batch can hold
         } else {
-            ++it;
+            ++it;         // fits a later batch only: pass over it
+            continue;
         }
+        batch.push_back(Piece{r, r->taken, take});
+        S->pending_bytes -= request_bytes(rest) - request_bytes(rest - take);
+        r->taken += take;
+        total += take;
+        S->queued -= take;
+        if (r->taken == r->n) it = S->queue.erase(it);
+        else break;  // the batch is full
     }
+    return batch.empty() ? 0 : batch_bytes(total, int64_t(batch.size()));
 }
 
 void worker_main(mlods_server_s* S, Worker* w)
@@ -257,22 +300,30 @@ void worker_main(mlods_server_s* S, Worker* w)
     std::vector<Piece> batch;
     for (;;) {
         batch.clear();
+        int64_t bytes = 0;
         {
             std::unique_lock<std::mutex> lock(S->mu);
-            while (!S->stopping && S->queue.empty()) S->cv_work.wait_for(lock, std::chrono::milliseconds(50));
-            if (S->stopping) return;
-            if (S->cfg.max_wait_us > 0 && S->queued < S->cfg.max_batch_queries)
-                S->cv_work.wait_for(lock, std::chrono::microseconds(S->cfg.max_wait_us),
-                                    [&] { return S->stopping || S->queued >= S->cfg.max_batch_queries; });
-            if (S->stopping) return;
-            form_batch(S, batch);
+            for (;;) {
+                while (!S->stopping && S->queue.empty()) S->cv_work.wait_for(lock, std::chrono::milliseconds(50));
+                if (S->stopping) return;
+                if (S->cfg.max_wait_us > 0 && S->queued < S->cfg.max_batch_queries)
+                    S->cv_work.wait_for(lock, std::chrono::microseconds(S->cfg.max_wait_us),
+                                        [&] { return S->stopping || S->queued >= S->cfg.max_batch_queries; });
+                if (S->stopping) return;
+                bytes = form_batch(S, batch);
+                if (!batch.empty()) break;
+                // nothing fits beside the batches in flight: wait for one to return
+                S->cv_work.wait_for(lock, std::chrono::milliseconds(50));
+            }
+            S->in_flight += bytes;
+            S->peak_in_flight = std::max(S->peak_in_flight, S->in_flight);
         }
-        if (batch.empty()) continue;
         const auto t0 = Clock::now();
         const int rc = run_batch(S, *w, batch);
         const auto t1 = Clock::now();
         const char* msg = mlods_last_error();
         std::lock_guard<std::mutex> lock(S->mu);
+        S->in_flight -= bytes;
         for (const Piece& pc : batch) {
             Request* r = pc.r;
             if (rc != MLODS_OK && r->piece_status == MLODS_OK) {
@@ -291,6 +342,7 @@ void worker_main(mlods_server_s* S, Worker* w)
         ++S->batches;
         S->busy_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
         S->cv_done.notify_all();
+        S->cv_work.notify_all();  // memory came back: a waiting worker may form its batch
     }
 }
 
@@ -302,14 +354,7 @@ void destroy_worker(Worker* w)
     cudaFreeHost(w->h_clouds);
     cudaFreeHost(w->h_offsets);
     cudaFreeHost(w->h_frames);
-    cudaFreeHost(w->h_chunks);
-    cudaFree(w->d_chunks);
-    cudaFree(w->d_buf);
-    cudaFree(w->d_clouds);
-    cudaFree(w->d_offsets);
-    cudaFree(w->d_frames);
     cudaFree(w->d_stats);
-    cudaFree(w->d_order);
     if (w->s) cudaStreamDestroy(w->s);
     delete w;
 }
@@ -335,6 +380,7 @@ void stop_server(mlods_server_s* S)
         }
         S->queue.clear();
         S->queued = 0;
+        S->pending_bytes = 0;
     }
     S->cv_work.notify_all();
     for (Worker* w : S->workers)
@@ -357,10 +403,18 @@ void mlods_server_default_config(mlods_server_config* c)
 {
     if (!c) return;
     c->n_streams = 2;
-    c->max_batch_queries = int64_t(1) << 21;
     c->max_batch_requests = 4096;
-    c->max_pending_queries = int64_t(1) << 26;
+    c->max_batch_queries = int64_t(1) << 18;
+    c->max_device_bytes = 0;
+    c->max_pending_bytes = 0;
     c->max_wait_us = 0;
+    c->reserved = 0;
+}
+
+int64_t mlods_server_batch_bytes(int64_t n_queries, int64_t n_requests)
+{
+    if (n_queries <= 0 || n_requests <= 0) return 0;
+    return batch_bytes(n_queries, n_requests);
 }
 
 int mlods_server_create(const mlods_tree* trees, int32_t n_trees, const mlods_server_config* cfg, mlods_server* out)
@@ -374,7 +428,8 @@ int mlods_server_create(const mlods_tree* trees, int32_t n_trees, const mlods_se
     mlods_server_default_config(&c);
     if (cfg) c = *cfg;
     if (c.n_streams < 1 || c.n_streams > 16 || c.max_batch_queries < 1 || c.max_batch_requests < 1 ||
-        c.max_pending_queries < 1 || c.max_wait_us < 0) {
+        c.max_batch_requests > kMaxServeGroups * kQueueMaxClouds ||
+        c.max_device_bytes < 0 || c.max_pending_bytes < 0 || c.max_wait_us < 0) {
         set_last_error("server create: bad configuration");
         return MLODS_ERR_INVALID;
     }
@@ -394,6 +449,19 @@ int mlods_server_create(const mlods_tree* trees, int32_t n_trees, const mlods_se
         }
     }
     MLODS_ON_DEVICE(trees[0]->device);
+    if (c.max_device_bytes == 0) {
+        size_t free_b = 0, total_b = 0;
+        MLODS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        c.max_device_bytes = int64_t(free_b / 2);
+    }
+    // a batch must be able to make progress on its own
+    const int64_t floor_bytes = batch_bytes(4096, 1);
+    if (c.max_device_bytes < floor_bytes) {
+        set_last_error("server create: max_device_bytes=%lld is below one batch of 4096 queries (%lld bytes)",
+                       (long long)c.max_device_bytes, (long long)floor_bytes);
+        return MLODS_ERR_CAPACITY;
+    }
+    if (c.max_pending_bytes == 0) c.max_pending_bytes = 8 * c.max_device_bytes;
     auto* S = new (std::nothrow) mlods_server_s();
     if (!S) {
         set_last_error("server create: host allocation failed");
@@ -459,22 +527,26 @@ int mlods_server_submit(mlods_server s, int32_t tree, int64_t n, const float* q,
             return krc;
         }
     }
+    const int64_t bytes = request_bytes(n);
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stopping) {
         delete r;
         set_last_error("server submit: server is stopping");
         return MLODS_ERR_STATE;
     }
-    if (s->queued + n > s->cfg.max_pending_queries) {
+    if (s->pending_bytes + bytes > s->cfg.max_pending_bytes) {
         delete r;
-        set_last_error("server submit: %lld queries queued, admitting %lld more would exceed max_pending_queries=%lld",
-                       (long long)s->queued, (long long)n, (long long)s->cfg.max_pending_queries);
+        set_last_error("server submit: queued work holds %lld bytes; admitting %lld queries (%lld bytes) would "
+                       "exceed max_pending_bytes=%lld (capacity)",
+                       (long long)s->pending_bytes, (long long)n, (long long)bytes,
+                       (long long)s->cfg.max_pending_bytes);
         return MLODS_ERR_CAPACITY;
     }
     r->ticket = s->next_ticket++;
     r->t_submit = Clock::now();
     s->queue.push_back(r);
     s->queued += n;
+    s->pending_bytes += bytes;
     s->live[r->ticket] = r;
     *ticket = r->ticket;
     s->cv_work.notify_one();
@@ -520,6 +592,22 @@ int mlods_server_stats(mlods_server s, int64_t* completed, int64_t* batches, int
     if (queries) *queries = s->queries;
     if (queued) *queued = s->queued;
     if (busy_ms) *busy_ms = s->busy_ms;
+    return MLODS_OK;
+}
+
+int mlods_server_memory(mlods_server s, int64_t* in_flight_bytes, int64_t* peak_in_flight_bytes,
+                        int64_t* pending_bytes, int64_t* max_device_bytes, int64_t* max_pending_bytes)
+{
+    if (!s) {
+        set_last_error("null server");
+        return MLODS_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (in_flight_bytes) *in_flight_bytes = s->in_flight;
+    if (peak_in_flight_bytes) *peak_in_flight_bytes = s->peak_in_flight;
+    if (pending_bytes) *pending_bytes = s->pending_bytes;
+    if (max_device_bytes) *max_device_bytes = s->cfg.max_device_bytes;
+    if (max_pending_bytes) *max_pending_bytes = s->cfg.max_pending_bytes;
     return MLODS_OK;
 }
 

@@ -291,6 +291,7 @@ def refgpu() -> C.CDLL:
         lib.refgpu_project.restype = C.c_double
         lib.refgpu_project.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, _P, _P]
         lib.refgpu_free.argtypes = [_P]
+        lib.refgpu_set_kernel.argtypes = [_P, C.c_int, C.c_float, C.c_float, C.c_float, _P, C.c_int]
         lib.refgpu_global_create.restype = _P
         lib.refgpu_global_create.argtypes = [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                              _P, C.c_int]
@@ -322,6 +323,12 @@ class RefGpu:
         if getattr(self, "_h", None):
             refgpu().refgpu_free(self._h)
             self._h = None
+
+    def set_kernel(self, kernel):
+        """APSS::updateKernel with a new kernel (the tree stays)."""
+        sig = np.ascontiguousarray(np.asarray(kernel.sigmas if len(kernel.sigmas) else [0.0], np.float32))
+        refgpu().refgpu_set_kernel(self._h, int(kernel.type), float(kernel.sigma), float(kernel.exponent),
+                                   float(kernel.constant_shift), _ptr(sig), len(kernel.sigmas))
 
     def project(self, q, calls=10, iters_per_call=1, step_max=-1.0):
         """(points, normals, device milliseconds of the project calls)."""

@@ -103,6 +103,19 @@ double refgpu_project(void* h, const float* q, int64_t n, int calls, int iters_p
     return double(ms);
 }
 
+// A new weight kernel for the same tree, through the reference's own
+// APSS::updateKernel (GPUUtils.cu:466-472), as scene::setNewKernel does.
+void refgpu_set_kernel(void* h, int ktype, float sigma, float exponent, float shift, const float* sigmas, int nsig)
+{
+    auto* r = static_cast<RefGpu*>(h);
+    r->kernel.type = ktype == 0 ? Kernel::GAUSSIAN : (ktype == 1 ? Kernel::SINGULAR : Kernel::GAUSSIAN_MULTIPLE);
+    r->kernel.sigma = sigma;
+    r->kernel.exponent = exponent;
+    r->kernel.constant_shift = shift;
+    r->kernel.sigmas.assign(sigmas, sigmas + nsig);
+    r->apss->updateKernel(r->kernel);
+}
+
 void refgpu_free(void* h)
 {
     auto* r = static_cast<RefGpu*>(h);

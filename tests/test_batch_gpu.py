@@ -99,7 +99,7 @@ def test_graph_replay_and_tuning(setup):
     b.tune(counts, d_q, d_p, d_n, 4)
     st = b.last_stats()
     assert st["grid_pct"] in (85, 100) and st["reorder"] in (0, 1)
-    assert st["queries_per_warp"] in (1, 2) and st["chunk"] % 4 == 0
+    assert st["queries_per_warp"] in (1, 2)
     d_p.fill_(float("nan"))
     b.project_device(counts, d_q, d_p, d_n, 4, use_graph=True)
     torch.cuda.synchronize()

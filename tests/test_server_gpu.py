@@ -144,7 +144,10 @@ def test_concurrent_submitters(projectors):
 
 def test_bounded_wait_admission_and_errors(projectors):
     f, pts, diag = projectors[0]
-    srv = ProjectionServer([f], n_streams=1, max_pending_queries=300000)
+    # room for about 300k queued queries: a request's footprint is its device
+    # bytes when it runs plus 36 bytes of pinned staging per query
+    budget = ProjectionServer.batch_bytes(300000) + 36 * 300000
+    srv = ProjectionServer([f], n_streams=1, max_pending_bytes=budget)
     try:
         q = synth.perturbed_queries(pts, 0.01, seed=77)
         big = np.concatenate([q] * 7)[:280000]
@@ -154,7 +157,7 @@ def test_bounded_wait_admission_and_errors(projectors):
         p, n, _ = srv.wait(t, timeout_ms=120000)  # the ticket is still valid after a timeout
         assert np.isfinite(p).all()
         with pytest.raises(MlodsError) as e:
-            srv.submit(0, np.concatenate([q] * 8)[:300001], 1)  # beyond max_pending_queries
+            srv.submit(0, np.concatenate([q] * 8)[:300001], 1)  # beyond max_pending_bytes
         assert e.value.code == capi.MLODS_ERR_CAPACITY
         with pytest.raises(MlodsError):
             srv.wait(987654321)  # unknown ticket
@@ -179,3 +182,32 @@ def test_close_with_queued_work_returns(projectors):
     for _ in range(6):
         srv.submit(0, big, 10)
     srv.close()
+
+
+def test_device_budget_bounds_the_batches_in_flight(projectors):
+    """Batches are formed within the device budget: with room for only a
+    few thousand queries in flight the server still answers every request
+    (large ones in pieces, requests waiting for memory to free up), the
+    bytes in flight never pass the budget, and results equal the requests
+    projected alone."""
+    f, pts, diag = projectors[0]
+    budget = ProjectionServer.batch_bytes(6000, 8)
+    srv = ProjectionServer([f], n_streams=2, max_device_bytes=budget)
+    try:
+        rng = np.random.default_rng(80)
+        q = synth.perturbed_queries(pts, 0.01, seed=80)
+        reqs = [q[rng.choice(len(q), int(m), replace=False)] for m in (100, 5000, 17000, 300, 2500, 9000)]
+        tickets = [srv.submit(0, r, 6) for r in reqs]
+        outs = [srv.wait(t, timeout_ms=120000) for t in tickets]
+        mem = srv.memory()
+        assert mem["max_device_bytes"] == budget
+        assert 0 < mem["peak_in_flight_bytes"] <= budget
+        assert mem["in_flight_bytes"] == 0 and mem["pending_bytes"] == 0
+        for r, (p, n, _) in zip(reqs, outs):
+            want_p = np.empty_like(r)
+            want_n = np.empty_like(r)
+            f.copyPointsToGPU(len(r), r)
+            f.project(len(r), want_p, want_n, 6)
+            assert np.array_equal(p, want_p) and np.array_equal(n, want_n)
+    finally:
+        srv.close()
