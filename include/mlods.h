@@ -367,7 +367,8 @@ int mlods_last_walk_counts(mlods_tree t, int64_t* lane_visits, int64_t* pruned);
  * settings and n_iterations stay the same (the stream must not be capturing).
  * mlods_batch_tune (the batch's autotuner) times, on the given buffers, walk
  * schedules (one or two queries per warp for every tree), Morton or input
- * order and the share of the resident grid --
+ * order, the share of the resident grid and the order of the trees in the
+ * launch --
  * each candidate run once untimed and once timed -- and keeps the fastest
  * for later calls.  The trees must outlive the batch and must not be rebuilt
  * while it exists. */
@@ -380,10 +381,24 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
                      int32_t n_iterations, void* stream);
 /* Statistics of the last batch launch (synchronises): query-node visits,
  * rounds, overflows, device time (ordering and kernel), the launch shape in
- * use (reorder, grid_pct, queries_per_warp) and node evaluations
- * (lane_visits, see mlods_last_walk_counts).  Any pointer may be NULL. */
+ * use (reorder, grid_pct, queries_per_warp, line_order: 0 = the trees with
+ * the most work first, 1 = grouped by walk specialisation) and node
+ * evaluations (lane_visits, see mlods_last_walk_counts).  Any pointer may be
+ * NULL. */
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
-                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int64_t* lane_visits);
+                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int32_t* line_order,
+                      int64_t* lane_visits);
+/* Sets the launch shape without tuning: queries_per_warp (0: each tree's own
+ * setting, the largest of them, at most 2; else 1 or 2 for every tree),
+ * reorder (1: Morton order inside each tree), grid_pct (share of the
+ * resident grid, 1-100) and line_order (0 or 1, see mlods_batch_stats). */
+int mlods_batch_set_schedule(mlods_batch b, int32_t queries_per_warp, int32_t reorder, int32_t grid_pct,
+                             int32_t line_order);
+/* The candidates of the last mlods_batch_tune and the device time of each:
+ * *n_candidates = their number; the first max_candidates are written to the
+ * arrays (any may be NULL). */
+int mlods_batch_tune_results(mlods_batch b, int32_t max_candidates, int32_t* queries_per_warp, int32_t* reorder,
+                             int32_t* grid_pct, int32_t* line_order, float* ms, int32_t* n_candidates);
 
 /* ---- projection without device allocation (extension) ----------------------
  * No counterpart in the reference.  Same computation and results as

@@ -177,7 +177,9 @@ SIGNATURES = {
     "mlods_batch_free": (C.c_int, [_P]),
     "mlods_batch_project": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, _P]),
     "mlods_batch_tune": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
-    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32, _I32, _I64]),
+    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32, _I32, _I32, _I64]),
+    "mlods_batch_set_schedule": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "mlods_batch_tune_results": (C.c_int, [_P, C.c_int32, _I32, _I32, _I32, _I32, C.POINTER(C.c_float), _I32]),
     "mlods_project_device_noalloc": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
     "mlods_dcgrid_adaptive": (C.c_int, [_P, C.c_int32, C.c_int32, _P, C.POINTER(_P)]),
     "mlods_dcgrid_xform": (C.c_int, [_P, _P, _I64]),

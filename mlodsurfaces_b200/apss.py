@@ -796,11 +796,32 @@ class FastapssBatch:
         ro = C.c_int32(0)
         gp = C.c_int32(0)
         qw = C.c_int32(0)
+        lo = C.c_int32(0)
         lv = C.c_int64(0)
         capi.check(self._lib.mlods_batch_stats(self._b, C.byref(v), C.byref(r), C.byref(o), C.byref(ms),
-                                               C.byref(ro), C.byref(gp), C.byref(qw), C.byref(lv)))
+                                               C.byref(ro), C.byref(gp), C.byref(qw), C.byref(lo), C.byref(lv)))
         return {"node_visits": v.value, "rounds": r.value, "overflows": o.value, "kernel_ms": ms.value,
-                "reorder": ro.value, "grid_pct": gp.value, "queries_per_warp": qw.value, "lane_visits": lv.value}
+                "reorder": ro.value, "grid_pct": gp.value, "queries_per_warp": qw.value,
+                "line_order": "by specialisation" if lo.value == 1 else "most work first", "lane_visits": lv.value}
+
+    def set_schedule(self, queries_per_warp: int = 0, reorder: bool = True, grid_pct: int = 100,
+                     by_specialisation: bool = False) -> None:
+        """Sets the launch shape without tuning (see :meth:`last_stats`)."""
+        capi.check(self._lib.mlods_batch_set_schedule(self._b, int(queries_per_warp), 1 if reorder else 0,
+                                                      int(grid_pct), 1 if by_specialisation else 0))
+
+    def tune_results(self):
+        """The candidates of the last :meth:`tune` with their device times (ms)."""
+        n = C.c_int32(0)
+        capi.check(self._lib.mlods_batch_tune_results(self._b, 0, None, None, None, None, None, C.byref(n)))
+        k = n.value
+        qw, ro, gp, lo = (C.c_int32 * max(k, 1))(), (C.c_int32 * max(k, 1))(), (C.c_int32 * max(k, 1))(), \
+            (C.c_int32 * max(k, 1))()
+        ms = (C.c_float * max(k, 1))()
+        capi.check(self._lib.mlods_batch_tune_results(self._b, k, qw, ro, gp, lo, ms, C.byref(n)))
+        return [{"queries_per_warp": qw[i], "query_order": "Morton" if ro[i] else "input", "grid_pct": gp[i],
+                 "line_order": "by specialisation" if lo[i] == 1 else "most work first", "ms": ms[i]}
+                for i in range(k)]
 
 
 class ProjectionServer:

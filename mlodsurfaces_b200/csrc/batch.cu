@@ -14,6 +14,7 @@
 // autotuner (mlods_batch_tune) times walk schedules (queries per warp),
 // query orders and grid sizes and keeps the fastest.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -37,6 +38,10 @@ struct mlods_batch_s {
     // launch shape (the tuner's pick)
     int reorder = 1;     // Morton order inside each tree
     int grid_pct = 100;  // share of the resident blocks launched
+    int line_order = mlods::kQueueMostWorkFirst;  // order of the trees along the launch's slot line
+    // the autotuner's last run: candidates {qpw, reorder, grid_pct, line_order} and their device ms
+    std::vector<std::array<int, 4>> tune_cands;
+    std::vector<float> tune_ms;
     int qpw = 0;         // queries per warp for every tree; 0: the trees' own setting (the largest, at most 2)
     int run_qpw = 1;     // the schedule the launches use
     // graph cache
@@ -49,6 +54,7 @@ struct mlods_batch_s {
     int g_iters = -1;
     int g_reorder = -1;
     int g_pct = -1;
+    int g_line = -1;
     int g_kernels = 0;  // kernels one replay runs
     bool ran = false;   // the events hold a launch
     // graphs are captured on this private stream (the legacy default stream
@@ -91,6 +97,7 @@ int enqueue(mlods_batch_s* b, const float* d_q, int64_t total, bool timed, cudaS
     a.order = order;
     a.counters = reinterpret_cast<unsigned long long*>(b->d_stats + 8);
     a.stats = b->d_stats;
+    a.line_order = b->line_order;
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev0, s));
     MLODS_CUDA(launch_mlod_queue(a, b->run_qpw, sm_count_for_current_device(), b->grid_pct, s));
     if (timed) MLODS_CUDA(cudaEventRecord(b->ev1, s));
@@ -179,7 +186,8 @@ int batch_run(mlods_batch_s* b, const float* d_q, float* d_p, float* d_n, int64_
 {
     if (!use_graph) return enqueue(b, d_q, total, true, s);
     const bool hit = b->exec && b->g_q == d_q && b->g_p == d_p && b->g_n == d_n && b->g_total == total &&
-                     b->g_iters == iters && b->g_reorder == b->reorder && b->g_pct == b->grid_pct;
+                     b->g_iters == iters && b->g_reorder == b->reorder && b->g_pct == b->grid_pct &&
+                     b->g_line == b->line_order;
     if (!hit) {
         drop_graph(b);
         if (!b->cap_stream) MLODS_CUDA(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
@@ -205,6 +213,7 @@ int batch_run(mlods_batch_s* b, const float* d_q, float* d_p, float* d_n, int64_
         b->g_iters = iters;
         b->g_reorder = b->reorder;
         b->g_pct = b->grid_pct;
+        b->g_line = b->line_order;
         b->g_kernels = kernels;
     }
     MLODS_CUDA(cudaEventRecord(b->ev0, s));
@@ -309,11 +318,15 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
     }
     MLODS_ON_DEVICE(b->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // walk schedule, query order and grid size
+    // walk schedule, query order, grid size and order of the trees
     struct Cand {
-        int qpw, reorder, pct;
+        int qpw, reorder, pct, line;
     };
-    const Cand cands[] = {{1, 1, 100}, {2, 1, 100}, {2, 0, 100}, {2, 1, 85}};
+    const Cand cands[] = {{1, 1, 100, kQueueMostWorkFirst},
+                          {2, 1, 100, kQueueMostWorkFirst},
+                          {2, 1, 100, kQueueBySpecialisation},
+                          {2, 0, 100, kQueueMostWorkFirst},
+                          {2, 1, 85, kQueueMostWorkFirst}};
     float best = INFINITY;
     Cand pick = cands[1];
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -324,10 +337,13 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
         return cuda_fail(ce, "batch_tune: events", __FILE__, __LINE__);
     }
     int rc = MLODS_OK;
+    b->tune_cands.clear();
+    b->tune_ms.clear();
     for (const Cand& c : cands) {
         b->qpw = c.qpw;
         b->reorder = c.reorder;
         b->grid_pct = c.pct;
+        b->line_order = c.line;
         int64_t total = 0;
         rc = batch_prepare(b, offsets, d_q, d_out_pts, d_out_nrm, n_iterations, s, &total);
         if (rc != MLODS_OK) break;
@@ -342,6 +358,8 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
         if (ce == cudaSuccess && rc == MLODS_OK) ce = cudaEventElapsedTime(&ms, t0, t1);
         if (ce != cudaSuccess) rc = cuda_fail(ce, "batch_tune: timing", __FILE__, __LINE__);
         if (rc != MLODS_OK) break;
+        b->tune_cands.push_back({c.qpw, c.reorder, c.pct, c.line});
+        b->tune_ms.push_back(ms);
         if (ms < best) {
             best = ms;
             pick = c;
@@ -352,12 +370,14 @@ int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, fl
     b->qpw = pick.qpw;
     b->reorder = pick.reorder;
     b->grid_pct = pick.pct;
+    b->line_order = pick.line;
     drop_graph(b);
     return rc;
 }
 
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
-                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int64_t* lane_visits)
+                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int32_t* line_order,
+                      int64_t* lane_visits)
 {
     if (!b) {
         set_last_error("null batch");
@@ -380,8 +400,50 @@ int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int6
     if (reorder) *reorder = b->reorder;
     if (grid_pct) *grid_pct = b->grid_pct;
     if (queries_per_warp) *queries_per_warp = b->run_qpw;
+    if (line_order) *line_order = b->line_order;
     if (lane_visits) *lane_visits = h[6];
     return MLODS_OK;
 }
 
 }  // extern "C"
+
+int mlods_batch_tune_results(mlods_batch b, int32_t max_candidates, int32_t* queries_per_warp, int32_t* reorder,
+                             int32_t* grid_pct, int32_t* line_order, float* ms, int32_t* n_candidates)
+{
+    if (!b || max_candidates < 0 || !n_candidates) {
+        set_last_error("batch_tune_results: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    const int n = int(b->tune_ms.size());
+    *n_candidates = n;
+    for (int i = 0; i < n && i < max_candidates; ++i) {
+        const std::array<int, 4>& c = b->tune_cands[size_t(i)];
+        if (queries_per_warp) queries_per_warp[i] = c[0];
+        if (reorder) reorder[i] = c[1];
+        if (grid_pct) grid_pct[i] = c[2];
+        if (line_order) line_order[i] = c[3];
+        if (ms) ms[i] = b->tune_ms[size_t(i)];
+    }
+    return MLODS_OK;
+}
+
+int mlods_batch_set_schedule(mlods_batch b, int32_t queries_per_warp, int32_t reorder, int32_t grid_pct,
+                             int32_t line_order)
+{
+    if (!b) {
+        set_last_error("null batch");
+        return MLODS_ERR_INVALID;
+    }
+    if (queries_per_warp < 0 || queries_per_warp > 2 || (reorder != 0 && reorder != 1) || grid_pct < 1 ||
+        grid_pct > 100 || (line_order != mlods::kQueueMostWorkFirst && line_order != mlods::kQueueBySpecialisation)) {
+        set_last_error("batch_set_schedule: queries_per_warp in {0, 1, 2}, reorder in {0, 1}, grid_pct in [1, 100], "
+                       "line_order in {0, 1}");
+        return MLODS_ERR_INVALID;
+    }
+    b->qpw = queries_per_warp;
+    b->reorder = reorder;
+    b->grid_pct = grid_pct;
+    b->line_order = line_order;
+    drop_graph(b);
+    return MLODS_OK;
+}

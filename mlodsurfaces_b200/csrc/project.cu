@@ -535,6 +535,7 @@ static_assert(sizeof(QueueLaunch) <= 32000, "queue launch parameters must fit th
 // The specialisation of the walk a cloud runs with: kernel family and number
 // of multi-Gaussian terms (2-6 and 8 have their own code, other counts share
 // one) and blend rule.
+constexpr int kWalkSpecs = 18;
 inline int walk_spec_id(const CloudArgs& c)
 {
     int k = 8;  // multi-Gaussian, terms counted at run time
@@ -763,9 +764,19 @@ cudaError_t launch_queue_typed(const QueueArgs& a, int sm_count, int grid_pct, c
             p.len[i] = a.q_offsets[c0 + i + 1] - a.q_offsets[c0 + i];
             p.spec[i] = walk_spec_id(p.clouds[i]);
         }
-        // the clouds with the most work first, so that the launch ends on small ones
+        // the clouds with the most work first, so that the launch ends on
+        // small ones; optionally grouped by specialisation first
         auto work = [&](int i) { return p.len[i] * int64_t(std::max(p.clouds[i].n_iter, 1)); };
-        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return work(x) > work(y); });
+        int64_t spec_work[kWalkSpecs] = {};
+        for (int i = 0; i < nc; ++i) spec_work[p.spec[i]] += work(i);
+        const bool by_spec = a.line_order == kQueueBySpecialisation;
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+            if (by_spec && p.spec[x] != p.spec[y]) {
+                const int64_t wx = spec_work[p.spec[x]], wy = spec_work[p.spec[y]];
+                return wx != wy ? wx > wy : p.spec[x] < p.spec[y];
+            }
+            return work(x) > work(y);
+        });
         int64_t v = 0;
         for (int j = 0; j < nc; ++j) {
             p.cloud_at[j] = idx[size_t(j)];

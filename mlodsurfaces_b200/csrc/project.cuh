@@ -74,7 +74,16 @@ struct QueueArgs {
     const uint32_t* order;     // device
     unsigned long long* counters;  // device: one 64-bit slot counter per launch group, zero before launch
     int64_t* stats;            // device, as ProjectArgs::stats
+    int line_order = 0;        // kQueueMostWorkFirst or kQueueBySpecialisation
 };
+
+// The order of the clouds along a launch's slot line: the clouds with the
+// most work (queries x iterations) first, or grouped by walk specialisation
+// (kernel family, terms, blend rule; the groups with the most work first,
+// the clouds inside each group likewise), so that the warps working at any
+// moment run the same code.
+constexpr int kQueueMostWorkFirst = 0;
+constexpr int kQueueBySpecialisation = 1;
 
 // Clouds per launch of the queue kernel: their launch arguments travel by
 // value in the kernel's parameters (within the 32 KB parameter limit); a

@@ -100,6 +100,11 @@ def test_graph_replay_and_tuning(setup):
     st = b.last_stats()
     assert st["grid_pct"] in (85, 100) and st["reorder"] in (0, 1)
     assert st["queries_per_warp"] in (1, 2)
+    cands = b.tune_results()
+    assert len(cands) == 5 and all(c["ms"] > 0 for c in cands)
+    best = min(cands, key=lambda c: c["ms"])
+    assert (best["queries_per_warp"], best["grid_pct"], best["line_order"]) == \
+        (st["queries_per_warp"], st["grid_pct"], st["line_order"])
     d_p.fill_(float("nan"))
     b.project_device(counts, d_q, d_p, d_n, 4, use_graph=True)
     torch.cuda.synchronize()
@@ -132,9 +137,11 @@ def test_graph_replay_and_tuning(setup):
     assert torch.equal(d_p, ref2_p)
 
 
-def test_batch_with_paired_walks_equals_per_tree(setup):
+@pytest.mark.parametrize("by_spec", [False, True])
+def test_batch_with_paired_walks_equals_per_tree(setup, by_spec):
     """Trees set to two queries per warp: the single launch pairs the same
-    queries as each tree's own launch (chunks start at multiples of 4)."""
+    queries as each tree's own launch (each tree's slots are padded to a
+    multiple of 4), whatever the order of the trees along the launch."""
     projectors, queries = setup
     saved = [f.queries_per_warp for f in projectors]
     try:
@@ -142,7 +149,9 @@ def test_batch_with_paired_walks_equals_per_tree(setup):
             f.queries_per_warp = 2
         ref_p, ref_n = _per_tree(projectors, queries, 5)
         b = FastapssBatch(projectors)
+        b.set_schedule(0, True, 100, by_specialisation=by_spec)
         p, n, _ = _batched(b, queries, 5)
+        assert b.last_stats()["line_order"] == ("by specialisation" if by_spec else "most work first")
     finally:
         for f, w in zip(projectors, saved):
             f.queries_per_warp = w
@@ -166,6 +175,10 @@ def test_batch_rejects_bad_input(setup):
     rc = lib.mlods_batch_project(b._b, capi.ptr(off), capi.ptr(d_q), capi.ptr(d_q), capi.ptr(d_q), 1, 0,
                                  C.c_void_p(0))
     assert rc == capi.MLODS_ERR_INVALID
+    with pytest.raises(MlodsError):
+        b.set_schedule(queries_per_warp=3)
+    with pytest.raises(MlodsError):
+        b.set_schedule(grid_pct=0)
     g = Fastapss(projectors[0].m_apssOctree)
     g.m_apssOctree.knnMode(True, 8)
     try:
