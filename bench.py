@@ -1060,10 +1060,37 @@ def run_batch(args, rank: int = 0, world: int = 1):
     if world > 1:
         torch.distributed.barrier()
     clk = clocks.stop()
+    st = b.last_stats()
+    # when the tuner gave the largest clouds launches of their own, the best
+    # single-launch schedule (every cloud in the one queue launch) as well
+    single = None
+    # (every rank takes the same collective steps: the decision is the max over ranks)
+    any_solo = max_over_ranks([1.0 if st["solo_min_queries"] > 0 else 0.0], world, dev)[0] > 0
+    if any_solo:
+        one = min((c for c in tune_results if c["solo_min_queries"] == 0), key=lambda c: c["ms"])
+        b.set_schedule(one["queries_per_warp"], bool(one["reorder"]), one["grid_pct"],
+                       one["line_order"] == "by specialisation", 0)
+        b.project_device(counts, d_q, d_p, d_n, iters, use_graph=True)
+        one_ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.project_device(counts, d_q, d_p, d_n, iters, use_graph=True)
+            e1.record(stream)
+            e1.synchronize()
+            one_ms.append(e0.elapsed_time(e1))
+        one_max = max_over_ranks([sum(one_ms)], world, dev)[0] / len(one_ms)
+        single = {"ms_per_step": one_max, "value": all_queries / (one_max / 1e3), "unit": "queries/s",
+                  "schedule": dict(one, ms=None), "walk_launches_per_step": b.last_stats()["walk_launches"]}
+        b.set_schedule(st["queries_per_warp"], bool(st["reorder"]), st["grid_pct"],
+                       st["line_order"] == "by specialisation", st["solo_min_queries"])
+        b.project_device(counts, d_q, d_p, d_n, iters, use_graph=True)  # the tuned outputs again
+        torch.cuda.synchronize()
     # the same work as one launch per cloud (the reference's one-object-per-call
     # form) with the batch's walk schedule and query order, warmed up and
     # timed like the batch, and its outputs compared
-    st = b.last_stats()
     for f in projectors:
         if st["queries_per_warp"]:
             f.queries_per_warp = st["queries_per_warp"]
@@ -1102,7 +1129,7 @@ def run_batch(args, rank: int = 0, world: int = 1):
     err = batch_fp64_sample(clouds, batch_p.cpu().numpy(), counts, iters) if rank == 0 else None
     ref_gpu = batch_reference_gpu(clouds, qs, iters, value) if (rank == 0 and args.ref_gpu) else None
     return {
-        "metric": "queries projected/s, 64 resident clouds in one graph launch",
+        "metric": "queries projected/s, 64 resident clouds in one graph-captured step",
         "value": value,
         "unit": "queries/s",
         "n_gpus": world,
@@ -1114,19 +1141,23 @@ def run_batch(args, rank: int = 0, world: int = 1):
         "vs_baseline": None,
         "dtype": "f32 (f64 sphere solve)",
         "data": "synthetic: seeded tori and RBF-blob surfaces, sizes log-uniform in [1e4, 4e6], random scales",
-        "config": {"workload": f"batched: {args.clouds} clouds, {all_points} points, one graph launch per step",
+        "config": {"workload": f"batched: {args.clouds} clouds, {all_points} points, one graph-captured step",
                    "n_points": all_points, "n_queries": all_queries, "iterations": iters, "cutoff": 2.0,
                    "parallelism": (f"whole clouds per GPU, {world} GPUs (rank 0: {len(clouds)} clouds, "
                                    f"{n_points} points)") if world > 1 else "1 GPU",
                    "kernels": "Gaussian / multi-Gaussian / rational drawn per cloud", "tree_depths": "7..10",
-                   "launch": "one persistent queue-kernel launch per step (after the Morton ordering), "
-                             "captured in a CUDA graph",
+                   "launch": "the Morton ordering, then one persistent queue-kernel launch for every cloud "
+                             "(or launches of their own for the largest clouds first, when the tuner picks it), "
+                             "captured in one CUDA graph",
                    "l2": "L2 flushed (256 MB write) before every timed step"},
         "schedule": {"queries_per_warp": st["queries_per_warp"],
                      "query_order": "Morton" if st["reorder"] else "input", "grid_pct": st["grid_pct"],
-                     "line_order": st["line_order"], "tuner_seconds": tune_s, "candidates": tune_results,
+                     "line_order": st["line_order"], "solo_min_queries": st["solo_min_queries"],
+                     "walk_launches_per_step": st["walk_launches"], "tuner_seconds": tune_s,
+                     "candidates": tune_results,
                      "note": "picked by mlods_batch_tune from the candidate launch shapes, each timed on a "
                              "2-iteration run"},
+        "single_launch": single if single is not None else "the tuned schedule is the single launch",
         "err_vs_fp64": err,
         "reference_gpu": ref_gpu,
         "one_launch_per_cloud_ms": per_cloud_ms,

@@ -360,45 +360,47 @@ int mlods_last_walk_counts(mlods_tree t, int64_t* lane_visits, int64_t* pruned);
  * Every tree must be in MLODS_MODE_MLOD with a kernel set; each tree's own
  * cutoff, min_depth, blend rule and convergence mode apply (pruning does not),
  * and the step clamp is each tree's root box radius.  Every tree is walked
- * with its own queries_per_warp (4 runs as 2) unless mlods_batch_tune picked
- * one schedule for all; results equal per-tree mlods_project_device calls
- * with the same schedule bit for bit.  With use_graph != 0 the work is
- * captured once in a CUDA graph and replayed while buffers, offsets, tree
- * settings and n_iterations stay the same (the stream must not be capturing).
- * mlods_batch_tune (the batch's autotuner) times, on the given buffers, walk
- * schedules (one or two queries per warp for every tree), Morton or input
- * order, the share of the resident grid and the order of the trees in the
- * launch --
- * each candidate run once untimed and once timed -- and keeps the fastest
- * for later calls.  The trees must outlive the batch and must not be rebuilt
- * while it exists. */
+ * with its own queries_per_warp (4 runs as 2) unless the schedule sets one
+ * for all; results equal per-tree mlods_project_device calls with the same
+ * schedule bit for bit.  With use_graph != 0 the work is captured once in a
+ * CUDA graph and replayed while buffers, offsets, tree settings, schedule and
+ * n_iterations stay the same (the stream must not be capturing).
+ * mlods_batch_tune (the batch's autotuner) times, on the given buffers, a set
+ * of schedules -- one or two queries per warp for every tree, Morton or input
+ * order, the share of the resident grid, the order of the trees in the
+ * launch, and launches of their own for the largest trees -- each run once
+ * untimed and once timed, and keeps the fastest for later calls.  The trees
+ * must outlive the batch and must not be rebuilt while it exists. */
 typedef struct mlods_batch_s* mlods_batch;
+/* The launch shape of a batch. */
+typedef struct {
+    int32_t queries_per_warp; /* 0: each tree's own setting (the largest of them, at most 2); else 1 or 2 for every tree */
+    int32_t reorder;          /* 1: Morton order inside each tree; 0: input order */
+    int32_t grid_pct;         /* share of the resident grid launched, 1-100 */
+    int32_t line_order;       /* 0: the trees with the most work first; 1: grouped by walk specialisation */
+    int64_t solo_min_queries; /* > 0: a tree with at least this many queries runs in a launch of its own
+                                 (the single-tree kernel) before the shared launch of the others; 0: none */
+} mlods_batch_schedule;
 int mlods_batch_create(const mlods_tree* trees, int32_t n_trees, mlods_batch* out);
 int mlods_batch_free(mlods_batch b);
 int mlods_batch_project(mlods_batch b, const int64_t* offsets, const float* d_q, float* d_out_pts, float* d_out_nrm,
                         int32_t n_iterations, int32_t use_graph, void* stream);
 int mlods_batch_tune(mlods_batch b, const int64_t* offsets, const float* d_q, float* d_out_pts, float* d_out_nrm,
                      int32_t n_iterations, void* stream);
-/* Statistics of the last batch launch (synchronises): query-node visits,
- * rounds, overflows, device time (ordering and kernel), the launch shape in
- * use (reorder, grid_pct, queries_per_warp, line_order: 0 = the trees with
- * the most work first, 1 = grouped by walk specialisation) and node
- * evaluations (lane_visits, see mlods_last_walk_counts).  Any pointer may be
- * NULL. */
+/* Statistics of the last batch call (synchronises): query-node visits,
+ * rounds, overflows, device time (ordering and kernels), node evaluations
+ * (lane_visits, see mlods_last_walk_counts) and the kernel launches it made.
+ * Any pointer may be NULL. */
 int mlods_batch_stats(mlods_batch b, int64_t* node_visits, int64_t* rounds, int64_t* overflows, float* kernel_ms,
-                      int32_t* reorder, int32_t* grid_pct, int32_t* queries_per_warp, int32_t* line_order,
-                      int64_t* lane_visits);
-/* Sets the launch shape without tuning: queries_per_warp (0: each tree's own
- * setting, the largest of them, at most 2; else 1 or 2 for every tree),
- * reorder (1: Morton order inside each tree), grid_pct (share of the
- * resident grid, 1-100) and line_order (0 or 1, see mlods_batch_stats). */
-int mlods_batch_set_schedule(mlods_batch b, int32_t queries_per_warp, int32_t reorder, int32_t grid_pct,
-                             int32_t line_order);
+                      int64_t* lane_visits, int32_t* walk_launches);
+/* The schedule in use / sets one without tuning. */
+int mlods_batch_get_schedule(mlods_batch b, mlods_batch_schedule* out);
+int mlods_batch_set_schedule(mlods_batch b, const mlods_batch_schedule* sched);
 /* The candidates of the last mlods_batch_tune and the device time of each:
- * *n_candidates = their number; the first max_candidates are written to the
- * arrays (any may be NULL). */
-int mlods_batch_tune_results(mlods_batch b, int32_t max_candidates, int32_t* queries_per_warp, int32_t* reorder,
-                             int32_t* grid_pct, int32_t* line_order, float* ms, int32_t* n_candidates);
+ * *n_candidates = their number; the first max_candidates are written to
+ * cands and ms (either may be NULL). */
+int mlods_batch_tune_results(mlods_batch b, int32_t max_candidates, mlods_batch_schedule* cands, float* ms,
+                             int32_t* n_candidates);
 
 /* ---- projection without device allocation (extension) ----------------------
  * No counterpart in the reference.  Same computation and results as

@@ -110,6 +110,16 @@ class mlods_server_config(C.Structure):
     ]
 
 
+class mlods_batch_schedule(C.Structure):
+    _fields_ = [
+        ("queries_per_warp", C.c_int32),
+        ("reorder", C.c_int32),
+        ("grid_pct", C.c_int32),
+        ("line_order", C.c_int32),
+        ("solo_min_queries", C.c_int64),
+    ]
+
+
 class mlods_tree_info(C.Structure):
     _fields_ = [
         ("n_points", C.c_int64),
@@ -177,9 +187,11 @@ SIGNATURES = {
     "mlods_batch_free": (C.c_int, [_P]),
     "mlods_batch_project": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, _P]),
     "mlods_batch_tune": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _P]),
-    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I32, _I32, _I32, _I32, _I64]),
-    "mlods_batch_set_schedule": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
-    "mlods_batch_tune_results": (C.c_int, [_P, C.c_int32, _I32, _I32, _I32, _I32, C.POINTER(C.c_float), _I32]),
+    "mlods_batch_stats": (C.c_int, [_P, _I64, _I64, _I64, C.POINTER(C.c_float), _I64, _I32]),
+    "mlods_batch_get_schedule": (C.c_int, [_P, C.POINTER(mlods_batch_schedule)]),
+    "mlods_batch_set_schedule": (C.c_int, [_P, C.POINTER(mlods_batch_schedule)]),
+    "mlods_batch_tune_results": (C.c_int, [_P, C.c_int32, C.POINTER(mlods_batch_schedule), C.POINTER(C.c_float),
+                                           _I32]),
     "mlods_project_device_noalloc": (C.c_int, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.c_float, _P]),
     "mlods_dcgrid_adaptive": (C.c_int, [_P, C.c_int32, C.c_int32, _P, C.POINTER(_P)]),
     "mlods_dcgrid_xform": (C.c_int, [_P, _P, _I64]),

@@ -788,40 +788,51 @@ class FastapssBatch:
         capi.check(self._lib.mlods_batch_tune(self._b, capi.ptr(off), capi.ptr(d_q), capi.ptr(d_out_p),
                                               capi.ptr(d_out_n), int(n_iterations), C.c_void_p(stream or 0)))
 
+    @staticmethod
+    def _schedule_dict(sc) -> dict:
+        return {"queries_per_warp": sc.queries_per_warp, "reorder": sc.reorder, "grid_pct": sc.grid_pct,
+                "line_order": "by specialisation" if sc.line_order == 1 else "most work first",
+                "solo_min_queries": sc.solo_min_queries}
+
+    def schedule(self) -> dict:
+        """The launch shape in use: walk schedule (queries per warp), Morton
+        order (reorder), share of the grid, order of the trees in the launch,
+        and the size from which a tree runs in a launch of its own (0: none)."""
+        sc = capi.mlods_batch_schedule()
+        capi.check(self._lib.mlods_batch_get_schedule(self._b, C.byref(sc)))
+        return self._schedule_dict(sc)
+
     def last_stats(self):
+        """Statistics of the last call, with the schedule it ran."""
         v = C.c_int64(0)
         r = C.c_int64(0)
         o = C.c_int64(0)
         ms = C.c_float(0)
-        ro = C.c_int32(0)
-        gp = C.c_int32(0)
-        qw = C.c_int32(0)
-        lo = C.c_int32(0)
         lv = C.c_int64(0)
+        nl = C.c_int32(0)
         capi.check(self._lib.mlods_batch_stats(self._b, C.byref(v), C.byref(r), C.byref(o), C.byref(ms),
-                                               C.byref(ro), C.byref(gp), C.byref(qw), C.byref(lo), C.byref(lv)))
-        return {"node_visits": v.value, "rounds": r.value, "overflows": o.value, "kernel_ms": ms.value,
-                "reorder": ro.value, "grid_pct": gp.value, "queries_per_warp": qw.value,
-                "line_order": "by specialisation" if lo.value == 1 else "most work first", "lane_visits": lv.value}
+                                               C.byref(lv), C.byref(nl)))
+        out = {"node_visits": v.value, "rounds": r.value, "overflows": o.value, "kernel_ms": ms.value,
+               "lane_visits": lv.value, "walk_launches": nl.value}
+        out.update(self.schedule())
+        return out
 
     def set_schedule(self, queries_per_warp: int = 0, reorder: bool = True, grid_pct: int = 100,
-                     by_specialisation: bool = False) -> None:
-        """Sets the launch shape without tuning (see :meth:`last_stats`)."""
-        capi.check(self._lib.mlods_batch_set_schedule(self._b, int(queries_per_warp), 1 if reorder else 0,
-                                                      int(grid_pct), 1 if by_specialisation else 0))
+                     by_specialisation: bool = False, solo_min_queries: int = 0) -> None:
+        """Sets the launch shape without tuning (see :meth:`schedule`)."""
+        sc = capi.mlods_batch_schedule(int(queries_per_warp), 1 if reorder else 0, int(grid_pct),
+                                       1 if by_specialisation else 0, int(solo_min_queries))
+        capi.check(self._lib.mlods_batch_set_schedule(self._b, C.byref(sc)))
 
     def tune_results(self):
         """The candidates of the last :meth:`tune` with their device times (ms)."""
         n = C.c_int32(0)
-        capi.check(self._lib.mlods_batch_tune_results(self._b, 0, None, None, None, None, None, C.byref(n)))
+        capi.check(self._lib.mlods_batch_tune_results(self._b, 0, None, None, C.byref(n)))
         k = n.value
-        qw, ro, gp, lo = (C.c_int32 * max(k, 1))(), (C.c_int32 * max(k, 1))(), (C.c_int32 * max(k, 1))(), \
-            (C.c_int32 * max(k, 1))()
+        cands = (capi.mlods_batch_schedule * max(k, 1))()
         ms = (C.c_float * max(k, 1))()
-        capi.check(self._lib.mlods_batch_tune_results(self._b, k, qw, ro, gp, lo, ms, C.byref(n)))
-        return [{"queries_per_warp": qw[i], "query_order": "Morton" if ro[i] else "input", "grid_pct": gp[i],
-                 "line_order": "by specialisation" if lo[i] == 1 else "most work first", "ms": ms[i]}
-                for i in range(k)]
+        capi.check(self._lib.mlods_batch_tune_results(self._b, k, cands, ms, C.byref(n)))
+        return [dict(self._schedule_dict(cands[i]), ms=ms[i]) for i in range(k)]
 
 
 class ProjectionServer:

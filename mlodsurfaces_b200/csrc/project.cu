@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(kProjectThreads, WalkShape<QPW>::kMinBlocks) m
 #pragma unroll
         for (int x = 0; x < QPW; ++x) {
             const uint32_t s = qs + uint32_t(x < nq ? x : 0);
-            qi[x] = a.order ? __ldg(a.order + s) : s;
+            qi[x] = a.order ? __ldg(a.order + s) - a.order_base : s;
         }
         WalkStats ws;
         project_queries<KTYPE, NSIG, RULE, CAP, QPW, PRUNE>(a.cloud, qi, nq, st, ws);
@@ -760,8 +760,8 @@ cudaError_t launch_queue_typed(const QueueArgs& a, int sm_count, int grid_pct, c
         for (int i = 0; i < nc; ++i) {
             idx[size_t(i)] = i;
             p.clouds[i] = a.clouds[c0 + i];
-            p.base[i] = a.q_offsets[c0 + i];
-            p.len[i] = a.q_offsets[c0 + i + 1] - a.q_offsets[c0 + i];
+            p.base[i] = a.base[c0 + i];
+            p.len[i] = a.len[c0 + i];
             p.spec[i] = walk_spec_id(p.clouds[i]);
         }
         // the clouds with the most work first, so that the launch ends on
@@ -803,6 +803,13 @@ cudaError_t launch_mlod_queue(const QueueArgs& a, int queries_per_warp, int sm_c
 {
     if (queries_per_warp == 2) return launch_queue_typed<2>(a, sm_count, grid_pct, s);
     return launch_queue_typed<1>(a, sm_count, grid_pct, s);
+}
+
+int64_t project_resident_queries(int queries_per_warp, int sm_count)
+{
+    const int per_sm = queries_per_warp == 4 ? WalkShape<4>::kMinBlocks
+                                             : (queries_per_warp == 2 ? WalkShape<2>::kMinBlocks : WalkShape<1>::kMinBlocks);
+    return int64_t(per_sm) * (kProjectThreads / 32) * queries_per_warp * sm_count;
 }
 
 size_t query_order_temp_bytes(int64_t n)

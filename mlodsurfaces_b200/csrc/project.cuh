@@ -58,18 +58,20 @@ struct ProjectArgs {
     int64_t* stats;         // [0] query-node visits, [1] max stack, [2] overflows, [3] counter, [4] rounds,
                             // [5] query-iterations, [6] lane visits (a node shared by a warp's queries once)
     int queries_per_warp = 1;  // 1, or 2: consecutive queries of `order` share one walk
+    uint32_t order_base = 0;   // subtracted from every entry of `order` (a tree's slice of a batch order)
 };
 
 // Many trees in ONE persistent launch.  The queries of cloud c occupy the
-// global range [q_offsets[c], q_offsets[c + 1]) of the concatenated buffers,
-// and the same range of slots of the batch order: order[slot] is the global
+// global range [base[c], base[c] + len[c]) of the concatenated buffers, and
+// the same range of slots of the batch order: order[slot] is the global
 // index of the query processed at that slot (nullptr: slot = query index).
 // The warps of the queue kernel take queries_per_warp consecutive slots of
 // one cloud at a time from a device counter, as the single-tree kernel does
 // over one cloud.
 struct QueueArgs {
     const CloudArgs* clouds;   // host array: each cloud's q_in / out_p / out_n address its own range
-    const int64_t* q_offsets;  // host array, n_clouds + 1 entries
+    const int64_t* base;       // host array: first global query of each cloud
+    const int64_t* len;        // host array: its query count
     int n_clouds;
     const uint32_t* order;     // device
     unsigned long long* counters;  // device: one 64-bit slot counter per launch group, zero before launch
@@ -96,6 +98,10 @@ inline int queue_groups(int n_clouds) { return (n_clouds + kQueueMaxClouds - 1) 
 // aligned to the cloud's first slot, so that results equal per-tree
 // launches with the same schedule bit for bit.
 cudaError_t launch_mlod_queue(const QueueArgs& a, int queries_per_warp, int sm_count, int grid_pct, cudaStream_t s);
+
+// Queries the single-tree walk holds in flight when every SM runs its
+// blocks (resident warps x queries per warp).
+int64_t project_resident_queries(int queries_per_warp, int sm_count);
 
 // Per-cloud frame used to key queries: the cloud's rank in the batch order
 // (clouds of a batch keep their own rank: their slots are their query range)

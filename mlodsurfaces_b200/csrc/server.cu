@@ -227,9 +227,12 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Piece>& batch)
     if (e == cudaSuccess)
         e = compute_batch_order(dq, total, d_offsets, int(nc), d_frames, true, order, mem + L.temp, w.s);
     if (e == cudaSuccess) {
+        std::vector<int64_t> lens(nc);
+        for (size_t i = 0; i < nc; ++i) lens[i] = w.h_offsets[i + 1] - w.h_offsets[i];
         QueueArgs a;
         a.clouds = w.h_clouds;
-        a.q_offsets = w.h_offsets;
+        a.base = w.h_offsets;
+        a.len = lens.data();
         a.n_clouds = int(nc);
         a.order = order;
         a.counters = reinterpret_cast<unsigned long long*>(w.d_stats + 8);

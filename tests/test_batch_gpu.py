@@ -101,10 +101,10 @@ def test_graph_replay_and_tuning(setup):
     assert st["grid_pct"] in (85, 100) and st["reorder"] in (0, 1)
     assert st["queries_per_warp"] in (1, 2)
     cands = b.tune_results()
-    assert len(cands) == 5 and all(c["ms"] > 0 for c in cands)
+    assert len(cands) == 7 and all(c["ms"] > 0 for c in cands)
     best = min(cands, key=lambda c: c["ms"])
-    assert (best["queries_per_warp"], best["grid_pct"], best["line_order"]) == \
-        (st["queries_per_warp"], st["grid_pct"], st["line_order"])
+    keys = ("queries_per_warp", "reorder", "grid_pct", "line_order", "solo_min_queries")
+    assert all(best[k] == st[k] for k in keys)
     d_p.fill_(float("nan"))
     b.project_device(counts, d_q, d_p, d_n, 4, use_graph=True)
     torch.cuda.synchronize()
@@ -137,24 +137,34 @@ def test_graph_replay_and_tuning(setup):
     assert torch.equal(d_p, ref2_p)
 
 
-@pytest.mark.parametrize("by_spec", [False, True])
-def test_batch_with_paired_walks_equals_per_tree(setup, by_spec):
+@pytest.mark.parametrize("by_spec,solo,reorder", [(False, 0, True), (True, 0, True), (True, 1000, True),
+                                                   (False, 1000, False)])
+def test_batch_with_paired_walks_equals_per_tree(setup, by_spec, solo, reorder):
     """Trees set to two queries per warp: the single launch pairs the same
     queries as each tree's own launch (each tree's slots are padded to a
-    multiple of 4), whatever the order of the trees along the launch."""
+    multiple of 4), whatever the order of the trees along the launch; trees
+    with at least `solo` queries run in launches of their own on their slice
+    of the batch order."""
     projectors, queries = setup
     saved = [f.queries_per_warp for f in projectors]
+    saved_order = [f.reorder for f in projectors]
     try:
         for f in projectors:
             f.queries_per_warp = 2
+            f.reorder = reorder
         ref_p, ref_n = _per_tree(projectors, queries, 5)
         b = FastapssBatch(projectors)
-        b.set_schedule(0, True, 100, by_specialisation=by_spec)
-        p, n, _ = _batched(b, queries, 5)
-        assert b.last_stats()["line_order"] == ("by specialisation" if by_spec else "most work first")
+        b.set_schedule(0, reorder, 100, by_specialisation=by_spec, solo_min_queries=solo)
+        p, n, _ = _batched(b, queries, 5, use_graph=bool(solo))
+        st = b.last_stats()
+        assert st["line_order"] == ("by specialisation" if by_spec else "most work first")
+        assert st["solo_min_queries"] == solo
+        # two trees hold >= 1000 queries (4000 and 3000), one fewer (700), one none
+        assert st["walk_launches"] == (3 if solo else 1)
     finally:
-        for f, w in zip(projectors, saved):
+        for f, w, r in zip(projectors, saved, saved_order):
             f.queries_per_warp = w
+            f.reorder = r
     assert torch.equal(p, ref_p) and torch.equal(n, ref_n)
 
 
@@ -179,6 +189,8 @@ def test_batch_rejects_bad_input(setup):
         b.set_schedule(queries_per_warp=3)
     with pytest.raises(MlodsError):
         b.set_schedule(grid_pct=0)
+    with pytest.raises(MlodsError):
+        b.set_schedule(solo_min_queries=-1)
     g = Fastapss(projectors[0].m_apssOctree)
     g.m_apssOctree.knnMode(True, 8)
     try:
