@@ -165,13 +165,14 @@ struct WalkStats {
 // blend weight, kernel weight -- and the node is opened for the queries that
 // find it near, or ends the walk as an aggregate for those that find it far.
 // Node loads, the pop / push bookkeeping and the leaf logic are paid once for
-// all the warp's queries.  Each query's arithmetic is exactly that of its own
-// walk (QPW = 1 is the one-query-per-warp walk); only the lane on which a
-// node's contribution is accumulated, and so the order of the float sums,
-// depends on the partner query.
-template <int KTYPE, int NSIG, int RULE, int CAP, int QPW, bool PRUNE = false>
-__device__ __forceinline__ void project_queries(const CloudArgs& c, const uint32_t (&qi)[QPW], int nq,
-                                                WarpStack<CAP, QPW>& st, WalkStats& ws)
+// all the warp's queries.  Each query's arithmetic is that of its own walk
+// (QPW = 1 is the one-query-per-warp walk; two queries per warp run the
+// packed form below); only the lane on which a node's contribution is
+// accumulated, and so the order of the float sums, depends on the partner
+// query.
+template <int KTYPE, int NSIG, int RULE, int CAP, int QPW, bool PRUNE>
+__device__ __forceinline__ void project_walk(const CloudArgs& c, const uint32_t (&qi)[QPW], int nq,
+                                             WarpStack<CAP, QPW>& st, WalkStats& ws)
 {
     static_assert(QPW >= 1 && QPW <= 4, "one to four queries per warp");
     const bool gpu_rule = RULE < 0 ? c.rule == MLODS_BLEND_GPU : RULE == MLODS_BLEND_GPU;
@@ -435,6 +436,356 @@ __device__ __forceinline__ void project_queries(const CloudArgs& c, const uint32
         on[1] = bad ? 0.f : nrm[1];
         on[2] = bad ? 0.f : nrm[2];
     }
+}
+
+// ---- two or four queries per warp in packed f32x2 arithmetic --------------
+// With several queries per warp every node is evaluated for each with the
+// same node data, so their arithmetic pairs up: sm_100's packed instructions
+// (FADD2 / FMUL2 / FFMA2) do two queries' operation in one issue slot, each
+// element rounded as the scalar instruction would.  The walk is otherwise the
+// general one; its stack entries hold each pair's values interleaved
+// ({f0, f1, A0, A1}, {dP0, dP1, g0, g1}) so that a pair sits in a register
+// pair.
+
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b, exactly as a scalar subtraction rounds it
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+template <int KTYPE, int NSIG>
+__device__ __forceinline__ float2 weight_pair(const KernelConsts& kc, float2 d2)
+{
+    if (KTYPE == MLODS_GAUSSIAN) {
+        const float2 t = mul2(d2, splat2(kc.g_scale));
+        return add2(make_float2(exp2f(t.x), exp2f(t.y)), splat2(kc.shift));
+    } else if (KTYPE == MLODS_GAUSSIAN_MULTIPLE && NSIG > 0) {
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < NSIG; ++i) {
+            const float2 t = mul2(d2, splat2(kc.ms_scale[i]));
+            s = fma2(make_float2(exp2f(t.x), exp2f(t.y)), splat2(kc.ms_w[i]), s);
+        }
+        return s;
+    } else if (KTYPE == MLODS_SINGULAR) {
+        const float2 u = add2(d2, splat2(kc.shift));
+        const float2 l = mul2(splat2(-kc.exponent), make_float2(__log2f(u.x), __log2f(u.y)));
+        return mul2(splat2(kc.num), make_float2(exp2f(l.x), exp2f(l.y)));
+    } else {
+        return make_float2(weight_n<KTYPE, NSIG>(kc, d2.x), weight_n<KTYPE, NSIG>(kc, d2.y));
+    }
+}
+
+template <int KTYPE, int NSIG, int RULE, int CAP, int NP, bool PRUNE>
+__device__ __forceinline__ void project_packed(const CloudArgs& c, const uint32_t (&qi)[2 * NP], int nq,
+                                               WarpStack<CAP, 2 * NP>& st, WalkStats& ws)
+{
+    constexpr int QPW = 2 * NP;
+    const bool gpu_rule = RULE < 0 ? c.rule == MLODS_BLEND_GPU : RULE == MLODS_BLEND_GPU;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t le_mask = lane == 31 ? kFull : ((2u << lane) - 1u);
+    const float4* __restrict__ ngeom = c.nodes.geom;
+    const float4* __restrict__ npm = c.nodes.pm;
+    const float4* __restrict__ nnc = c.nodes.nc;
+    const float4* __restrict__ naux = c.nodes.aux;
+    const float cutoff = c.cutoff;
+    const int min_depth = c.min_depth;
+
+    // lane x < nq holds the iterate of query x in the tree's local frame, in
+    // double; the other lanes shadow query 0 (their results are not written)
+    uint32_t my_q = qi[0];
+#pragma unroll
+    for (int x = 1; x < QPW; ++x)
+        if (lane == x && x < nq) my_q = qi[x];
+    double qd[3] = {double(c.q_in[3 * int64_t(my_q)]) - c.o0, double(c.q_in[3 * int64_t(my_q) + 1]) - c.o1,
+                    double(c.q_in[3 * int64_t(my_q) + 2]) - c.o2};
+    float nrm[3] = {0.f, 0.f, 0.f};
+    uint32_t live = (1u << nq) - 1u;  // queries still iterating (warp-uniform)
+    uint32_t failed = 0;
+    for (int it = 0; it < c.n_iter && live; ++it) {
+        // queries 2j and 2j + 1 form pair j
+        float2 qx[NP], qy[NP], qz[NP];
+        {
+            const float mx = float(qd[0]), my = float(qd[1]), mz = float(qd[2]);
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                qx[j] = make_float2(__shfl_sync(kFull, mx, 2 * j), __shfl_sync(kFull, mx, 2 * j + 1));
+                qy[j] = make_float2(__shfl_sync(kFull, my, 2 * j), __shfl_sync(kFull, my, 2 * j + 1));
+                qz[j] = make_float2(__shfl_sync(kFull, mz, 2 * j), __shfl_sync(kFull, mz, 2 * j + 1));
+            }
+        }
+        float2 acc[NP][9];
+#pragma unroll
+        for (int j = 0; j < NP; ++j)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc[j][k] = make_float2(0.f, 0.f);
+        int top = 1;
+        if (lane == 0) {
+            const uint32_t w0 = 1u | kEntNoBlend | (live << kEntLiveShift);
+            st.h[0] = make_uint2(0u, w0);
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                st.v[0][2 * j] = make_float4(1.f, 1.f, 0.f, 0.f);  // f f A A
+                st.v[0][2 * j + 1] = make_float4(0.f, 0.f, 0.f, 0.f);  // dP dP g g
+            }
+            st.cnt[0] = w0;
+        }
+        __syncwarp();
+        while (top > 0) {
+            // ---- pop sibling ranges from the top until 32 lanes are filled
+            int cn = 0;
+            if (lane < top) cn = int(st.cnt[top - 1 - lane] & kEntCount);
+            const int incl = warp_incl_scan_i(cn);
+            const uint32_t fit = __ballot_sync(kFull, lane < top && incl <= 32);
+            const int npop = __popc(fit);
+            const bool partial = npop == 0;  // top range wider than a warp (multi-point leaf)
+            const int total = partial ? 32 : __shfl_sync(kFull, incl, npop - 1);
+            const uint32_t heads = partial ? 1u : __reduce_or_sync(kFull, lane < npop ? (1u << (incl - cn)) : 0u);
+            const bool active = lane < total;
+            const uint32_t hb = heads & le_mask;
+            const int e = __popc(hb) - 1;
+            const int r_start = 31 - __clz(hb);
+            const int slot = top - 1 - e;
+            const uint2 E = st.h[slot];
+            float4 VA[NP], VB[NP];  // {f, f, A, A} and {dP, dP, g, g} of each pair
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                VA[j] = st.v[slot][2 * j];
+                VB[j] = st.v[slot][2 * j + 1];
+            }
+            const uint32_t r_first = E.x, r_cnt = E.y;
+            const uint32_t r_live = (r_cnt >> kEntLiveShift) & ((1u << QPW) - 1u);
+            const int r_len = partial ? 32 : int(r_cnt & kEntCount);
+            const int old_top = top;
+            if (!partial) top -= npop;
+            ws.lane_visits += uint32_t(total);
+            ws.visits += __reduce_add_sync(kFull, active ? uint32_t(__popc(r_live)) : 0u);
+            ++ws.rounds;
+
+            // ---- evaluate one node per lane, for every query at once
+            const uint32_t node = r_first + uint32_t(lane - r_start);
+            float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f), p4 = g4;
+            float4 x4 = make_float4(0.f, 0.f, __uint_as_float(kLeafBit | 1u), 0.f);
+            if (active) {
+                g4 = __ldg(ngeom + node);
+                p4 = __ldg(npm + node);
+                x4 = __ldg(naux + node);
+            }
+            const float cr = cutoff * g4.w;
+            const bool blend = active && !(r_cnt & kEntNoBlend);
+            const int seg_end = r_start + r_len;
+            float2 dist[NP], f[NP], A[NP];
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                const float2 cx = sub2(splat2(g4.x), qx[j]), cy = sub2(splat2(g4.y), qy[j]),
+                             cz = sub2(splat2(g4.z), qz[j]);
+                const float2 dd = fma2(cx, cx, fma2(cy, cy, mul2(cz, cz)));
+                dist[j] = make_float2(sqrtf(dd.x), sqrtf(dd.y));
+                float2 beta = make_float2(1.f, 1.f), kcon = make_float2(0.f, 0.f);
+                if (blend) {
+                    const float2 dCs = sub2(dist[j], splat2(cr));
+                    const float2 dC = make_float2(fmaxf(dCs.x, 0.f), fmaxf(dCs.y, 0.f));
+                    const float2 dP = make_float2(VB[j].x, VB[j].y);
+                    const float2 den = add2(dP, dC);
+                    const float2 t = mul2(dP, make_float2(__fdividef(1.f, den.x), __fdividef(1.f, den.y)));
+                    const float2 a = mul2(splat2(kPiRef), t);
+                    beta = fma2(splat2(-0.5f), make_float2(__cosf(a.x), __cosf(a.y)), splat2(0.5f));
+                    kcon = mul2(sub2(splat2(1.f), beta), make_float2(VB[j].z, VB[j].w));
+                    if (gpu_rule) kcon = mul2(kcon, splat2(p4.w));
+                    // a query the range is not live for takes no part
+                    if (!((r_live >> (2 * j)) & 1u)) {
+                        beta.x = 1.f;
+                        kcon.x = 0.f;
+                    }
+                    if (!((r_live >> (2 * j + 1)) & 1u)) {
+                        beta.y = 1.f;
+                        kcon.y = 0.f;
+                    }
+                }
+                // segmented sums over the range (blend ranges hold <= 8 lanes)
+#pragma unroll
+                for (int o = 1; o < 8; o <<= 1) {
+                    const float2 nv =
+                        make_float2(__shfl_down_sync(kFull, kcon.x, o), __shfl_down_sync(kFull, kcon.y, o));
+                    if (lane + o < seg_end) kcon = add2(kcon, nv);
+                }
+                const float2 K =
+                    make_float2(__shfl_sync(kFull, kcon.x, r_start), __shfl_sync(kFull, kcon.y, r_start));
+                f[j] = mul2(make_float2(VA[j].x, VA[j].y), beta);
+                A[j] = add2(make_float2(VA[j].z, VA[j].w), K);
+            }
+            if (!gpu_rule && (r_cnt & kEntLastOnly) && (partial || node != r_first + uint32_t(r_len) - 1u))
+#pragma unroll
+                for (int j = 0; j < NP; ++j) f[j] = make_float2(0.f, 0.f);
+
+            const uint32_t info = __float_as_uint(x4.z);
+            const uint32_t nfirst = __float_as_uint(x4.y);
+            const bool leaf = (info & kLeafBit) != 0;
+            const bool multi = (info & kMultiBit) != 0;
+            const uint32_t cnt = node_count(info);
+            // opened for every live query whatever its distance: the points of
+            // a multi-point leaf, the children of a node above min_depth
+            const bool opens_all = leaf ? multi : node_depth(info) < min_depth;
+            uint32_t term = 0, near = 0;
+            if (active && !opens_all) {
+#pragma unroll
+                for (int x = 0; x < QPW; ++x) {
+                    if (!((r_live >> x) & 1u)) continue;
+                    const float d = (x & 1) ? dist[x >> 1].y : dist[x >> 1].x;
+                    if (leaf || d > cr) term |= 1u << x;
+                    else near |= 1u << x;
+                }
+            }
+            if (PRUNE && near) {
+                // kernel-weight pruning (extension, off by default), as in the
+                // general walk
+#pragma unroll
+                for (int x = 0; x < QPW; ++x) {
+                    if (!((near >> x) & 1u)) continue;
+                    const float d = (x & 1) ? dist[x >> 1].y : dist[x >> 1].x;
+                    const float fx = (x & 1) ? f[x >> 1].y : f[x >> 1].x;
+                    const float dmin = fmaxf(d - g4.w, 0.f);
+                    const float wub = weight_n<KTYPE, NSIG>(c.kc, dmin * dmin);
+                    if (fx * wub * p4.w < c.prune_thr) {
+                        near &= ~(1u << x);
+                        term |= 1u << x;
+                        ++ws.pruned;
+                    }
+                }
+            }
+            const uint32_t child_live = active ? (opens_all ? r_live : near) : 0u;
+            const bool push = child_live != 0;
+            const uint32_t p_cnt = cnt | (child_live << kEntLiveShift) |
+                                   (opens_all ? (kEntNoBlend | (leaf && !gpu_rule ? kEntLastOnly : 0u)) : 0u);
+
+            const float inv_m = __fdividef(1.f, gpu_rule ? p4.w : float(cnt));
+            float4 n4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (term) n4 = __ldg(nnc + node);
+            float2 pv_dP[NP], pv_g[NP];
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                const float2 px = sub2(splat2(p4.x), qx[j]), py = sub2(splat2(p4.y), qy[j]),
+                             pz = sub2(splat2(p4.z), qz[j]);
+                const float2 d2 = fma2(px, px, fma2(py, py, mul2(pz, pz)));
+                const float2 w = weight_pair<KTYPE, NSIG>(c.kc, d2);
+                pv_dP[j] = sub2(splat2(cr), dist[j]);
+                pv_g[j] = mul2(mul2(f[j], w), splat2(inv_m));
+                const uint32_t tj = (term >> (2 * j)) & 3u;
+                if (tj) {
+                    const float2 cf = fma2(f[j], w, A[j]);
+                    // a query for which the node is not an aggregate adds zero
+                    const float2 coef = make_float2((tj & 1u) ? cf.x : 0.f, (tj & 2u) ? cf.y : 0.f);
+                    const float2 cm = mul2(coef, splat2(p4.w));
+                    acc[j][0] = add2(acc[j][0], cm);
+                    acc[j][1] = fma2(coef, splat2(n4.x), acc[j][1]);
+                    acc[j][2] = fma2(coef, splat2(n4.y), acc[j][2]);
+                    acc[j][3] = fma2(coef, splat2(n4.z), acc[j][3]);
+                    acc[j][4] = fma2(cm, px, acc[j][4]);
+                    acc[j][5] = fma2(cm, py, acc[j][5]);
+                    acc[j][6] = fma2(cm, pz, acc[j][6]);
+                    acc[j][7] = fma2(
+                        coef, fma2(px, splat2(n4.x), fma2(py, splat2(n4.y), fma2(pz, splat2(n4.z), splat2(n4.w)))),
+                        acc[j][7]);
+                    acc[j][8] = fma2(coef, fma2(d2, splat2(p4.w), splat2(x4.x)), acc[j][8]);
+                }
+            }
+            // ---- push child ranges (every lane has read its entry: the
+            // shuffles above depend on those reads)
+            __syncwarp();
+            if (partial && lane == 0) {
+                uint2 rest = st.h[old_top - 1];
+                rest.x += 32u;
+                rest.y -= 32u;
+                st.h[old_top - 1] = rest;
+                st.cnt[old_top - 1] = rest.y;
+            }
+            const uint32_t pmask = __ballot_sync(kFull, push);
+            const int npush = __popc(pmask);
+            if (top + npush > CAP) {
+                ws.overflow = true;  // the warp's live queries are reported as failed
+            } else {
+                if (push) {
+                    const int pos = top + __popc(pmask & lt_mask);
+                    st.h[pos] = make_uint2(nfirst, p_cnt);
+#pragma unroll
+                    for (int j = 0; j < NP; ++j) {
+                        st.v[pos][2 * j] = make_float4(f[j].x, f[j].y, A[j].x, A[j].y);
+                        st.v[pos][2 * j + 1] = make_float4(pv_dP[j].x, pv_dP[j].y, pv_g[j].x, pv_g[j].y);
+                    }
+                    st.cnt[pos] = p_cnt;
+                }
+                top += npush;
+            }
+            if (top > ws.max_top) ws.max_top = top;
+            __syncwarp();
+        }
+        ws.iterations += uint32_t(__popc(live));
+        // warp sums; lane x then fits query x (the other lanes repeat query 0)
+        float sv[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            sv[k] = warp_sum_f(acc[0][k].x);
+#pragma unroll
+            for (int x = 1; x < QPW; ++x) {
+                const float t = warp_sum_f((x & 1) ? acc[x >> 1][k].y : acc[x >> 1][k].x);
+                if (lane == x) sv[k] = t;
+            }
+        }
+        const bool mine = lane < QPW && ((live >> lane) & 1u);
+        double xr[3] = {0.0, 0.0, 0.0};
+        const bool ok = !ws.overflow && fit_sphere(sv, double(c.step_max), gpu_rule, xr, nrm);
+        bool stop = false;
+        if (mine && !ok) {
+            failed |= 1u << lane;
+            stop = true;
+        } else if (mine) {
+            // the projection of the float query just evaluated
+            const float fx = float(qd[0]), fy = float(qd[1]), fz = float(qd[2]);
+            qd[0] = double(fx) + xr[0];
+            qd[1] = double(fy) + xr[1];
+            qd[2] = double(fz) + xr[2];
+            if (c.conv_mode == MLODS_CONVERGE_EXACT) {
+                // the next iteration would evaluate the same float query:
+                // every remaining iteration returns this result again
+                stop = float(qd[0]) == fx && float(qd[1]) == fy && float(qd[2]) == fz;
+            } else if (c.conv_mode == MLODS_CONVERGE_TOL) {
+                stop = xr[0] * xr[0] + xr[1] * xr[1] + xr[2] * xr[2] < double(c.conv_tol) * double(c.conv_tol);
+            }
+        }
+        live &= ~__ballot_sync(kFull, mine && stop);
+    }
+    failed = __reduce_or_sync(kFull, failed);
+    if (lane < nq) {
+        float* op = c.out_p + 3 * int64_t(my_q);
+        float* on = c.out_n + 3 * int64_t(my_q);
+        // on failure (Fastapss.cu:385-391) the point stays where the failing
+        // iteration started and the normal is zero
+        const bool bad = (failed >> lane) & 1u;
+        if (c.local_out) {
+            op[0] = float(qd[0]);
+            op[1] = float(qd[1]);
+            op[2] = float(qd[2]);
+        } else {
+            op[0] = float(qd[0] + c.o0);
+            op[1] = float(qd[1] + c.o1);
+            op[2] = float(qd[2] + c.o2);
+        }
+        on[0] = bad ? 0.f : nrm[0];
+        on[1] = bad ? 0.f : nrm[1];
+        on[2] = bad ? 0.f : nrm[2];
+    }
+}
+
+// Projects the nq (<= QPW) queries qi[0..nq) of one tree together (the
+// general walk for one query per warp, the packed form for two or four).
+template <int KTYPE, int NSIG, int RULE, int CAP, int QPW, bool PRUNE = false>
+__device__ __forceinline__ void project_queries(const CloudArgs& c, const uint32_t (&qi)[QPW], int nq,
+                                                WarpStack<CAP, QPW>& st, WalkStats& ws)
+{
+    if constexpr (QPW == 2 || QPW == 4) project_packed<KTYPE, NSIG, RULE, CAP, QPW / 2, PRUNE>(c, qi, nq, st, ws);
+    else project_walk<KTYPE, NSIG, RULE, CAP, QPW, PRUNE>(c, qi, nq, st, ws);
 }
 
 // Per-warp totals of the walks, kept in 64 bits across queries.
