@@ -201,18 +201,20 @@ PRUNE_TOLS = (1e-6, 1e-3, 1e-1)  # tolerances of the reported kernel-weight prun
 # scaled to 200k points (one launch, -k mlod_project -s 3 -c 1): the limits
 # the algorithmic-bytes figure does not show.
 PROFILED_COUNTERS = {
-    "precision": {"capture": "ncu --set full, precision workload at 200k points, two queries per warp, one launch",
-                  "issue_slots_active_pct": 76.4, "warp_instructions_per_query_node_visit": 7.44,
-                  "threads_active_per_instruction": 28.43, "warps_active_per_sm": 27.6,
-                  "l2_sector_throughput_gbs": 3010.0, "l2_throughput_pct": 12.3, "l2_hit_rate_pct": 98.76,
-                  "l1_throughput_pct": 54.2, "fp32_fma_pipe_pct": 27.6, "alu_pipe_pct": 50.5, "xu_pipe_pct": 35.0,
-                  "fp64_pipe_pct": 2.76, "top_stalls_per_issue": {"wait": 2.13, "short_scoreboard": 1.72,
-                                                                  "not_selected": 1.71, "long_scoreboard": 1.10}},
+    "precision": {"capture": "ncu --set full, precision workload at 200k points, two queries per warp (packed "
+                             "f32x2 arithmetic), one launch",
+                  "issue_slots_active_pct": 74.9, "warp_instructions_per_query_node_visit": 6.6,
+                  "threads_active_per_instruction": 28.71, "warps_active_per_sm": 27.6,
+                  "l2_sector_throughput_gbs": 4040.0, "l2_throughput_pct": 15.3, "l2_hit_rate_pct": 99.11,
+                  "l1_throughput_pct": 65.3, "fp32_fma_pipe_cycles_pct": 35.0, "alu_pipe_pct": 55.3,
+                  "xu_pipe_pct": 38.8, "fp64_pipe_pct": 3.06,
+                  "top_stalls_per_issue": {"wait": 2.22, "short_scoreboard": 1.91, "not_selected": 1.53,
+                                           "long_scoreboard": 0.94}},
 }
 # L2 sector throughput peak of the B200 as ncu reports it (lts__t_sectors:
 # 3 sectors per cycle per slice at the L2 clock), from the capture above:
-# 94.07 sectors/ns at 8.68 % of peak
-L2_PEAK_GBS = 94.07 * 32 / 0.0868
+# 126.26 sectors/ns at 11.66 % of peak
+L2_PEAK_GBS = 126.26 * 32 / 0.1166
 
 
 def max_over_ranks(values, world: int, device):
@@ -547,8 +549,9 @@ def run_ours(args, rank, world, local_rank):
     mean_visits = statistics.mean(visits)
     bytes_per_launch = len(q) * (12 + 24) + 64 * mean_visits
     roof_note = (f"algorithmic bytes = 36 per query + 64 per node visit ({mean_visits / len(q) / args.iters:.0f}"
-                 f" visits per query-iteration); traffic = DRAM bytes per launch from ncu: the node arrays are read "
-                 f"from DRAM about once, later visits hit L1/L2")
+                 f" visits per query-iteration, the reference walk's); a warp walking two queries loads a node they "
+                 f"share once, so frac can exceed 1 (node_evaluations: the bytes of the loads made); traffic = DRAM "
+                 f"bytes per launch from ncu: the node arrays are read from DRAM about once, later visits hit L1/L2")
     if spec.get("knn"):  # the k neighbours' positions and normals, every iteration
         bytes_per_launch = len(q) * (12 + 24) + len(q) * args.iters * spec["knn"] * 24
         roof_note = (f"algorithmic bytes = 36 per query + {spec['knn']} neighbours x 24 bytes per query-iteration "
@@ -565,6 +568,14 @@ def run_ours(args, rank, world, local_rank):
         roofline["served_from"] = "L1/L2: the algorithmic node bytes are rereads of records already on chip"
         roofline["l2"] = {"achieved": achieved, "peak": L2_PEAK_GBS, "unit": "GB/s", "frac": achieved / L2_PEAK_GBS,
                           "note": "the same algorithmic bytes against the L2 sector peak ncu reports"}
+        # a warp walking several queries loads a node once for all of them:
+        # the bytes of the node evaluations it actually makes
+        ev = statistics.mean(lane_visits)
+        loaded = (len(q) * 36 + 64 * ev) / (kms / 1e3) / 1e9
+        roofline["node_evaluations"] = {
+            "achieved": loaded, "peak": peak, "unit": "GB/s", "frac": loaded / peak,
+            "note": f"36 B per query + 64 B per node evaluation ({ev / len(q) / args.iters:.0f} per query-iteration: "
+                    f"a node the queries of one warp share is loaded once), against the HBM peak"}
         # flops per query-iteration: per node visit 14 (distance, blend) + 18
         # (moment terms) + the kernel's (10 per Gaussian term, 20 rational),
         # and about 60 for the sphere solve
