@@ -104,10 +104,17 @@ namespace mlods
 namespace
 {
 inline size_t al256(size_t v) { return (v + 255) / 256 * 256; }
-// statistics, then a 64-bit slot counter for each launch group of
-// kQueueMaxClouds pieces (max_batch_requests is at most kMaxServeGroups groups)
+// statistics, a 64-bit slot counter for each launch group of
+// kQueueMaxClouds pieces (max_batch_requests is at most kMaxServeGroups
+// groups), then a 32-bit work counter for each piece that runs in a launch
+// of its own
 constexpr int kMaxServeGroups = 64;
-constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + kMaxServeGroups * sizeof(uint64_t);
+constexpr size_t kStatsBytes = 8 * sizeof(int64_t) + kMaxServeGroups * sizeof(uint64_t) +
+                               size_t(kMaxServeGroups) * kQueueMaxClouds * sizeof(unsigned int);
+// A piece of at least this many times the queries the walk holds in flight
+// on the whole GPU runs in a launch of its own (the single-tree kernel, whose
+// arguments sit in the constant bank) before the shared launch of the rest.
+constexpr int64_t kSoloFill = 16;
 
 // Device layout of one batch of n queries from r requests or pieces.
 struct BatchLayout {
@@ -227,17 +234,42 @@ int run_batch(mlods_server_s* S, Worker& w, const std::vector<Piece>& batch)
     if (e == cudaSuccess)
         e = compute_batch_order(dq, total, d_offsets, int(nc), d_frames, true, order, mem + L.temp, w.s);
     if (e == cudaSuccess) {
-        std::vector<int64_t> lens(nc);
-        for (size_t i = 0; i < nc; ++i) lens[i] = w.h_offsets[i + 1] - w.h_offsets[i];
-        QueueArgs a;
-        a.clouds = w.h_clouds;
-        a.base = w.h_offsets;
-        a.len = lens.data();
-        a.n_clouds = int(nc);
-        a.order = order;
-        a.counters = reinterpret_cast<unsigned long long*>(w.d_stats + 8);
-        a.stats = w.d_stats;
-        e = launch_mlod_queue(a, qpw, sm_count_for_current_device(), 100, w.s);
+        const int sm = sm_count_for_current_device();
+        const int64_t solo_min = kSoloFill * project_resident_queries(qpw, sm);
+        std::vector<CloudArgs> qclouds;
+        std::vector<int64_t> qbase, qlen;
+        unsigned int* solo_counters = reinterpret_cast<unsigned int*>(w.d_stats + 8 + kMaxServeGroups);
+        int n_solo = 0;
+        for (size_t i = 0; i < nc && e == cudaSuccess; ++i) {
+            const int64_t len = w.h_offsets[i + 1] - w.h_offsets[i];
+            if (len >= solo_min) {
+                // a large piece: the single-tree kernel on its slice of the order
+                ProjectArgs pa;
+                pa.cloud = w.h_clouds[i];
+                pa.order = order + w.h_offsets[i];
+                pa.order_base = uint32_t(w.h_offsets[i]);
+                pa.nq = len;
+                pa.counter = solo_counters + n_solo++;
+                pa.stats = w.d_stats;
+                pa.queries_per_warp = qpw;
+                e = launch_mlod_project(pa, pa.cloud.kc.type, pa.cloud.rule, sm, w.s);
+            } else {
+                qclouds.push_back(w.h_clouds[i]);
+                qbase.push_back(w.h_offsets[i]);
+                qlen.push_back(len);
+            }
+        }
+        if (e == cudaSuccess && !qclouds.empty()) {
+            QueueArgs a;
+            a.clouds = qclouds.data();
+            a.base = qbase.data();
+            a.len = qlen.data();
+            a.n_clouds = int(qclouds.size());
+            a.order = order;
+            a.counters = reinterpret_cast<unsigned long long*>(w.d_stats + 8);
+            a.stats = w.d_stats;
+            e = launch_mlod_queue(a, qpw, sm, 100, w.s);
+        }
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(hp, dp, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hn, dn, size_t(total) * 12, cudaMemcpyDeviceToHost, w.s);

@@ -211,3 +211,40 @@ def test_device_budget_bounds_the_batches_in_flight(projectors):
             assert np.array_equal(p, want_p) and np.array_equal(n, want_n)
     finally:
         srv.close()
+
+
+def test_large_pieces_alone_and_paired_walks(projectors):
+    """A piece large enough to fill the GPU many times over runs in a launch
+    of its own (the single-tree kernel) beside the shared launch of the
+    small ones, with the same results as the requests projected alone.  With
+    two queries per warp a request that runs whole is still bit-identical;
+    one cut into pieces pairs its queries within each piece, so it agrees
+    with the projection alone to float rounding of the moment sums."""
+    f, pts, diag = projectors[0]
+    q = synth.perturbed_queries(pts, 0.01, seed=81)
+    big = np.ascontiguousarray(np.concatenate([q + np.float32(1e-4 * diag * k) for k in range(5)]), np.float32)
+    small = q[:3000]
+    saved = f.queries_per_warp
+    try:
+        for qpw in (1, 2):
+            f.queries_per_warp = qpw
+            want = [direct(f, r, 3) for r in (big, small)]
+            srv = ProjectionServer([f], n_streams=1)  # 2^18-query batches: the 200k request runs whole
+            try:
+                outs = [srv.wait(srv.submit(0, r, 3), timeout_ms=120000) for r in (big, small)]
+            finally:
+                srv.close()
+            for (p, n, _), (wp, wn) in zip(outs, want):
+                assert np.array_equal(p, wp) and np.array_equal(n, wn)
+        # cut into 60000-query pieces: within the tolerance of the projection alone
+        wp, wn = direct(f, big, 3)
+        srv = ProjectionServer([f], n_streams=2, max_batch_queries=60000)
+        try:
+            p, n, _ = srv.wait(srv.submit(0, big, 3), timeout_ms=120000)
+        finally:
+            srv.close()
+        dev = np.linalg.norm(p.astype(np.float64) - wp, axis=1) / diag
+        assert dev.max() < 1e-5
+        assert ((n * wn).sum(1) > 1 - 1e-4).mean() > 0.999
+    finally:
+        f.queries_per_warp = saved
