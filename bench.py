@@ -1338,7 +1338,6 @@ def run_serve(args):
     stats = srv.stats()
     memory = srv.memory()
     srv.close()
-    total_q = done_q[0]
     # served results against each request projected alone (the reference-facing
     # protocol with the request's kernel): bit-identical for a request that
     # ran whole; one cut into pieces pairs its queries within each piece, so

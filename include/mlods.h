@@ -89,7 +89,7 @@ typedef struct mlods_params {
                             average sample at the query, w(0) * mean area.  Fewer node visits;
                             results move by at most what the dropped subtrees could weigh.
                             Applies to projections of one tree (queries_per_warp 1 or 2, which
-                            it requires); the grouped launches of a batch walk without it. */
+                            it requires); batched and served projections walk without it. */
     int32_t converge;    /* MLODS_CONVERGE_* (default MLODS_CONVERGE_OFF) */
     float converge_tol;  /* step length for MLODS_CONVERGE_TOL (absolute units) */
     int32_t local_output; /* extension, default 0.  1: MLoD results are written relative to the
