@@ -198,7 +198,7 @@ class ClockSampler:
 # (2M points, 2M queries, 10 iterations), from a single-pass ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum of mlod_project_kernel on that
 # workload (python bench.py --steps 2 --warmup 1 under ncu --metrics ...).
-PROFILED_TRAFFIC = {("precision", 2_000_000, 10): 515.25e6 + 168.89e6}
+PROFILED_TRAFFIC = {("precision", 2_000_000, 10): 503.71e6 + 146.34e6}
 PRUNE_TOLS = (1e-6, 1e-3, 1e-1)  # tolerances of the reported kernel-weight pruning runs
 # Counters of the same kernel from a `--set full` capture of the workload
 # scaled to 200k points (one launch, -k mlod_project -s 3 -c 1): the limits
