@@ -477,7 +477,7 @@ __device__ __forceinline__ float2 weight_pair(const KernelConsts& kc, float2 d2)
     }
 }
 
-template <int KTYPE, int NSIG, int RULE, int CAP, int NP, bool PRUNE>
+template <int KTYPE, int NSIG, int RULE, int CAP, int NP, bool PRUNE, bool EARLY_NC>
 __device__ __forceinline__ void project_packed(const CloudArgs& c, const uint32_t (&qi)[2 * NP], int nq,
                                                WarpStack<CAP, 2 * NP>& st, WalkStats& ws)
 {
@@ -568,14 +568,15 @@ __device__ __forceinline__ void project_packed(const CloudArgs& c, const uint32_
             const uint32_t node = r_first + uint32_t(lane - r_start);
             float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f), p4 = g4;
             float4 x4 = make_float4(0.f, 0.f, __uint_as_float(kLeafBit | 1u), 0.f);
-            // the normal record is needed only where the node ends a walk, but
-            // loading it with the others hides its latency (measured faster)
+            // the normal record is needed only where the node ends a walk;
+            // loading it with the others hides its latency, which measured
+            // faster in the single-tree kernel and slower in the queue kernel
             float4 n4 = make_float4(0.f, 0.f, 0.f, 0.f);
             if (active) {
                 g4 = __ldg(ngeom + node);
                 p4 = __ldg(npm + node);
                 x4 = __ldg(naux + node);
-                n4 = __ldg(nnc + node);
+                if (EARLY_NC) n4 = __ldg(nnc + node);
             }
             const float cr = cutoff * g4.w;
             const bool blend = active && !(r_cnt & kEntNoBlend);
@@ -665,6 +666,7 @@ __device__ __forceinline__ void project_packed(const CloudArgs& c, const uint32_
                                    (opens_all ? (kEntNoBlend | (leaf && !gpu_rule ? kEntLastOnly : 0u)) : 0u);
 
             const float inv_m = __fdividef(1.f, gpu_rule ? p4.w : float(cnt));
+            if (!EARLY_NC && term) n4 = __ldg(nnc + node);
             float2 pv_dP[NP], pv_g[NP];
 #pragma unroll
             for (int j = 0; j < NP; ++j) {
@@ -782,11 +784,12 @@ __device__ __forceinline__ void project_packed(const CloudArgs& c, const uint32_
 
 // Projects the nq (<= QPW) queries qi[0..nq) of one tree together (the
 // general walk for one query per warp, the packed form for two or four).
-template <int KTYPE, int NSIG, int RULE, int CAP, int QPW, bool PRUNE = false>
+template <int KTYPE, int NSIG, int RULE, int CAP, int QPW, bool PRUNE = false, bool EARLY_NC = true>
 __device__ __forceinline__ void project_queries(const CloudArgs& c, const uint32_t (&qi)[QPW], int nq,
                                                 WarpStack<CAP, QPW>& st, WalkStats& ws)
 {
-    if constexpr (QPW == 2 || QPW == 4) project_packed<KTYPE, NSIG, RULE, CAP, QPW / 2, PRUNE>(c, qi, nq, st, ws);
+    if constexpr (QPW == 2 || QPW == 4)
+        project_packed<KTYPE, NSIG, RULE, CAP, QPW / 2, PRUNE, EARLY_NC>(c, qi, nq, st, ws);
     else project_walk<KTYPE, NSIG, RULE, CAP, QPW, PRUNE>(c, qi, nq, st, ws);
 }
 
@@ -904,15 +907,15 @@ __device__ __forceinline__ void walk_k(int k, const CloudArgs& c, const uint32_t
                                        WarpStack<CAP, QPW>& st, WalkStats& ws)
 {
     switch (k) {
-    case 0: project_queries<MLODS_GAUSSIAN, 0, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    case 1: project_queries<MLODS_SINGULAR, 0, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    case 2: project_queries<MLODS_GAUSSIAN_MULTIPLE, 2, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    case 3: project_queries<MLODS_GAUSSIAN_MULTIPLE, 3, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    case 4: project_queries<MLODS_GAUSSIAN_MULTIPLE, 4, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    case 5: project_queries<MLODS_GAUSSIAN_MULTIPLE, 5, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    case 6: project_queries<MLODS_GAUSSIAN_MULTIPLE, 6, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    case 7: project_queries<MLODS_GAUSSIAN_MULTIPLE, 8, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
-    default: project_queries<MLODS_GAUSSIAN_MULTIPLE, 0, RULE, CAP, QPW>(c, qi, nq, st, ws); break;
+    case 0: project_queries<MLODS_GAUSSIAN, 0, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    case 1: project_queries<MLODS_SINGULAR, 0, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    case 2: project_queries<MLODS_GAUSSIAN_MULTIPLE, 2, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    case 3: project_queries<MLODS_GAUSSIAN_MULTIPLE, 3, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    case 4: project_queries<MLODS_GAUSSIAN_MULTIPLE, 4, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    case 5: project_queries<MLODS_GAUSSIAN_MULTIPLE, 5, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    case 6: project_queries<MLODS_GAUSSIAN_MULTIPLE, 6, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    case 7: project_queries<MLODS_GAUSSIAN_MULTIPLE, 8, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
+    default: project_queries<MLODS_GAUSSIAN_MULTIPLE, 0, RULE, CAP, QPW, false, false>(c, qi, nq, st, ws); break;
     }
 }
 
