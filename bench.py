@@ -686,6 +686,12 @@ def run_dc(args):
     f.setScalingProtectionSphere(2.0)
     torch.cuda.synchronize()
     build_ms = 1e3 * (time.perf_counter() - t0)
+    # the walk schedule for every projection of the pipeline, tuned on a
+    # sample of the cloud's points (one iteration, as the corner field runs)
+    rs = np.random.default_rng(17)
+    d_s = torch.from_numpy(np.ascontiguousarray(pts[rs.choice(len(pts), min(len(pts), 262144), replace=False)])).cuda()
+    schedule = f.tune_schedule(d_s, 1)
+    del d_s
     t0 = time.perf_counter()
     grid = DCGrid.adaptive(f, args.dc_depth)
     grid_ms = 1e3 * (time.perf_counter() - t0)
@@ -726,6 +732,9 @@ def run_dc(args):
                        "< prune_tol * w(0) * mean sample area; deviation measured against the unpruned field"}
     ok_off = ~np.isnan(field_off)
     strong = ok_off & (np.abs(field_off) > 1e-5 * diag)
+    qpw_tuned = f.queries_per_warp
+    f.queries_per_warp = min(qpw_tuned, 2)  # the pruning variant walks one or two queries per warp
+    pruning["queries_per_warp"] = f.queries_per_warp
     for tol in PRUNE_TOLS:
         f.prune_tol = tol
         f.dc_evaluate_device(d_cells, grid.max_depth, grid.xform)  # warm-up
@@ -748,6 +757,7 @@ def run_dc(args):
             "nan_pattern_equal": bool(np.array_equal(np.isnan(fp), ~ok_off)),
             "sign_agreement_where_abs_f_above_1e-5_diag": float(np.mean((fp[strong] < 0) == (field_off[strong] < 0)))})
     f.prune_tol = 0.0
+    f.queries_per_warp = qpw_tuned
     # end to end through the host-buffer call (cells from host memory, results to host memory)
     e2e_ms = []
     for _ in range(max(args.steps, 1)):
@@ -826,6 +836,7 @@ def run_dc(args):
                       "mesh_pipeline_runs": [round(v_, 1) for v_ in mesh_runs],
                       "mesh_parts_host_path": {k: round(v_, 1) for k, v_ in parts.items()}},
         "mesh": {"vertices": int(len(v)), "triangles": int(len(tri))},
+        "schedule": dict(schedule, note="mlods_tune_schedule on 262144 of the cloud's points, 1 iteration"),
         "pruning": pruning,
         "e2e": {"value": n_unique * len(e2e_ms) / (sum(e2e_ms) / 1e3), "unit": "corners/s",
                 "h2d_bytes_per_step": int(grid.cells.nbytes), "d2h_bytes_per_step": int(cf.nbytes + vx.nbytes + nc.nbytes),
