@@ -206,18 +206,18 @@ PRUNE_TOLS = (1e-6, 1e-3, 1e-1)  # tolerances of the reported kernel-weight prun
 PROFILED_COUNTERS = {
     "precision": {"capture": "ncu --set full, precision workload at 200k points, two queries per warp (packed "
                              "f32x2 arithmetic), one launch",
-                  "issue_slots_active_pct": 74.9, "warp_instructions_per_query_node_visit": 6.6,
-                  "threads_active_per_instruction": 28.71, "warps_active_per_sm": 27.6,
-                  "l2_sector_throughput_gbs": 4040.0, "l2_throughput_pct": 15.3, "l2_hit_rate_pct": 99.11,
-                  "l1_throughput_pct": 65.3, "fp32_fma_pipe_cycles_pct": 35.0, "alu_pipe_pct": 55.3,
-                  "xu_pipe_pct": 38.8, "fp64_pipe_pct": 3.06,
-                  "top_stalls_per_issue": {"wait": 2.22, "short_scoreboard": 1.91, "not_selected": 1.53,
-                                           "long_scoreboard": 0.94}},
+                  "issue_slots_active_pct": 76.8, "warp_instructions_per_query_node_visit": 6.77,
+                  "threads_active_per_instruction": 28.32, "warps_active_per_sm": 27.6,
+                  "l2_sector_throughput_gbs": 4138.0, "l2_throughput_pct": 15.7, "l2_hit_rate_pct": 99.09,
+                  "l1_throughput_pct": 65.5, "fp32_fma_pipe_cycles_pct": 36.7, "alu_pipe_pct": 56.0,
+                  "xu_pipe_pct": 40.4, "fp64_pipe_pct": 3.06,
+                  "top_stalls_per_issue": {"wait": 2.25, "not_selected": 1.71, "short_scoreboard": 1.57,
+                                           "long_scoreboard": 0.73}},
 }
 # L2 sector throughput peak of the B200 as ncu reports it (lts__t_sectors:
 # 3 sectors per cycle per slice at the L2 clock), from the capture above:
-# 126.26 sectors/ns at 11.66 % of peak
-L2_PEAK_GBS = 126.26 * 32 / 0.1166
+# 129.30 sectors/ns at 11.97 % of peak
+L2_PEAK_GBS = 129.30 * 32 / 0.1197
 
 
 def max_over_ranks(values, world: int, device):
