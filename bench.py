@@ -206,18 +206,18 @@ PRUNE_TOLS = (1e-6, 1e-3, 1e-1)  # tolerances of the reported kernel-weight prun
 PROFILED_COUNTERS = {
     "precision": {"capture": "ncu --set full, precision workload at 200k points, two queries per warp (packed "
                              "f32x2 arithmetic), one launch",
-                  "issue_slots_active_pct": 76.8, "warp_instructions_per_query_node_visit": 6.77,
-                  "threads_active_per_instruction": 28.32, "warps_active_per_sm": 27.6,
-                  "l2_sector_throughput_gbs": 4138.0, "l2_throughput_pct": 15.7, "l2_hit_rate_pct": 99.09,
-                  "l1_throughput_pct": 65.5, "fp32_fma_pipe_cycles_pct": 36.7, "alu_pipe_pct": 56.0,
-                  "xu_pipe_pct": 40.4, "fp64_pipe_pct": 3.06,
-                  "top_stalls_per_issue": {"wait": 2.25, "not_selected": 1.71, "short_scoreboard": 1.57,
-                                           "long_scoreboard": 0.73}},
+                  "issue_slots_active_pct": 76.7, "warp_instructions_per_query_node_visit": 6.61,
+                  "threads_active_per_instruction": 28.74, "warps_active_per_sm": 27.6,
+                  "l2_sector_throughput_gbs": 4193.0, "l2_throughput_pct": 15.7, "l2_hit_rate_pct": 99.09,
+                  "l1_throughput_pct": 66.8, "fp32_fma_pipe_cycles_pct": 35.9, "alu_pipe_pct": 56.5,
+                  "xu_pipe_pct": 39.9, "fp64_pipe_pct": 3.13,
+                  "top_stalls_per_issue": {"wait": 2.25, "short_scoreboard": 1.67, "not_selected": 1.66,
+                                           "long_scoreboard": 0.75}},
 }
 # L2 sector throughput peak of the B200 as ncu reports it (lts__t_sectors:
 # 3 sectors per cycle per slice at the L2 clock), from the capture above:
-# 129.30 sectors/ns at 11.97 % of peak
-L2_PEAK_GBS = 129.30 * 32 / 0.1197
+# 131.05 sectors/ns at 12.09 % of peak
+L2_PEAK_GBS = 131.05 * 32 / 0.1209
 
 
 def max_over_ranks(values, world: int, device):
