@@ -212,6 +212,9 @@ int mlods_project_device(mlods_tree t, int64_t n, const float* d_q, float* d_out
  * float rounding.  Synchronises. */
 int mlods_tune_schedule(mlods_tree t, int64_t n, const float* d_q, int32_t n_iterations, void* stream,
                         int32_t* chosen, float* ms);
+/* The same on n host queries (xyz floats), staged in library scratch memory. */
+int mlods_tune_schedule_host(mlods_tree t, int64_t n, const float* q, int32_t n_iterations, int32_t* chosen,
+                             float* ms);
 
 /* ---- neighbour gathers -----------------------------------------------------
  * k nearest neighbours of n device query points (world xyz), as the

@@ -332,6 +332,20 @@ public:
     const APSSOctree* CPU() { return m_apssOctree; }
 
     int blend_rule = MLODS_BLEND_GPU;  // extension: select the CPU blend rule on the device
+    // extension: the MLoD walk schedule (mlods_params.queries_per_warp): 1, 2
+    // or 4 Morton-adjacent queries share one walk of the tree
+    int queries_per_warp = 1;
+
+    // extension: times the walk schedules on n sample queries (host array)
+    // with n_iterations steps and keeps the fastest in queries_per_warp
+    int tuneSchedule(unsigned int n, const vec3* sample, unsigned int n_iterations)
+    {
+        sync_params();
+        int32_t chosen = queries_per_warp;
+        check(mlods_tune_schedule_host(tree(), int64_t(n), &sample[0].x, int32_t(n_iterations), &chosen, nullptr));
+        queries_per_warp = chosen;
+        return chosen;
+    }
 
 protected:
     virtual int32_t mode() const
@@ -355,6 +369,7 @@ protected:
         p.knn = int32_t(m_apssOctree->m_knn);
         p.ball_radius = m_apssOctree->m_ballRadius;
         p.blend_rule = blend_rule;
+        p.queries_per_warp = queries_per_warp;
         check(mlods_set_params(tree(), &p));
     }
 

@@ -172,6 +172,7 @@ SIGNATURES = {
     "mlods_last_walk_counts": (C.c_int, [_P, _I64, _I64]),
     "mlods_tune_schedule": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, C.POINTER(C.c_int32),
                                       C.POINTER(C.c_float)]),
+    "mlods_tune_schedule_host": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _I32, C.POINTER(C.c_float)]),
     "mlods_kernel_launches": (C.c_int64, []),
     "mlods_release_scratch": (C.c_int, []),
     "mlods_knn": (C.c_int, [_P, C.c_int64, _P, C.c_int32, _P, _P, _P]),

@@ -897,6 +897,26 @@ int mlods_tune_schedule(mlods_tree t, int64_t n, const float* d_q, int32_t n_ite
     return MLODS_OK;
 }
 
+int mlods_tune_schedule_host(mlods_tree t, int64_t n, const float* q, int32_t n_iterations, int32_t* chosen,
+                             float* ms)
+{
+    CHECK_TREE(t);
+    if (!q || n <= 0) {
+        set_last_error("tune schedule: bad arguments");
+        return MLODS_ERR_INVALID;
+    }
+    // the sample staged in scratch memory on the legacy stream, then tuned there
+    float* d = nullptr;
+    MLODS_CUDA(scratch_alloc(reinterpret_cast<void**>(&d), size_t(n) * 12, nullptr));
+    cudaError_t e = cudaMemcpyAsync(d, q, size_t(n) * 12, cudaMemcpyHostToDevice, nullptr);
+    const int rc = e == cudaSuccess ? mlods_tune_schedule(t, n, d, n_iterations, nullptr, chosen, ms) : MLODS_OK;
+    const cudaError_t ef = scratch_free(d, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "tune schedule: upload", __FILE__, __LINE__);
+    if (rc != MLODS_OK) return rc;
+    if (ef != cudaSuccess) return cuda_fail(ef, "tune schedule: free", __FILE__, __LINE__);
+    return MLODS_OK;
+}
+
 int mlods_knn(mlods_tree t, int64_t n, const float* d_q, int32_t k, int32_t* d_idx, float* d_d2, void* stream)
 {
     CHECK_TREE(t);

@@ -5,6 +5,7 @@
 // writes the projections for the test to compare.
 #include <cstdio>
 #include <cstdlib>
+#include <cmath>
 #include <thread>
 #include <vector>
 
@@ -70,6 +71,23 @@ int main(int argc, char** argv)
             std::fprintf(stderr, "threaded projectCPU differs from the serial result at query %zu\n", i);
             return 4;
         }
+    // the walk schedule tuned on the queries, then the same ten project calls:
+    // any schedule agrees with one query per warp to float rounding
+    const int chosen = apss.tuneSchedule(unsigned(q.size()), q.data(), 10);
+    if (chosen != 1 && chosen != 2 && chosen != 4) return 5;
+    apss.queries_per_warp = 2;
+    apss.copyPointsToGPU(unsigned(q.size()), q.data());
+    for (int tick = 0; tick < 10; ++tick) apss.project(unsigned(q.size()), nullptr, nullptr, 1, k);
+    std::vector<vec3> out2(q.size()), out2n(q.size());
+    apss.project(unsigned(q.size()), out2.data(), out2n.data(), 0, k);
+    const float r = tree->getBoundingBox().radius();
+    for (size_t i = 0; i < q.size(); ++i) {
+        const float dx = out2[i].x - out[i].x, dy = out2[i].y - out[i].y, dz = out2[i].z - out[i].z;
+        if (std::sqrt(dx * dx + dy * dy + dz * dz) > 2e-5f * r) {  // 1e-5 of the diagonal
+            std::fprintf(stderr, "two queries per warp differ from one at query %zu\n", i);
+            return 6;
+        }
+    }
     if (argc > 7) {  // APSSOctree::cpuSphere at the queries: u0, u123, u4 per query
         std::vector<float> u;
         for (const vec3& x : q) {
