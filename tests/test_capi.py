@@ -69,3 +69,28 @@ def test_apss_lifecycle_methods_without_a_gpu():
     f.stop()
     f.eraseAndRestart()
     assert isinstance(f.CPU(), APSSOctree) and f.CPU() is not t
+
+
+def test_new_entry_points_reject_null_handles_without_a_gpu():
+    lib = capi.load()
+    ci = C.c_int32(0)
+    assert lib.mlods_tune_schedule(None, 10, None, 1, None, C.byref(ci), None) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_tune_schedule_host(None, 10, None, 1, C.byref(ci), None) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_last_walk_counts(None, None, None) == capi.MLODS_ERR_INVALID
+    sched = capi.mlods_batch_schedule(2, 1, 100, 0, 0)
+    assert lib.mlods_batch_set_schedule(None, C.byref(sched)) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_batch_get_schedule(None, C.byref(sched)) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_batch_tune_results(None, 0, None, None, C.byref(ci)) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_batch_stats(None, None, None, None, None, None, None) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_batch_create(None, 0, C.byref(C.c_void_p())) == capi.MLODS_ERR_INVALID
+    assert lib.mlods_batch_free(None) == capi.MLODS_OK
+
+
+def test_server_batch_footprint_grows_with_the_batch():
+    """mlods_server_batch_bytes is host arithmetic: a batch's device bytes
+    grow with its queries and requests."""
+    lib = capi.load()
+    small = lib.mlods_server_batch_bytes(4096, 1)
+    assert small > 4096 * 36
+    assert lib.mlods_server_batch_bytes(8192, 1) > small
+    assert lib.mlods_server_batch_bytes(4096, 64) > small
